@@ -1,0 +1,110 @@
+// Stage (d): per-tile front-to-back blending -- splat/splat_blend.slang:236-578
+// (splatBlend = blendPixel<composite=false, matte=false, traced=false>) -- with
+// the P layer (usd/aov_position.slang:34-52) as its epilogue.
+//
+// One block a 16x16 tile, one thread a pixel. The tile's records are staged in
+// shared memory 256 at a time (:287-312); a pixel stops at T < 1e-4 after
+// accumulating (:501-505); the block stops loading once every pixel is done,
+// counted with a block-wide ballot (__syncthreads_count). Per pixel the walk
+// is sequential in the tile's (depth key, slot) order, so the result is the
+// CPU restatement's to the bit (built with --fmad=false; see splat_math.cuh).
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "raster_types.cuh"
+#include "splat_math.cuh"
+
+namespace ath {
+namespace {
+
+constexpr uint32_t kBlendThreads = kTile * kTile;
+
+__global__ void __launch_bounds__(kBlendThreads)
+    blendKernel(const FrameConst F, const uint2* __restrict__ ranges, const uint32_t* __restrict__ pairValues,
+                const float4* __restrict__ recs, float4* __restrict__ colour, float* __restrict__ depth,
+                float4* __restrict__ position, float* __restrict__ finalT, uint32_t* __restrict__ lastContrib) {
+    __shared__ float4 sScreen[kBlendThreads];
+    __shared__ float4 sConic[kBlendThreads];
+    __shared__ float4 sColour[kBlendThreads];
+
+    const uint32_t tile = blockIdx.x;
+    const uint32_t tx = tile % F.tilesX, ty = tile / F.tilesX;
+    const uint32_t px = tx * kTile + (threadIdx.x % kTile);
+    const uint32_t py = ty * kTile + (threadIdx.x / kTile);
+    const bool inside = px < F.width && py < F.height;
+    const uint2 range = ranges[tile];
+    const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+
+    float r = 0.0f, g = 0.0f, bl = 0.0f;
+    float T = 1.0f, depthSum = 0.0f, depthAt = -1.0f;
+    uint32_t last = 0;
+    bool done = !inside;
+    for (uint32_t first = range.x; first < range.y; first += kBlendThreads) {
+        if (__syncthreads_count(done) == kBlendThreads) break;
+        const uint32_t mine = first + threadIdx.x;
+        if (mine < range.y) {
+            const uint32_t s = pairValues[mine];
+            sScreen[threadIdx.x] = recs[(size_t)s * 3 + 0];
+            sConic[threadIdx.x] = recs[(size_t)s * 3 + 1];
+            sColour[threadIdx.x] = recs[(size_t)s * 3 + 2];
+        }
+        __syncthreads();
+        const uint32_t count = min(kBlendThreads, range.y - first);
+        for (uint32_t j = 0; j < count && !done; ++j) {
+            const float4 sc = sScreen[j];
+            const float4 k = sConic[j];
+            const float dx = pxc - sc.x;
+            const float dy = pyc - sc.y;
+            const float power = ((k.x * dx) * dx + ((2.0f * k.y) * dx) * dy) + (k.z * dy) * dy;
+            if (power > sc.w) continue;
+            const float alpha = fminf(0.99f, falloffAlpha(fabsf(k.w), exp_f((-0.5f) * power)));
+            if (alpha < kFaint) continue;
+            const float weight = T * alpha;
+            const float4 c = sColour[j];
+            r = r + weight * c.x;
+            g = g + weight * c.y;
+            bl = bl + weight * c.z;
+            depthSum = depthSum + weight * sc.z;
+            T = T * (1.0f - alpha);
+            last = first - range.x + j + 1;
+            if (depthAt < 0.0f && 1.0f - T >= F.depthThreshold) depthAt = sc.z;
+            if (T < 1e-4f) done = true;
+        }
+    }
+    if (!inside) return;
+    const uint32_t at = py * F.width + px;
+    const float coverage = 1.0f - T;
+    colour[at] = make_float4(r + T * F.bg[0], g + T * F.bg[1], bl + T * F.bg[2], coverage + T * F.bg[3]);
+    const float z = F.depthMode == 0 ? (coverage > 1e-6f ? depthSum / coverage : 0.0f) : fmaxf(depthAt, 0.0f);
+    depth[at] = z;
+    if (finalT) finalT[at] = T;
+    if (lastContrib) lastContrib[at] = last;
+    if (position) {
+        // usd/aov_position.slang:40-51
+        if (!(z > 0.0f)) {
+            position[at] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else {
+            const float scale = F.orthographic != 0 ? 1.0f : z;
+            const float v0 = ((pxc - F.centreX) / F.focalX) * scale;
+            const float v1 = ((pyc - F.centreY) / F.focalY) * scale;
+            const float* m = F.viewToWorld;
+            position[at] = make_float4(((m[0] * v0 + m[1] * v1) + m[2] * z) + m[3] * 1.0f,
+                                       ((m[4] * v0 + m[5] * v1) + m[6] * z) + m[7] * 1.0f,
+                                       ((m[8] * v0 + m[9] * v1) + m[10] * z) + m[11] * 1.0f, 1.0f);
+        }
+    }
+}
+
+}   // namespace
+
+cudaError_t launchBlend(const FrameConst& F, const uint2* ranges, const uint32_t* pairValues, const float4* recs,
+                        float4* colour, float* depth, float4* position, float* finalT, uint32_t* lastContrib,
+                        cudaStream_t stream) {
+    const uint32_t tiles = F.tilesX * F.tilesY;
+    if (tiles == 0) return cudaSuccess;
+    blendKernel<<<tiles, kBlendThreads, 0, stream>>>(F, ranges, pairValues, recs, colour, depth, position, finalT,
+                                                    lastContrib);
+    return cudaGetLastError();
+}
+
+}   // namespace ath

@@ -1,0 +1,45 @@
+// Host-side entry points of the stage kernels (one .cu each), called by the
+// rasteriser's host code (host.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/athenea_raster.h"
+
+namespace ath {
+
+struct FrameConst;
+struct InstanceConst;
+
+// project.cu
+uint32_t projectBlocks(uint32_t slots);
+cudaError_t launchProject(const FrameConst& F, const InstanceConst* inst, uint32_t nInst, uint32_t slots,
+                          bool countCulls, float4* recs, uint2* rects, uint32_t* keys, uint32_t* offsets,
+                          uint64_t* flags, uint32_t* words, cudaStream_t stream);
+cudaError_t launchEmit(const FrameConst& F, uint32_t slots, const float4* recs, const uint2* rects,
+                       const uint32_t* keys, const uint32_t* offsets, const uint32_t* words, uint64_t capacity,
+                       uint64_t* pairKeys, uint32_t* pairValues, cudaStream_t stream);
+cudaError_t launchRanges(uint32_t pairs, const uint64_t* pairKeys, uint2* ranges, cudaStream_t stream);
+
+// sort.cu
+uint32_t sortPasses(uint32_t bits);
+uint32_t sortTiles(uint32_t n);
+size_t sortFlagWords(uint32_t n, uint32_t bits);
+uint32_t sortResultIndex(uint32_t n, uint32_t bits);
+cudaError_t sortPrepare();
+cudaError_t launchSort(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_t bits, uint32_t* hist,
+                       uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream);
+
+// blend.cu
+cudaError_t launchBlend(const FrameConst& F, const uint2* ranges, const uint32_t* pairValues, const float4* recs,
+                        float4* colour, float* depth, float4* position, float* finalT, uint32_t* lastContrib,
+                        cudaStream_t stream);
+
+// decode.cu
+uint32_t decodeBlocks(uint32_t count);
+cudaError_t launchDecode(const float* records, uint32_t count, const ath_encoding& E, float4* positions, uint4* shape,
+                         uint32_t* sh, uint64_t* flags, uint32_t* words, cudaStream_t stream);
+
+}   // namespace ath

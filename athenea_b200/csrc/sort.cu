@@ -1,0 +1,217 @@
+// Stage (c): a stable LSD radix sort of 64-bit keys with 32-bit values, eight
+// bits a pass, in the onesweep form (Adinets and Merrill, "Onesweep: A Faster
+// Least Significant Digit Radix Sort for GPUs", 2022): one read of the keys
+// makes every pass's digit histogram, then each pass is a single kernel whose
+// tiles rank their keys in shared memory, find where each digit of theirs
+// starts by a decoupled look-back over the tiles before them, and scatter.
+//
+// It replaces the reference's RadixSort (modules/gpu/src/algo/RadixSort.cpp:
+// 95-261; shaders/athenea/algo/radix_*.slang), which the rasteriser runs twice
+// (24-bit depth keys, then tile keys). Same contract: stable, so equal keys
+// keep their input order (algo/radix_common.slang:18-22), and only the low
+// `bits` of a key take part.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "raster_types.cuh"
+
+namespace ath {
+namespace {
+
+constexpr uint32_t kRadix = 256;
+constexpr uint32_t kSortThreads = 256;
+constexpr uint32_t kWarps = kSortThreads / 32;
+constexpr uint32_t kItems = 16;
+constexpr uint32_t kTileKeys = kSortThreads * kItems;   // 4096
+constexpr uint32_t kMaxPasses = 8;
+
+__global__ void __launch_bounds__(256)
+    histogramKernel(const uint64_t* __restrict__ keys, uint32_t n, uint32_t passes, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t sHist[kMaxPasses * kRadix];
+    for (uint32_t j = threadIdx.x; j < passes * kRadix; j += blockDim.x) sHist[j] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[i];
+        for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p * kRadix + (uint32_t)((key >> (8 * p)) & 0xFFu)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < passes * kRadix; j += blockDim.x)
+        if (sHist[j]) atomicAdd(&hist[j], sHist[j]);
+}
+
+// Exclusive scan of one value a thread over the block (256 threads).
+__device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* sWarp) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += u;
+    }
+    if (lane == 31) sWarp[warp] = incl;
+    __syncthreads();
+    uint32_t base = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kWarps; ++w) base += w < warp ? sWarp[w] : 0u;
+    __syncthreads();
+    return base + incl - v;
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+    onesweepKernel(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
+                   uint64_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, uint32_t n, uint32_t shift,
+                   const uint32_t* __restrict__ globalHist, uint64_t* __restrict__ flags, uint32_t* __restrict__ ticket,
+                   uint32_t* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
+    uint32_t* sVals = reinterpret_cast<uint32_t*>(sKeys + kTileKeys);
+    uint32_t* sWarpCnt = sVals + kTileKeys;   // kWarps x kRadix
+    __shared__ uint32_t sTile;
+    __shared__ uint32_t sStart[kRadix];
+    __shared__ uint32_t sAdjust[kRadix];
+    __shared__ uint32_t sScan[kWarps];
+
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    if (tid == 0) sTile = atomicAdd(ticket, 1u);
+    for (uint32_t j = tid; j < kWarps * kRadix; j += kSortThreads) sWarpCnt[j] = 0;
+    __syncthreads();
+    const uint32_t tile = sTile;
+    const uint32_t base = tile * kTileKeys;
+    const uint32_t ltMask = (1u << lane) - 1u;
+
+    // Rank: warp `warp` owns keys [base + warp*32*kItems, +32*kItems), item k of
+    // lane l being the (k*32 + l)-th; walking k then l is input order, so the
+    // ranks are stable.
+    uint64_t key[kItems];
+    uint32_t val[kItems];
+    uint32_t rank[kItems];
+#pragma unroll
+    for (uint32_t k = 0; k < kItems; ++k) {
+        const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
+        const bool valid = idx < n;
+        key[k] = valid ? keysIn[idx] : 0ull;
+        val[k] = valid ? valsIn[idx] : 0u;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < kItems; ++k) {
+        const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t d = valid ? (uint32_t)((key[k] >> shift) & 0xFFu) : kRadix + lane;
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        uint32_t before = 0;
+        if (valid) before = sWarpCnt[warp * kRadix + d];
+        __syncwarp();
+        if (valid && lane == (uint32_t)(__ffs(peers) - 1)) sWarpCnt[warp * kRadix + d] = before + __popc(peers);
+        __syncwarp();
+        rank[k] = before + __popc(peers & ltMask);
+    }
+    __syncthreads();
+
+    // One thread a digit: the warps' counts to exclusive offsets, the tile's count.
+    const uint32_t t = tid;
+    uint32_t count = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kWarps; ++w) {
+        const uint32_t c = sWarpCnt[w * kRadix + t];
+        sWarpCnt[w * kRadix + t] = count;
+        count += c;
+    }
+    // Where this tile's share of digit t starts in the output.
+    uint64_t* flag = flags + (size_t)tile * kRadix + t;
+    uint32_t exclusive;
+    if (tile == 0) {
+        exclusive = blockExclusiveScan(globalHist[t], sScan);
+        storeRelaxed(flag, kFlagInclusive | (uint64_t)(exclusive + count));
+    } else {
+        storeRelaxed(flag, kFlagAggregate | (uint64_t)count);
+        uint64_t sum = 0;
+        int64_t j = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (j >= 0) {
+            const uint64_t v = loadRelaxed(flags + (size_t)j * kRadix + t);
+            const uint32_t st = (uint32_t)(v >> 62);
+            if (st == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicOr(status, kStatusLookbackTimeout);
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            sum += v & kFlagValue;
+            if (st == 2) break;
+            --j;
+        }
+        exclusive = (uint32_t)sum;
+        storeRelaxed(flag, kFlagInclusive | (uint64_t)(exclusive + count));
+    }
+    const uint32_t start = blockExclusiveScan(count, sScan);
+    sStart[t] = start;
+    sAdjust[t] = exclusive - start;
+    __syncthreads();
+
+    // Scatter into shared memory in the tile's sorted order, then out.
+#pragma unroll
+    for (uint32_t k = 0; k < kItems; ++k) {
+        const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (uint32_t)((key[k] >> shift) & 0xFFu);
+            const uint32_t s = sStart[d] + sWarpCnt[warp * kRadix + d] + rank[k];
+            sKeys[s] = key[k];
+            sVals[s] = val[k];
+        }
+    }
+    __syncthreads();
+    const uint32_t tileN = min(kTileKeys, n - base);
+    for (uint32_t s = tid; s < tileN; s += kSortThreads) {
+        const uint64_t k = sKeys[s];
+        const uint32_t dst = sAdjust[(uint32_t)((k >> shift) & 0xFFu)] + s;
+        keysOut[dst] = k;
+        valsOut[dst] = sVals[s];
+    }
+}
+
+constexpr size_t kOnesweepSmem = (size_t)kTileKeys * 8 + (size_t)kTileKeys * 4 + (size_t)kWarps * kRadix * 4;
+
+}   // namespace
+
+uint32_t sortPasses(uint32_t bits) { return (bits + 7) / 8; }
+uint32_t sortTiles(uint32_t n) { return (n + kTileKeys - 1) / kTileKeys; }
+size_t sortFlagWords(uint32_t n, uint32_t bits) { return (size_t)sortTiles(n) * kRadix * sortPasses(bits); }
+
+cudaError_t sortPrepare() {
+    return cudaFuncSetAttribute(onesweepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOnesweepSmem);
+}
+
+// keys/vals[0] hold the input; the sorted result lands in keys/vals[passes & 1]
+// (the caller reads sortResultIndex). hist: kMaxPasses*256 words, flags:
+// sortFlagWords words, tickets: one word a pass; all three are zeroed here.
+cudaError_t launchSort(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_t bits, uint32_t* hist,
+                       uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream) {
+    if (n <= 1) return cudaSuccess;
+    const uint32_t passes = sortPasses(bits);
+    if (passes > kMaxPasses) return cudaErrorInvalidValue;
+    const uint32_t tiles = sortTiles(n);
+    cudaError_t err = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kRadix * passes, stream);
+    if (err != cudaSuccess) return err;
+    err = cudaMemsetAsync(flags, 0, sizeof(uint64_t) * (size_t)tiles * kRadix * passes, stream);
+    if (err != cudaSuccess) return err;
+    err = cudaMemsetAsync(tickets, 0, sizeof(uint32_t) * passes, stream);
+    if (err != cudaSuccess) return err;
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const uint32_t hblocks = min((n + 255) / 256, (uint32_t)sms * 4);
+    histogramKernel<<<hblocks, 256, 0, stream>>>(keys[0], n, passes, hist);
+    for (uint32_t p = 0; p < passes; ++p) {
+        const uint32_t in = p & 1u, out = in ^ 1u;
+        onesweepKernel<<<tiles, kSortThreads, kOnesweepSmem, stream>>>(
+            keys[in], vals[in], keys[out], vals[out], n, 8 * p, hist + p * kRadix,
+            flags + (size_t)p * tiles * kRadix, tickets + p, status);
+    }
+    return cudaGetLastError();
+}
+
+uint32_t sortResultIndex(uint32_t n, uint32_t bits) { return n <= 1 ? 0u : (sortPasses(bits) & 1u); }
+
+}   // namespace ath

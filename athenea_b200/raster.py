@@ -1,0 +1,326 @@
+"""The reference's rasteriser interface, over the C ABI.
+
+Mirrors render::TileRasterizer (modules/render/include/athenea/render/
+TileRasterizer.h:452-487), its settings and targets (:248-450), the camera
+(Camera.h) and scene::CloudLoader::upload's decode (scene/GpuClouds.h:366), with
+the same names, argument meaning and errors (failures raise AtheneaError
+carrying the ErrorCode the reference would return). Device memory is torch's:
+clouds and targets are CUDA tensors the caller owns.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native as N
+from ._native import AtheneaError, check
+
+
+def _ptr(t: torch.Tensor | None):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise AtheneaError(3, "device memory expected: pass CUDA tensors")
+    if not t.is_contiguous():
+        raise AtheneaError(3, "contiguous tensors expected")
+    return C.c_void_p(t.data_ptr())
+
+
+def _mat(m) -> np.ndarray:
+    return np.asarray(m, dtype=np.float64).reshape(4, 4)
+
+
+# ---- camera (Camera.h / Camera.cpp) ----------------------------------------
+@dataclass
+class Lens:
+    """Camera.h:89-117."""
+    orthographic: bool = False
+    focal: float = 50.0
+    haperture: float = 24.576
+    vaperture: float = 18.672
+    near_z: float = 0.1
+    far_z: float = 10000.0
+    window_translate: tuple = (0.0, 0.0)
+    window_scale: tuple = (1.0, 1.0)
+    window_roll: float = 0.0
+
+
+@dataclass
+class Camera:
+    """Camera.h:119-126: camera_to_world is row-major, acting on column vectors."""
+    camera_to_world: np.ndarray = field(default_factory=lambda: np.eye(4))
+    lens: Lens = field(default_factory=Lens)
+
+    @staticmethod
+    def looking_at(eye, target, up=(0.0, 1.0, 0.0)) -> "Camera":
+        """Camera::lookingAt (Camera.cpp:9-25)."""
+        c = N.Camera()
+        check(N.lib().ath_camera_looking_at(np.asarray(eye, np.float64).ctypes.data_as(C.c_void_p),
+                                            np.asarray(target, np.float64).ctypes.data_as(C.c_void_p),
+                                            np.asarray(up, np.float64).ctypes.data_as(C.c_void_p), C.byref(c)))
+        cam = Camera(np.array(c.camera_to_world[:]).reshape(4, 4))
+        cam.lens.near_z = c.near_z
+        return cam
+
+    def _native(self) -> N.Camera:
+        c = N.Camera()
+        c.camera_to_world[:] = list(_mat(self.camera_to_world).reshape(16))
+        c.orthographic = 1 if self.lens.orthographic else 0
+        c.focal, c.haperture = self.lens.focal, self.lens.haperture
+        c.near_z, c.far_z = self.lens.near_z, self.lens.far_z
+        c.window_translate[:] = list(self.lens.window_translate)
+        c.window_scale[:] = list(self.lens.window_scale)
+        c.window_roll = self.lens.window_roll
+        return c
+
+    def projection_for(self, width: int, height: int) -> N.Projection:
+        """projectionFor (Camera.cpp:32-64)."""
+        p = N.Projection()
+        check(N.lib().ath_projection_for(C.byref(self._native()), width, height, C.byref(p)))
+        return p
+
+
+def pinhole_for_vertical_fov(eye, target, width, height, vfov_degrees, up=(0.0, 1.0, 0.0)) -> Camera:
+    """A lookingAt camera whose focal length gives `vfov_degrees` vertically over `height`
+    pixels (square pixels: focal_px = (height / 2) / tan(vfov / 2))."""
+    cam = Camera.looking_at(eye, target, up)
+    focal_px = (height * 0.5) / math.tan(math.radians(vfov_degrees) * 0.5)
+    cam.lens.focal = cam.lens.haperture * focal_px / width
+    return cam
+
+
+# ---- the cloud (scene/GpuClouds.h) -----------------------------------------
+@dataclass
+class GpuSplats:
+    """scene::GpuSplats (GpuClouds.h:44-52): the packed layout of common/packing.slang."""
+    positions: torch.Tensor          # (count, 4) float32
+    shape: torch.Tensor              # (count, 4) int32 (uint32 bits)
+    sh: torch.Tensor                 # (count, sh_words) int32 (uint32 bits)
+    count: int
+    rest_per_colour: int
+    sh_words: int
+    linear: bool = False
+    antialiased: int = -1            # what the file said: -1 nothing
+
+    def degree(self) -> int:
+        r = self.rest_per_colour
+        return 3 if r >= 15 else 2 if r >= 8 else 1 if r >= 3 else 0
+
+
+# 3DGS record layouts (io::SplatEncoding) the decode reads.
+def encoding_3dgs(rest_per_colour: int, stride: int | None = None, **fields) -> dict:
+    """The field layout of a 3DGS PLY record: x y z nx ny nz f_dc(3) f_rest(3 r) opacity scale(3) rot(4)."""
+    rest = 3 * rest_per_colour
+    e = dict(x=0, y=1, z=2, dc0=6, dc1=7, dc2=8, rest_base=9, file_per_colour=rest_per_colour,
+             opacity=9 + rest, scale0=10 + rest, scale1=11 + rest, scale2=12 + rest, rot_w=13 + rest,
+             rot_x=14 + rest, rot_y=15 + rest, rot_z=16 + rest)
+    e["stride"] = stride if stride is not None else 17 + rest
+    e.update(fields)
+    return e
+
+
+PER_DEGREE = (0, 3, 8, 15)
+
+
+class CloudLoader:
+    """scene::CloudLoader::upload (GpuClouds.h:366): records -> packed splats, on the GPU."""
+
+    @staticmethod
+    def upload(records: torch.Tensor, encoding: dict, max_degree: int = 3, linear: bool = False,
+               stream: torch.cuda.Stream | None = None) -> GpuSplats:
+        if records.dtype != torch.float32 or not records.is_cuda:
+            raise AtheneaError(3, "records must be a CUDA float32 tensor")
+        stride = encoding["stride"]
+        count = records.numel() // stride
+        keep = min(encoding["file_per_colour"], PER_DEGREE[min(max_degree, 3)])
+        sh_words = 1 if keep == 0 else (keep * 3 + 1) // 2
+        dev = records.device
+        positions = torch.empty((max(count, 1), 4), dtype=torch.float32, device=dev)
+        shape = torch.empty((max(count, 1), 4), dtype=torch.int32, device=dev)
+        sh = torch.zeros((max(count, 1), sh_words), dtype=torch.int32, device=dev)
+        e = N.Encoding(keep_per_colour=keep, **{k: encoding[k] for k in (
+            "stride", "x", "y", "z", "opacity", "scale0", "scale1", "scale2", "rot_w", "rot_x", "rot_y", "rot_z",
+            "dc0", "dc1", "dc2", "rest_base", "file_per_colour")})
+        kept = C.c_uint32(0)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        check(N.lib().ath_decode_records(_ptr(records.contiguous()), count, C.byref(e), _ptr(positions),
+                                         _ptr(shape), _ptr(sh), C.byref(kept), C.c_void_p(s.cuda_stream)))
+        n = kept.value
+        return GpuSplats(positions[:max(n, 1)], shape[:max(n, 1)], sh[:max(n, 1)], n, keep, sh_words, linear)
+
+
+# ---- settings, instances, targets (TileRasterizer.h) -----------------------
+@dataclass
+class SplatEdit:
+    """TileRasterizer.h:38-60."""
+    active: bool = False
+    shape: int = 0
+    mode: int = 2
+    centre: tuple = (0.0, 0.0, 0.0)
+    size: tuple = (1.0, 1.0, 1.0)
+    tint: tuple = (1.0, 1.0, 1.0)
+    saturation: float = 1.0
+    brightness: float = 1.0
+    opacity: float = 1.0
+    min_opacity: float = 0.0
+    max_scale: float = 0.0
+    invert: bool = False
+
+
+@dataclass
+class SplatInstance:
+    """TileRasterizer.h:85-172 (its plain-path fields)."""
+    splats: GpuSplats | None
+    object_to_world: np.ndarray = field(default_factory=lambda: np.eye(4))
+    edit: SplatEdit = field(default_factory=SplatEdit)
+
+
+@dataclass
+class RenderSettings:
+    """TileRasterizer.h:248-371 (its plain-path fields)."""
+    width: int = 1920
+    height: int = 1080
+    antialias: bool = True
+    antialias_override: bool | None = None
+    made_spread: float = 0.0
+    surfels: bool = True
+    max_sh_degree: int = 3
+    background: tuple = (0.0, 0.0, 0.0, 0.0)
+    depth_mode: int = 0           # 0 Mean, 1 Threshold
+    depth_threshold: float = 0.5
+    time_stages: bool = False
+    count_splats: bool = False
+    counters_tag: int = 0
+
+    def _native(self) -> N.Settings:
+        s = N.Settings()
+        s.width, s.height = self.width, self.height
+        s.antialias = 1 if self.antialias else 0
+        s.antialias_override = -1 if self.antialias_override is None else int(bool(self.antialias_override))
+        s.made_spread = self.made_spread
+        s.surfels = 1 if self.surfels else 0
+        s.max_sh_degree = self.max_sh_degree
+        s.background[:] = list(self.background)
+        s.depth_mode = self.depth_mode
+        s.depth_threshold = self.depth_threshold
+        s.time_stages = 1 if self.time_stages else 0
+        s.count_splats = 1 if self.count_splats else 0
+        s.counters_tag = self.counters_tag
+        return s
+
+
+@dataclass
+class RenderTargets:
+    """TileRasterizer.h:421-450 plus P: CUDA tensors, bottom row first."""
+    width: int = 0
+    height: int = 0
+    colour: torch.Tensor | None = None     # (h*w, 4) float32, premultiplied linear
+    depth: torch.Tensor | None = None      # (h*w,) float32, view z
+    position: torch.Tensor | None = None   # (h*w, 4) float32, world xyz (optional)
+
+    @staticmethod
+    def make(width: int, height: int, position: bool = False, device="cuda") -> "RenderTargets":
+        n = width * height
+        return RenderTargets(width, height, torch.empty((n, 4), dtype=torch.float32, device=device),
+                             torch.empty(n, dtype=torch.float32, device=device),
+                             torch.empty((n, 4), dtype=torch.float32, device=device) if position else None)
+
+
+def _instances(instances) -> tuple:
+    arr = (N.Instance * max(len(instances), 1))()
+    for k, inst in enumerate(instances):
+        s = inst.splats
+        a = arr[k]
+        if s is not None and s.count:
+            a.positions = _ptr(s.positions)
+            a.shape = _ptr(s.shape)
+            a.sh = _ptr(s.sh)
+            a.count = s.count
+            a.rest_per_colour = s.rest_per_colour
+            a.sh_words = s.sh_words
+            a.linear = 1 if s.linear else 0
+            a.antialiased = s.antialiased
+        a.object_to_world[:] = list(_mat(inst.object_to_world).reshape(16))
+        e = inst.edit
+        a.edit.active = 1 if e.active else 0
+        a.edit.shape, a.edit.mode, a.edit.invert = e.shape, e.mode, 1 if e.invert else 0
+        a.edit.centre[:], a.edit.size[:], a.edit.tint[:] = list(e.centre), list(e.size), list(e.tint)
+        a.edit.saturation, a.edit.brightness, a.edit.opacity = e.saturation, e.brightness, e.opacity
+        a.edit.min_opacity, a.edit.max_scale = e.min_opacity, e.max_scale
+    return arr, len(instances)
+
+
+@dataclass
+class FrameStats:
+    """TileRasterizer.h:408-419."""
+    splats: int = 0
+    visible: int = 0
+    pairs: int = 0
+    project_ms: float = 0.0
+    counts_ms: float = 0.0
+    depth_sort_ms: float = 0.0
+    emit_ms: float = 0.0
+    tile_sort_ms: float = 0.0
+    blend_ms: float = 0.0
+    total_ms: float = 0.0
+
+
+@dataclass
+class SplatCounters:
+    """TileRasterizer.h:333-401."""
+    tag: int
+    slots: int
+    visible: int
+    pairs: int
+    max_tiles: int
+    culled: list
+
+
+class TileRasterizer:
+    """render::TileRasterizer (TileRasterizer.h:452-487)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @staticmethod
+    def create() -> "TileRasterizer":
+        h = C.c_void_p()
+        check(N.lib().ath_raster_create(C.byref(h)))
+        return TileRasterizer(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            N.lib().ath_raster_destroy(h)
+            self._h = None
+
+    def render(self, camera, instances, settings: RenderSettings, targets: RenderTargets,
+               stream: torch.cuda.Stream | None = None) -> FrameStats:
+        """render(const Camera&/const Projection&, ...) -> FrameStats (TileRasterizer.cpp:287-1295)."""
+        proj = camera.projection_for(settings.width, settings.height) if isinstance(camera, Camera) else camera
+        arr, n = _instances(instances)
+        t = N.Targets(targets.width, targets.height, _ptr(targets.colour), _ptr(targets.depth),
+                      _ptr(targets.position))
+        stats = N.FrameStats()
+        dev = targets.colour.device if targets.colour is not None else torch.device("cuda")
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        check(N.lib().ath_raster_render(self._h, C.byref(proj), arr, n, C.byref(settings._native()), C.byref(t),
+                                        C.byref(stats), C.c_void_p(s.cuda_stream)))
+        return FrameStats(*[getattr(stats, f) for f, _ in N.FrameStats._fields_])
+
+    def latest_counters(self) -> SplatCounters | None:
+        """latestCounters (TileRasterizer.h:478): None until a counted frame finished."""
+        c = N.SplatCounters()
+        status = N.lib().ath_raster_latest_counters(self._h, C.byref(c))
+        if status == 2:
+            return None
+        check(status)
+        return SplatCounters(c.tag, c.slots, c.visible, c.pairs, c.max_tiles, list(c.culled))
+
+    def release_scratch(self) -> None:
+        """releaseScratch (TileRasterizer.h:482)."""
+        check(N.lib().ath_raster_release_scratch(self._h))

@@ -1,0 +1,252 @@
+/*
+ * athenea-b200: the Gaussian-splat tile rasteriser of athenea, for B200
+ * (sm_100a), behind a C ABI.
+ *
+ * Each entry point replaces one member of the reference's
+ * render::TileRasterizer (modules/render/include/athenea/render/TileRasterizer.h)
+ * or of the camera helpers it is driven by (modules/render/src/Camera.cpp); the
+ * comment above each names the interface and file:line it stands in for.
+ *
+ * Conventions (the reference's, splat/frame.slang:22-30): view +z forward, x
+ * right, y up; images bottom row first; pixel centres at +0.5; colour is
+ * premultiplied linear RGBA.
+ *
+ * Memory: every pointer a caller passes that a kernel reads or writes is device
+ * memory the caller owns (GpuSplats and RenderTargets are the caller's in the
+ * reference too). The rasteriser owns its scratch, grows it by half again when
+ * a frame needs more (TileRasterizer.cpp:30-36) and gives it back on
+ * ath_raster_release_scratch (:178-191).
+ *
+ * Errors: every function returns an ath_status; the message of the last failure
+ * on the calling thread is ath_last_error_message(). Nothing throws across the
+ * ABI. A handle is one camera's frame at a time and is not re-entrant
+ * (TileRasterizer.h:316-317): use one handle per thread or stream.
+ */
+#ifndef ATHENEA_RASTER_H
+#define ATHENEA_RASTER_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* core/Error.h:14-26 (ErrorCode), in its order, after ATH_OK; plus ATH_E_TIMEOUT
+ * for a bounded device wait that gave up (the sort's look-back) and
+ * ATH_E_CAPACITY for a frame whose pairs outgrew a caller-fixed capacity. */
+typedef enum {
+    ATH_OK = 0,
+    ATH_E_UNKNOWN = 1,
+    ATH_E_NOT_FOUND = 2,
+    ATH_E_INVALID_ARGUMENT = 3,
+    ATH_E_UNSUPPORTED = 4,
+    ATH_E_IO_FAILURE = 5,
+    ATH_E_DEVICE_FAILURE = 6,
+    ATH_E_SHADER_FAILURE = 7,
+    ATH_E_PLUGIN_FAILURE = 8,
+    ATH_E_OUT_OF_MEMORY = 9,
+    ATH_E_CANCELLED = 10,
+    ATH_E_INTERNAL = 11,
+    ATH_E_TIMEOUT = 12,
+    ATH_E_CAPACITY = 13
+} ath_status;
+
+typedef struct ath_raster ath_raster;
+
+/* Camera.h:89-117 (Lens) and :119-126 (Camera). Matrices are row-major 4x4
+ * acting on column vectors (p' = M p). */
+typedef struct {
+    double camera_to_world[16];
+    int32_t orthographic;
+    double focal;             /* mm */
+    double haperture;         /* mm */
+    double near_z, far_z;
+    double window_translate[2];
+    double window_scale[2];
+    double window_roll;       /* degrees, counter-clockwise */
+} ath_camera;
+
+/* Camera.h:129-155 (Projection): what the kernels need of a camera for one image size. */
+typedef struct {
+    double world_to_view[16]; /* +z forward */
+    double focal_x, focal_y;  /* pixels per unit of x/z (perspective) or per world unit (ortho) */
+    double centre_x, centre_y;
+    double near_z, far_z;
+    int32_t orthographic;
+    double eye_world[3];
+} ath_projection;
+
+/* TileRasterizer.h:38-60 (SplatEdit); common/edit.slang. */
+typedef struct {
+    int32_t active;
+    uint32_t shape;           /* 0 box, 1 sphere */
+    uint32_t mode;            /* 0 keep inside, 1 remove inside, 2 grade inside */
+    int32_t invert;
+    float centre[3], size[3], tint[3];
+    float saturation, brightness, opacity, min_opacity, max_scale;
+} ath_edit;
+
+/* scene::GpuSplats (scene/GpuClouds.h:44-52) with SplatInstance
+ * (TileRasterizer.h:85-172): device pointers in the reference's packed layout
+ * (common/packing.slang:5-27):
+ *   positions  float4 a splat: xyz, opacity
+ *   shape      uint4 a splat:  [0] 10-bit smallest-three quaternion, [1] f16 ln sx | ln sy,
+ *                              [2] f16 ln sz | base r, [3] base g | base b
+ *   sh         sh_words uint a splat: f16 rest coefficients, rgb per basis */
+typedef struct {
+    const float* positions;
+    const uint32_t* shape;
+    const uint32_t* sh;
+    uint32_t count;
+    uint32_t rest_per_colour;  /* 0, 3, 8 or 15 */
+    uint32_t sh_words;         /* rest_per_colour == 0 ? 1 : (3 rest_per_colour + 1) / 2 */
+    int32_t linear;            /* 1: colours are linear light; 0: sRGB, decoded per splat */
+    int32_t antialiased;       /* what the cloud's file said: -1 nothing, 0 no, 1 yes */
+    double object_to_world[16];
+    ath_edit edit;
+} ath_instance;
+
+/* The plain-path subset of RenderSettings (TileRasterizer.h:248-371). */
+typedef struct {
+    uint32_t width, height;
+    int32_t antialias;          /* default 1 */
+    int32_t antialias_override; /* -1 none, else 0/1 */
+    float made_spread;
+    int32_t surfels;            /* default 1 */
+    uint32_t max_sh_degree;     /* default 3 */
+    float background[4];        /* premultiplied linear */
+    uint32_t depth_mode;        /* 0 alpha-weighted mean, 1 first threshold crossing */
+    float depth_threshold;      /* default 0.5 */
+    int32_t time_stages;        /* wait after each stage and fill the *_ms stats */
+    int32_t count_splats;       /* count culls by reason (ath_raster_latest_counters) */
+    uint64_t counters_tag;
+} ath_settings;
+
+/* RenderTargets (TileRasterizer.h:421-450) plus the P layer
+ * (usd/aov_position.slang): caller-owned device buffers of width*height,
+ * bottom row first. position may be NULL. */
+typedef struct {
+    uint32_t width, height;
+    float* colour;    /* float4, premultiplied linear */
+    float* depth;     /* float, view z */
+    float* position;  /* float4 world xyz, 1 (zeros where nothing drew); optional */
+} ath_targets;
+
+/* FrameStats (TileRasterizer.h:408-419). */
+typedef struct {
+    uint32_t splats, visible, pairs;
+    double project_ms, counts_ms, depth_sort_ms, emit_ms, tile_sort_ms, blend_ms, total_ms;
+} ath_frame_stats;
+
+/* SplatCounters (TileRasterizer.h:333-401); culled[] in splat/frame.slang:42-49's numbering. */
+typedef struct {
+    uint64_t tag;
+    uint32_t slots, visible, pairs, max_tiles;
+    uint32_t culled[7];
+} ath_splat_counters;
+
+/* ---- camera helpers ----------------------------------------------------- */
+
+/* Camera::lookingAt (Camera.cpp:9-25). up may be NULL for +Y. */
+ath_status ath_camera_looking_at(const double eye[3], const double target[3], const double up[3], ath_camera* out);
+/* A camera with the reference's defaults (Camera.h:89-121): at the origin, looking down -Z. */
+ath_status ath_camera_default(ath_camera* out);
+/* projectionFor (Camera.cpp:32-64). */
+ath_status ath_projection_for(const ath_camera* camera, uint32_t width, uint32_t height, ath_projection* out);
+/* RenderSettings' defaults (TileRasterizer.h:248-371). */
+ath_status ath_settings_default(ath_settings* out);
+
+/* ---- the rasteriser ------------------------------------------------------ */
+
+/* TileRasterizer::create (TileRasterizer.h:454). Binds the current CUDA device. */
+ath_status ath_raster_create(ath_raster** out);
+/* ~TileRasterizer: frees the scratch; the handle is gone. */
+void ath_raster_destroy(ath_raster* r);
+/* TileRasterizer::releaseScratch (TileRasterizer.h:482; TileRasterizer.cpp:178-191). */
+ath_status ath_raster_release_scratch(ath_raster* r);
+
+/* TileRasterizer::render(const Projection&, span<const SplatInstance>,
+ * const RenderSettings&, RenderTargets&) (TileRasterizer.h:468-474;
+ * TileRasterizer.cpp:296-1295). Enqueued on `stream` (a cudaStream_t; NULL:
+ * the legacy default stream). Like the reference it reads the frame's visible
+ * and pair totals back once mid-frame to size the pairs exactly; `stats` is
+ * filled from those. Targets must be width x height of `settings`. */
+ath_status ath_raster_render(ath_raster* r, const ath_projection* projection, const ath_instance* instances,
+                             uint32_t instance_count, const ath_settings* settings, ath_targets* targets,
+                             ath_frame_stats* stats, void* stream);
+
+/* TileRasterizer::latestCounters (TileRasterizer.h:478). ATH_E_NOT_FOUND
+ * until a frame drawn with count_splats has finished. */
+ath_status ath_raster_latest_counters(ath_raster* r, ath_splat_counters* out);
+
+/* The last frame's intermediate buffers, for inspection (what the reference's
+ * tests read through its Buffer handles). Device pointers owned by the
+ * rasteriser, valid until its next render or release_scratch:
+ *   records    12 floats a slot: screen (centre xy, view z, cutoff), conic (a b c, alpha),
+ *              colour (rgb, 0) -- splat/frame.slang:269-281's ProjRecord without the surfel
+ *              word; written for kept slots only
+ *   rects      2 words a slot: x0 | y0 << 16, x1 | y1 << 16 (inclusive tiles; kept slots)
+ *   keys       a slot: the 24-bit depth key, or 0xFF000000 | cull reason (frame.slang:42-49)
+ *   offsets    a slot: its first pair (exclusive scan of tiles touched)
+ *   pair_keys, pair_splats   the sorted pairs: tile << 24 | depth key, and the slot
+ *   ranges     2 a tile: [start, end) into the sorted pairs (splat_ranges.slang) */
+typedef struct {
+    uint32_t slots, pairs, tiles;
+    const float* records;
+    const uint32_t* rects;
+    const uint32_t* keys;
+    const uint32_t* offsets;
+    const uint64_t* pair_keys;
+    const uint32_t* pair_splats;
+    const uint32_t* ranges;
+} ath_frame_buffers;
+
+ath_status ath_raster_frame_buffers(ath_raster* r, ath_frame_buffers* out);
+
+/* ---- the radix sort: gpu::RadixSort (modules/gpu/include/athenea/gpu/algo/RadixSort.h;
+ * RadixSort.cpp:95-261) ---------------------------------------------------- */
+
+typedef struct ath_sorter ath_sorter;
+
+/* RadixSort::create. Owns the sort's working memory (histograms, look-back words). */
+ath_status ath_sorter_create(ath_sorter** out);
+void ath_sorter_destroy(ath_sorter* s);
+
+/* RadixSort::sort(batch, SortBuffers, count, keyBits): sorts the first `count`
+ * (key, value) pairs stably by the low `key_bits` bits (1..64) of the key,
+ * eight bits a pass. keys/values hold the input and receive the result; the
+ * scratch pair (as SortBuffers' scratchKeys/scratchValues) holds count
+ * entries each. An odd number of passes ends with a copy back. Enqueued on
+ * `stream`, not waited for. */
+ath_status ath_sorter_sort(ath_sorter* s, uint64_t* keys, uint32_t* values, uint64_t* scratch_keys,
+                           uint32_t* scratch_values, uint32_t count, uint32_t key_bits, void* stream);
+
+/* ---- decode: scene::CloudLoader::upload's kernels ------------------------ */
+
+/* scene/splat_validate.slang:16-31 + scene/splat_decode.slang:45-173 for
+ * 3DGS-encoded float records (io::SplatEncoding: logit opacity, log scale,
+ * wxyz rotation, SH DC, rest colour-outer). `records` is device memory,
+ * `count` records of `stride` floats; field indices as named. The valid
+ * records are written compacted, in file order, to positions/shape/sh (room
+ * for `count` splats); *kept receives how many (a device-to-host read). */
+typedef struct {
+    uint32_t stride;
+    uint32_t x, y, z, opacity, scale0, scale1, scale2, rot_w, rot_x, rot_y, rot_z, dc0, dc1, dc2;
+    uint32_t rest_base, file_per_colour, keep_per_colour;
+} ath_encoding;
+
+ath_status ath_decode_records(const float* records, uint32_t count, const ath_encoding* encoding, float* positions,
+                              uint32_t* shape, uint32_t* sh, uint32_t* kept, void* stream);
+
+/* ---- diagnostics --------------------------------------------------------- */
+
+/* The message of the last failure on this thread ("" when none). */
+const char* ath_last_error_message(void);
+/* Version of this library, "major.minor.patch". */
+const char* ath_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

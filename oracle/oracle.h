@@ -1,0 +1,185 @@
+/*
+ * ORACLE -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A CPU restatement of athenea's Gaussian-splat tile rasteriser (the plain
+ * path of render::TileRasterizer and the Slang kernels it dispatches), written
+ * from the reference's shader sources and used as the checker for the CUDA
+ * product. Nothing in the product links, loads or calls this code: only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg do.
+ *
+ * Parity status: the reference cannot run here (it needs Slang, slang-rhi and a
+ * GPU). The restatement is pinned against the reference's own known-answer
+ * tests (tests/render/test_splat_render.cpp:130-206, :1831-1917,
+ * tests/scene/test_loading.cpp:91-166, tests/gpu/test_algo.cpp:347-379), which
+ * the test suite re-runs against it. Bit-level parity with the Slang build is
+ * unpinned where Slang maps exp/log/pow to a vendor library: this restatement
+ * uses its own exp/log (Cody-Waite reduction, Taylor and atanh series), and so
+ * does the product, which is what makes keys, rects, counts, ranges and images
+ * comparable bit for bit between the two.
+ *
+ * Arithmetic rules (so the CUDA side can reproduce every bit): IEEE float32,
+ * no contraction of a*b+c into fma (built with -ffp-contract=off), expressions
+ * evaluated left to right exactly as the Slang source writes them.
+ */
+#ifndef ATHENEA_ORACLE_H
+#define ATHENEA_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* common/edit.slang:23-36 (EditParams). */
+typedef struct {
+    uint32_t active, shape, mode, invert;
+    float centre[3];
+    float size[3];
+    float tint[3];
+    float saturation, brightness, opacity, minOpacity, maxScale;
+} orc_edit;
+
+/* The subset of splat/frame.slang:51-230 (FrameParams) the plain path reads,
+ * as setFrame/setObject/setCloudSpace fill it (modules/render/src/FrameParams.h:32-117). */
+typedef struct {
+    uint32_t width, height, tilesX, tilesY;
+    float focalX, focalY, centreX, centreY, nearZ, farZ;
+    uint32_t orthographic, antialias;
+    float paidAt;
+    uint32_t surfels;
+    float m[12];      /* object -> view, rows of a 3x4 */
+    float eye[3];     /* the camera in the cloud's own space */
+    uint32_t restPerColour, shWords, shLimit, linearCloud;
+    uint32_t depthMode;
+    float depthThreshold;
+    float bg[4];
+    orc_edit edit;
+} orc_frame;
+
+/* 3DGS record layout (io::SplatEncoding) for the decode. Field indices into a
+ * record of `stride` floats; rest coefficients colour-outer (r..., g..., b...). */
+typedef struct {
+    uint32_t stride;
+    uint32_t x, y, z, opacity, scale0, scale1, scale2, rotW, rotX, rotY, rotZ, dc0, dc1, dc2;
+    uint32_t restBase, filePerColour, keepPerColour;
+} orc_encoding;
+
+/* ---- scalar helpers the product must agree with (exposed for unit tests) ---- */
+float orc_exp(float x);
+float orc_log(float x);
+float orc_pow(float x, float y);
+uint16_t orc_f32_to_f16(float v);
+float orc_f16_to_f32(uint16_t h);
+uint32_t orc_encode_quaternion(const float q[4]);
+void orc_decode_quaternion(uint32_t word, float q[4]);
+
+/* ---- decode: scene/splat_validate.slang + scene/splat_decode.slang ----
+ * Records that fail validation are dropped and the rest compacted in file
+ * order. Returns the number kept. shWords = keep == 0 ? 1 : (3 keep + 1) / 2. */
+uint32_t orc_decode(const float* records, uint32_t count, const orc_encoding* e, float* positions,
+                    uint32_t* shape, uint32_t* sh, uint32_t* origin);
+
+/* ---- camera: modules/render/src/Camera.cpp:9-64 (double precision) ---- */
+typedef struct {
+    double cameraToWorld[16]; /* row-major, column vectors (p' = M p) */
+    uint32_t orthographic;
+    double focal, haperture, nearZ, farZ;
+    double windowTranslate[2], windowScale[2], windowRoll;
+} orc_camera;
+
+typedef struct {
+    double worldToView[16];
+    double focalX, focalY, centreX, centreY, nearZ, farZ;
+    uint32_t orthographic;
+    double eyeWorld[3];
+} orc_projection;
+
+void orc_camera_looking_at(const double eye[3], const double target[3], const double up[3], orc_camera* out);
+void orc_projection_for(const orc_camera* camera, uint32_t width, uint32_t height, orc_projection* out);
+/* setFrame + setObject + setCloudSpace for one instance (FrameParams.h:32-117;
+ * TileRasterizer.cpp:599-601). antialiased: -1 when the cloud's file says nothing. */
+void orc_frame_for(const orc_projection* p, const double objectToWorld[16], uint32_t width, uint32_t height,
+                   uint32_t antialias, int32_t antialiased, float madeSpread, uint32_t surfels,
+                   uint32_t maxShDegree, uint32_t restPerColour, uint32_t shWords, uint32_t linearCloud,
+                   const float bg[4], uint32_t depthMode, float depthThreshold, const orc_edit* edit,
+                   orc_frame* out);
+
+/* ---- (a) projection: splat/splat_project.slang:497-785,1080-1129 (projectSplat<0>) ----
+ * Per slot base+i: record (12 floats: screen xyzw, conic xyzw, colour rgb + mark),
+ * tile rect (4), tiles touched, depth key (or 0xFF000000 | cull reason), visible. */
+void orc_project(const orc_frame* f, uint32_t count, uint32_t base, const float* positions,
+                 const uint32_t* shape, const uint32_t* sh, float* records, uint32_t* rects,
+                 uint32_t* touched, uint32_t* depthKeys, uint32_t* visible, int threads);
+
+/* ---- (b)+(c) binning, the reference's two-sort form (TileRasterizer.cpp:1088-1176):
+ * compact -> stable 24-bit depth sort -> gather -> scan -> emit -> stable tile sort -> ranges.
+ * pairTiles/pairSplats need `pairs` entries (the sum of touched); ranges 2 per tile.
+ * Returns the number of pairs written. */
+uint64_t orc_bin(const orc_frame* f, uint32_t slots, const float* records, const uint32_t* rects,
+                 const uint32_t* touched, const uint32_t* depthKeys, const uint32_t* visible,
+                 uint32_t* pairTiles, uint32_t* pairSplats, uint32_t* ranges, uint32_t* visibleCount);
+
+/* ---- (d) blend: splat/splat_blend.slang:236-578 (blendPixel<false,false,false>) ----
+ * colour float4 and depth per pixel, bottom row first. finalT / lastContrib
+ * (optional, may be NULL): the transmittance the walk ended with and one past
+ * the index into the tile's pair range of the last record blended (0: none).
+ * Returns the number of (pixel, record) evaluations the walks made. */
+uint64_t orc_blend(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                   const float* records, float* colour, float* depth, float* finalT, uint32_t* lastContrib,
+                   int threads);
+
+/* contributionMode 4 (splat_blend.slang:381-398): per slot four signed words,
+ * weight * dLdPixel.rgb in 1/256 with hash-dithered rounding, and the weight. */
+void orc_colour_gradient(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                         const float* records, const float* dLdPixel, int32_t* contribution);
+
+/* contributionMode 1: the weight each slot blended with, in 1/4096 of a pixel. */
+void orc_contribution_weight(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                             const float* records, uint32_t* contribution);
+
+/* P: usd/aov_position.slang:34-52; viewToWorld rows (3x4, float). */
+void orc_position(uint32_t width, uint32_t height, uint32_t orthographic, float focalX, float focalY,
+                  float centreX, float centreY, const float viewToWorld[12], const float* depth,
+                  float* position);
+
+/* ---- FP64 oracle ----
+ * The same plain path evaluated in double from the same packed inputs (fp16
+ * fields widened exactly), binned with the exact tile test, sorted per tile by
+ * (view depth, slot) -- reference/reference_blend.slang's order -- and blended
+ * in double. `near` (optional) receives, per pixel, 1 where a blend decision
+ * (cutoff, 1/255, T < 1e-4) of some record lies within `margin` relative of
+ * its threshold: a pixel where float rounding may legitimately decide
+ * otherwise. One instance per call, as the FP32 path's orc_project. */
+typedef struct {
+    double focalX, focalY, centreX, centreY, nearZ, farZ;
+    uint32_t width, height, orthographic, antialias;
+    double paidAt;
+    double m[12];
+    double eye[3];
+    uint32_t restPerColour, shWords, shLimit, linearCloud;
+    double bg[4];
+} orc_frame64;
+
+void orc_frame64_from(const orc_projection* p, const double objectToWorld[16], uint32_t width, uint32_t height,
+                      uint32_t antialias, uint32_t maxShDegree, uint32_t restPerColour, uint32_t shWords,
+                      uint32_t linearCloud, const double bg[4], orc_frame64* out);
+
+/* Renders `count` splats; only pixels whose tile index satisfies
+ * tile % tileStride == tileOffset are written (a sampled check at scale);
+ * others are left as they are. */
+void orc_render_f64(const orc_frame64* f, uint32_t count, const float* positions, const uint32_t* shape,
+                    const uint32_t* sh, double* colour, double* depth, uint8_t* nearDecision, double margin,
+                    uint32_t tileStride, uint32_t tileOffset, int threads);
+
+/* The same FP64 path from FP32 training parameters (means, log-scales,
+ * quaternion wxyz unnormalised, opacity logit, 48 SH floats a splat rgb per
+ * basis with the DC first): the function the gradients are checked against. */
+void orc_render_params_f64(const orc_frame64* f, uint32_t count, const double* means, const double* logScales,
+                           const double* quats, const double* logits, const double* shs, uint32_t shDegree,
+                           double* colour, double* depth, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
