@@ -20,9 +20,10 @@ namespace {
 constexpr uint32_t kBlendThreads = kTile * kTile;
 
 __global__ void __launch_bounds__(kBlendThreads)
-    blendKernel(const FrameConst F, const uint2* __restrict__ ranges, const uint32_t* __restrict__ pairValues,
-                const float4* __restrict__ recs, float4* __restrict__ colour, float* __restrict__ depth,
-                float4* __restrict__ position, float* __restrict__ finalT, uint32_t* __restrict__ lastContrib) {
+    blendKernel(const FrameConst F, uint32_t pairs, uint32_t slots, const uint2* __restrict__ ranges,
+                const uint32_t* __restrict__ pairValues, const float4* __restrict__ recs, float4* __restrict__ colour,
+                float* __restrict__ depth, float4* __restrict__ position, float* __restrict__ finalT,
+                uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ status) {
     __shared__ float4 sScreen[kBlendThreads];
     __shared__ float4 sConic[kBlendThreads];
     __shared__ float4 sColour[kBlendThreads];
@@ -32,7 +33,11 @@ __global__ void __launch_bounds__(kBlendThreads)
     const uint32_t px = tx * kTile + (threadIdx.x % kTile);
     const uint32_t py = ty * kTile + (threadIdx.x / kTile);
     const bool inside = px < F.width && py < F.height;
-    const uint2 range = ranges[tile];
+    uint2 range = ranges[tile];
+    if (range.y > pairs || range.x > range.y) {   // never, for ranges the sort wrote
+        if (threadIdx.x == 0) atomicOr(status, kStatusIndexRange);
+        range = make_uint2(0, 0);
+    }
     const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
 
     float r = 0.0f, g = 0.0f, bl = 0.0f;
@@ -43,7 +48,11 @@ __global__ void __launch_bounds__(kBlendThreads)
         if (__syncthreads_count(done) == kBlendThreads) break;
         const uint32_t mine = first + threadIdx.x;
         if (mine < range.y) {
-            const uint32_t s = pairValues[mine];
+            uint32_t s = pairValues[mine];
+            if (s >= slots) {
+                atomicOr(status, kStatusIndexRange);
+                s = 0;
+            }
             sScreen[threadIdx.x] = recs[(size_t)s * 3 + 0];
             sConic[threadIdx.x] = recs[(size_t)s * 3 + 1];
             sColour[threadIdx.x] = recs[(size_t)s * 3 + 2];
@@ -97,13 +106,13 @@ __global__ void __launch_bounds__(kBlendThreads)
 
 }   // namespace
 
-cudaError_t launchBlend(const FrameConst& F, const uint2* ranges, const uint32_t* pairValues, const float4* recs,
-                        float4* colour, float* depth, float4* position, float* finalT, uint32_t* lastContrib,
-                        cudaStream_t stream) {
+cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
+                        const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
+                        float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream) {
     const uint32_t tiles = F.tilesX * F.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blendKernel<<<tiles, kBlendThreads, 0, stream>>>(F, ranges, pairValues, recs, colour, depth, position, finalT,
-                                                    lastContrib);
+    blendKernel<<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, depth,
+                                                    position, finalT, lastContrib, status);
     return cudaGetLastError();
 }
 

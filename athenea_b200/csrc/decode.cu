@@ -111,6 +111,10 @@ __global__ void __launch_bounds__(kDecodeThreads)
     __syncthreads();
     if (!valid) return;
     const uint32_t j = (uint32_t)sPrefix + warpBase + __popc(ballot & ((1u << lane) - 1u));
+    if (j >= count) {   // never, for a look-back that completed
+        atomicOr(&words[1], kStatusIndexRange);
+        return;
+    }
     positions[j] = make_float4(p[0], p[1], p[2], clampf(a, 0.0f, 5.0f));
     const float q0 = r[E.rot_x], q1 = r[E.rot_y], q2 = r[E.rot_z], q3 = r[E.rot_w];
     const float qLength = sqrtf(((q0 * q0 + q1 * q1) + q2 * q2) + q3 * q3);

@@ -427,11 +427,14 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
     if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
     if (err != cudaSuccess) return failCuda(err, "projecting the splats");
     mark(2);
-    if (wordsHost[kWordSticky] & kStatusLookbackTimeout) {
-        // Raised by the sort of a frame that did not wait for its end: that
-        // frame is not valid, and neither is this one's report of it.
+    if (wordsHost[kWordSticky] & (kStatusLookbackTimeout | kStatusIndexRange)) {
+        // Raised after the read of a frame that did not wait for its end: that
+        // frame is not valid, and this call reports it.
+        const uint32_t bits = wordsHost[kWordSticky];
         cudaMemsetAsync(words + kWordSticky, 0, sizeof(uint32_t), stream);
-        return fail(ATH_E_TIMEOUT, "a look-back wait of the previous frame's sort gave up (bounded spin)");
+        if (bits & kStatusLookbackTimeout)
+            return fail(ATH_E_TIMEOUT, "a look-back wait of the previous frame's sort gave up (bounded spin)");
+        return fail(ATH_E_INTERNAL, "the previous frame met an index outside its buffers (skipped, not written)");
     }
     if (wordsHost[kWordStatus] & kStatusLookbackTimeout)
         return fail(ATH_E_TIMEOUT, "a look-back wait gave up (bounded spin); the frame is not valid");
@@ -455,13 +458,15 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
                          stream);
     const uint32_t sorted = sortResultIndex(pairs, bits);
     if (err == cudaSuccess) err = cudaMemsetAsync(r->ranges.ptr, 0, (size_t)tiles * 8, stream);
-    if (err == cudaSuccess) err = launchRanges(pairs, keysBuf[sorted], static_cast<uint2*>(r->ranges.ptr), stream);
+    if (err == cudaSuccess)
+        err = launchRanges(pairs, tiles, keysBuf[sorted], static_cast<uint2*>(r->ranges.ptr), words + kWordSticky, stream);
     mark(4);
     // --- blend ---------------------------------------------------------------
     if (err == cudaSuccess)
-        err = launchBlend(F, static_cast<const uint2*>(r->ranges.ptr), valsBuf[sorted],
+        err = launchBlend(F, pairs, slots, static_cast<const uint2*>(r->ranges.ptr), valsBuf[sorted],
                           static_cast<const float4*>(r->recs.ptr), reinterpret_cast<float4*>(targets->colour),
-                          targets->depth, reinterpret_cast<float4*>(targets->position), nullptr, nullptr, stream);
+                          targets->depth, reinterpret_cast<float4*>(targets->position), nullptr, nullptr,
+                          words + kWordSticky, stream);
     mark(5);
     if (err != cudaSuccess) return failCuda(err, "drawing the frame");
     r->lastSlots = slots;
@@ -478,9 +483,12 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
         err = cudaMemcpyAsync(wordsHost, words, (kFrameWords + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
         if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
         if (err != cudaSuccess) return failCuda(err, "reading the frame's counters");
-        if (wordsHost[kWordSticky] & kStatusLookbackTimeout) {
+        if (wordsHost[kWordSticky] & (kStatusLookbackTimeout | kStatusIndexRange)) {
+            const uint32_t bits = wordsHost[kWordSticky];
             cudaMemsetAsync(words + kWordSticky, 0, sizeof(uint32_t), stream);
-            return fail(ATH_E_TIMEOUT, "a look-back wait in the sort gave up (bounded spin); the frame is not valid");
+            if (bits & kStatusLookbackTimeout)
+                return fail(ATH_E_TIMEOUT, "a look-back wait in the sort gave up (bounded spin); the frame is not valid");
+            return fail(ATH_E_INTERNAL, "the frame met an index outside its buffers (skipped, not written)");
         }
         if (s.count_splats) {
             ath_splat_counters& c = r->counters;
@@ -568,9 +576,11 @@ extern "C" ath_status ath_sorter_sort(ath_sorter* s, uint64_t* keys, uint32_t* v
     cudaError_t err = cudaMemcpyAsync(s->wordsHost.ptr, words, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
     if (err != cudaSuccess) return failCuda(err, "ath_sorter_sort");
-    if (static_cast<uint32_t*>(s->wordsHost.ptr)[8] & kStatusLookbackTimeout) {
+    if (const uint32_t bits = static_cast<uint32_t*>(s->wordsHost.ptr)[8]; bits != 0) {
         cudaMemsetAsync(words + 8, 0, sizeof(uint32_t), stream);
-        return fail(ATH_E_TIMEOUT, "a look-back wait of an earlier sort gave up (bounded spin)");
+        if (bits & kStatusLookbackTimeout)
+            return fail(ATH_E_TIMEOUT, "a look-back wait of an earlier sort gave up (bounded spin)");
+        return fail(ATH_E_INTERNAL, "an earlier sort met an index outside its buffers (skipped)");
     }
     err = s->flags.reserve(sortFlagWords(count, keyBits) * 8);
     if (err != cudaSuccess) return failCuda(err, "reserving the sort's look-back words");
@@ -624,6 +634,7 @@ extern "C" ath_status ath_decode_records(const float* records, uint32_t count, c
     if (err != cudaSuccess) return failCuda(err, "decoding the records");
     const uint32_t* w = static_cast<const uint32_t*>(host.ptr);
     if (w[1] & kStatusLookbackTimeout) return fail(ATH_E_TIMEOUT, "the decode's compaction gave up waiting");
+    if (w[1] & kStatusIndexRange) return fail(ATH_E_INTERNAL, "the decode's compaction went outside its buffers");
     *kept = w[2];
     return ATH_OK;
 }

@@ -21,7 +21,8 @@ cudaError_t launchProject(const FrameConst& F, const InstanceConst* inst, uint32
 cudaError_t launchEmit(const FrameConst& F, uint32_t slots, const float4* recs, const uint2* rects,
                        const uint32_t* keys, const uint32_t* offsets, const uint32_t* words, uint64_t capacity,
                        uint64_t* pairKeys, uint32_t* pairValues, cudaStream_t stream);
-cudaError_t launchRanges(uint32_t pairs, const uint64_t* pairKeys, uint2* ranges, cudaStream_t stream);
+cudaError_t launchRanges(uint32_t pairs, uint32_t tiles, const uint64_t* pairKeys, uint2* ranges, uint32_t* status,
+                         cudaStream_t stream);
 
 // sort.cu
 uint32_t sortPasses(uint32_t bits);
@@ -33,9 +34,9 @@ cudaError_t launchSort(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_
                        uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream);
 
 // blend.cu
-cudaError_t launchBlend(const FrameConst& F, const uint2* ranges, const uint32_t* pairValues, const float4* recs,
-                        float4* colour, float* depth, float4* position, float* finalT, uint32_t* lastContrib,
-                        cudaStream_t stream);
+cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
+                        const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
+                        float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream);
 
 // decode.cu
 uint32_t decodeBlocks(uint32_t count);

@@ -326,10 +326,15 @@ __global__ void __launch_bounds__(256)
 // splat_ranges.slang:11-25 over the sorted keys; ranges were cleared first
 // (splat_tiles_clear.slang).
 __global__ void __launch_bounds__(256)
-    rangesKernel(uint32_t pairs, const uint64_t* __restrict__ pairKeys, uint2* __restrict__ ranges) {
+    rangesKernel(uint32_t pairs, uint32_t tiles, const uint64_t* __restrict__ pairKeys, uint2* __restrict__ ranges,
+                 uint32_t* __restrict__ status) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pairs) return;
     const uint32_t t = (uint32_t)(pairKeys[i] >> 24);
+    if (t >= tiles) {
+        atomicOr(status, kStatusIndexRange);
+        return;
+    }
     if (i == 0 || (uint32_t)(pairKeys[i - 1] >> 24) != t) ranges[t].x = i;
     if (i + 1 == pairs || (uint32_t)(pairKeys[i + 1] >> 24) != t) ranges[t].y = i + 1;
 }
@@ -357,9 +362,10 @@ cudaError_t launchEmit(const FrameConst& F, uint32_t slots, const float4* recs, 
     return cudaGetLastError();
 }
 
-cudaError_t launchRanges(uint32_t pairs, const uint64_t* pairKeys, uint2* ranges, cudaStream_t stream) {
+cudaError_t launchRanges(uint32_t pairs, uint32_t tiles, const uint64_t* pairKeys, uint2* ranges, uint32_t* status,
+                         cudaStream_t stream) {
     if (pairs == 0) return cudaSuccess;
-    rangesKernel<<<(pairs + 255) / 256, 256, 0, stream>>>(pairs, pairKeys, ranges);
+    rangesKernel<<<(pairs + 255) / 256, 256, 0, stream>>>(pairs, tiles, pairKeys, ranges, status);
     return cudaGetLastError();
 }
 

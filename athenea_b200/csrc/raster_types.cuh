@@ -54,13 +54,20 @@ enum FrameWord : uint32_t {
 enum StatusBit : uint32_t {
     kStatusLookbackTimeout = 1u,   // a look-back gave up waiting (bounded spin)
     kStatusPairOverflow = 2u,      // more pairs than the pair buffers hold
+    kStatusIndexRange = 4u,        // a data-dependent index fell outside its buffer (skipped)
 };
 
 // A look-back word: two status bits over a 62-bit count.
 constexpr uint64_t kFlagAggregate = 1ull << 62;
 constexpr uint64_t kFlagInclusive = 2ull << 62;
 constexpr uint64_t kFlagValue = (1ull << 62) - 1;
-constexpr uint32_t kSpinLimit = 1u << 22;   // ~0.3 s at 64 ns a spin before giving up
+constexpr uint32_t kSpinLimit = 1u << 20;   // spins before a wait gives up (tens of ms)
+
+// Whether some block has already given up: the rest stop waiting at once, so
+// one failure costs one time-out, not one a block.
+__device__ __forceinline__ bool gaveUp(const uint32_t* status) {
+    return (*reinterpret_cast<const volatile uint32_t*>(status) & 1u) != 0;
+}
 
 __device__ __forceinline__ void storeRelaxed(uint64_t* p, uint64_t v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
@@ -105,7 +112,7 @@ __device__ __forceinline__ uint64_t lookbackExclusive(uint64_t* flags, uint32_t 
         const uint32_t first = inclusive ? (uint32_t)(__ffs(inclusive) - 1) : 32u;
         const uint32_t need = first >= 31 ? 0xFFFFFFFFu : ((2u << first) - 1u);
         if (notReady & need) {
-            if (++spins > kSpinLimit) {
+            if (++spins > kSpinLimit || ((spins & 255u) == 0 && gaveUp(status))) {
                 if (lane == 0) atomicOr(status, kStatusLookbackTimeout);
                 break;
             }

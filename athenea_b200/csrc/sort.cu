@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kSortThreads)
             const uint64_t v = loadRelaxed(flags + (size_t)j * kRadix + t);
             const uint32_t st = (uint32_t)(v >> 62);
             if (st == 0) {
-                if (++spins > kSpinLimit) {
+                if (++spins > kSpinLimit || ((spins & 255u) == 0 && gaveUp(status))) {
                     atomicOr(status, kStatusLookbackTimeout);
                     break;
                 }
@@ -166,8 +166,12 @@ __global__ void __launch_bounds__(kSortThreads)
     for (uint32_t s = tid; s < tileN; s += kSortThreads) {
         const uint64_t k = sKeys[s];
         const uint32_t dst = sAdjust[(uint32_t)((k >> shift) & 0xFFu)] + s;
-        keysOut[dst] = k;
-        valsOut[dst] = sVals[s];
+        if (dst < n) {
+            keysOut[dst] = k;
+            valsOut[dst] = sVals[s];
+        } else {
+            atomicOr(status, kStatusIndexRange);
+        }
     }
 }
 

@@ -15,7 +15,7 @@ class _DeviceView:
     """A device buffer the library owns, as torch sees one (__cuda_array_interface__)."""
 
     def __init__(self, ptr: int, shape, typestr: str):
-        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), True),
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
                                          "version": 3, "strides": None}
 
 
