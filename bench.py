@@ -132,6 +132,7 @@ def run_ours(args) -> dict | None:
     recs, enc = make_scene(20261203 + 1)
     cloud = A.CloudLoader.upload(torch.from_numpy(recs.reshape(-1)).to(dev), enc, 3)
     del recs
+    torch.cuda.empty_cache()
     V = WORKLOAD["views"]
     W, H = WORKLOAD["width"], WORKLOAD["height"]
     projs = view_cameras(V, first=rank * V)
@@ -229,7 +230,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--views", type=int, default=WORKLOAD["views"], help="views a GPU draws a step")
+    ap.add_argument("--gaussians", type=int, default=WORKLOAD["count"], help="Gaussians in the scene")
     args = ap.parse_args()
+    WORKLOAD["views"] = args.views
+    WORKLOAD["count"] = args.gaussians
     args.warmup = max(args.warmup, 3)
     rank, world, _ = dist_env()
 
