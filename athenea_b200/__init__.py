@@ -5,10 +5,11 @@ package is the Python mirror of the reference's rasteriser interface over its
 C ABI (include/athenea_raster.h).
 """
 from ._native import AtheneaError  # noqa: F401
-from .raster import (Camera, CloudLoader, FrameStats, GpuSplats, Lens, RenderSettings, RenderTargets,  # noqa: F401
-                     SplatCounters, SplatEdit, SplatInstance, TileRasterizer, encoding_3dgs,
+from .raster import (Camera, CloudLoader, FrameStats, GpuSplats, Lens, Params, RenderSettings,  # noqa: F401
+                     RenderTargets, SplatCounters, SplatEdit, SplatInstance, TileRasterizer, encoding_3dgs, l2_loss,
                      pinhole_for_vertical_fov)
 
-__all__ = ["AtheneaError", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "RenderSettings",
+__all__ = ["AtheneaError", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "Params", "l2_loss",
+           "RenderSettings",
            "RenderTargets", "SplatCounters", "SplatEdit", "SplatInstance", "TileRasterizer", "encoding_3dgs",
            "pinhole_for_vertical_fov"]

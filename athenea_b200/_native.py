@@ -79,7 +79,17 @@ class SplatCounters(C.Structure):
 class FrameBuffers(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("pairs", C.c_uint32), ("tiles", C.c_uint32), ("records", C.c_void_p),
                 ("rects", C.c_void_p), ("keys", C.c_void_p), ("offsets", C.c_void_p), ("pair_keys", C.c_void_p),
-                ("pair_splats", C.c_void_p), ("ranges", C.c_void_p)]
+                ("pair_splats", C.c_void_p), ("ranges", C.c_void_p), ("grads", C.c_void_p)]
+
+
+class Params(C.Structure):
+    _fields_ = [("means", C.c_void_p), ("scales", C.c_void_p), ("quats", C.c_void_p), ("sh", C.c_void_p),
+                ("count", C.c_uint32), ("sh_degree", C.c_uint32), ("sh_stride", C.c_uint32), ("linear", C.c_int32),
+                ("object_to_world", C.c_double * 16)]
+
+
+class ParamGrads(C.Structure):
+    _fields_ = [("means", C.c_void_p), ("scales", C.c_void_p), ("quats", C.c_void_p), ("sh", C.c_void_p)]
 
 
 class Encoding(C.Structure):
@@ -101,6 +111,10 @@ SIGNATURES = {
     "ath_raster_render": (C.c_int32, [_P, C.POINTER(Projection), _P, C.c_uint32, C.POINTER(Settings),
                                       C.POINTER(Targets), C.POINTER(FrameStats), _P]),
     "ath_raster_latest_counters": (C.c_int32, [_P, C.POINTER(SplatCounters)]),
+    "ath_raster_render_params": (C.c_int32, [_P, C.POINTER(Projection), C.POINTER(Params), C.POINTER(Settings),
+                                             C.POINTER(Targets), C.POINTER(FrameStats), _P]),
+    "ath_raster_backward": (C.c_int32, [_P, _P, _P, C.POINTER(ParamGrads), _P]),
+    "ath_l2_loss": (C.c_int32, [_P, _P, C.c_uint32, _P, _P, _P]),
     "ath_raster_frame_buffers": (C.c_int32, [_P, C.POINTER(FrameBuffers)]),
     "ath_sorter_create": (C.c_int32, [C.POINTER(C.c_void_p)]),
     "ath_sorter_destroy": (None, [_P]),

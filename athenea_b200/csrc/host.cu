@@ -16,6 +16,7 @@
 #include "../../include/athenea_raster.h"
 #include "host_util.h"
 #include "kernels.h"
+#include "gauss.cuh"
 #include "raster_types.cuh"
 
 using namespace ath;
@@ -34,6 +35,12 @@ struct ath_raster {
     ath_splat_counters counters{};
     cudaEvent_t marks[8] = {};
     uint32_t lastSlots = 0, lastPairs = 0, lastTiles = 0, lastSorted = 0;   // what frame_buffers describes
+    FrameConst lastFrame{};
+    // the differentiable frame's state (ath_raster_render_params -> ath_raster_backward)
+    DeviceBuffer finalT, lastContrib, grads;
+    bool trainingValid = false;
+    InstanceConst trainingInstance{};
+    const float* trainingDepth = nullptr;
 };
 
 struct ath_sorter {
@@ -307,8 +314,9 @@ extern "C" ath_status ath_raster_release_scratch(ath_raster* r) {
     r->slotCapacity = r->pairCapacity = r->tileCapacity = r->instanceCapacity = 0;
     for (DeviceBuffer* b : {&r->recs, &r->rects, &r->keys, &r->offsets, &r->projectFlags, &r->instances,
                             &r->pairKeys[0], &r->pairKeys[1], &r->pairVals[0], &r->pairVals[1], &r->sortHist,
-                            &r->sortFlags, &r->ranges})
+                            &r->sortFlags, &r->ranges, &r->finalT, &r->lastContrib, &r->grads})
         b->release();
+    r->trainingValid = false;
     r->instanceStage.release();
     return ATH_OK;
 }
@@ -354,32 +362,27 @@ ath_status reservePairs(ath_raster* r, uint32_t pairs, uint32_t bits) {   // res
 
 }   // namespace
 
-extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* projection, const ath_instance* instances,
-                                        uint32_t instanceCount, const ath_settings* settings, ath_targets* targets,
-                                        ath_frame_stats* stats, void* streamPtr) {
-    if (!r || !projection || !settings || !targets || (instanceCount && !instances))
-        return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render: null argument");
-    const auto frameStart = std::chrono::steady_clock::now();
-    const ath_settings& s = *settings;
+namespace {
+
+ath_status checkFrame(const ath_settings& s, const ath_targets& targets) {
     // TileRasterizer.cpp:302-325
     if (s.width == 0 || s.height == 0) return fail(ATH_E_INVALID_ARGUMENT, "a frame needs a size");
     if (s.width > 0xFFFFu * kTileSize || s.height > 0xFFFFu * kTileSize)
         return fail(ATH_E_UNSUPPORTED, "a frame wider or taller than 65535 tiles");
-    if (targets->width != s.width || targets->height != s.height)
+    if (targets.width != s.width || targets.height != s.height)
         return fail(ATH_E_INVALID_ARGUMENT, "the targets are not the frame's size");
-    if (!targets->colour || !targets->depth) return fail(ATH_E_INVALID_ARGUMENT, "the targets need colour and depth");
-    uint64_t total = 0;
-    for (uint32_t k = 0; k < instanceCount; ++k) {
-        const ath_status v = validInstance(instances[k], k);
-        if (v != ATH_OK) return v;
-        total += instances[k].count;
-    }
-    if (total > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 splats in one frame");
-    const uint32_t slots = (uint32_t)total;
-    DeviceGuard guard(r->device);
-    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (!targets.colour || !targets.depth) return fail(ATH_E_INVALID_ARGUMENT, "the targets need colour and depth");
+    return ATH_OK;
+}
 
-    const FrameConst F = frameConstFor(*projection, s);
+// One frame: project (scan fused), the one mid-frame read, emit, sort, ranges,
+// blend. `staged` is the instance table in host memory (pinned staging).
+// `training` also keeps, per pixel, the final transmittance and the last
+// record blended, for the backward.
+ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, uint32_t instanceCount,
+                     uint32_t slots, uint32_t layout, const ath_settings& s, ath_targets* targets,
+                     ath_frame_stats* stats, cudaStream_t stream, bool training) {
+    const auto frameStart = std::chrono::steady_clock::now();
     const uint32_t tiles = F.tilesX * F.tilesY;
     const uint32_t bits = 24 + F.tileBits;
     ath_status st = reserveSlots(r, std::max(slots, 1u));
@@ -389,18 +392,11 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
             return failCuda(err, "reserving the tiles' ranges");
         r->tileCapacity = tiles;
     }
-    if (instanceCount > r->instanceCapacity || !r->instances.bytes) {
-        const uint32_t n = std::max(instanceCount, 4u);
-        cudaError_t err = r->instances.reserve((size_t)n * sizeof(InstanceConst));
-        if (err == cudaSuccess) err = r->instanceStage.reserve((size_t)n * sizeof(InstanceConst));
-        if (err != cudaSuccess) return failCuda(err, "reserving the instance table");
-        r->instanceCapacity = n;
-    }
-    InstanceConst* staged = static_cast<InstanceConst*>(r->instanceStage.ptr);
-    uint32_t base = 0;
-    for (uint32_t k = 0; k < instanceCount; ++k) {
-        staged[k] = instanceConstFor(*projection, s, instances[k], base);
-        base += instances[k].count;
+    if (training) {
+        const size_t pixels = (size_t)F.width * F.height;
+        cudaError_t err = r->finalT.reserve(pixels * 4);
+        if (err == cudaSuccess) err = r->lastContrib.reserve(pixels * 4);
+        if (err != cudaSuccess) return failCuda(err, "reserving the backward's per-pixel state");
     }
     uint32_t* words = static_cast<uint32_t*>(r->words.ptr);
     uint32_t* wordsHost = static_cast<uint32_t*>(r->wordsHost.ptr);
@@ -416,7 +412,7 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
         err = cudaMemcpyAsync(r->instances.ptr, staged, instanceCount * sizeof(InstanceConst), cudaMemcpyHostToDevice,
                               stream);
     if (err == cudaSuccess)
-        err = launchProject(F, static_cast<const InstanceConst*>(r->instances.ptr), instanceCount, slots,
+        err = launchProject(F, static_cast<const InstanceConst*>(r->instances.ptr), instanceCount, slots, layout,
                             s.count_splats != 0, static_cast<float4*>(r->recs.ptr), static_cast<uint2*>(r->rects.ptr),
                             static_cast<uint32_t*>(r->keys.ptr), static_cast<uint32_t*>(r->offsets.ptr),
                             static_cast<uint64_t*>(r->projectFlags.ptr), words, stream);
@@ -430,9 +426,9 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
     if (wordsHost[kWordSticky] & (kStatusLookbackTimeout | kStatusIndexRange)) {
         // Raised after the read of a frame that did not wait for its end: that
         // frame is not valid, and this call reports it.
-        const uint32_t bits = wordsHost[kWordSticky];
+        const uint32_t b = wordsHost[kWordSticky];
         cudaMemsetAsync(words + kWordSticky, 0, sizeof(uint32_t), stream);
-        if (bits & kStatusLookbackTimeout)
+        if (b & kStatusLookbackTimeout)
             return fail(ATH_E_TIMEOUT, "a look-back wait of the previous frame's sort gave up (bounded spin)");
         return fail(ATH_E_INTERNAL, "the previous frame met an index outside its buffers (skipped, not written)");
     }
@@ -465,14 +461,16 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
     if (err == cudaSuccess)
         err = launchBlend(F, pairs, slots, static_cast<const uint2*>(r->ranges.ptr), valsBuf[sorted],
                           static_cast<const float4*>(r->recs.ptr), reinterpret_cast<float4*>(targets->colour),
-                          targets->depth, reinterpret_cast<float4*>(targets->position), nullptr, nullptr,
-                          words + kWordSticky, stream);
+                          targets->depth, reinterpret_cast<float4*>(targets->position),
+                          training ? static_cast<float*>(r->finalT.ptr) : nullptr,
+                          training ? static_cast<uint32_t*>(r->lastContrib.ptr) : nullptr, words + kWordSticky, stream);
     mark(5);
     if (err != cudaSuccess) return failCuda(err, "drawing the frame");
     r->lastSlots = slots;
     r->lastPairs = pairs;
     r->lastTiles = tiles;
     r->lastSorted = sorted;
+    r->lastFrame = F;
 
     ath_frame_stats out{};
     out.splats = slots;
@@ -484,9 +482,9 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
         if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
         if (err != cudaSuccess) return failCuda(err, "reading the frame's counters");
         if (wordsHost[kWordSticky] & (kStatusLookbackTimeout | kStatusIndexRange)) {
-            const uint32_t bits = wordsHost[kWordSticky];
+            const uint32_t b = wordsHost[kWordSticky];
             cudaMemsetAsync(words + kWordSticky, 0, sizeof(uint32_t), stream);
-            if (bits & kStatusLookbackTimeout)
+            if (b & kStatusLookbackTimeout)
                 return fail(ATH_E_TIMEOUT, "a look-back wait in the sort gave up (bounded spin); the frame is not valid");
             return fail(ATH_E_INTERNAL, "the frame met an index outside its buffers (skipped, not written)");
         }
@@ -519,6 +517,142 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
     return ATH_OK;
 }
 
+ath_status reserveInstances(ath_raster* r, uint32_t instanceCount) {
+    if (instanceCount > r->instanceCapacity || !r->instances.bytes) {
+        const uint32_t n = std::max(instanceCount, 4u);
+        cudaError_t err = r->instances.reserve((size_t)n * sizeof(InstanceConst));
+        if (err == cudaSuccess) err = r->instanceStage.reserve((size_t)n * sizeof(InstanceConst));
+        if (err != cudaSuccess) return failCuda(err, "reserving the instance table");
+        r->instanceCapacity = n;
+    }
+    return ATH_OK;
+}
+
+}   // namespace
+
+extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* projection, const ath_instance* instances,
+                                        uint32_t instanceCount, const ath_settings* settings, ath_targets* targets,
+                                        ath_frame_stats* stats, void* streamPtr) {
+    if (!r || !projection || !settings || !targets || (instanceCount && !instances))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render: null argument");
+    const ath_settings& s = *settings;
+    ath_status st = checkFrame(s, *targets);
+    if (st != ATH_OK) return st;
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < instanceCount; ++k) {
+        const ath_status v = validInstance(instances[k], k);
+        if (v != ATH_OK) return v;
+        total += instances[k].count;
+    }
+    if (total > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 splats in one frame");
+    DeviceGuard guard(r->device);
+    if ((st = reserveInstances(r, instanceCount)) != ATH_OK) return st;
+    InstanceConst* staged = static_cast<InstanceConst*>(r->instanceStage.ptr);
+    uint32_t base = 0;
+    for (uint32_t k = 0; k < instanceCount; ++k) {
+        staged[k] = instanceConstFor(*projection, s, instances[k], base);
+        base += instances[k].count;
+    }
+    r->trainingValid = false;
+    return drawFrame(r, frameConstFor(*projection, s), staged, instanceCount, (uint32_t)total, kLayoutPacked, s,
+                     targets, stats, static_cast<cudaStream_t>(streamPtr), false);
+}
+
+namespace ath {
+
+// The training layout as an instance (setObject/setCloudSpace as for a packed cloud).
+InstanceConst instanceConstForParams(const ath_projection& p, const ath_settings& s, const ath_params& in) {
+    ath_instance packed{};
+    packed.count = in.count;
+    packed.rest_per_colour = in.sh_degree >= 3 ? 15 : in.sh_degree == 2 ? 8 : in.sh_degree == 1 ? 3 : 0;
+    packed.sh_words = 1;
+    packed.linear = in.linear;
+    packed.antialiased = -1;
+    std::memcpy(packed.object_to_world, in.object_to_world, sizeof(packed.object_to_world));
+    InstanceConst I = instanceConstFor(p, s, packed, 0);
+    I.positions = nullptr;
+    I.shape = nullptr;
+    I.sh = nullptr;
+    I.means = in.means;
+    I.scales = in.scales;
+    I.quats = in.quats;
+    I.shf = in.sh;
+    I.shStride = in.sh_stride;
+    return I;
+}
+
+}   // namespace ath
+
+extern "C" ath_status ath_raster_render_params(ath_raster* r, const ath_projection* projection, const ath_params* params,
+                                               const ath_settings* settings, ath_targets* targets,
+                                               ath_frame_stats* stats, void* streamPtr) {
+    if (!r || !projection || !params || !settings || !targets)
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render_params: null argument");
+    const ath_settings& s = *settings;
+    ath_status st = checkFrame(s, *targets);
+    if (st != ATH_OK) return st;
+    const ath_params& P = *params;
+    if (P.count && (!P.means || !P.scales || !P.quats || !P.sh))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render_params: a cloud needs means, scales, quats and sh");
+    if (P.sh_degree > 3) return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render_params: sh_degree must be 0..3");
+    const uint32_t rest = P.sh_degree >= 3 ? 15 : P.sh_degree == 2 ? 8 : P.sh_degree == 1 ? 3 : 0;
+    if (P.sh_stride < 3 + 3 * rest) return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render_params: sh_stride too small");
+    for (const float* ptr : {P.means, P.scales, P.quats})
+        if (reinterpret_cast<uintptr_t>(ptr) & 15)
+            return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render_params: means, scales and quats must be 16-byte aligned");
+    DeviceGuard guard(r->device);
+    if ((st = reserveInstances(r, 1)) != ATH_OK) return st;
+    InstanceConst* staged = static_cast<InstanceConst*>(r->instanceStage.ptr);
+    staged[0] = instanceConstForParams(*projection, s, P);
+    r->trainingValid = false;
+    st = drawFrame(r, frameConstFor(*projection, s), staged, 1, P.count, kLayoutParams, s, targets, stats,
+                   static_cast<cudaStream_t>(streamPtr), true);
+    if (st != ATH_OK) return st;
+    r->trainingInstance = staged[0];
+    r->trainingDepth = targets->depth;
+    r->trainingValid = true;
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_raster_backward(ath_raster* r, const float* dlDcolour, const float* dlDdepth,
+                                          ath_param_grads* grads, void* streamPtr) {
+    if (!r || !dlDcolour || !grads || !grads->means || !grads->scales || !grads->quats || !grads->sh)
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_backward: null argument");
+    if (!r->trainingValid)
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_backward: no ath_raster_render_params frame to differentiate");
+    DeviceGuard guard(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    const FrameConst& F = r->lastFrame;
+    const InstanceConst& I = r->trainingInstance;
+    const uint32_t slots = r->lastSlots;
+    cudaError_t err = r->grads.reserve((size_t)std::max(slots, 1u) * kGradWords * sizeof(float));
+    if (err == cudaSuccess) err = cudaMemsetAsync(r->grads.ptr, 0, (size_t)slots * kGradWords * sizeof(float), stream);
+    uint32_t* words = static_cast<uint32_t*>(r->words.ptr);
+    if (err == cudaSuccess)
+        err = launchBlendBackward(F, r->lastPairs, slots, static_cast<const uint2*>(r->ranges.ptr),
+                                  static_cast<const uint32_t*>(r->pairVals[r->lastSorted].ptr),
+                                  static_cast<const float4*>(r->recs.ptr), static_cast<const float*>(r->finalT.ptr),
+                                  static_cast<const uint32_t*>(r->lastContrib.ptr),
+                                  reinterpret_cast<const float4*>(dlDcolour), dlDdepth, r->trainingDepth,
+                                  static_cast<float*>(r->grads.ptr), words + kWordSticky, stream);
+    if (err == cudaSuccess)
+        err = launchProjectBackward(F, I, static_cast<const uint32_t*>(r->keys.ptr), static_cast<const float*>(r->grads.ptr),
+                                    reinterpret_cast<float4*>(grads->means), reinterpret_cast<float4*>(grads->scales),
+                                    reinterpret_cast<float4*>(grads->quats), grads->sh, stream);
+    if (err != cudaSuccess) return failCuda(err, "the backward");
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_l2_loss(const float* colour, const float* target, uint32_t pixels, float* dlDcolour,
+                                  float* loss, void* streamPtr) {
+    if (pixels && (!colour || !target || !dlDcolour || !loss))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_l2_loss: null argument");
+    const cudaError_t err = launchL2Loss(reinterpret_cast<const float4*>(colour), target, pixels,
+                                         reinterpret_cast<float4*>(dlDcolour), loss, static_cast<cudaStream_t>(streamPtr));
+    if (err != cudaSuccess) return failCuda(err, "ath_l2_loss");
+    return ATH_OK;
+}
+
 extern "C" ath_status ath_raster_frame_buffers(ath_raster* r, ath_frame_buffers* out) {
     if (!r || !out) return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_frame_buffers: null argument");
     if (!r->recs.ptr) return fail(ATH_E_NOT_FOUND, "no frame has been drawn since the scratch was made");
@@ -532,6 +666,7 @@ extern "C" ath_status ath_raster_frame_buffers(ath_raster* r, ath_frame_buffers*
     out->pair_keys = static_cast<const uint64_t*>(r->pairKeys[r->lastSorted].ptr);
     out->pair_splats = static_cast<const uint32_t*>(r->pairVals[r->lastSorted].ptr);
     out->ranges = static_cast<const uint32_t*>(r->ranges.ptr);
+    out->grads = static_cast<const float*>(r->grads.ptr);
     return ATH_OK;
 }
 

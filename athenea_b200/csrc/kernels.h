@@ -16,8 +16,8 @@ struct InstanceConst;
 // project.cu
 uint32_t projectBlocks(uint32_t slots);
 cudaError_t launchProject(const FrameConst& F, const InstanceConst* inst, uint32_t nInst, uint32_t slots,
-                          bool countCulls, float4* recs, uint2* rects, uint32_t* keys, uint32_t* offsets,
-                          uint64_t* flags, uint32_t* words, cudaStream_t stream);
+                          uint32_t layout, bool countCulls, float4* recs, uint2* rects, uint32_t* keys,
+                          uint32_t* offsets, uint64_t* flags, uint32_t* words, cudaStream_t stream);
 cudaError_t launchEmit(const FrameConst& F, uint32_t slots, const float4* recs, const uint2* rects,
                        const uint32_t* keys, const uint32_t* offsets, const uint32_t* words, uint64_t capacity,
                        uint64_t* pairKeys, uint32_t* pairValues, cudaStream_t stream);
@@ -37,6 +37,17 @@ cudaError_t launchSort(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
                         const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
                         float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream);
+
+// backward.cu
+cudaError_t launchBlendBackward(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
+                                const uint32_t* pairValues, const float4* recs, const float* finalT,
+                                const uint32_t* lastContrib, const float4* dLdColour, const float* dLdDepth,
+                                const float* depthOut, float* grads, uint32_t* status, cudaStream_t stream);
+cudaError_t launchProjectBackward(const FrameConst& F, const InstanceConst& I, const uint32_t* keys,
+                                  const float* grads, float4* gMeans, float4* gScales, float4* gQuats, float* gSh,
+                                  cudaStream_t stream);
+cudaError_t launchL2Loss(const float4* colour, const float* target, uint32_t pixels, float4* dLdColour, float* loss,
+                         cudaStream_t stream);
 
 // decode.cu
 uint32_t decodeBlocks(uint32_t count);

@@ -9,6 +9,7 @@
 // Built with --fmad=false: see splat_math.cuh.
 #include <cuda_runtime.h>
 
+#include "gauss.cuh"
 #include "kernels.h"
 #include "raster_types.cuh"
 #include "splat_math.cuh"
@@ -59,13 +60,9 @@ __device__ void editGrade(const EditConst& e, float c[3]) {
     for (int k = 0; k < 3; ++k) c[k] = fmaxf(luma + (g[k] - luma) * e.saturation, 0.0f);
 }
 
-// common/sh.slang:25-51 for one channel `ch` of the rest coefficients at `row`.
-__device__ __forceinline__ float shHalf(const uint32_t* __restrict__ row, uint32_t index) {
-    const uint32_t word = __ldg(row + index / 2);
-    return (index & 1u) == 0u ? lowHalf(word) : highHalf(word);
-}
-
-__device__ void evaluateRest(const uint32_t* __restrict__ row, uint32_t degree, float x, float y, float z,
+// common/sh.slang:25-51, the view-dependent part of the colour, channel by channel.
+template <uint32_t L>
+__device__ void evaluateRest(const InstanceConst& I, uint32_t i, uint32_t degree, float x, float y, float z,
                              float out[3]) {
     const float kC1 = 0.4886025119029199f;
 #pragma unroll
@@ -74,25 +71,24 @@ __device__ void evaluateRest(const uint32_t* __restrict__ row, uint32_t degree, 
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
         const uint32_t c = (uint32_t)ch;
-        float r = (((-kC1) * y) * shHalf(row, 0 + c) + (kC1 * z) * shHalf(row, 3 + c)) - (kC1 * x) * shHalf(row, 6 + c);
+        auto B = [&](uint32_t k) { return restAt<L>(I, i, k * 3 + c); };
+        float r = (((-kC1) * y) * B(0) + (kC1 * z) * B(1)) - (kC1 * x) * B(2);
         if (degree >= 2) {
             const float xx = x * x, yy = y * y, zz = z * z;
             const float xy = x * y, yz = y * z, xz = x * z;
-            const float t = (((((1.0925484305920792f * xy) * shHalf(row, 9 + c) +
-                                (-1.0925484305920792f * yz) * shHalf(row, 12 + c)) +
-                               (0.31539156525252005f * ((2.0f * zz - xx) - yy)) * shHalf(row, 15 + c)) +
-                              (-1.0925484305920792f * xz) * shHalf(row, 18 + c)) +
-                             (0.5462742152960396f * (xx - yy)) * shHalf(row, 21 + c));
+            const float t = (((((1.0925484305920792f * xy) * B(3) + (-1.0925484305920792f * yz) * B(4)) +
+                               (0.31539156525252005f * ((2.0f * zz - xx) - yy)) * B(5)) +
+                              (-1.0925484305920792f * xz) * B(6)) +
+                             (0.5462742152960396f * (xx - yy)) * B(7));
             r = r + t;
             if (degree >= 3) {
-                const float u =
-                    ((((((((-0.5900435899266435f * y) * (3.0f * xx - yy)) * shHalf(row, 24 + c) +
-                          ((2.890611442640554f * xy) * z) * shHalf(row, 27 + c)) +
-                         ((-0.4570457994644658f * y) * ((4.0f * zz - xx) - yy)) * shHalf(row, 30 + c)) +
-                        ((0.3731763325901154f * z) * ((2.0f * zz - 3.0f * xx) - 3.0f * yy)) * shHalf(row, 33 + c)) +
-                       ((-0.4570457994644658f * x) * ((4.0f * zz - xx) - yy)) * shHalf(row, 36 + c)) +
-                      ((1.445305721320277f * z) * (xx - yy)) * shHalf(row, 39 + c)) +
-                     ((-0.5900435899266435f * x) * (xx - 3.0f * yy)) * shHalf(row, 42 + c));
+                const float u = ((((((((-0.5900435899266435f * y) * (3.0f * xx - yy)) * B(8) +
+                                     ((2.890611442640554f * xy) * z) * B(9)) +
+                                    ((-0.4570457994644658f * y) * ((4.0f * zz - xx) - yy)) * B(10)) +
+                                   ((0.3731763325901154f * z) * ((2.0f * zz - 3.0f * xx) - 3.0f * yy)) * B(11)) +
+                                  ((-0.4570457994644658f * x) * ((4.0f * zz - xx) - yy)) * B(12)) +
+                                 ((1.445305721320277f * z) * (xx - yy)) * B(13)) +
+                                ((-0.5900435899266435f * x) * (xx - 3.0f * yy)) * B(14));
                 r = r + u;
             }
         }
@@ -107,121 +103,45 @@ struct Projected {
 
 // One splat: projectSplat<0>. Writes the record and the rect of a splat that
 // is kept; a culled one writes nothing here (its key says why).
+template <uint32_t L>
 __device__ Projected projectSlot(const FrameConst& F, const InstanceConst& I, uint32_t i, uint32_t slot,
                                  float4* __restrict__ recs, uint2* __restrict__ rects) {
-    const float4 po = __ldg(I.positions + i);
-    const uint4 sh4 = __ldg(I.shape + i);
-    const float scale[3] = {exp_f(lowHalf(sh4.y)), exp_f(highHalf(sh4.y)), exp_f(lowHalf(sh4.z))};
-    const Fate fate = editFate(I.edit, po.x, po.y, po.z, po.w, scale);
+    const Gauss g = loadGauss<L>(I, i);
+    const Fate fate = editFate(I.edit, g.px, g.py, g.pz, g.opacity, g.scale);
     if (fate.removed) return {0, kCulledKey | kCullEdit};
-    const float opacity = fate.opacity;
-    const float* m = I.m;
-    const float tx = ((m[0] * po.x + m[1] * po.y) + m[2] * po.z) + m[3];
-    const float ty = ((m[4] * po.x + m[5] * po.y) + m[6] * po.z) + m[7];
-    const float tz = ((m[8] * po.x + m[9] * po.y) + m[10] * po.z) + m[11];
-    if (!(tz > F.nearZ) || tz > F.farZ) return {0, kCulledKey | kCullDepth};
-
-    float q[4];
-    decodeQuaternion(sh4.x, q);
-    const float x = q[0], y = q[1], z = q[2], w = q[3];
-    const float r00 = 1.0f - 2.0f * (y * y + z * z), r01 = 2.0f * (x * y - w * z), r02 = 2.0f * (x * z + w * y);
-    const float r10 = 2.0f * (x * y + w * z), r11 = 1.0f - 2.0f * (x * x + z * z), r12 = 2.0f * (y * z - w * x);
-    const float r20 = 2.0f * (x * z - w * y), r21 = 2.0f * (y * z + w * x), r22 = 1.0f - 2.0f * (x * x + y * y);
-    const float M[3][3] = {{r00 * scale[0], r01 * scale[1], r02 * scale[2]},
-                           {r10 * scale[0], r11 * scale[1], r12 * scale[2]},
-                           {r20 * scale[0], r21 * scale[1], r22 * scale[2]}};
-
-    float jx0, jx2, jy1, jy2, cx, cy;
-    if (F.orthographic != 0) {
-        jx0 = F.focalX; jx2 = 0.0f;
-        jy1 = F.focalY; jy2 = 0.0f;
-        cx = F.focalX * tx + F.centreX;
-        cy = F.focalY * ty + F.centreY;
-    } else {
-        const float invZ = 1.0f / tz;
-        cx = (F.focalX * tx) * invZ + F.centreX;
-        cy = (F.focalY * ty) * invZ + F.centreY;
-        const float limLoX = ((-0.15f) * (float)F.width - F.centreX) / F.focalX;
-        const float limHiX = (1.15f * (float)F.width - F.centreX) / F.focalX;
-        const float limLoY = ((-0.15f) * (float)F.height - F.centreY) / F.focalY;
-        const float limHiY = (1.15f * (float)F.height - F.centreY) / F.focalY;
-        const float txc = clampf(tx * invZ, limLoX, limHiX) * tz;
-        const float tyc = clampf(ty * invZ, limLoY, limHiY) * tz;
-        jx0 = F.focalX * invZ;
-        jx2 = (((-F.focalX) * txc) * invZ) * invZ;
-        jy1 = F.focalY * invZ;
-        jy2 = (((-F.focalY) * tyc) * invZ) * invZ;
-    }
-    // mul(jx, W) with jx = (jx0, 0, jx2): the zero terms are kept as the
-    // row-vector product writes them, so the sums round exactly as there.
-    float t3[3], u3[3], ax[3], ay[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        t3[j] = (jx0 * m[j] + 0.0f * m[4 + j]) + jx2 * m[8 + j];
-        u3[j] = (0.0f * m[j] + jy1 * m[4 + j]) + jy2 * m[8 + j];
-    }
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        ax[j] = (t3[0] * M[0][j] + t3[1] * M[1][j]) + t3[2] * M[2][j];
-        ay[j] = (u3[0] * M[0][j] + u3[1] * M[1][j]) + u3[2] * M[2][j];
-    }
-    float a = (ax[0] * ax[0] + ax[1] * ax[1]) + ax[2] * ax[2];
-    const float b = (ax[0] * ay[0] + ax[1] * ay[1]) + ax[2] * ay[2];
-    float c = (ay[0] * ay[0] + ay[1] * ay[1]) + ay[2] * ay[2];
-    const float detBefore = a * c - b * b;
-    a = a + 0.3f;
-    c = c + 0.3f;
-    const float det = a * c - b * b;
-    if (!(det > 1e-12f)) return {0, kCulledKey | kCullDegenerate};
-    const float filtered = sqrtf(fmaxf(detBefore, 0.0f) / det);
-    const float paid = I.antialias != 0 ? filtered : I.paidAt > 0.0f ? fminf(filtered / I.paidAt, 1.0f) : 1.0f;
-    const float alpha = opacity > 1.0f ? opacity : paidOpacity(opacity, paid);
-    if (!(alpha >= kFaint)) return {0, kCulledKey | kCullFaint};
-
-    const float boundDet = a * c - b * b;
-    const float ca = c / boundDet, cb = (-b) / boundDet, cc = a / boundDet;
-    const float cutoff = alpha > 1.0f ? falloffCutoff(alpha) : cutoffPower(alpha);
-    const float det2 = ca * cc - cb * cb;
-    const float inv = det2 > 1e-20f ? 1.0f / det2 : 0.0f;
-    const float ex = sqrtf(fmaxf((cutoff * cc) * inv, 0.0f));
-    const float ey = sqrtf(fmaxf((cutoff * ca) * inv, 0.0f));
-    const float x1 = cx - ex, y1 = cy - ey, x2 = cx + ex, y2 = cy + ey;
-    if (x2 < 0.0f || y2 < 0.0f || x1 >= (float)F.width || y1 >= (float)F.height) return {0, kCulledKey | kCullOffscreen};
-    const uint32_t rx0 = (uint32_t)fmaxf(x1, 0.0f) / kTile;
-    const uint32_t ry0 = (uint32_t)fmaxf(y1, 0.0f) / kTile;
-    const uint32_t rx1 = (uint32_t)fminf(x2, (float)F.width - 1.0f) / kTile;
-    const uint32_t ry1 = (uint32_t)fminf(y2, (float)F.height - 1.0f) / kTile;
-    if (rx0 > rx1 || ry0 > ry1) return {0, kCulledKey | kCullOffscreen};
-
+    const Geometry G = projectGeometry(F, I, g, fate.opacity);
+    if (G.cull) return {0, kCulledKey | G.cull};
+    uint32_t rx0, ry0, rx1, ry1;
+    if (!tileRectOf(F, G, rx0, ry0, rx1, ry1)) return {0, kCulledKey | kCullOffscreen};
     uint32_t touched = 0;
-    for (uint32_t ty2 = ry0; ty2 <= ry1; ++ty2)
-        for (uint32_t tx2 = rx0; tx2 <= rx1; ++tx2)
-            touched += tileTouched(F.width, F.height, cx, cy, ca, cb, cc, cutoff, tx2, ty2) ? 1u : 0u;
+    for (uint32_t ty = ry0; ty <= ry1; ++ty)
+        for (uint32_t tx = rx0; tx <= rx1; ++tx)
+            touched += tileTouched(F.width, F.height, G.cx, G.cy, G.ca, G.cb, G.cc, G.cutoff, tx, ty) ? 1u : 0u;
     if (touched == 0) return {0, kCulledKey | kCullNoTile};
 
-    const float base[3] = {highHalf(sh4.z), lowHalf(sh4.w), highHalf(sh4.w)};
     const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
-    const float dx = po.x - I.eye[0], dy = po.y - I.eye[1], dz = po.z - I.eye[2];
+    const float dx = g.px - I.eye[0], dy = g.py - I.eye[1], dz = g.pz - I.eye[2];
     const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
     float rest[3];
-    evaluateRest(I.sh + (size_t)i * I.shWords, degree, dx / len, dy / len, dz / len, rest);
+    evaluateRest<L>(I, i, degree, dx / len, dy / len, dz / len, rest);
     float colour[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const float v = base[k] + rest[k];
+        const float v = g.base[k] + rest[k];
         colour[k] = I.linear != 0 ? fmaxf(v, 0.0f) : srgbToLinear(v);
     }
     if (fate.graded) editGrade(I.edit, colour);
 
-    recs[(size_t)slot * 3 + 0] = make_float4(cx, cy, tz, cutoff);
-    recs[(size_t)slot * 3 + 1] = make_float4(ca, cb, cc, alpha);
+    recs[(size_t)slot * 3 + 0] = make_float4(G.cx, G.cy, G.tz, G.cutoff);
+    recs[(size_t)slot * 3 + 1] = make_float4(G.ca, G.cb, G.cc, G.alpha);
     recs[(size_t)slot * 3 + 2] = make_float4(colour[0], colour[1], colour[2], 0.0f);
     rects[slot] = make_uint2(rx0 | (ry0 << 16), rx1 | (ry1 << 16));
-    return {touched, __float_as_uint(tz) >> 7};
+    return {touched, __float_as_uint(G.tz) >> 7};
 }
 
 constexpr uint32_t kProjectThreads = 256;
 
+template <uint32_t L>
 __global__ void __launch_bounds__(kProjectThreads)
     projectKernel(const FrameConst F, const InstanceConst* __restrict__ inst, uint32_t nInst, uint32_t slots,
                   uint32_t countCulls, float4* __restrict__ recs, uint2* __restrict__ rects,
@@ -241,7 +161,7 @@ __global__ void __launch_bounds__(kProjectThreads)
     if (slot < slots) {
         uint32_t k = 0;
         while (k + 1 < nInst && slot >= inst[k + 1].base) ++k;
-        const Projected p = projectSlot(F, inst[k], slot - inst[k].base, slot, recs, rects);
+        const Projected p = projectSlot<L>(F, inst[k], slot - inst[k].base, slot, recs, rects);
         keys[slot] = p.key;
         touched = p.touched;
         kept = p.key < kCulledKey;
@@ -342,12 +262,20 @@ __global__ void __launch_bounds__(256)
 }   // namespace
 
 cudaError_t launchProject(const FrameConst& F, const InstanceConst* inst, uint32_t nInst, uint32_t slots,
-                          bool countCulls, float4* recs, uint2* rects, uint32_t* keys, uint32_t* offsets,
-                          uint64_t* flags, uint32_t* words, cudaStream_t stream) {
+                          uint32_t layout, bool countCulls, float4* recs, uint2* rects, uint32_t* keys,
+                          uint32_t* offsets, uint64_t* flags, uint32_t* words, cudaStream_t stream) {
     if (slots == 0) return cudaSuccess;
     const uint32_t blocks = (slots + kProjectThreads - 1) / kProjectThreads;
-    projectKernel<<<blocks, kProjectThreads, 0, stream>>>(F, inst, nInst, slots, countCulls ? 1u : 0u, recs, rects,
-                                                         keys, offsets, flags, words);
+    const uint32_t cc = countCulls ? 1u : 0u;
+    if (layout == kLayoutPacked)
+        projectKernel<kLayoutPacked><<<blocks, kProjectThreads, 0, stream>>>(F, inst, nInst, slots, cc, recs, rects,
+                                                                            keys, offsets, flags, words);
+    else if (layout == kLayoutParams)
+        projectKernel<kLayoutParams><<<blocks, kProjectThreads, 0, stream>>>(F, inst, nInst, slots, cc, recs, rects,
+                                                                            keys, offsets, flags, words);
+    else
+        projectKernel<kLayoutMixed><<<blocks, kProjectThreads, 0, stream>>>(F, inst, nInst, slots, cc, recs, rects,
+                                                                           keys, offsets, flags, words);
     return cudaGetLastError();
 }
 

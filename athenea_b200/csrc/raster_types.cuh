@@ -25,12 +25,21 @@ struct FrameConst {
 };
 
 // The per-instance part (setObject, setCloudSpace, setEdit: FrameParams.h:84-165),
-// with the cloud's device buffers (scene/GpuClouds.h:44-52).
+// with the cloud's device buffers in one of the layouts of gauss.cuh.
 struct InstanceConst {
+    // the reference's packed layout (scene/GpuClouds.h:44-52)
     const float4* positions;
     const uint4* shape;
     const uint32_t* sh;
-    uint32_t count, base, restPerColour, shWords, linear, antialias;
+    // FP32 training parameters, and the mixed-precision layout's SH
+    const float* means;     // float4: x y z, opacity logit
+    const float* scales;    // float4: log scales
+    const float* quats;     // float4: w x y z
+    const float* shf;       // shStride floats: DC rgb, rest rgb per basis
+    const void* shLow;      // mixed: 12 bf16 a Gaussian (DC, band 1)
+    const void* shHigh;     // mixed: 36 e4m3 a Gaussian (bands 2-3)
+    const float* shScale;   // mixed: the bands' scale a Gaussian
+    uint32_t count, base, restPerColour, shWords, shStride, linear, antialias;
     float paidAt;
     float m[12];
     float eye[3];
@@ -55,6 +64,16 @@ enum StatusBit : uint32_t {
     kStatusLookbackTimeout = 1u,   // a look-back gave up waiting (bounded spin)
     kStatusPairOverflow = 2u,      // more pairs than the pair buffers hold
     kStatusIndexRange = 4u,        // a data-dependent index fell outside its buffer (skipped)
+};
+
+// The backward's gradient with respect to one record: ten floats a slot.
+enum GradWord : uint32_t {
+    kGradCx = 0, kGradCy = 1,               // screen centre
+    kGradA = 2, kGradB2 = 3, kGradC = 4,    // conic a, b, c
+    kGradAlpha = 5,                         // the record's opacity (after the payback)
+    kGradR = 6, kGradG = 7, kGradB = 8,     // colour
+    kGradZ = 9,                             // view depth (the depth layer's)
+    kGradWords = 10,
 };
 
 // A look-back word: two status bits over a 62-bit count.

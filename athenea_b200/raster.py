@@ -324,3 +324,75 @@ class TileRasterizer:
     def release_scratch(self) -> None:
         """releaseScratch (TileRasterizer.h:482)."""
         check(N.lib().ath_raster_release_scratch(self._h))
+
+
+# ---- differentiation -----------------------------------------------------------
+@dataclass
+class Params:
+    """A cloud as FP32 training parameters (ath_params): CUDA tensors, one Gaussian a row.
+
+    means (N, 4): x y z, opacity logit; scales (N, 4): log scales (4th unused);
+    quats (N, 4): w x y z; sh (N, stride): DC rgb, then the rest rgb per basis.
+    """
+    means: torch.Tensor
+    scales: torch.Tensor
+    quats: torch.Tensor
+    sh: torch.Tensor
+    sh_degree: int = 3
+    linear: bool = False
+    object_to_world: np.ndarray = field(default_factory=lambda: np.eye(4))
+
+    @property
+    def count(self) -> int:
+        return int(self.means.shape[0])
+
+    def zeros_like(self) -> "Params":
+        return Params(torch.zeros_like(self.means), torch.zeros_like(self.scales), torch.zeros_like(self.quats),
+                      torch.zeros_like(self.sh), self.sh_degree, self.linear, self.object_to_world)
+
+    def _native(self) -> N.Params:
+        p = N.Params()
+        p.means, p.scales, p.quats, p.sh = _ptr(self.means), _ptr(self.scales), _ptr(self.quats), _ptr(self.sh)
+        p.count = self.count
+        p.sh_degree = self.sh_degree
+        p.sh_stride = int(self.sh.shape[1])
+        p.linear = 1 if self.linear else 0
+        p.object_to_world[:] = list(_mat(self.object_to_world).reshape(16))
+        return p
+
+
+def _render_params(self, camera, params: Params, settings: RenderSettings, targets: RenderTargets,
+                   stream: torch.cuda.Stream | None = None) -> FrameStats:
+    """A differentiable frame (ath_raster_render_params): render() for one cloud of training
+    parameters, keeping what backward() needs."""
+    proj = camera.projection_for(settings.width, settings.height) if isinstance(camera, Camera) else camera
+    t = N.Targets(targets.width, targets.height, _ptr(targets.colour), _ptr(targets.depth), _ptr(targets.position))
+    stats = N.FrameStats()
+    s = stream if stream is not None else torch.cuda.current_stream(targets.colour.device)
+    self._params_keep = params   # the backward reads them again
+    check(N.lib().ath_raster_render_params(self._h, C.byref(proj), C.byref(params._native()),
+                                           C.byref(settings._native()), C.byref(t), C.byref(stats),
+                                           C.c_void_p(s.cuda_stream)))
+    return FrameStats(*[getattr(stats, f) for f, _ in N.FrameStats._fields_])
+
+
+def _backward(self, dl_dcolour: torch.Tensor, grads: Params, dl_ddepth: torch.Tensor | None = None,
+              stream: torch.cuda.Stream | None = None) -> None:
+    """ath_raster_backward: adds dL/dparameters of the last render_params frame into `grads`."""
+    g = N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
+    s = stream if stream is not None else torch.cuda.current_stream(dl_dcolour.device)
+    check(N.lib().ath_raster_backward(self._h, _ptr(dl_dcolour), _ptr(dl_ddepth), C.byref(g),
+                                      C.c_void_p(s.cuda_stream)))
+
+
+TileRasterizer.render_params = _render_params
+TileRasterizer.backward = _backward
+
+
+def l2_loss(colour: torch.Tensor, target: torch.Tensor, dl_dcolour: torch.Tensor, loss: torch.Tensor,
+            stream: torch.cuda.Stream | None = None) -> None:
+    """ath_l2_loss: mean over pixels and rgb of (colour - target)^2 added into `loss` (a 1-element
+    CUDA tensor); dL/dcolour written (float4 a pixel, alpha 0)."""
+    s = stream if stream is not None else torch.cuda.current_stream(colour.device)
+    check(N.lib().ath_l2_loss(_ptr(colour), _ptr(target), int(colour.shape[0]), _ptr(dl_dcolour), _ptr(loss),
+                              C.c_void_p(s.cuda_stream)))

@@ -44,35 +44,57 @@ WORKLOADS = {
 MIXED_RESOLUTIONS = ((320, 180), (640, 360), (960, 540), (1280, 720), (1920, 1080))
 
 
-def records(count: int, clustered: bool, seed: int, sh_degree: int = 3) -> tuple[np.ndarray, dict]:
-    """`count` 3DGS records: means uniform in [-1,1]^3, or from a mixture of 8
+def gaussians(count: int, clustered: bool, seed: int, sh_degree: int = 3) -> dict:
+    """`count` Gaussians: means uniform in [-1,1]^3, or from a mixture of 8
     isotropic normals (sigma 0.3) centred uniformly in [-1,1]^3; log-scales
-    N(-4.5, 0.5) per axis; rotations uniform (a normalised 4D gaussian);
-    opacity sigmoid(N(0,1)); SH of `sh_degree`, N(0, 0.3) with 0.5 added to the DC."""
+    N(-4.5, 0.5) per axis; rotations uniform (a normalised 4D gaussian, w x y z);
+    opacity logits N(0, 1) (opacity sigmoid(N(0,1))); SH of `sh_degree`, N(0, 0.3)
+    with 0.5 added to the DC, rgb per basis with the DC first."""
     rng = np.random.default_rng(seed)
     rest = (0, 3, 8, 15)[sh_degree]
-    enc = encoding_3dgs(rest)
-    out = np.zeros((count, enc["stride"]), np.float32)
     if clustered:
         centres = rng.uniform(-1.0, 1.0, size=(8, 3))
         which = rng.integers(0, 8, size=count)
         means = centres[which] + rng.normal(0.0, 0.3, size=(count, 3))
     else:
         means = rng.uniform(-1.0, 1.0, size=(count, 3))
-    out[:, 0:3] = means
     shs = rng.normal(0.0, 0.3, size=(count, 3 + 3 * rest))
     shs[:, 0:3] += 0.5
-    out[:, enc["dc0"]:enc["dc0"] + 3] = shs[:, 0:3]
-    if rest:
-        # f_rest is colour-outer: all red, then green, then blue (a 3DGS PLY)
-        restv = shs[:, 3:].reshape(count, rest, 3)          # basis-major, rgb inner
-        out[:, enc["rest_base"]:enc["rest_base"] + 3 * rest] = restv.transpose(0, 2, 1).reshape(count, 3 * rest)
-    out[:, enc["opacity"]] = rng.normal(0.0, 1.0, size=count)
-    out[:, enc["scale0"]:enc["scale0"] + 3] = rng.normal(-4.5, 0.5, size=(count, 3))
+    logits = rng.normal(0.0, 1.0, size=count)
+    log_scales = rng.normal(-4.5, 0.5, size=(count, 3))
     q = rng.normal(0.0, 1.0, size=(count, 4))
     q /= np.linalg.norm(q, axis=1, keepdims=True)
-    out[:, enc["rot_w"]:enc["rot_w"] + 4] = q
+    return dict(means=means, logits=logits, log_scales=log_scales, quats=q, sh=shs, rest=rest)
+
+
+def records(count: int, clustered: bool, seed: int, sh_degree: int = 3) -> tuple[np.ndarray, dict]:
+    """The Gaussians of `gaussians` as 3DGS records (f_rest colour-outer, as a PLY has them)."""
+    g = gaussians(count, clustered, seed, sh_degree)
+    rest = g["rest"]
+    enc = encoding_3dgs(rest)
+    out = np.zeros((count, enc["stride"]), np.float32)
+    out[:, 0:3] = g["means"]
+    out[:, enc["dc0"]:enc["dc0"] + 3] = g["sh"][:, 0:3]
+    if rest:
+        restv = g["sh"][:, 3:].reshape(count, rest, 3)          # basis-major, rgb inner
+        out[:, enc["rest_base"]:enc["rest_base"] + 3 * rest] = restv.transpose(0, 2, 1).reshape(count, 3 * rest)
+    out[:, enc["opacity"]] = g["logits"]
+    out[:, enc["scale0"]:enc["scale0"] + 3] = g["log_scales"]
+    out[:, enc["rot_w"]:enc["rot_w"] + 4] = g["quats"]
     return out, enc
+
+
+def params(count: int, clustered: bool, seed: int, sh_degree: int = 3) -> dict:
+    """The Gaussians of `gaussians` in the FP32 training layout (ath_params): means (N,4) with the
+    opacity logit fourth, scales (N,4) log scales, quats (N,4) w x y z, sh (N, 3 + 3 rest)."""
+    g = gaussians(count, clustered, seed, sh_degree)
+    means = np.zeros((count, 4), np.float32)
+    means[:, :3] = g["means"]
+    means[:, 3] = g["logits"]
+    scales = np.zeros((count, 4), np.float32)
+    scales[:, :3] = g["log_scales"]
+    return dict(means=means, scales=scales, quats=g["quats"].astype(np.float32),
+                sh=np.ascontiguousarray(g["sh"], np.float32), sh_degree=sh_degree)
 
 
 def circle_eye(view: int, views: int, radius: float = 3.0, height: float = 0.0) -> tuple:

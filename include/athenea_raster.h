@@ -175,6 +175,56 @@ ath_status ath_raster_render(ath_raster* r, const ath_projection* projection, co
                              uint32_t instance_count, const ath_settings* settings, ath_targets* targets,
                              ath_frame_stats* stats, void* stream);
 
+/* ---- differentiation (no counterpart in the reference's API: it only has
+ * the colour gradient of splat_blend.slang:381-398, contributionMode 4) ------ */
+
+/* A cloud as FP32 training parameters: one Gaussian a row of each array.
+ * The projection decodes them as the reference's upload would: opacity =
+ * sigmoid(logit), scale = exp(log scale), rotation = the unit quaternion,
+ * base colour = 0.5 + SH0 * DC. */
+typedef struct {
+    const float* means;    /* float4: x y z, opacity logit (16-byte aligned) */
+    const float* scales;   /* float4: log scale x y z, unused */
+    const float* quats;    /* float4: w x y z, any length */
+    const float* sh;       /* sh_stride floats: DC rgb, then the rest coefficients rgb per basis */
+    uint32_t count;
+    uint32_t sh_degree;    /* 0..3 */
+    uint32_t sh_stride;    /* floats a Gaussian: at least 3 (1 + 3, 8 or 15 bases) */
+    int32_t linear;        /* 1: colours are linear light; 0: sRGB, decoded per splat */
+    double object_to_world[16];
+} ath_params;
+
+/* Gradients with respect to ath_params, in its layout (means' fourth float is
+ * the opacity logit's). Added into: zero them before a batch. */
+typedef struct {
+    float* means;
+    float* scales;
+    float* quats;
+    float* sh;
+} ath_param_grads;
+
+/* The forward of a differentiable frame: ath_raster_render for one cloud of
+ * training parameters, keeping what the backward needs (per pixel the final
+ * transmittance and one past the last record blended; the frame's pairs and
+ * records). The backward must follow before the next render on this handle. */
+ath_status ath_raster_render_params(ath_raster* r, const ath_projection* projection, const ath_params* params,
+                                    const ath_settings* settings, ath_targets* targets, ath_frame_stats* stats,
+                                    void* stream);
+
+/* The backward of the last ath_raster_render_params: from dL/dcolour (float4 a
+ * pixel, premultiplied rgba) and optionally dL/ddepth (a float a pixel, may be
+ * NULL), adds dL/dparameters into `grads`. Reverse-order blend recomputed from
+ * the stored transmittances, then the projection's adjoint. The targets and
+ * parameters of the forward must be unchanged. */
+ath_status ath_raster_backward(ath_raster* r, const float* dl_dcolour, const float* dl_ddepth, ath_param_grads* grads,
+                               void* stream);
+
+/* L = mean over pixels and the three colour channels of (colour - target)^2:
+ * writes dL/dcolour (float4 a pixel, alpha 0) and adds L into *loss (device).
+ * colour: float4 a pixel, target: float3 a pixel. */
+ath_status ath_l2_loss(const float* colour, const float* target, uint32_t pixels, float* dl_dcolour, float* loss,
+                       void* stream);
+
 /* TileRasterizer::latestCounters (TileRasterizer.h:478). ATH_E_NOT_FOUND
  * until a frame drawn with count_splats has finished. */
 ath_status ath_raster_latest_counters(ath_raster* r, ath_splat_counters* out);
@@ -189,7 +239,9 @@ ath_status ath_raster_latest_counters(ath_raster* r, ath_splat_counters* out);
  *   keys       a slot: the 24-bit depth key, or 0xFF000000 | cull reason (frame.slang:42-49)
  *   offsets    a slot: its first pair (exclusive scan of tiles touched)
  *   pair_keys, pair_splats   the sorted pairs: tile << 24 | depth key, and the slot
- *   ranges     2 a tile: [start, end) into the sorted pairs (splat_ranges.slang) */
+ *   ranges     2 a tile: [start, end) into the sorted pairs (splat_ranges.slang)
+ *   grads      after ath_raster_backward, 10 floats a slot: dL/d(centre x y, conic a b c,
+ *              alpha, colour r g b, view z) -- the colour part is contributionMode 4's sums */
 typedef struct {
     uint32_t slots, pairs, tiles;
     const float* records;
@@ -199,6 +251,7 @@ typedef struct {
     const uint64_t* pair_keys;
     const uint32_t* pair_splats;
     const uint32_t* ranges;
+    const float* grads;
 } ath_frame_buffers;
 
 ath_status ath_raster_frame_buffers(ath_raster* r, ath_frame_buffers* out);

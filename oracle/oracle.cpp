@@ -154,9 +154,10 @@ float fromHalf(uint16_t h) {
 inline float lowHalf(uint32_t w) { return fromHalf((uint16_t)(w & 0xFFFFu)); }
 inline float highHalf(uint32_t w) { return fromHalf((uint16_t)(w >> 16)); }
 inline uint32_t packHalves(float a, float b) { return (uint32_t)toHalf(a) | ((uint32_t)toHalf(b) << 16); }
-inline float halfSafe(float v) { return std::min(std::max(v, -65000.0f), 65000.0f); }   // packing.slang:328
+// Slang's min/max/clamp are IEEE minNum/maxNum (a NaN operand yields the other).
+inline float halfSafe(float v) { return std::fmin(std::fmax(v, -65000.0f), 65000.0f); }   // packing.slang:328
 
-inline float clampf(float v, float lo, float hi) { return std::min(std::max(v, lo), hi); }
+inline float clampf(float v, float lo, float hi) { return std::fmin(std::fmax(v, lo), hi); }
 
 // common/packing.slang:59-76
 void decodeQuaternion(uint32_t word, float q[4]) {
@@ -312,7 +313,8 @@ inline float halfAt(const uint32_t* sh, uint32_t row, uint32_t index) {
     return (index & 1u) == 0u ? lowHalf(word) : highHalf(word);
 }
 
-void evaluateRest(const uint32_t* sh, uint32_t row, uint32_t degree, float x, float y, float z, float out[3]) {
+template <typename Coef>
+void evaluateRest(Coef coef, uint32_t degree, float x, float y, float z, float out[3]) {
     const float kC1 = 0.4886025119029199f;
     const float kC2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f, -1.0925484305920792f,
                           0.5462742152960396f};
@@ -321,7 +323,7 @@ void evaluateRest(const uint32_t* sh, uint32_t row, uint32_t degree, float x, fl
     for (int ch = 0; ch < 3; ++ch) out[ch] = 0.0f;
     if (degree == 0) return;
     for (int ch = 0; ch < 3; ++ch) {
-        auto B = [&](uint32_t k) { return halfAt(sh, row, k * 3 + (uint32_t)ch); };
+        auto B = [&](uint32_t k) { return coef(k * 3 + (uint32_t)ch); };
         float r = (((-kC1) * y) * B(0) + (kC1 * z) * B(1)) - (kC1 * x) * B(2);
         if (degree >= 2) {
             const float xx = x * x, yy = y * y, zz = z * z;
@@ -358,15 +360,61 @@ void cullSlot(uint32_t slot, uint32_t reason, float* records, uint32_t* rects, u
     for (int k = 0; k < 12; ++k) records[slot * 12 + k] = 0.0f;
 }
 
-void projectOne(const orc_frame& f, uint32_t i, uint32_t slot, const float* positions, const uint32_t* shape,
-                const uint32_t* sh, float* records, uint32_t* rects, uint32_t* touchedOut, uint32_t* depthKeys,
-                uint32_t* visible) {
-    // splat_project.slang:497-523
-    const float px = positions[i * 4 + 0], py = positions[i * 4 + 1], pz = positions[i * 4 + 2];
-    float opacity = positions[i * 4 + 3];
+// One Gaussian as the projection reads it (position, opacity, linear scales,
+// unit quaternion x y z w, the constant term's colour).
+struct G32 {
+    float px, py, pz, opacity;
+    float scale[3];
+    float q[4];
+    float base[3];
+};
+
+G32 loadPacked(const float* positions, const uint32_t* shape, uint32_t i) {
+    G32 g;
+    g.px = positions[i * 4 + 0];
+    g.py = positions[i * 4 + 1];
+    g.pz = positions[i * 4 + 2];
+    g.opacity = positions[i * 4 + 3];
     const uint32_t row = i * 4;
-    const float scale[3] = {expf_(lowHalf(shape[row + 1])), expf_(highHalf(shape[row + 1])),
-                            expf_(lowHalf(shape[row + 2]))};
+    g.scale[0] = expf_(lowHalf(shape[row + 1]));
+    g.scale[1] = expf_(highHalf(shape[row + 1]));
+    g.scale[2] = expf_(lowHalf(shape[row + 2]));
+    decodeQuaternion(shape[row], g.q);
+    g.base[0] = highHalf(shape[row + 2]);
+    g.base[1] = lowHalf(shape[row + 3]);
+    g.base[2] = highHalf(shape[row + 3]);
+    return g;
+}
+
+// The FP32 training layout: means float4 (xyz, opacity logit), scales float4
+// (log scales), quats float4 (w x y z, any length), sh: DC rgb then rest rgb
+// per basis. Decoded as the upload would: sigmoid, exp, normalise, 0.5 + SH0 dc.
+G32 loadParams(const float* means, const float* scales, const float* quats, const float* sh, uint32_t stride,
+               uint32_t i) {
+    G32 g;
+    g.px = means[i * 4 + 0];
+    g.py = means[i * 4 + 1];
+    g.pz = means[i * 4 + 2];
+    g.opacity = 1.0f / (1.0f + expf_(-means[i * 4 + 3]));
+    for (int k = 0; k < 3; ++k) g.scale[k] = expf_(scales[i * 4 + k]);
+    const float* q = quats + (size_t)i * 4;
+    const float len = std::sqrt(((q[0] * q[0] + q[1] * q[1]) + q[2] * q[2]) + q[3] * q[3]);
+    g.q[0] = q[1] / len;
+    g.q[1] = q[2] / len;
+    g.q[2] = q[3] / len;
+    g.q[3] = q[0] / len;
+    const float* c = sh + (size_t)i * stride;
+    for (int k = 0; k < 3; ++k) g.base[k] = 0.5f + kSH0 * c[k];
+    return g;
+}
+
+template <typename RestFn>
+void projectCore(const orc_frame& f, const G32& g, RestFn rest3, uint32_t slot, float* records, uint32_t* rects,
+                 uint32_t* touchedOut, uint32_t* depthKeys, uint32_t* visible) {
+    // splat_project.slang:497-523
+    const float px = g.px, py = g.py, pz = g.pz;
+    float opacity = g.opacity;
+    const float* scale = g.scale;
     const float pos[3] = {px, py, pz};
     const Fate fate = editFate(f.edit, pos, opacity, scale);
     if (fate.removed) {
@@ -383,9 +431,7 @@ void projectOne(const orc_frame& f, uint32_t i, uint32_t slot, const float* posi
         return;
     }
     // :526-532
-    float q[4];
-    decodeQuaternion(shape[row], q);
-    const float x = q[0], y = q[1], z = q[2], w = q[3];
+    const float x = g.q[0], y = g.q[1], z = g.q[2], w = g.q[3];
     const float r[3][3] = {{1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - w * z), 2.0f * (x * z + w * y)},
                            {2.0f * (x * y + w * z), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z - w * x)},
                            {2.0f * (x * z - w * y), 2.0f * (y * z + w * x), 1.0f - 2.0f * (x * x + y * y)}};
@@ -478,15 +524,14 @@ void projectOne(const orc_frame& f, uint32_t i, uint32_t slot, const float* posi
         return;
     }
     // :781-785
-    const float base[3] = {highHalf(shape[row + 2]), lowHalf(shape[row + 3]), highHalf(shape[row + 3])};
     const uint32_t degree = std::min(degreeOf(f.restPerColour), f.shLimit);
     const float dx = px - f.eye[0], dy = py - f.eye[1], dz = pz - f.eye[2];
     const float len = std::sqrt((dx * dx + dy * dy) + dz * dz);
-    float rest[3];
-    evaluateRest(sh, i * f.shWords, degree, dx / len, dy / len, dz / len, rest);
+    float restv[3];
+    rest3(degree, dx / len, dy / len, dz / len, restv);
     float colour[3];
     for (int k = 0; k < 3; ++k) {
-        const float v = base[k] + rest[k];
+        const float v = g.base[k] + restv[k];
         colour[k] = f.linearCloud != 0 ? std::max(v, 0.0f) : srgbToLinear(v);
     }
     if (fate.graded) editGrade(f.edit, colour);
@@ -502,6 +547,18 @@ void projectOne(const orc_frame& f, uint32_t i, uint32_t slot, const float* posi
     touchedOut[slot] = touched;
     visible[slot] = 1;
     depthKeys[slot] = bitsOf(tz) >> 7;
+}
+
+void projectOne(const orc_frame& f, uint32_t i, uint32_t slot, const float* positions, const uint32_t* shape,
+                const uint32_t* sh, float* records, uint32_t* rects, uint32_t* touchedOut, uint32_t* depthKeys,
+                uint32_t* visible) {
+    const G32 g = loadPacked(positions, shape, i);
+    projectCore(f, g,
+                [&](uint32_t degree, float x, float y, float z, float out[3]) {
+                    evaluateRest([&](uint32_t index) { return halfAt(sh, i * f.shWords, index); }, degree, x, y, z,
+                                 out);
+                },
+                slot, records, rects, touchedOut, depthKeys, visible);
 }
 
 // One pixel's walk: splat_blend.slang:236-578 with composite, matte, trace off.
@@ -763,6 +820,42 @@ void orc_project(const orc_frame* f, uint32_t count, uint32_t base, const float*
     for (int64_t i = 0; i < (int64_t)count; ++i) {
         projectOne(*f, (uint32_t)i, base + (uint32_t)i, positions, shape, sh, records, rects, touched, depthKeys,
                    visible);
+    }
+}
+
+void orc_project_params(const orc_frame* f, uint32_t count, uint32_t base, const float* means, const float* scales,
+                        const float* quats, const float* sh, uint32_t shStride, float* records, uint32_t* rects,
+                        uint32_t* touched, uint32_t* depthKeys, uint32_t* visible, int threads) {
+#pragma omp parallel for schedule(static, 4096) num_threads(threadsOr(threads))
+    for (int64_t ii = 0; ii < (int64_t)count; ++ii) {
+        const uint32_t i = (uint32_t)ii;
+        const G32 g = loadParams(means, scales, quats, sh, shStride, i);
+        const float* row = sh + (size_t)i * shStride + 3;
+        projectCore(*f, g,
+                    [&](uint32_t degree, float x, float y, float z, float out[3]) {
+                        evaluateRest([&](uint32_t index) { return row[index]; }, degree, x, y, z, out);
+                    },
+                    base + i, records, rects, touched, depthKeys, visible);
+    }
+}
+
+void orc_colour_gradient_exact(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                               const float* records, const float* dLdPixel, double* gradient) {
+    const uint32_t tiles = f->tilesX * f->tilesY;
+    for (uint32_t t = 0; t < tiles; ++t) {
+        const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
+        for (uint32_t ly = 0; ly < kTile; ++ly) {
+            for (uint32_t lx = 0; lx < kTile; ++lx) {
+                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+                if (px >= f->width || py >= f->height) continue;
+                const uint32_t at = py * f->width + px;
+                walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
+                          (float)py + 0.5f, [&](uint32_t s, float weight) {
+                              for (uint32_t c = 0; c < 3; ++c)
+                                  gradient[s * 3 + c] += (double)weight * (double)dLdPixel[at * 4 + c];
+                          });
+            }
+        }
     }
 }
 

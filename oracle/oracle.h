@@ -111,6 +111,14 @@ void orc_project(const orc_frame* f, uint32_t count, uint32_t base, const float*
                  const uint32_t* shape, const uint32_t* sh, float* records, uint32_t* rects,
                  uint32_t* touched, uint32_t* depthKeys, uint32_t* visible, int threads);
 
+/* The same projection from FP32 training parameters: means float4 (xyz, opacity
+ * logit), scales float4 (log scales), quats float4 (w x y z, any length), sh
+ * shStride floats (DC rgb, then rest rgb per basis). Decoded as an upload
+ * would: sigmoid, exp, normalise, 0.5 + SH0 * DC. */
+void orc_project_params(const orc_frame* f, uint32_t count, uint32_t base, const float* means, const float* scales,
+                        const float* quats, const float* sh, uint32_t shStride, float* records, uint32_t* rects,
+                        uint32_t* touched, uint32_t* depthKeys, uint32_t* visible, int threads);
+
 /* ---- (b)+(c) binning, the reference's two-sort form (TileRasterizer.cpp:1088-1176):
  * compact -> stable 24-bit depth sort -> gather -> scan -> emit -> stable tile sort -> ranges.
  * pairTiles/pairSplats need `pairs` entries (the sum of touched); ranges 2 per tile.
@@ -132,6 +140,10 @@ uint64_t orc_blend(const orc_frame* f, const uint32_t* ranges, const uint32_t* p
  * weight * dLdPixel.rgb in 1/256 with hash-dithered rounding, and the weight. */
 void orc_colour_gradient(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
                          const float* records, const float* dLdPixel, int32_t* contribution);
+
+/* The same sums unquantised, in double: gradient[slot*3 + c] = sum of weight * dLdPixel. */
+void orc_colour_gradient_exact(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                               const float* records, const float* dLdPixel, double* gradient);
 
 /* contributionMode 1: the weight each slot blended with, in 1/4096 of a pixel. */
 void orc_contribution_weight(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
@@ -177,6 +189,17 @@ void orc_render_f64(const orc_frame64* f, uint32_t count, const float* positions
 void orc_render_params_f64(const orc_frame64* f, uint32_t count, const double* means, const double* logScales,
                            const double* quats, const double* logits, const double* shs, uint32_t shDegree,
                            double* colour, double* depth, int threads);
+
+/* Central finite differences (step eps) of L = mean over pixels and r g b of
+ * (colour - target)^2, in double, for the Gaussians `which`: out[k*59 + j] for
+ * parameter j of which[k] in the order means x y z, logit, log scales x y z,
+ * quat w x y z, sh[48]. The blend's decisions (which records each pixel blends
+ * and where its walk stops) are frozen at the base parameters. target: float3
+ * a pixel. *lossOut receives L at the base. */
+void orc_fd_gradients_f64(const orc_frame64* f, uint32_t count, const double* means, const double* logScales,
+                          const double* quats, const double* logits, const double* shs, uint32_t shDegree,
+                          const float* target, const uint32_t* which, uint32_t nWhich, double eps, double* out,
+                          double* lossOut, int threads);
 
 #ifdef __cplusplus
 }

@@ -97,6 +97,11 @@ def lib():
                                     C.c_float, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P,
                                     C.c_uint32, C.c_float, C.POINTER(Edit), C.POINTER(Frame)]
         L.orc_project.argtypes = [C.POINTER(Frame), C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, C.c_int]
+        L.orc_project_params.argtypes = [C.POINTER(Frame), C.c_uint32, C.c_uint32, _P, _P, _P, _P, C.c_uint32,
+                                         _P, _P, _P, _P, _P, C.c_int]
+        L.orc_colour_gradient_exact.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
+        L.orc_fd_gradients_f64.argtypes = [C.POINTER(Frame64), C.c_uint32, _P, _P, _P, _P, _P, C.c_uint32, _P, _P,
+                                           C.c_uint32, C.c_double, _P, C.POINTER(C.c_double), C.c_int]
         L.orc_bin.restype = C.c_uint64
         L.orc_bin.argtypes = [C.POINTER(Frame), C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         L.orc_blend.restype = C.c_uint64
@@ -224,6 +229,51 @@ def project(f: Frame, positions, shape, sh, slots=None, base=0, out=None, thread
                           _ptr(out["records"]), _ptr(out["rects"]), _ptr(out["touched"]), _ptr(out["keys"]),
                           _ptr(out["visible"]), threads)
     return out
+
+
+def project_params(f: Frame, means, scales, quats, sh, sh_stride, out=None, base=0, threads=0):
+    """The projection from FP32 training parameters (float4 means/scales/quats, sh rows)."""
+    n = means.shape[0]
+    slots = base + n
+    if out is None:
+        out = dict(records=np.zeros((slots, 12), np.float32), rects=np.zeros((slots, 4), np.uint32),
+                   touched=np.zeros(slots, np.uint32), keys=np.zeros(slots, np.uint32),
+                   visible=np.zeros(slots, np.uint32))
+    if n:
+        lib().orc_project_params(C.byref(f), n, base, _ptr(np.ascontiguousarray(means, np.float32)),
+                                 _ptr(np.ascontiguousarray(scales, np.float32)),
+                                 _ptr(np.ascontiguousarray(quats, np.float32)),
+                                 _ptr(np.ascontiguousarray(sh, np.float32)), sh_stride, _ptr(out["records"]),
+                                 _ptr(out["rects"]), _ptr(out["touched"]), _ptr(out["keys"]), _ptr(out["visible"]),
+                                 threads)
+    return out
+
+
+def colour_gradient_exact(f: Frame, binned: dict, proj: dict, dl_dpixel: np.ndarray) -> np.ndarray:
+    """Per slot, sum over pixels of weight * dL/dpixel (rgb), in double."""
+    slots = proj["touched"].shape[0]
+    out = np.zeros((slots, 3), np.float64)
+    ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
+    lib().orc_colour_gradient_exact(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]),
+                                    _ptr(np.ascontiguousarray(dl_dpixel, np.float32)), _ptr(out))
+    return out
+
+
+def fd_gradients_f64(f64: Frame64, means, log_scales, quats, logits, shs, sh_degree, target, which, eps,
+                     threads=0):
+    """FP64 central differences of the mean-L2 loss (decisions frozen at the base), 59 a Gaussian:
+    means xyz, logit, log scales xyz, quat wxyz, sh[48]. Returns (grads (K, 59), loss)."""
+    which = np.ascontiguousarray(which, np.uint32)
+    out = np.zeros((which.shape[0], 59), np.float64)
+    loss = C.c_double(0.0)
+    lib().orc_fd_gradients_f64(C.byref(f64), means.shape[0], _ptr(np.ascontiguousarray(means, np.float64)),
+                               _ptr(np.ascontiguousarray(log_scales, np.float64)),
+                               _ptr(np.ascontiguousarray(quats, np.float64)),
+                               _ptr(np.ascontiguousarray(logits, np.float64)),
+                               _ptr(np.ascontiguousarray(shs, np.float64)), sh_degree,
+                               _ptr(np.ascontiguousarray(target, np.float32)), _ptr(which), which.shape[0], eps,
+                               _ptr(out), C.byref(loss), threads)
+    return out, loss.value
 
 
 def bin_(f: Frame, proj: dict):

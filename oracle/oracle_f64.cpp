@@ -383,3 +383,154 @@ void orc_render_params_f64(const orc_frame64* f, uint32_t count, const double* m
 }
 
 }   // extern "C"
+
+// ---------------------------------------------------------------------------
+// Central finite differences of the mean-L2 loss in double, with the blend's
+// decisions frozen at the base parameters: which records each pixel blends
+// (power within the cutoff, alpha at least 1/255) and where its walk stops.
+// Those decisions are piecewise constant, so the derivative the analytic
+// backward computes is the derivative of the frozen walk; differencing the
+// unfrozen image instead would count every pixel a footprint's edge crosses.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kParamsPerGaussian = 59;   // means 3, logit 1, log scales 3, quat 4 (w x y z), sh 48
+
+struct ParamSet {
+    const double *means, *logScales, *quats, *logits, *shs;
+    uint32_t degree;
+};
+
+Gauss64 gaussOf(const ParamSet& P, uint32_t i, int perturbed, double delta) {
+    double v[kParamsPerGaussian];
+    v[0] = P.means[i * 3 + 0]; v[1] = P.means[i * 3 + 1]; v[2] = P.means[i * 3 + 2];
+    v[3] = P.logits[i];
+    v[4] = P.logScales[i * 3 + 0]; v[5] = P.logScales[i * 3 + 1]; v[6] = P.logScales[i * 3 + 2];
+    for (int k = 0; k < 4; ++k) v[7 + k] = P.quats[i * 4 + k];
+    for (int k = 0; k < 48; ++k) v[11 + k] = P.shs[(size_t)i * 48 + k];
+    if (perturbed >= 0) v[perturbed] += delta;
+    Gauss64 g{};
+    for (int k = 0; k < 3; ++k) {
+        g.p[k] = v[k];
+        g.scale[k] = std::exp(v[4 + k]);
+    }
+    g.opacity = sigmoid(v[3]);
+    const double n = std::sqrt(v[7] * v[7] + v[8] * v[8] + v[9] * v[9] + v[10] * v[10]);
+    g.q[0] = v[8] / n;
+    g.q[1] = v[9] / n;
+    g.q[2] = v[10] / n;
+    g.q[3] = v[7] / n;
+    for (int k = 0; k < 3; ++k) g.base[k] = 0.5 + kSH0 * v[11 + k];
+    for (int b = 0; b < 15; ++b)
+        for (int ch = 0; ch < 3; ++ch) g.rest[b][ch] = v[11 + 3 + b * 3 + ch];
+    g.degree = P.degree;
+    return g;
+}
+
+// A pixel's frozen walk: the records it blended, in order.
+struct FrozenPixel {
+    std::vector<uint32_t> slots;
+};
+
+double pixelColourWith(const orc_frame64& f, const FrozenPixel& fp, const std::vector<Rec64>& recs, uint32_t px,
+                       uint32_t py, uint32_t overrideSlot, const Rec64* overrideRec, double out[3]) {
+    const double pxc = px + 0.5, pyc = py + 0.5;
+    double rgb[3] = {0, 0, 0}, T = 1.0;
+    for (uint32_t s : fp.slots) {
+        const Rec64& r = (s == overrideSlot && overrideRec) ? *overrideRec : recs[s];
+        const double dx = pxc - r.cx, dy = pyc - r.cy;
+        const double power = r.a * dx * dx + 2.0 * r.b * dx * dy + r.c * dy * dy;
+        const double alpha = std::min(0.99, r.alpha * std::exp(-0.5 * power));
+        const double w = T * alpha;
+        for (int k = 0; k < 3; ++k) rgb[k] += w * r.colour[k];
+        T *= 1.0 - alpha;
+    }
+    for (int k = 0; k < 3; ++k) out[k] = rgb[k] + T * f.bg[k];
+    return T;
+}
+
+}   // namespace
+
+extern "C" void orc_fd_gradients_f64(const orc_frame64* f, uint32_t count, const double* means,
+                                     const double* logScales, const double* quats, const double* logits,
+                                     const double* shs, uint32_t shDegree, const float* target, const uint32_t* which,
+                                     uint32_t nWhich, double eps, double* out, double* lossOut, int threads) {
+    const ParamSet P{means, logScales, quats, logits, shs, shDegree};
+    Frame64 fr;
+    fr.recs.resize(count);
+#pragma omp parallel for schedule(static, 1024) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (int64_t i = 0; i < (int64_t)count; ++i) {
+        fr.recs[i] = project64(*f, gaussOf(P, (uint32_t)i, -1, 0.0), 0.0);
+        fr.recs[i].slot = (uint32_t)i;
+    }
+    bin64(*f, fr, 0.0, 1, 0);
+    const uint32_t W = f->width, H = f->height;
+    std::vector<FrozenPixel> frozen((size_t)W * H);
+    std::vector<double> base((size_t)W * H * 3);
+    double loss = 0.0;
+    const double scale = 1.0 / (3.0 * (double)W * (double)H);
+    const uint32_t tiles = fr.tilesX * fr.tilesY;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : loss) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (int64_t ti = 0; ti < (int64_t)tiles; ++ti) {
+        const uint32_t t = (uint32_t)ti, tx = t % fr.tilesX, ty = t / fr.tilesX;
+        for (uint32_t ly = 0; ly < kTile; ++ly)
+            for (uint32_t lx = 0; lx < kTile; ++lx) {
+                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+                if (px >= W || py >= H) continue;
+                const size_t at = (size_t)py * W + px;
+                FrozenPixel& fp = frozen[at];
+                double T = 1.0;
+                for (uint32_t s : fr.lists[t]) {
+                    const Rec64& r = fr.recs[s];
+                    if (!r.live) continue;
+                    const double dx = px + 0.5 - r.cx, dy = py + 0.5 - r.cy;
+                    const double power = r.a * dx * dx + 2.0 * r.b * dx * dy + r.c * dy * dy;
+                    if (power > r.cutoff) continue;
+                    const double alpha = std::min(0.99, r.alpha * std::exp(-0.5 * power));
+                    if (alpha < 1.0 / 255.0) continue;
+                    fp.slots.push_back(s);
+                    T *= 1.0 - alpha;
+                    if (T < 1e-4) break;
+                }
+                double c[3];
+                pixelColourWith(*f, fp, fr.recs, px, py, ~0u, nullptr, c);
+                for (int k = 0; k < 3; ++k) {
+                    base[at * 3 + k] = c[k];
+                    const double e = c[k] - target[at * 3 + k];
+                    loss += e * e * scale;
+                }
+            }
+    }
+    if (lossOut) *lossOut = loss;
+    // the pixels each perturbed Gaussian reaches
+    std::vector<std::vector<uint32_t>> reach(nWhich);
+    {
+        std::vector<int64_t> index(count, -1);
+        for (uint32_t k = 0; k < nWhich; ++k) index[which[k]] = k;
+        for (size_t at = 0; at < frozen.size(); ++at)
+            for (uint32_t s : frozen[at].slots)
+                if (index[s] >= 0) reach[index[s]].push_back((uint32_t)at);
+    }
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (int64_t kk = 0; kk < (int64_t)nWhich; ++kk) {
+        const uint32_t g = which[kk];
+        for (int j = 0; j < kParamsPerGaussian; ++j) {
+            double d[2] = {0.0, 0.0};
+            for (int sgn = 0; sgn < 2; ++sgn) {
+                Rec64 rec = project64(*f, gaussOf(P, g, j, sgn == 0 ? eps : -eps), 1.0);
+                double delta = 0.0;
+                for (uint32_t at : reach[kk]) {
+                    double c[3];
+                    pixelColourWith(*f, frozen[at], fr.recs, at % W, at / W, g, &rec, c);
+                    for (int k = 0; k < 3; ++k) {
+                        const double e1 = c[k] - target[(size_t)at * 3 + k];
+                        const double e0 = base[(size_t)at * 3 + k] - target[(size_t)at * 3 + k];
+                        delta += (e1 * e1 - e0 * e0) * scale;
+                    }
+                }
+                d[sgn] = delta;
+            }
+            out[(size_t)kk * kParamsPerGaussian + j] = (d[0] - d[1]) / (2.0 * eps);
+        }
+    }
+}
