@@ -133,10 +133,15 @@ def test_colour_gradient_is_the_references(oracle, raster):
     ours = grads10[:, 6:9].astype(np.float64)
     scale = np.abs(exact).max()
     assert np.abs(ours - exact).max() <= 1e-4 * scale
-    quant = oracle.colour_gradient(f, binned, pr, dln)[:, :3] / 256.0
-    # hash-dithered rounding: unbiased, a step of 1/256 at most per pixel
-    assert np.abs(quant - exact).mean() < 1.0 / 256.0
-    assert np.corrcoef(quant.ravel(), exact.ravel())[0, 1] > 0.99
+    # The quantised form, at the per-pixel scale it is made for (a derivative of
+    # order one a pixel: the sum of squares, not its mean): hash-dithered rounding
+    # to 1/256 is unbiased, so the sums agree to about sqrt(pixels)/256.
+    big = dln * (3.0 * W * H)
+    quant = oracle.colour_gradient(f, binned, pr, big)[:, :3] / 256.0
+    exact_big = oracle.colour_gradient_exact(f, binned, pr, big)
+    live = np.abs(exact_big) > 0
+    assert np.corrcoef(quant[live], exact_big[live])[0, 1] > 0.99
+    assert np.abs(quant - exact_big).mean() < 0.1
 
 
 def test_gradients_match_fp64_finite_differences(oracle, raster):
