@@ -119,6 +119,7 @@ SIGNATURES = {
     "ath_sorter_create": (C.c_int32, [C.POINTER(C.c_void_p)]),
     "ath_sorter_destroy": (None, [_P]),
     "ath_sorter_sort": (C.c_int32, [_P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, _P]),
+    "ath_sort_pairs_static": (C.c_int32, [_P, _P, _P, _P, C.c_uint32, C.c_uint32, _P]),
     "ath_decode_records": (C.c_int32, [_P, C.c_uint32, C.POINTER(Encoding), _P, _P, _P, C.POINTER(C.c_uint32), _P]),
     "ath_last_error_message": (C.c_char_p, []),
     "ath_version": (C.c_char_p, []),

@@ -274,6 +274,19 @@ void ath_sorter_destroy(ath_sorter* s);
 ath_status ath_sorter_sort(ath_sorter* s, uint64_t* keys, uint32_t* values, uint64_t* scratch_keys,
                            uint32_t* scratch_values, uint32_t count, uint32_t key_bits, void* stream);
 
+/* The same sort for callers that cannot allocate device memory while they
+ * sort: a plugin held to its host application's memory budget mid-frame, or a
+ * caller capturing its own work into a CUDA graph. It has no counterpart in
+ * the reference. The sort's own working memory (histograms, look-back words,
+ * tickets) is a fixed 4 MiB array every GPU that loads the library holds until
+ * exit; nothing is allocated. At most 1,048,576 pairs a call (larger counts
+ * return ATH_E_INVALID_ARGUMENT). The first call on a device finds that array's
+ * address and sets the kernel up: make it before any stream capture. Every call
+ * shares the array, so calls that overlap on the GPU race; keys/values and the
+ * scratch pair are as for ath_sorter_sort. */
+ath_status ath_sort_pairs_static(uint64_t* keys, uint32_t* values, uint64_t* scratch_keys, uint32_t* scratch_values,
+                                 uint32_t count, uint32_t key_bits, void* stream);
+
 /* ---- decode: scene::CloudLoader::upload's kernels ------------------------ */
 
 /* scene/splat_validate.slang:16-31 + scene/splat_decode.slang:45-173 for
