@@ -30,6 +30,26 @@ __device__ __forceinline__ float warpSum(float v) {
     return v;
 }
 
+// Sums 16 values over the warp's 32 lanes in 16 shuffles (not 16 x 5): at each
+// butterfly step a lane keeps one half of its values and sends the other, so
+// the values a lane carries halve while the lanes summed double. Afterwards
+// value k's total sits in the lanes whose bits 1..4 spell k (lane >> 1 == k:
+// lanes 2k and 2k + 1 both hold it).
+__device__ __forceinline__ float warpSum16(float v[16]) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int half = 8, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
+        const bool upper = (lane & (uint32_t)bit) != 0;
+#pragma unroll
+        for (int k = 0; k < half; ++k) {
+            const float send = upper ? v[k] : v[k + half];
+            const float keep = upper ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, bit);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xFFFFFFFFu, v[0], 1);
+}
+
 // dL/d(record) of every slot: centre x y, conic a b c, alpha, colour r g b, view z.
 __global__ void __launch_bounds__(kBwdThreads)
     blendBackwardKernel(const FrameConst F, uint32_t pairs, uint32_t slots, const uint2* __restrict__ ranges,
@@ -143,11 +163,12 @@ __global__ void __launch_bounds__(kBwdThreads)
                 }
             }
             if (__any_sync(0xFFFFFFFFu, live)) {
+                float v16[16];
 #pragma unroll
-                for (int k = 0; k < (int)kGradWords; ++k) {
-                    const float v = warpSum(g[k]);
-                    if (lane == 0 && v != 0.0f) atomicAdd(&sAcc[j * kGradWords + k], v);
-                }
+                for (int k = 0; k < 16; ++k) v16[k] = k < (int)kGradWords ? g[k] : 0.0f;
+                const float v = warpSum16(v16);
+                const uint32_t k = lane >> 1;   // lanes 2k and 2k + 1 hold value k's total
+                if ((lane & 1u) == 0 && k < kGradWords && v != 0.0f) atomicAdd(&sAcc[j * kGradWords + k], v);
             }
         }
         __syncthreads();
@@ -235,7 +256,9 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
         float v = g.base[ch];
-        for (uint32_t k = 0; k < bases; ++k) v += Y[k] * shRow[3 + k * 3 + ch];
+#pragma unroll
+        for (uint32_t k = 0; k < 15; ++k)
+            if (k < bases) v += Y[k] * shRow[3 + k * 3 + ch];
         float dcdv;
         if (I.linear != 0) {
             dcdv = v > 0.0f ? 1.0f : 0.0f;
@@ -244,7 +267,9 @@ __global__ void __launch_bounds__(128)
         }
         const float dv = gc[ch] * dcdv;
         gRow[ch] += kSH0 * dv;
-        for (uint32_t k = 0; k < bases; ++k) {
+#pragma unroll
+        for (uint32_t k = 0; k < 15; ++k) {
+            if (k >= bases) continue;
             gRow[3 + k * 3 + ch] += Y[k] * dv;
             const float coef = shRow[3 + k * 3 + ch] * dv;
             dDir[0] += dY[k][0] * coef;
@@ -397,8 +422,16 @@ __global__ void __launch_bounds__(256)
         l = (er * er + eg * eg + eb * eb) * scale;
         dLdColour[p] = make_float4(2.0f * scale * er, 2.0f * scale * eg, 2.0f * scale * eb, 0.0f);
     }
+    __shared__ float sPart[8];
     l = warpSum(l);
-    if ((threadIdx.x & 31u) == 0 && l != 0.0f) atomicAdd(loss, l);
+    if ((threadIdx.x & 31u) == 0) sPart[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float b = 0.0f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) b += sPart[w];
+        if (b != 0.0f) atomicAdd(loss, b);
+    }
 }
 
 }   // namespace

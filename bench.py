@@ -118,36 +118,68 @@ def view_cameras(views: int, first: int = 0):
 
 
 # ---------------------------------------------------------------------------
+class PlainTrainer:
+    """The plain FP32 path: per view, a differentiable frame (ath_raster_render_params),
+    the mean-L2 loss's gradient (ath_l2_loss) and the backward (ath_raster_backward), one
+    view after another, gradients added into one set."""
+
+    def __init__(self, params, projs, targets_dev, W, H, dev):
+        import torch
+        import athenea_b200 as A
+        self.A = A
+        self.P = params
+        self.projs = projs
+        self.targets = targets_dev
+        self.W, self.H = W, H
+        self.raster = A.TileRasterizer.create()
+        self.settings = A.RenderSettings(width=W, height=H)
+        self.frames = A.RenderTargets.make(W, H, device=dev)
+        self.dl = torch.empty((W * H, 4), dtype=torch.float32, device=dev)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.grads = params.zeros_like()
+
+    def step(self, stream, targets=None, ready=None):
+        targets = targets if targets is not None else self.targets
+        self.loss.zero_()
+        for g in (self.grads.means, self.grads.scales, self.grads.quats, self.grads.sh):
+            g.zero_()
+        stats = None
+        for v, proj in enumerate(self.projs):
+            if ready is not None:
+                stream.wait_event(ready[v])
+            stats = self.raster.render_params(proj, self.P, self.settings, self.frames, stream=stream)
+            self.A.l2_loss(self.frames.colour, targets[v], self.dl, self.loss, stream=stream)
+            self.raster.backward(self.dl, self.grads, stream=stream)
+        return stats
+
+
 def run_ours(args) -> dict | None:
     import torch
     import torch.distributed as dist
 
     import athenea_b200 as A
+    from athenea_b200 import scenes
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device("cuda", local)
-    recs, enc = make_scene(20261203 + 1)
-    cloud = A.CloudLoader.upload(torch.from_numpy(recs.reshape(-1)).to(dev), enc, 3)
-    del recs
-    torch.cuda.empty_cache()
     V = WORKLOAD["views"]
     W, H = WORKLOAD["width"], WORKLOAD["height"]
+    p = scenes.params(WORKLOAD["count"], WORKLOAD["clustered"], 20261203 + 1, WORKLOAD["sh_degree"])
+    params = A.Params(*[torch.from_numpy(p[k]).to(dev) for k in ("means", "scales", "quats", "sh")],
+                      sh_degree=p["sh_degree"])
+    del p
     projs = view_cameras(V, first=rank * V)
-    raster = A.TileRasterizer.create()
-    settings = A.RenderSettings(width=W, height=H)
-    targets = [A.RenderTargets.make(W, H, device=dev) for _ in range(V)]
-    inst = [A.SplatInstance(cloud)]
+    gen = torch.Generator().manual_seed(20261203 + 7 + rank)
+    host_targets = [torch.rand((W * H, 3), generator=gen).pin_memory() for _ in range(V)]
+    dev_targets = [t.to(dev) for t in host_targets]
     stream = torch.cuda.current_stream(dev)
-
-    def step():
-        for v in range(V):
-            raster.render(projs[v], inst, settings, targets[v], stream=stream)
+    trainer = PlainTrainer(params, projs, dev_targets, W, H, dev)
 
     for _ in range(args.warmup):
-        step()
+        trainer.step(stream)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -156,7 +188,7 @@ def run_ours(args) -> dict | None:
     with ClockSampler(local) as clocks:
         start.record(stream)
         for _ in range(args.steps):
-            step()
+            trainer.step(stream)
         end.record(stream)
         torch.cuda.synchronize()
     ms = start.elapsed_time(end)
@@ -167,60 +199,81 @@ def run_ours(args) -> dict | None:
         dist.barrier()
     torch.cuda.synchronize()
     ms_per_step = ms / args.steps
-    views_total = V * world
 
-    # e2e: through the public API from host memory -- each view's camera goes
-    # in, its image comes back to pinned host memory.
-    host = [torch.empty((W * H, 4), dtype=torch.float32, pin_memory=True) for _ in range(V)]
+    # e2e: through the public API, each step's target images copied in from pinned
+    # host memory (on a copy stream, each view's copy overlapping the views before
+    # it) and the loss read back to the host.
+    copy = torch.cuda.Stream(dev)
+    staged = [torch.empty_like(t) for t in dev_targets]
+    loss_host = torch.empty(1, dtype=torch.float32, pin_memory=True)
     e2e_start, e2e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e2e_start.record(stream)
     for _ in range(args.steps):
+        copy.wait_stream(stream)
+        ready = []
         for v in range(V):
-            raster.render(projs[v], inst, settings, targets[v], stream=stream)
-            host[v].copy_(targets[v].colour, non_blocking=True)
+            with torch.cuda.stream(copy):
+                staged[v].copy_(host_targets[v], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(copy)
+            ready.append(ev)
+        trainer.step(stream, targets=staged, ready=ready)
+        loss_host.copy_(trainer.loss, non_blocking=True)
     e2e_end.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e2e_start.elapsed_time(e2e_end) / args.steps
 
-    # per-stage times of one frame (events between the stages, waited for)
+    # per-stage times of one forward (events between the stages, waited for)
     timed = A.RenderSettings(width=W, height=H, time_stages=True)
-    st = raster.render(projs[0], inst, timed, targets[0], stream=stream)
+    st = trainer.raster.render_params(projs[0], params, timed, trainer.frames, stream=stream)
+    bw0, bw1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    A.l2_loss(trainer.frames.colour, dev_targets[0], trainer.dl, trainer.loss, stream=stream)
+    bw0.record(stream)
+    trainer.raster.backward(trainer.dl, trainer.grads, stream=stream)
+    bw1.record(stream)
+    torch.cuda.synchronize()
     stages = {"project_ms": st.project_ms, "emit_ms": st.emit_ms, "sort_and_ranges_ms": st.tile_sort_ms,
-              "blend_ms": st.blend_ms}
+              "blend_ms": st.blend_ms, "backward_ms": bw0.elapsed_time(bw1)}
     passes = math.ceil((24 + max(1, math.ceil(math.log2(max(2, ((W + 15) // 16) * ((H + 15) // 16)))))) / 8)
-    launches_per_view = 5 + passes   # project, emit, histogram, passes, ranges, blend
-    out = dict(ms_per_step=ms_per_step, views=views_total, stats=st, stages=stages, e2e_ms=e2e_ms,
+    launches_per_view = 5 + passes + 3   # project, emit, histogram, passes, ranges, blend; loss, 2 backward
+    out = dict(ms_per_step=ms_per_step, views=V * world, stats=st, stages=stages, e2e_ms=e2e_ms,
                clocks=clocks.summary(), launches=launches_per_view * V * args.steps,
-               sh_words=cloud.sh_words, count=cloud.count, passes=passes)
+               sh_words=23, count=params.count, passes=passes, loss=float(loss_host.item()),
+               h2d=sum(t.numel() * 4 for t in host_targets), d2h=4)
     if world > 1:
         dist.destroy_process_group()
     return out if rank == 0 else None
 
 
 def cpu_baseline(threads: int = 0) -> dict:
-    """The CPU restatement (oracle/, the reference's method in C++) timed on one view."""
+    """The CPU restatement (oracle/: the reference's method in C++, OpenMP) on one view of the
+    same workload: the forward from the same FP32 parameters, the mean-L2 loss's gradient, and
+    the reference's own backward, the per-Gaussian colour gradient of its blend's
+    contributionMode 4 (splat_blend.slang:381-398)."""
     from oracle import oracle as O
-    O.build()
-    recs, enc = make_scene(20261203 + 1)
-    e = dict(stride=enc["stride"], x=0, y=1, z=2, opacity=enc["opacity"], scale0=enc["scale0"],
-             scale1=enc["scale1"], scale2=enc["scale2"], rotW=enc["rot_w"], rotX=enc["rot_x"], rotY=enc["rot_y"],
-             rotZ=enc["rot_z"], dc0=enc["dc0"], dc1=enc["dc1"], dc2=enc["dc2"], restBase=enc["rest_base"],
-             filePerColour=enc["file_per_colour"])
-    pos, shape, sh, _, shw = O.decode(recs.reshape(-1), e, 15)
-    del recs
-    W, H = WORKLOAD["width"], WORKLOAD["height"]
     from athenea_b200 import scenes
+    O.build()
+    p = scenes.params(WORKLOAD["count"], WORKLOAD["clustered"], 20261203 + 1, WORKLOAD["sh_degree"])
+    W, H = WORKLOAD["width"], WORKLOAD["height"]
     eye = scenes.circle_eye(0, WORKLOAD["views"] * 4, 3.0, 0.3)
     cam = O.looking_at(eye, (0, 0, 0))
     cam.focal = cam.haperture * ((H * 0.5) / math.tan(math.radians(WORKLOAD["vfov"]) * 0.5)) / W
     proj = O.projection_for(cam, W, H)
+    target = np.random.default_rng(20261203 + 7).uniform(0, 1, size=(W * H, 3)).astype(np.float32)
     t0 = time.perf_counter()
-    out = O.render([(pos, shape, sh, 15, shw, np.eye(4), 0)], proj, W, H, threads=threads)
+    f = O.frame_for(proj, np.eye(4), W, H, rest_per_colour=15, sh_words=23)
+    pr = O.project_params(f, p["means"], p["scales"], p["quats"], p["sh"], p["sh"].shape[1], threads=threads)
+    binned = O.bin_(f, pr)
+    out = O.blend(f, binned, pr, threads=threads)
+    err = out["colour"][:, :3] - target
+    dl = np.zeros((W * H, 4), np.float32)
+    dl[:, :3] = 2.0 * err / (3.0 * W * H)
+    O.colour_gradient(f, binned, pr, dl)
     dt = time.perf_counter() - t0
     cores = threads or os.cpu_count()
-    return dict(ms=dt * 1000.0, cores=cores, evaluated=out["evaluated"], pairs=out["binned"]["pairs"],
-                visible=out["binned"]["visible"])
+    return dict(ms=dt * 1000.0, cores=cores, evaluated=out["evaluated"], pairs=binned["pairs"],
+                visible=binned["visible"])
 
 
 def main():
@@ -242,18 +295,19 @@ def main():
         if rank != 0:
             return
         runs = []
-        for _ in range(args.warmup if args.warmup < 1 else 1):
-            cpu_baseline()
+        cpu_baseline()   # one untimed run: builds the checker, pages the scene in
         for _ in range(args.steps):
             runs.append(cpu_baseline())
         ms = statistics.median(r["ms"] for r in runs)
         line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms/view", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "clustered-1.5M-1920x1080, forward of one view, CPU restatement",
-                           "gaussians": WORKLOAD["count"], "width": WORKLOAD["width"], "height": WORKLOAD["height"]},
+                "config": {"workload": "clustered-1.5M-1920x1080", "gaussians": WORKLOAD["count"],
+                           "width": WORKLOAD["width"], "height": WORKLOAD["height"],
+                           "path": "the CPU restatement of the reference's path (oracle/, OpenMP): forward, "
+                                   "mean-L2 loss gradient, the reference's colour-gradient backward"},
                 "cpu_baseline": {"value": ms, "unit": "ms/view", "cores": runs[0]["cores"], "kind": "port",
-                                 "sample": "one 1920x1080 view of the 1.5M-Gaussian scene, forward"},
+                                 "sample": "one 1920x1080 view of the 1.5M-Gaussian scene a step"},
                 "e2e": {"value": ms, "unit": "ms/view", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -267,19 +321,20 @@ def main():
     dominant = max(stages, key=stages.get)
     W, H = WORKLOAD["width"], WORKLOAD["height"]
     # algorithmic bytes a launch, per stage (DESIGN.md states each figure)
-    per_slot_read = 16 + 16 + 4 * res["sh_words"]
+    per_slot_read = 16 + 16 + 16 + 4 * 48      # FP32 training parameters a Gaussian
     bytes_ = {
         "project_ms": res["count"] * (per_slot_read + 4 + 4) + st.visible * (48 + 8),
         "emit_ms": st.visible * (48 + 8 + 8) + st.pairs * 12,
         "sort_and_ranges_ms": st.pairs * (8 + 24 * res["passes"] + 8 + 8),
     }
     cpu = None if args.no_cpu else cpu_baseline()
-    if dominant == "blend_ms":
+    if dominant in ("blend_ms", "backward_ms"):
         flops = (cpu["evaluated"] if cpu else st.pairs * 256) * 20
         achieved = flops / (stages[dominant] * 1e-3) / 1e12
         fp32_peak = 148 * 128 * 2 * (P.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
         roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                    "frac": achieved / fp32_peak, "traffic": None, "kernel": "blendKernel",
+                    "frac": achieved / fp32_peak, "traffic": None,
+                    "kernel": "blendKernel" if dominant == "blend_ms" else "blendBackwardKernel",
                     "peak_source": "nominal FP32 FMA rate at the measured max SM clock (no FP32 peak is measured)"}
     else:
         achieved = bytes_[dominant] / (stages[dominant] * 1e-3) / 1e9
@@ -292,20 +347,23 @@ def main():
         "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset)",
         "config": {"workload": "clustered-1.5M-1920x1080", "gaussians": WORKLOAD["count"], "width": W, "height": H,
-                   "views_per_gpu": WORKLOAD["views"], "sh_degree": 3, "tile": 16, "path": "plain forward, FP32",
+                   "views_per_gpu": WORKLOAD["views"], "sh_degree": 3, "tile": 16,
+                   "path": "plain FP32, one view at a time: forward, mean-L2 loss, backward",
+                   "loss": "mean L2 against a target uniform in [0,1]^3",
                    "parallelism": f"views sharded over {world} GPU(s)",
-                   "l2": "inputs larger than L2 (packed Gaussians 186 MB > 126 MB)",
-                   "note": "forward only: the backward and the batched/mixed path are not in this measurement"},
+                   "l2": "inputs larger than L2 (FP32 parameters 360 MB > 126 MB)",
+                   "note": "the batched/mixed-precision path is not in this measurement yet"},
         "stages_ms": stages, "visible": st.visible, "pairs": st.pairs,
         "roofline": roofline,
-        "e2e": {"value": res["e2e_ms"] / WORKLOAD["views"], "unit": "ms/view", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": W * H * 16 * WORKLOAD["views"]},
+        "e2e": {"value": res["e2e_ms"] / WORKLOAD["views"], "unit": "ms/view",
+                "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
         "gpu_launches": res["launches"],
         "clocks": res["clocks"],
     }
     if cpu:
         line["cpu_baseline"] = {"value": cpu["ms"], "unit": "ms/view", "cores": cpu["cores"], "kind": "port",
-                                "sample": "one 1920x1080 view of the same scene, forward (project, bin, blend)"}
+                                "sample": "one 1920x1080 view of the same scene: forward, loss gradient and the "
+                                          "reference's colour-gradient backward"}
     print(json.dumps(line))
 
 
