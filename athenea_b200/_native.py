@@ -92,6 +92,27 @@ class ParamGrads(C.Structure):
     _fields_ = [("means", C.c_void_p), ("scales", C.c_void_p), ("quats", C.c_void_p), ("sh", C.c_void_p)]
 
 
+class MixedParams(C.Structure):
+    _fields_ = [("means", C.c_void_p), ("scales", C.c_void_p), ("quats", C.c_void_p), ("sh_low", C.c_void_p),
+                ("sh_high", C.c_void_p), ("sh_scale", C.c_void_p), ("count", C.c_uint32), ("sh_degree", C.c_uint32),
+                ("linear", C.c_int32), ("object_to_world", C.c_double * 16)]
+
+
+class View(C.Structure):
+    _fields_ = [("projection", Projection), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("pairs", C.c_uint64), ("capacity", C.c_uint64), ("kept", C.c_uint32), ("tile", C.c_uint32),
+                ("block_batch", C.c_uint32), ("ms_per_step", C.c_float)]
+
+
+class BatchBuffers(C.Structure):
+    _fields_ = [("pairs", C.c_uint64), ("key_shift", C.c_uint32), ("slot_bits", C.c_uint32),
+                ("total_tiles", C.c_uint32), ("views", C.c_uint32), ("sorted_pairs", C.c_void_p),
+                ("ranges", C.c_void_p), ("tile_bases", C.POINTER(C.c_uint32))]
+
+
 class Encoding(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("stride", "x", "y", "z", "opacity", "scale0", "scale1", "scale2", "rot_w",
                                           "rot_x", "rot_y", "rot_z", "dc0", "dc1", "dc2", "rest_base",
@@ -115,6 +136,17 @@ SIGNATURES = {
                                              C.POINTER(Targets), C.POINTER(FrameStats), _P]),
     "ath_raster_backward": (C.c_int32, [_P, _P, _P, C.POINTER(ParamGrads), _P]),
     "ath_l2_loss": (C.c_int32, [_P, _P, C.c_uint32, _P, _P, _P]),
+    "ath_params_to_mixed": (C.c_int32, [C.POINTER(Params), _P, _P, _P, _P]),
+    "ath_batch_create": (C.c_int32, [C.POINTER(C.c_void_p)]),
+    "ath_batch_destroy": (None, [_P]),
+    "ath_batch_set_views": (C.c_int32, [_P, _P, C.c_uint32, C.POINTER(Settings)]),
+    "ath_batch_set_tuning": (C.c_int32, [_P, C.c_uint32, C.c_uint32]),
+    "ath_batch_pixels": (C.c_int32, [_P, C.POINTER(C.c_uint32)]),
+    "ath_batch_train_step": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads), _P]),
+    "ath_batch_check": (C.c_int32, [_P, C.POINTER(BatchStats), _P]),
+    "ath_batch_buffers_of": (C.c_int32, [_P, C.POINTER(BatchBuffers), _P]),
+    "ath_batch_tune": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads), C.c_uint32,
+                                   C.POINTER(BatchStats), _P]),
     "ath_raster_frame_buffers": (C.c_int32, [_P, C.POINTER(FrameBuffers)]),
     "ath_sorter_create": (C.c_int32, [C.POINTER(C.c_void_p)]),
     "ath_sorter_destroy": (None, [_P]),

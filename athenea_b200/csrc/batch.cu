@@ -1,0 +1,1113 @@
+// The batched, mixed-precision training step: every view of a batch through
+// each stage in one launch, with nothing read back between stages, so the
+// whole step (forward, loss, backward) is captured once in a CUDA graph and
+// replayed.
+//
+//   projectEmit   one block = 256 Gaussians x one view (blocks of the same
+//                 Gaussians for every view run back to back, so the cloud is
+//                 read from DRAM once and from L2 after): the exact projection
+//                 geometry, the tiles touched (each division of the tile test
+//                 done once a rect row and once a tile), the scan over every
+//                 view's pairs by an epoch-tagged look-back, and the pairs,
+//                 written from a tile mask kept in registers.
+//   sort          one onesweep sort of every view's pairs, packed into one
+//                 64-bit word (global tile | 24-bit depth key | Gaussian), on
+//                 the tile and depth bits only: stability keeps each tile's
+//                 ties in Gaussian order, the reference's (frame.slang:17-20).
+//   blend         a persistent kernel over every view's tiles (a tile queue),
+//                 tile size 8, 16 or 32 and a record batch of 64, 128 or 256.
+//   loss          mean L2 a view against its target, summed over views.
+//   blendAdjoint  the same queue, reverse order, as backward.cu.
+//   projectAdjoint one thread a Gaussian over every view, its gradient kept in
+//                 registers and written once.
+//
+// The geometry that decides footprints, tiles and depth keys is the plain
+// path's to the bit (this file builds with --fmad=false and calls the same
+// projectGeometry): pairs, their order and the tile ranges are the reference's.
+// Colour (SH in BF16/FP8 from the mixed layout), the blend's exponential and
+// its divisions use the fast hardware paths; the image error that costs is
+// measured against an FP64 oracle.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cuda_runtime.h>
+
+#include "../../include/athenea_raster.h"
+#include "adjoint.cuh"
+#include "batch_kernels.cuh"
+#include "host_util.h"
+#include "kernels.h"
+
+namespace ath {
+namespace {
+
+constexpr uint32_t kProjThreads = 256;
+
+// ---- the step's first kernel: a new epoch, the step's counters cleared ------
+__global__ void beginStepKernel(uint32_t* words) {
+    words[kBatchEpoch] = (words[kBatchEpoch] + 1u) & 0x3FFFFFFFu;
+    words[kBatchTicket] = 0;
+    words[kBatchPairsLo] = 0;
+    words[kBatchPairsHi] = 0;
+    words[kBatchBlendTicket] = 0;
+    words[kBatchBackTicket] = 0;
+    words[kBatchKept] = 0;
+    for (int p = 0; p < 8; ++p) words[kBatchSortTickets + p] = 0;
+}
+
+// The decoupled look-back of lookbackExclusive with epoch-tagged 32-bit values.
+__device__ uint32_t lookbackEpoch(uint64_t* flags, uint32_t b, uint32_t aggregate, uint32_t epoch, uint32_t* status) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (b == 0) {
+        if (lane == 0) storeRelaxed(flags, tagged(epoch, 2, aggregate));
+        return 0;
+    }
+    if (lane == 0) storeRelaxed(flags + b, tagged(epoch, 1, aggregate));
+    uint64_t exclusive = 0;
+    int64_t window = (int64_t)b - 1;
+    uint32_t spins = 0;
+    while (true) {
+        const int64_t idx = window - (int64_t)lane;
+        const uint64_t v = idx >= 0 ? loadRelaxed(flags + idx) : tagged(epoch, 2, 0);
+        const uint32_t st = (uint32_t)(v >> 34) == (epoch & 0x3FFFFFFFu) ? (uint32_t)(v >> 32) & 3u : 0u;
+        const uint32_t notReady = __ballot_sync(0xFFFFFFFFu, st == 0);
+        const uint32_t inclusive = __ballot_sync(0xFFFFFFFFu, st == 2);
+        const uint32_t first = inclusive ? (uint32_t)(__ffs(inclusive) - 1) : 32u;
+        const uint32_t need = first >= 31 ? 0xFFFFFFFFu : ((2u << first) - 1u);
+        if (notReady & need) {
+            if (++spins > kSpinLimit || ((spins & 255u) == 0 && gaveUp(status))) {
+                if (lane == 0) atomicOr(status, kStatusLookbackTimeout);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        exclusive += warpSum64(lane <= first ? (v & 0xFFFFFFFFull) : 0ull);
+        if (first < 32) break;
+        window -= 32;
+    }
+    if (exclusive + aggregate > 0xFFFFFFFFull) atomicOr(status, kStatusPairOverflow);
+    if (lane == 0) storeRelaxed(flags + b, tagged(epoch, 2, (uint32_t)(exclusive + aggregate)));
+    return (uint32_t)exclusive;
+}
+
+// frame.slang:354-379 for tile size T, its divisions shared: x* = -b x / c of a
+// column's two x edges are computed once a rect row... the per-edge values are
+// the same operations minPowerOverBox performs, so the result is its result.
+__device__ __forceinline__ float quad(float a, float b, float c, float x, float y) {
+    return ((a * x) * x + ((2.0f * b) * x) * y) + (c * y) * y;
+}
+
+template <uint32_t L>
+__device__ void colourFast(const InstanceConst& I, const Gauss& g, uint32_t i, uint32_t degree, float dx, float dy,
+                           float dz, float colour[3]) {
+    const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
+    const float inv = fastRcp(len);
+    const float x = dx * inv, y = dy * inv, z = dz * inv;
+    float Y[15];
+    const float C1 = 0.4886025119029199f;
+    Y[0] = -C1 * y; Y[1] = C1 * z; Y[2] = -C1 * x;
+    const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+    Y[3] = 1.0925484305920792f * xy; Y[4] = -1.0925484305920792f * yz;
+    Y[5] = 0.31539156525252005f * (2.0f * zz - xx - yy); Y[6] = -1.0925484305920792f * xz;
+    Y[7] = 0.5462742152960396f * (xx - yy);
+    Y[8] = -0.5900435899266435f * y * (3.0f * xx - yy); Y[9] = 2.890611442640554f * xy * z;
+    Y[10] = -0.4570457994644658f * y * (4.0f * zz - xx - yy);
+    Y[11] = 0.3731763325901154f * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+    Y[12] = -0.4570457994644658f * x * (4.0f * zz - xx - yy); Y[13] = 1.445305721320277f * z * (xx - yy);
+    Y[14] = -0.5900435899266435f * x * (xx - 3.0f * yy);
+    const uint32_t bases = degree == 3 ? 15 : degree == 2 ? 8 : degree == 1 ? 3 : 0;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        float v = g.base[ch];
+#pragma unroll
+        for (uint32_t k = 0; k < 15; ++k)
+            if (k < bases) v = __fmaf_rn(Y[k], restAt<L>(I, i, k * 3 + (uint32_t)ch), v);
+        if (I.linear) {
+            colour[ch] = fmaxf(v, 0.0f);
+        } else {
+            const float c = fmaxf(v, 0.0f);
+            colour[ch] = c <= 0.04045f ? c * (1.0f / 12.92f) : __powf((c + 0.055f) * (1.0f / 1.055f), 2.4f);
+        }
+    }
+}
+
+template <uint32_t L>
+__global__ void __launch_bounds__(kProjThreads)
+    projectEmitKernel(const BatchConst B, const BatchView* __restrict__ views, float4* __restrict__ recs,
+                      uint64_t* __restrict__ pairs, uint64_t* __restrict__ flags, uint32_t* __restrict__ words,
+                      uint32_t gaussBlocks) {
+    __shared__ uint32_t sTicket;
+    __shared__ uint32_t sWarp[kProjThreads / 32];
+    __shared__ uint32_t sPrefix;
+    __shared__ BatchView sView;
+    __shared__ FrameConst sF;
+    if (threadIdx.x == 0) sTicket = atomicAdd(&words[kBatchTicket], 1u);
+    __syncthreads();
+    const uint32_t t = sTicket;
+    const uint32_t gb = t / B.views, v = t % B.views;
+    if (threadIdx.x == 0) {
+        sView = views[v];
+        FrameConst F{};
+        F.width = sView.width; F.height = sView.height; F.tilesX = sView.tilesX; F.tilesY = sView.tilesY;
+        F.focalX = sView.focalX; F.focalY = sView.focalY; F.centreX = sView.centreX; F.centreY = sView.centreY;
+        F.nearZ = sView.nearZ; F.farZ = sView.farZ; F.orthographic = sView.orthographic; F.shLimit = B.shLimit;
+        sF = F;
+    }
+    __syncthreads();
+    const uint32_t epoch = words[kBatchEpoch];
+    const FrameConst& F = sF;
+    InstanceConst I = B.inst;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) I.m[k] = sView.m[k];
+    I.eye[0] = sView.eye[0]; I.eye[1] = sView.eye[1]; I.eye[2] = sView.eye[2];
+    const uint32_t T = B.tile;
+    const uint32_t i = gb * kProjThreads + threadIdx.x;
+    uint32_t touched = 0, depthKey = 0, rx0 = 0, ry0 = 0, rx1 = 0, ry1 = 0;
+    uint64_t mask = 0;
+    float cx = 0, cy = 0, ca = 0, cb = 0, cc = 0, cutoff = 0;
+    if (i < B.count && gb < gaussBlocks) {
+        const Gauss g = loadGauss<L>(I, i);
+        const Geometry G = projectGeometry(F, I, g, g.opacity);
+        if (!G.cull) {
+            // frame.slang:383-402 for tile size T
+            const float det2 = G.ca * G.cc - G.cb * G.cb;
+            const float inv = det2 > 1e-20f ? 1.0f / det2 : 0.0f;
+            const float ex = sqrtf(fmaxf((G.cutoff * G.cc) * inv, 0.0f));
+            const float ey = sqrtf(fmaxf((G.cutoff * G.ca) * inv, 0.0f));
+            const float x1 = G.cx - ex, y1 = G.cy - ey, x2 = G.cx + ex, y2 = G.cy + ey;
+            if (!(x2 < 0.0f || y2 < 0.0f || x1 >= (float)F.width || y1 >= (float)F.height)) {
+                rx0 = (uint32_t)fmaxf(x1, 0.0f) / T;
+                ry0 = (uint32_t)fmaxf(y1, 0.0f) / T;
+                rx1 = (uint32_t)fminf(x2, (float)F.width - 1.0f) / T;
+                ry1 = (uint32_t)fminf(y2, (float)F.height - 1.0f) / T;
+                cx = G.cx; cy = G.cy; ca = G.ca; cb = G.cb; cc = G.cc; cutoff = G.cutoff;
+                const uint32_t cols = rx1 - rx0 + 1;
+                uint32_t bit = 0;
+                for (uint32_t ty = ry0; ty <= ry1; ++ty) {
+                    const float loy = ((float)(ty * T) + 0.5f) - cy;
+                    const float hiy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
+                    // the row's x* = -b y / a at its two y edges
+                    const float xLo = ca > 1e-12f ? ((-cb) * loy) / ca : 0.0f;
+                    const float xHi = ca > 1e-12f ? ((-cb) * hiy) / ca : 0.0f;
+                    for (uint32_t tx = rx0; tx <= rx1; ++tx, ++bit) {
+                        const float lox = ((float)(tx * T) + 0.5f) - cx;
+                        const float hix = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
+                        float best;
+                        if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) {
+                            best = 0.0f;
+                        } else {
+                            best = 3.4e38f;
+                            const float yl = cc > 1e-12f ? clampf(((-cb) * lox) / cc, loy, hiy) : loy;
+                            best = fminf(best, quad(ca, cb, cc, lox, yl));
+                            const float yh = cc > 1e-12f ? clampf(((-cb) * hix) / cc, loy, hiy) : loy;
+                            best = fminf(best, quad(ca, cb, cc, hix, yh));
+                            const float xl = ca > 1e-12f ? clampf(xLo, lox, hix) : lox;
+                            best = fminf(best, quad(ca, cb, cc, xl, loy));
+                            const float xh = ca > 1e-12f ? clampf(xHi, lox, hix) : lox;
+                            best = fminf(best, quad(ca, cb, cc, xh, hiy));
+                        }
+                        if (best <= cutoff) {
+                            touched += 1;
+                            if (bit < 64) mask |= 1ull << bit;
+                        }
+                    }
+                }
+                (void)cols;
+                if (touched) {
+                    const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
+                    float colour[3];
+                    colourFast<L>(I, g, i, degree, g.px - I.eye[0], g.py - I.eye[1], g.pz - I.eye[2], colour);
+                    const size_t r = ((size_t)v * B.count + i) * 3;
+                    recs[r + 0] = make_float4(G.cx, G.cy, G.tz, G.cutoff);
+                    recs[r + 1] = make_float4(G.ca, G.cb, G.cc, G.alpha);
+                    recs[r + 2] = make_float4(colour[0], colour[1], colour[2], 0.0f);
+                    depthKey = __float_as_uint(G.tz) >> 7;
+                }
+            }
+        }
+    }
+    // the scan of every view's pairs, in (Gaussian block, view, thread) order
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = touched;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += u;
+    }
+    if (lane == 31) sWarp[warp] = incl;
+    const uint32_t kept = __syncthreads_count(touched > 0);
+    uint32_t warpBase = 0, blockTotal = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kProjThreads / 32; ++w) {
+        warpBase += w < warp ? sWarp[w] : 0u;
+        blockTotal += sWarp[w];
+    }
+    if (warp == 0) {
+        const uint32_t prefix = lookbackEpoch(flags, t, blockTotal, epoch, &words[kBatchStatus]);
+        if (lane == 0) {
+            sPrefix = prefix;
+            if (kept) atomicAdd(&words[kBatchKept], kept);
+            if (t == gridDim.x - 1) {
+                const uint64_t total = (uint64_t)prefix + blockTotal;
+                words[kBatchPairsLo] = (uint32_t)total;
+                words[kBatchPairsHi] = (uint32_t)(total >> 32);
+                if (total > B.capacity) atomicOr(&words[kBatchStatus], kStatusPairOverflow);
+            }
+        }
+    }
+    __syncthreads();
+    if (!touched) return;
+    // the pairs, in the rect's row-major order (splat_emit.slang:37-49)
+    uint64_t at = (uint64_t)sPrefix + warpBase + (incl - touched);
+    const uint64_t head = ((uint64_t)(sView.tileBase) << B.keyShift) | ((uint64_t)depthKey << B.slotBits) | i;
+    const uint32_t cols = rx1 - rx0 + 1;
+    const uint32_t area = cols * (ry1 - ry0 + 1);
+    if (area <= 64) {
+        uint64_t m = mask;
+        while (m) {
+            const uint32_t bit = (uint32_t)__ffsll((long long)m) - 1u;
+            m &= m - 1;
+            const uint32_t tx = rx0 + bit % cols, ty = ry0 + bit / cols;
+            if (at < B.capacity) pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
+            ++at;
+        }
+    } else {
+        for (uint32_t ty = ry0; ty <= ry1; ++ty)
+            for (uint32_t tx = rx0; tx <= rx1; ++tx) {
+                const float lx = ((float)(tx * T) + 0.5f) - cx, ly = ((float)(ty * T) + 0.5f) - cy;
+                const float hx = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
+                const float hy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
+                if (minPowerOverBox(ca, cb, cc, lx, ly, hx, hy) <= cutoff) {
+                    if (at < B.capacity) pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
+                    ++at;
+                }
+            }
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    rangesBatchKernel(uint64_t capacity, const uint32_t* __restrict__ words, uint32_t keyShift, uint32_t totalTiles,
+                      const uint64_t* __restrict__ pairs, uint2* __restrict__ ranges, uint32_t* __restrict__ status) {
+    const uint64_t n = min((uint64_t)words[kBatchPairsLo] | ((uint64_t)words[kBatchPairsHi] << 32), capacity);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = (uint32_t)(pairs[i] >> keyShift);
+        if (t >= totalTiles) {
+            atomicOr(status, kStatusIndexRange);
+            continue;
+        }
+        if (i == 0 || (uint32_t)(pairs[i - 1] >> keyShift) != t) ranges[t].x = (uint32_t)i;
+        if (i + 1 == n || (uint32_t)(pairs[i + 1] >> keyShift) != t) ranges[t].y = (uint32_t)(i + 1);
+    }
+}
+
+// ---- the persistent blend ------------------------------------------------------
+// One block of T*T threads takes tiles off a queue; a thread is a pixel.
+template <uint32_t T, uint32_t NB>
+__global__ void __launch_bounds__(T * T)
+    blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
+                     const uint64_t* __restrict__ pairs, const float4* __restrict__ recs,
+                     float4* __restrict__ colour, float* __restrict__ depth, float* __restrict__ finalT,
+                     uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ words) {
+    constexpr uint32_t kThreads = T * T;
+    __shared__ float4 sScreen[NB];
+    __shared__ float4 sConic[NB];
+    __shared__ float4 sColour[NB];
+    __shared__ uint32_t sTileBase[kMaxBatchViews];
+    __shared__ uint32_t sTile;
+    for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
+    const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
+    const float kL2e = 1.4426950408889634f;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) sTile = atomicAdd(&words[kBatchBlendTicket], 1u);
+        __syncthreads();
+        const uint32_t tile = sTile;
+        if (tile >= B.totalTiles) break;
+        const uint32_t v = viewOf(sTileBase, B.views, tile);
+        const BatchView& V = views[v];
+        const uint32_t local = tile - V.tileBase;
+        const uint32_t tx = local % V.tilesX, ty = local / V.tilesX;
+        const uint32_t px = tx * T + threadIdx.x % T, py = ty * T + threadIdx.x / T;
+        const bool inside = px < V.width && py < V.height;
+        const uint2 range = ranges[tile];
+        const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+        const size_t recBase = (size_t)v * B.count;
+        float r = 0.0f, g = 0.0f, bl = 0.0f, Tr = 1.0f, depthSum = 0.0f;
+        uint32_t last = 0;
+        bool done = !inside;
+        for (uint32_t first = range.x; first < range.y; first += NB) {
+            if (__syncthreads_count(done) == kThreads) break;
+            for (uint32_t k = threadIdx.x; k < NB; k += kThreads) {
+                const uint32_t mine = first + k;
+                if (mine < range.y) {
+                    const size_t s = (recBase + (pairs[mine] & slotMask)) * 3;
+                    sScreen[k] = recs[s + 0];
+                    const float4 c = recs[s + 1];
+                    // the conic pre-scaled by -log2(e)/2: power in base-2 exponent units
+                    const float kx = c.x * (-0.5f * kL2e), ky = c.y * (-kL2e), kz = c.z * (-0.5f * kL2e);
+                    sConic[k] = make_float4(kx, ky, kz, c.w);
+                    sColour[k] = recs[s + 2];
+                }
+            }
+            __syncthreads();
+            const uint32_t count = min(NB, range.y - first);
+            for (uint32_t j = 0; j < count && !done; ++j) {
+                const float4 sc = sScreen[j];
+                const float4 k = sConic[j];
+                const float dx = pxc - sc.x, dy = pyc - sc.y;
+                // e = -log2(e)/2 * power; power > cutoff  <=>  e < -log2(e)/2 * cutoff
+                const float e = __fmaf_rn(k.x * dx, dx, __fmaf_rn(k.y * dx, dy, k.z * dy * dy));   // kx ky kz
+                if (e < (-0.5f * kL2e) * sc.w) continue;
+                const float alpha = fminf(0.99f, k.w * fastExp2(e));
+                if (alpha < kFaint) continue;
+                const float w = Tr * alpha;
+                const float4 c = sColour[j];
+                r = __fmaf_rn(w, c.x, r);
+                g = __fmaf_rn(w, c.y, g);
+                bl = __fmaf_rn(w, c.z, bl);
+                depthSum = __fmaf_rn(w, sc.z, depthSum);
+                Tr = Tr * (1.0f - alpha);
+                last = first - range.x + j + 1;
+                if (Tr < 1e-4f) done = true;
+            }
+        }
+        if (inside) {
+            const uint32_t at = V.pixelBase + py * V.width + px;
+            const float coverage = 1.0f - Tr;
+            colour[at] = make_float4(r + Tr * B.bg[0], g + Tr * B.bg[1], bl + Tr * B.bg[2], coverage + Tr * B.bg[3]);
+            if (depth) depth[at] = coverage > 1e-6f ? depthSum / coverage : 0.0f;
+            finalT[at] = Tr;
+            lastContrib[at] = last;
+        }
+    }
+}
+
+// ---- the loss: a view's mean L2 over its pixels and r g b, summed over views ----
+__global__ void __launch_bounds__(256)
+    lossBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float4* __restrict__ colour,
+                    const float* __restrict__ target, float4* __restrict__ dL, float* __restrict__ loss) {
+    __shared__ uint32_t sPixelBase[kMaxBatchViews];
+    __shared__ float sPart[8];
+    for (uint32_t k = threadIdx.x; k < B.views; k += blockDim.x) sPixelBase[k] = views[k].pixelBase;
+    __syncthreads();
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (p < B.totalPixels) {
+        const float scale = views[viewOf(sPixelBase, B.views, p)].lossScale;
+        const float4 c = colour[p];
+        const float er = c.x - target[(size_t)p * 3 + 0], eg = c.y - target[(size_t)p * 3 + 1],
+                    eb = c.z - target[(size_t)p * 3 + 2];
+        l = (er * er + eg * eg + eb * eb) * scale;
+        dL[p] = make_float4(2.0f * scale * er, 2.0f * scale * eg, 2.0f * scale * eb, 0.0f);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xFFFFFFFFu, l, o);
+    if ((threadIdx.x & 31u) == 0) sPart[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float b = 0.0f;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) b += sPart[w];
+        if (b != 0.0f) atomicAdd(loss, b);
+    }
+}
+
+// backward.cu's transpose reduction: lanes 2k and 2k + 1 end with value k's warp total.
+__device__ __forceinline__ float warpSum16b(float v[16]) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int half = 8, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
+        const bool upper = (lane & (uint32_t)bit) != 0;
+#pragma unroll
+        for (int k = 0; k < half; ++k) {
+            const float send = upper ? v[k] : v[k + half];
+            const float keep = upper ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, bit);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xFFFFFFFFu, v[0], 1);
+}
+
+// ---- the blend's adjoint, over the same tile queue ------------------------------
+template <uint32_t T, uint32_t NB>
+__global__ void __launch_bounds__(T * T)
+    blendAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
+                            const uint64_t* __restrict__ pairs, const float4* __restrict__ recs,
+                            const float* __restrict__ finalT, const uint32_t* __restrict__ lastContrib,
+                            const float4* __restrict__ dLdColour, float* __restrict__ grads,
+                            uint32_t* __restrict__ words) {
+    constexpr uint32_t kThreads = T * T;
+    constexpr uint32_t kWords = 9;   // centre x y, conic a b c, alpha, colour r g b (no depth loss)
+    __shared__ float4 sScreen[NB];
+    __shared__ float4 sConic[NB];
+    __shared__ float4 sColour[NB];
+    __shared__ uint32_t sRec[NB];
+    __shared__ float sAcc[NB * kWords];
+    __shared__ uint32_t sTileBase[kMaxBatchViews];
+    __shared__ uint32_t sTile, sMaxLast;
+    for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
+    const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
+    const float kL2e = 1.4426950408889634f;
+    const uint32_t lane = threadIdx.x & 31u;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sTile = atomicAdd(&words[kBatchBackTicket], 1u);
+            sMaxLast = 0;
+        }
+        __syncthreads();
+        const uint32_t tile = sTile;
+        if (tile >= B.totalTiles) break;
+        const uint32_t v = viewOf(sTileBase, B.views, tile);
+        const BatchView& V = views[v];
+        const uint32_t local = tile - V.tileBase;
+        const uint32_t tx = local % V.tilesX, ty = local / V.tilesX;
+        const uint32_t px = tx * T + threadIdx.x % T, py = ty * T + threadIdx.x / T;
+        const bool inside = px < V.width && py < V.height;
+        const uint2 range = ranges[tile];
+        const uint32_t at = inside ? V.pixelBase + py * V.width + px : 0u;
+        const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+        const float Tfinal = inside ? finalT[at] : 1.0f;
+        const uint32_t last = inside ? min(lastContrib[at], range.y - range.x) : 0u;
+        const float4 dC = inside ? dLdColour[at] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float dAlphaOut = dC.w * Tfinal * (1.0f - B.bg[3]);
+        if (last) atomicMax(&sMaxLast, last);
+        __syncthreads();
+        const uint32_t end = range.x + sMaxLast;
+        const size_t recBase = (size_t)v * B.count;
+        float Tr = Tfinal, Sr = B.bg[0], Sg = B.bg[1], Sb = B.bg[2];
+        for (uint32_t batchEnd = end; batchEnd > range.x;) {
+            const uint32_t batchStart = batchEnd - range.x > NB ? batchEnd - NB : range.x;
+            const uint32_t count = batchEnd - batchStart;
+            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
+                const uint32_t s = (uint32_t)(pairs[batchStart + k] & slotMask);
+                sRec[k] = s;
+                const size_t q = (recBase + s) * 3;
+                sScreen[k] = recs[q + 0];
+                sConic[k] = recs[q + 1];
+                sColour[k] = recs[q + 2];
+            }
+            for (uint32_t k = threadIdx.x; k < NB * kWords; k += kThreads) sAcc[k] = 0.0f;
+            __syncthreads();
+            for (int j = (int)count - 1; j >= 0; --j) {
+                const uint32_t rel = batchStart + (uint32_t)j - range.x;
+                float gv[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
+                bool live = false;
+                if (rel < last) {
+                    const float4 sc = sScreen[j];
+                    const float4 k = sConic[j];
+                    const float dx = pxc - sc.x, dy = pyc - sc.y;
+                    // the forward's exponent, operation for operation (so the same records pass)
+                    const float kx = k.x * (-0.5f * kL2e), ky = k.y * (-kL2e), kz = k.z * (-0.5f * kL2e);
+                    const float e = __fmaf_rn(kx * dx, dx, __fmaf_rn(ky * dx, dy, kz * dy * dy));
+                    if (e >= (-0.5f * kL2e) * sc.w) {
+                        const float G = fastExp2(e);
+                        const float raw = k.w * G;
+                        const float alpha = fminf(0.99f, raw);
+                        if (alpha >= kFaint) {
+                            live = true;
+                            const float4 c = sColour[j];
+                            const float oneMinus = 1.0f - alpha;
+                            const float inv = fastRcp(oneMinus);
+                            const float Tb = Tr * inv;
+                            const float w = Tb * alpha;
+                            gv[6] = w * dC.x;
+                            gv[7] = w * dC.y;
+                            gv[8] = w * dC.z;
+                            const float dAlpha =
+                                Tb * ((c.x - Sr) * dC.x + (c.y - Sg) * dC.y + (c.z - Sb) * dC.z) + dAlphaOut * inv;
+                            Sr = __fmaf_rn(alpha, c.x - Sr, Sr);
+                            Sg = __fmaf_rn(alpha, c.y - Sg, Sg);
+                            Sb = __fmaf_rn(alpha, c.z - Sb, Sb);
+                            Tr = Tb;
+                            if (raw < 0.99f && k.w <= 1.0f) {
+                                gv[5] = dAlpha * G;
+                                const float dPower = -0.5f * alpha * dAlpha;
+                                gv[2] = dPower * (dx * dx);
+                                gv[3] = dPower * (2.0f * dx * dy);
+                                gv[4] = dPower * (dy * dy);
+                                gv[0] = dPower * (-2.0f * (k.x * dx + k.y * dy));
+                                gv[1] = dPower * (-2.0f * (k.y * dx + k.z * dy));
+                            }
+                        }
+                    }
+                }
+                if (__any_sync(0xFFFFFFFFu, live)) {
+                    const float s = warpSum16b(gv);
+                    const uint32_t k = lane >> 1;
+                    if ((lane & 1u) == 0 && k < kWords && s != 0.0f) atomicAdd(&sAcc[j * kWords + k], s);
+                }
+            }
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < count * kWords; k += kThreads) {
+                const float s = sAcc[k];
+                if (s != 0.0f)
+                    atomicAdd(&grads[(recBase + sRec[k / kWords]) * kGradWords + k % kWords], s);
+            }
+            __syncthreads();   // the next batch's loads overwrite what the flush reads
+            batchEnd = batchStart;
+        }
+    }
+}
+
+
+// ---- the projection's adjoint over every view: one thread a Gaussian ---------
+template <uint32_t L>
+__global__ void __launch_bounds__(128)
+    projectAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float* __restrict__ grads,
+                              float4* __restrict__ gMeans, float4* __restrict__ gScales, float4* __restrict__ gQuats,
+                              float* __restrict__ gSh, uint32_t shStride) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B.count) return;
+    ParamGrad acc;
+    acc.clear();
+    for (uint32_t v = 0; v < B.views; ++v) {
+        const float* gr = grads + ((size_t)v * B.count + i) * kGradWords;
+        float gw[kGradWords];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < (int)kGradWords; ++k) {
+            gw[k] = gr[k];
+            any |= gw[k] != 0.0f;
+        }
+        if (!any) continue;
+        const BatchView& V = views[v];
+        FrameConst F{};
+        F.width = V.width; F.height = V.height; F.tilesX = V.tilesX; F.tilesY = V.tilesY;
+        F.focalX = V.focalX; F.focalY = V.focalY; F.centreX = V.centreX; F.centreY = V.centreY;
+        F.nearZ = V.nearZ; F.farZ = V.farZ; F.orthographic = V.orthographic; F.shLimit = B.shLimit;
+        InstanceConst I = B.inst;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) I.m[k] = V.m[k];
+        I.eye[0] = V.eye[0]; I.eye[1] = V.eye[1]; I.eye[2] = V.eye[2];
+        projectAdjoint<L>(F, I, i, gw, acc);
+    }
+    acc.addTo(i, shStride, gMeans, gScales, gQuats, gSh, true);
+}
+
+// ---- FP32 SH -> the mixed layout ------------------------------------------------
+// DC and band 1 (12 values) to BF16; bands 2-3 (36 values) to FP8 e4m3 over a
+// per-Gaussian scale, the largest magnitude over e4m3's largest finite (448).
+__global__ void __launch_bounds__(256)
+    toMixedKernel(const float* __restrict__ sh, uint32_t count, uint32_t stride, uint32_t degree,
+                  __nv_bfloat16* __restrict__ low, __nv_fp8_e4m3* __restrict__ high, float* __restrict__ scale) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float* row = sh + (size_t)i * stride;
+    const uint32_t rest = degree >= 3 ? 45 : degree == 2 ? 24 : degree == 1 ? 9 : 0;
+#pragma unroll
+    for (uint32_t k = 0; k < 12; ++k) low[(size_t)i * 12 + k] = __float2bfloat16_rn(k < 3 + rest ? row[k] : 0.0f);
+    float most = 0.0f;
+    for (uint32_t k = 9; k < rest; ++k) most = fmaxf(most, fabsf(row[3 + k]));
+    const float s = most > 0.0f ? most / 448.0f : 1.0f;
+    scale[i] = s;
+    const float inv = 1.0f / s;
+    for (uint32_t k = 0; k < 36; ++k) high[(size_t)i * 36 + k] = __nv_fp8_e4m3(9 + k < rest ? row[12 + k] * inv : 0.0f);
+}
+
+}   // namespace
+}   // namespace ath
+
+// ===========================================================================
+// Host side
+// ===========================================================================
+using namespace ath;
+
+struct ath_batch {
+    int device = 0;
+    int sms = 148;
+    std::vector<BatchView> views;
+    DeviceBuffer viewsDev;
+    uint32_t totalTiles = 0, totalPixels = 0, tileBits = 0;
+    uint32_t tile = 16, blockBatch = 256;
+    float bg[4] = {0, 0, 0, 0};
+    uint32_t shLimit = 3, antialias = 1;
+    std::vector<ath_projection> projections;
+    std::vector<uint32_t> widths, heights, tileBases;
+    uint32_t lastSorted = 0, lastSlotBits = 0;
+    // scratch
+    DeviceBuffer words, recs, grads, projFlags, pairs[2], sortHist, sortFlags, ranges, finalT, lastContrib, dL;
+    uint32_t count = 0;
+    uint64_t capacity = 0;
+    bool resize = true;
+    // the captured step
+    cudaStream_t captureStream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uintptr_t graphKey[12] = {};
+};
+
+namespace {
+
+uint32_t bitsForValues(uint64_t values) {   // FrameParams.h:18-24
+    uint32_t bits = 1;
+    while (bits < 63 && (uint64_t{1} << bits) < values) ++bits;
+    return bits;
+}
+
+void dropGraph(ath_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+}
+
+ath_status buildViews(ath_batch* b) {
+    const uint32_t T = b->tile;
+    b->views.clear();
+    uint32_t tileBase = 0, pixelBase = 0;
+    ath_settings s{};
+    ath_settings_default(&s);
+    for (size_t v = 0; v < b->projections.size(); ++v) {
+        const ath_projection& p = b->projections[v];
+        BatchView V{};
+        V.width = b->widths[v];
+        V.height = b->heights[v];
+        V.tilesX = (V.width + T - 1) / T;
+        V.tilesY = (V.height + T - 1) / T;
+        s.width = V.width;
+        s.height = V.height;
+        const FrameConst F = frameConstFor(p, s);
+        V.focalX = F.focalX; V.focalY = F.focalY; V.centreX = F.centreX; V.centreY = F.centreY;
+        V.nearZ = F.nearZ; V.farZ = F.farZ; V.orthographic = F.orthographic;
+        V.tileBase = tileBase;
+        V.pixelBase = pixelBase;
+        V.lossScale = 1.0f / (3.0f * (float)V.width * (float)V.height);
+        tileBase += V.tilesX * V.tilesY;
+        pixelBase += V.width * V.height;
+        b->views.push_back(V);
+    }
+    b->totalTiles = tileBase;
+    b->totalPixels = pixelBase;
+    b->tileBases.clear();
+    for (const BatchView& V : b->views) b->tileBases.push_back(V.tileBase);
+    b->tileBits = bitsForValues(tileBase);
+    return ATH_OK;
+}
+
+// The per-view object -> view rows and eye for a cloud placed by `objectToWorld`.
+void placeCloud(ath_batch* b, const double objectToWorld[16]) {
+    ath_settings s{};
+    ath_settings_default(&s);
+    ath_instance in{};
+    std::memcpy(in.object_to_world, objectToWorld, sizeof(in.object_to_world));
+    for (size_t v = 0; v < b->views.size(); ++v) {
+        const InstanceConst I = instanceConstFor(b->projections[v], s, in, 0);
+        std::memcpy(b->views[v].m, I.m, sizeof(I.m));
+        std::memcpy(b->views[v].eye, I.eye, sizeof(I.eye));
+    }
+}
+
+BatchConst batchConst(const ath_batch* b, const ath_mixed_params& P) {
+    BatchConst B{};
+    B.views = (uint32_t)b->views.size();
+    B.count = P.count;
+    B.tile = b->tile;
+    B.slotBits = bitsForValues(std::max<uint64_t>(P.count, 2));
+    B.keyShift = 24 + B.slotBits;
+    B.totalTiles = b->totalTiles;
+    B.totalPixels = b->totalPixels;
+    B.shLimit = b->shLimit;
+    B.antialias = b->antialias;
+    B.linear = P.linear ? 1u : 0u;
+    B.restPerColour = P.sh_degree >= 3 ? 15 : P.sh_degree == 2 ? 8 : P.sh_degree == 1 ? 3 : 0;
+    for (int k = 0; k < 4; ++k) B.bg[k] = b->bg[k];
+    B.capacity = b->capacity;
+    InstanceConst& I = B.inst;
+    I = InstanceConst{};
+    I.means = P.means;
+    I.scales = P.scales;
+    I.quats = P.quats;
+    I.shLow = P.sh_low;
+    I.shHigh = P.sh_high;
+    I.shScale = P.sh_scale;
+    I.count = P.count;
+    I.restPerColour = B.restPerColour;
+    I.linear = B.linear;
+    I.antialias = b->antialias;
+    return B;
+}
+
+template <typename K>
+int residentBlocks(K kernel, int threads, int sms) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0);
+    return std::max(n, 1) * sms;
+}
+
+template <uint32_t T, uint32_t NB>
+cudaError_t launchBlends(const ath_batch* b, const BatchConst& B, uint32_t sorted, cudaStream_t stream, bool forward,
+                         float4* colour, float4* dL, float* grads) {
+    const BatchView* views = static_cast<const BatchView*>(b->viewsDev.ptr);
+    const uint2* ranges = static_cast<const uint2*>(b->ranges.ptr);
+    const uint64_t* pairs = static_cast<const uint64_t*>(b->pairs[sorted].ptr);
+    const float4* recs = static_cast<const float4*>(b->recs.ptr);
+    uint32_t* words = static_cast<uint32_t*>(b->words.ptr);
+    if (forward) {
+        const int grid = residentBlocks(blendBatchKernel<T, NB>, T * T, b->sms);
+        blendBatchKernel<T, NB><<<grid, T * T, 0, stream>>>(B, views, ranges, pairs, recs, colour, nullptr,
+                                                            static_cast<float*>(b->finalT.ptr),
+                                                            static_cast<uint32_t*>(b->lastContrib.ptr), words);
+    } else {
+        const int grid = residentBlocks(blendAdjointBatchKernel<T, NB>, T * T, b->sms);
+        blendAdjointBatchKernel<T, NB><<<grid, T * T, 0, stream>>>(
+            B, views, ranges, pairs, recs, static_cast<const float*>(b->finalT.ptr),
+            static_cast<const uint32_t*>(b->lastContrib.ptr), dL, grads, words);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t sorted, cudaStream_t stream, bool forward,
+                            float4* colour, float4* dL, float* grads) {
+#define ATH_BLEND_CASE(T_, NB_) \
+    if (b->tile == T_ && b->blockBatch == NB_) return launchBlends<T_, NB_>(b, B, sorted, stream, forward, colour, dL, grads);
+    ATH_BLEND_CASE(8, 64) ATH_BLEND_CASE(8, 128) ATH_BLEND_CASE(8, 256)
+    ATH_BLEND_CASE(16, 64) ATH_BLEND_CASE(16, 128) ATH_BLEND_CASE(16, 256)
+    ATH_BLEND_CASE(32, 64) ATH_BLEND_CASE(32, 128) ATH_BLEND_CASE(32, 256)
+#undef ATH_BLEND_CASE
+    return cudaErrorInvalidValue;
+}
+
+// One step, enqueued (captured or not). `countOnly`: the projection alone, to size the pairs.
+cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* target, float4* colour, float* loss,
+                        ath_param_grads& g, cudaStream_t stream, bool countOnly) {
+    BatchConst B = batchConst(b, P);
+    if (countOnly) B.capacity = 0;
+    uint32_t* words = static_cast<uint32_t*>(b->words.ptr);
+    const uint32_t V = B.views;
+    const uint32_t gaussBlocks = (P.count + kProjThreads - 1) / kProjThreads;
+    beginStepKernel<<<1, 1, 0, stream>>>(words);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess && P.count)
+        projectEmitKernel<kLayoutMixed><<<gaussBlocks * V, kProjThreads, 0, stream>>>(
+            B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<float4*>(b->recs.ptr),
+            static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint64_t*>(b->projFlags.ptr), words, gaussBlocks);
+    if (err == cudaSuccess) err = cudaGetLastError();
+    if (countOnly || err != cudaSuccess) return err;
+    uint64_t* keys[2] = {static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint64_t*>(b->pairs[1].ptr)};
+    const uint32_t bits = 24 + b->tileBits;
+    err = launchSortDevice(keys, nullptr, (uint32_t)b->capacity, words + kBatchPairsLo, words + kBatchEpoch,
+                           B.slotBits, bits, static_cast<uint32_t*>(b->sortHist.ptr),
+                           static_cast<uint64_t*>(b->sortFlags.ptr), words + kBatchSortTickets, words + kBatchStatus,
+                           stream);
+    const uint32_t sorted = sortResultIndex(2, bits);
+    b->lastSorted = sorted;
+    b->lastSlotBits = B.slotBits;
+    if (err == cudaSuccess) err = cudaMemsetAsync(b->ranges.ptr, 0, (size_t)b->totalTiles * 8, stream);
+    if (err == cudaSuccess) {
+        const uint32_t grid = std::max<uint32_t>(1, std::min<uint64_t>((b->capacity + 255) / 256, (uint64_t)b->sms * 8));
+        rangesBatchKernel<<<grid, 256, 0, stream>>>(b->capacity, words, B.keyShift, b->totalTiles, keys[sorted],
+                                                    static_cast<uint2*>(b->ranges.ptr), words + kBatchStatus);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = launchBlendsFor(b, B, sorted, stream, true, colour, nullptr, nullptr);
+    if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
+    if (err == cudaSuccess) {
+        lossBatchKernel<<<(b->totalPixels + 255) / 256, 256, 0, stream>>>(
+            B, static_cast<const BatchView*>(b->viewsDev.ptr), colour, target, static_cast<float4*>(b->dL.ptr), loss);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess)
+        err = cudaMemsetAsync(b->grads.ptr, 0, (size_t)V * P.count * kGradWords * sizeof(float), stream);
+    if (err == cudaSuccess)
+        err = launchBlendsFor(b, B, sorted, stream, false, nullptr, static_cast<float4*>(b->dL.ptr),
+                              static_cast<float*>(b->grads.ptr));
+    if (err == cudaSuccess && P.count) {
+        projectAdjointBatchKernel<kLayoutMixed><<<(P.count + 127) / 128, 128, 0, stream>>>(
+            B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
+            reinterpret_cast<float4*>(g.means), reinterpret_cast<float4*>(g.scales), reinterpret_cast<float4*>(g.quats),
+            g.sh, 48);
+        err = cudaGetLastError();
+    }
+    return err;
+}
+
+ath_status reserveBatch(ath_batch* b, uint32_t count) {
+    const uint32_t V = (uint32_t)b->views.size();
+    const uint32_t gaussBlocks = (count + kProjThreads - 1) / kProjThreads;
+    cudaError_t err = b->words.reserve(kBatchWords * sizeof(uint32_t));
+    if (err == cudaSuccess && b->count == 0) err = cudaMemset(b->words.ptr, 0, kBatchWords * sizeof(uint32_t));
+    if (err == cudaSuccess) err = b->recs.reserve((size_t)V * count * 48);
+    if (err == cudaSuccess) err = b->grads.reserve((size_t)V * count * kGradWords * sizeof(float));
+    if (err == cudaSuccess) err = b->projFlags.reserve((size_t)std::max(1u, gaussBlocks * V) * 8);
+    if (err == cudaSuccess) err = b->ranges.reserve((size_t)std::max(1u, b->totalTiles) * 8);
+    if (err == cudaSuccess) err = b->finalT.reserve((size_t)std::max(1u, b->totalPixels) * 4);
+    if (err == cudaSuccess) err = b->lastContrib.reserve((size_t)std::max(1u, b->totalPixels) * 4);
+    if (err == cudaSuccess) err = b->dL.reserve((size_t)std::max(1u, b->totalPixels) * 16);
+    if (err == cudaSuccess) err = b->sortHist.reserve(8 * 256 * sizeof(uint32_t));
+    if (err == cudaSuccess) err = b->viewsDev.reserve(std::max<size_t>(1, b->views.size()) * sizeof(BatchView));
+    if (err != cudaSuccess) return failCuda(err, "reserving the batch's scratch");
+    b->count = count;
+    return ATH_OK;
+}
+
+// Sizes the pairs: the projection alone, its total read back (the one host read,
+// made before capture), and the pair buffers grown to 1.15 times it.
+ath_status sizePairs(ath_batch* b, const ath_mixed_params& P, cudaStream_t stream) {
+    ath_param_grads none{};
+    cudaError_t err = enqueueStep(b, P, nullptr, nullptr, nullptr, none, stream, true);
+    uint32_t w[kBatchWords];
+    if (err == cudaSuccess) err = cudaMemcpyAsync(w, b->words.ptr, sizeof(w), cudaMemcpyDeviceToHost, stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) return failCuda(err, "sizing the batch's pairs");
+    if (w[kBatchStatus] & kStatusLookbackTimeout) return fail(ATH_E_TIMEOUT, "a look-back wait gave up while sizing");
+    const uint64_t pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
+    const uint64_t want = pairs + pairs / 7 + 65536;
+    if (want > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 pairs in one batched step");
+    if (want > b->capacity || !b->pairs[0].ptr) {
+        for (int k = 0; k < 2; ++k)
+            if ((err = b->pairs[k].reserve((size_t)want * 8)) != cudaSuccess) return failCuda(err, "reserving the pairs");
+        b->capacity = want;
+    }
+    const uint32_t bits = 24 + b->tileBits;
+    err = b->sortFlags.reserve(sortFlagWords((uint32_t)b->capacity, bits) * 8);
+    if (err != cudaSuccess) return failCuda(err, "reserving the sort's look-back words");
+    // the look-back words carry epochs: start them all at "not ready"
+    err = cudaMemsetAsync(b->sortFlags.ptr, 0, sortFlagWords((uint32_t)b->capacity, bits) * 8, stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(b->words.ptr, 0, kBatchWords * sizeof(uint32_t), stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(b->projFlags.ptr, 0, b->projFlags.bytes, stream);
+    if (err != cudaSuccess) return failCuda(err, "clearing the batch's look-back words");
+    b->resize = false;
+    return ATH_OK;
+}
+
+}   // namespace
+
+extern "C" ath_status ath_params_to_mixed(const ath_params* in, void* shLow, void* shHigh, float* shScale,
+                                          void* stream) {
+    if (!in || (in->count && (!in->sh || !shLow || !shHigh || !shScale)))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_params_to_mixed: null argument");
+    if (in->sh_degree > 3 || in->sh_stride < 3u + 3u * (in->sh_degree >= 3 ? 15u : in->sh_degree == 2 ? 8u : in->sh_degree == 1 ? 3u : 0u))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_params_to_mixed: sh_degree / sh_stride");
+    if (in->count == 0) return ATH_OK;
+    toMixedKernel<<<(in->count + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        in->sh, in->count, in->sh_stride, in->sh_degree, static_cast<__nv_bfloat16*>(shLow),
+        static_cast<__nv_fp8_e4m3*>(shHigh), shScale);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? ATH_OK : failCuda(err, "ath_params_to_mixed");
+}
+
+extern "C" ath_status ath_batch_create(ath_batch** out) {
+    if (!out) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_create: null output");
+    *out = nullptr;
+    ath_batch* b = new (std::nothrow) ath_batch();
+    if (!b) return fail(ATH_E_OUT_OF_MEMORY, "ath_batch_create: host allocation failed");
+    cudaError_t err = cudaGetDevice(&b->device);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (err == cudaSuccess) err = sortPrepare();
+    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&b->captureStream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) {
+        delete b;
+        return failCuda(err, "ath_batch_create");
+    }
+    *out = b;
+    return ATH_OK;
+}
+
+extern "C" void ath_batch_destroy(ath_batch* b) {
+    if (!b) return;
+    dropGraph(b);
+    if (b->captureStream) cudaStreamDestroy(b->captureStream);
+    delete b;
+}
+
+extern "C" ath_status ath_batch_set_views(ath_batch* b, const ath_view* views, uint32_t count,
+                                          const ath_settings* settings) {
+    if (!b || (count && !views)) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_views: null argument");
+    if (count == 0 || count > kMaxBatchViews)
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_views: 1 to 256 views a batch");
+    uint64_t pixels = 0;
+    for (uint32_t v = 0; v < count; ++v) {
+        if (views[v].width == 0 || views[v].height == 0) return fail(ATH_E_INVALID_ARGUMENT, "a view needs a size");
+        pixels += (uint64_t)views[v].width * views[v].height;
+    }
+    if (pixels > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 pixels in one batch");
+    b->projections.clear();
+    b->widths.clear();
+    b->heights.clear();
+    for (uint32_t v = 0; v < count; ++v) {
+        b->projections.push_back(views[v].projection);
+        b->widths.push_back(views[v].width);
+        b->heights.push_back(views[v].height);
+    }
+    if (settings) {
+        for (int k = 0; k < 4; ++k) b->bg[k] = settings->background[k];
+        b->shLimit = settings->max_sh_degree;
+        b->antialias = settings->antialias_override >= 0 ? (uint32_t)(settings->antialias_override != 0)
+                                                         : (uint32_t)(settings->antialias != 0);
+    }
+    buildViews(b);
+    b->resize = true;
+    dropGraph(b);
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_batch_set_tuning(ath_batch* b, uint32_t tile, uint32_t blockBatch) {
+    if (!b) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_tuning: null handle");
+    if ((tile != 8 && tile != 16 && tile != 32) || (blockBatch != 64 && blockBatch != 128 && blockBatch != 256))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_tuning: tile 8, 16 or 32; block batch 64, 128 or 256");
+    if (tile != b->tile || blockBatch != b->blockBatch) {
+        b->tile = tile;
+        b->blockBatch = blockBatch;
+        if (!b->projections.empty()) buildViews(b);
+        b->resize = true;
+        dropGraph(b);
+    }
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_batch_pixels(ath_batch* b, uint32_t* pixels) {
+    if (!b || !pixels) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_pixels: null argument");
+    *pixels = b->totalPixels;
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target,
+                                           float* colour, float* loss, ath_param_grads* grads, void* streamPtr) {
+    if (!b || !params || !target || !colour || !loss || !grads || !grads->means || !grads->scales || !grads->quats ||
+        !grads->sh)
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: null argument");
+    if (b->views.empty()) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: no views (ath_batch_set_views)");
+    const ath_mixed_params& P = *params;
+    if (P.count && (!P.means || !P.scales || !P.quats || !P.sh_low || !P.sh_high || !P.sh_scale))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: a cloud needs every array of the mixed layout");
+    if (P.sh_degree > 3) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: sh_degree must be 0..3");
+    const uint32_t slotBits = bitsForValues(std::max<uint64_t>(P.count, 2));
+    if (24 + slotBits + b->tileBits > 64)
+        return fail(ATH_E_UNSUPPORTED, "ath_batch_train_step: tiles, depth key and Gaussian index exceed 64 bits");
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    ath_status st = ATH_OK;
+    if (P.count != b->count) {
+        if ((st = reserveBatch(b, P.count)) != ATH_OK) return st;
+        b->resize = true;
+        dropGraph(b);
+    }
+    placeCloud(b, P.object_to_world);
+    cudaError_t err = cudaMemcpyAsync(b->viewsDev.ptr, b->views.data(), b->views.size() * sizeof(BatchView),
+                                      cudaMemcpyHostToDevice, stream);
+    if (err != cudaSuccess) return failCuda(err, "ath_batch_train_step");
+    if (b->resize) {
+        if ((st = sizePairs(b, P, stream)) != ATH_OK) return st;
+        dropGraph(b);
+    }
+    const uintptr_t key[12] = {(uintptr_t)P.means, (uintptr_t)P.scales, (uintptr_t)P.quats, (uintptr_t)P.sh_low,
+                               (uintptr_t)P.sh_high, (uintptr_t)P.sh_scale, (uintptr_t)target, (uintptr_t)colour,
+                               (uintptr_t)loss, (uintptr_t)grads->means, (uintptr_t)grads->sh, (uintptr_t)P.count};
+    if (!b->exec || std::memcmp(key, b->graphKey, sizeof(key)) != 0) {
+        dropGraph(b);
+        // Capture on the batch's own stream (the caller's may be the legacy one),
+        // ordered after the caller's work so far.
+        cudaEvent_t ready;
+        err = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+        if (err == cudaSuccess) err = cudaEventRecord(ready, stream);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(b->captureStream, ready, 0);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(b->captureStream);
+        cudaEventDestroy(ready);
+        cudaGraph_t graph = nullptr;
+        if (err == cudaSuccess) err = cudaStreamBeginCapture(b->captureStream, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+            ath_param_grads g = *grads;
+            const cudaError_t enq =
+                enqueueStep(b, P, target, reinterpret_cast<float4*>(colour), loss, g, b->captureStream, false);
+            err = cudaStreamEndCapture(b->captureStream, &graph);
+            if (enq != cudaSuccess) err = enq;
+        }
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&b->exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (err != cudaSuccess) {
+            b->exec = nullptr;
+            return failCuda(err, "capturing the batched step");
+        }
+        std::memcpy(b->graphKey, key, sizeof(key));
+    }
+    err = cudaGraphLaunch(b->exec, stream);
+    if (err != cudaSuccess) return failCuda(err, "launching the batched step");
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* streamPtr) {
+    if (!b || !out) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_check: null argument");
+    if (!b->words.ptr) return fail(ATH_E_NOT_FOUND, "ath_batch_check: no step has run");
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    uint32_t w[kBatchWords];
+    cudaError_t err = cudaMemcpyAsync(w, b->words.ptr, sizeof(w), cudaMemcpyDeviceToHost, stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) return failCuda(err, "ath_batch_check");
+    out->pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
+    out->kept = w[kBatchKept];
+    out->tile = b->tile;
+    out->block_batch = b->blockBatch;
+    out->capacity = b->capacity;
+    if (w[kBatchStatus]) {
+        const uint32_t bits = w[kBatchStatus];
+        cudaMemsetAsync(static_cast<uint32_t*>(b->words.ptr) + kBatchStatus, 0, sizeof(uint32_t), stream);
+        if (bits & kStatusPairOverflow) {
+            b->resize = true;   // the next step sizes the pairs again
+            return fail(ATH_E_CAPACITY, "a step had more pairs than its buffers; the next step grows them");
+        }
+        if (bits & kStatusLookbackTimeout) return fail(ATH_E_TIMEOUT, "a look-back wait of a batched step gave up");
+        return fail(ATH_E_INTERNAL, "a batched step met an index outside its buffers");
+    }
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_batch_buffers_of(ath_batch* b, ath_batch_buffers* out, void* streamPtr) {
+    if (!b || !out) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_buffers_of: null argument");
+    if (!b->words.ptr || !b->pairs[0].ptr) return fail(ATH_E_NOT_FOUND, "ath_batch_buffers_of: no step has run");
+    uint32_t w[kBatchWords];
+    cudaError_t err = cudaMemcpyAsync(w, b->words.ptr, sizeof(w), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(streamPtr));
+    if (err == cudaSuccess) err = cudaStreamSynchronize(static_cast<cudaStream_t>(streamPtr));
+    if (err != cudaSuccess) return failCuda(err, "ath_batch_buffers_of");
+    out->pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
+    out->key_shift = 24 + b->lastSlotBits;
+    out->slot_bits = b->lastSlotBits;
+    out->total_tiles = b->totalTiles;
+    out->views = (uint32_t)b->views.size();
+    out->sorted_pairs = static_cast<const uint64_t*>(b->pairs[b->lastSorted].ptr);
+    out->ranges = static_cast<const uint32_t*>(b->ranges.ptr);
+    out->tile_bases = b->tileBases.data();
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* params, const float* target,
+                                     float* colour, float* loss, ath_param_grads* grads, uint32_t repeats,
+                                     ath_batch_stats* best, void* streamPtr) {
+    if (!b || !params) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_tune: null argument");
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    const uint32_t tiles[3] = {8, 16, 32}, batches[3] = {64, 128, 256};
+    float bestMs = 1e30f;
+    uint32_t bestTile = b->tile, bestBatch = b->blockBatch;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (uint32_t t : tiles) {
+        for (uint32_t nb : batches) {
+            ath_status st = ath_batch_set_tuning(b, t, nb);
+            if (st == ATH_OK) st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);
+            if (st != ATH_OK) continue;   // e.g. too many tile bits for this tile size
+            cudaEventRecord(e0, stream);
+            for (uint32_t r = 0; r < std::max(repeats, 1u); ++r)
+                st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);
+            cudaEventRecord(e1, stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ath_batch_stats s{};
+            if (st == ATH_OK && ath_batch_check(b, &s, streamPtr) == ATH_OK && ms < bestMs) {
+                bestMs = ms;
+                bestTile = t;
+                bestBatch = nb;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ath_status st = ath_batch_set_tuning(b, bestTile, bestBatch);
+    if (st == ATH_OK) st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);
+    if (st == ATH_OK && best) st = ath_batch_check(b, best, streamPtr);
+    if (best) best->ms_per_step = bestMs / (float)std::max(repeats, 1u);
+    return st;
+}

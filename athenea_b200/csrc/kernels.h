@@ -13,6 +13,10 @@ namespace ath {
 struct FrameConst;
 struct InstanceConst;
 
+// host.cu: FrameParams' setters (modules/render/src/FrameParams.h:32-117)
+FrameConst frameConstFor(const ath_projection& p, const ath_settings& s);
+InstanceConst instanceConstFor(const ath_projection& p, const ath_settings& s, const ath_instance& in, uint32_t base);
+
 // project.cu
 uint32_t projectBlocks(uint32_t slots);
 cudaError_t launchProject(const FrameConst& F, const InstanceConst* inst, uint32_t nInst, uint32_t slots,
@@ -32,6 +36,13 @@ uint32_t sortResultIndex(uint32_t n, uint32_t bits);
 cudaError_t sortPrepare();
 cudaError_t launchSort(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_t bits, uint32_t* hist,
                        uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream);
+cudaError_t launchSortBits(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_t firstBit, uint32_t bits,
+                           uint32_t* hist, uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream);
+// The same with the key count on the device (at most n) and, when epochDevice is
+// given, epoch-tagged look-back words that need no clearing (a captured step).
+cudaError_t launchSortDevice(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, const uint32_t* nDevice,
+                             const uint32_t* epochDevice, uint32_t firstBit, uint32_t bits, uint32_t* hist,
+                             uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream);
 
 // blend.cu
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,

@@ -25,13 +25,21 @@ constexpr uint32_t kItems = 16;
 constexpr uint32_t kTileKeys = kSortThreads * kItems;   // 4096
 constexpr uint32_t kMaxPasses = 8;
 
+// `nDevice`, when given, holds the key count (a count only the device knows, as
+// in a step captured in a CUDA graph); `n` is then a bound on it.
+__device__ __forceinline__ uint32_t countOf(uint32_t n, const uint32_t* nDevice) {
+    return nDevice ? min(n, *nDevice) : n;
+}
+
 __global__ void __launch_bounds__(256)
-    histogramKernel(const uint64_t* __restrict__ keys, uint32_t n, uint32_t passes, uint32_t* __restrict__ hist) {
+    histogramKernel(const uint64_t* __restrict__ keys, uint32_t n, const uint32_t* __restrict__ nDevice,
+                    uint32_t firstBit, uint32_t passes, uint32_t* __restrict__ hist) {
     __shared__ uint32_t sHist[kMaxPasses * kRadix];
+    n = countOf(n, nDevice);
     for (uint32_t j = threadIdx.x; j < passes * kRadix; j += blockDim.x) sHist[j] = 0;
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint64_t key = keys[i];
+        const uint64_t key = keys[i] >> firstBit;
         for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p * kRadix + (uint32_t)((key >> (8 * p)) & 0xFFu)], 1u);
     }
     __syncthreads();
@@ -57,26 +65,33 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* sWa
     return base + incl - v;
 }
 
+template <bool kValues>
 __global__ void __launch_bounds__(kSortThreads)
     onesweepKernel(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
                    uint64_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, uint32_t n, uint32_t shift,
                    const uint32_t* __restrict__ globalHist, uint64_t* __restrict__ flags, uint32_t* __restrict__ ticket,
-                   uint32_t* __restrict__ status) {
+                   uint32_t* __restrict__ status, const uint32_t* __restrict__ nDevice,
+                   const uint32_t* __restrict__ epochDevice) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(sKeys + kTileKeys);
-    uint32_t* sWarpCnt = sVals + kTileKeys;   // kWarps x kRadix
+    uint32_t* sWarpCnt = kValues ? sVals + kTileKeys : sVals;   // kWarps x kRadix
     __shared__ uint32_t sTile;
     __shared__ uint32_t sStart[kRadix];
     __shared__ uint32_t sAdjust[kRadix];
     __shared__ uint32_t sScan[kWarps];
 
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    n = countOf(n, nDevice);
+    // Look-back words are [epoch:30][status:2][value:32]; a word of another
+    // epoch reads as not ready. Without an epoch (0) the caller clears them.
+    const uint32_t epoch = epochDevice ? (*epochDevice & 0x3FFFFFFFu) : 0u;
     if (tid == 0) sTile = atomicAdd(ticket, 1u);
     for (uint32_t j = tid; j < kWarps * kRadix; j += kSortThreads) sWarpCnt[j] = 0;
     __syncthreads();
     const uint32_t tile = sTile;
     const uint32_t base = tile * kTileKeys;
+    if (base >= n) return;   // a tile past the keys (the grid was sized for a bound)
     const uint32_t ltMask = (1u << lane) - 1u;
 
     // Rank: warp `warp` owns keys [base + warp*32*kItems, +32*kItems), item k of
@@ -90,7 +105,7 @@ __global__ void __launch_bounds__(kSortThreads)
         const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
         const bool valid = idx < n;
         key[k] = valid ? keysIn[idx] : 0ull;
-        val[k] = valid ? valsIn[idx] : 0u;
+        if constexpr (kValues) val[k] = valid ? valsIn[idx] : 0u;
     }
 #pragma unroll
     for (uint32_t k = 0; k < kItems; ++k) {
@@ -119,17 +134,18 @@ __global__ void __launch_bounds__(kSortThreads)
     // Where this tile's share of digit t starts in the output.
     uint64_t* flag = flags + (size_t)tile * kRadix + t;
     uint32_t exclusive;
+    const uint64_t tag = (uint64_t)epoch << 34;
     if (tile == 0) {
         exclusive = blockExclusiveScan(globalHist[t], sScan);
-        storeRelaxed(flag, kFlagInclusive | (uint64_t)(exclusive + count));
+        storeRelaxed(flag, tag | (2ull << 32) | (uint64_t)(exclusive + count));
     } else {
-        storeRelaxed(flag, kFlagAggregate | (uint64_t)count);
+        storeRelaxed(flag, tag | (1ull << 32) | (uint64_t)count);
         uint64_t sum = 0;
         int64_t j = (int64_t)tile - 1;
         uint32_t spins = 0;
         while (j >= 0) {
             const uint64_t v = loadRelaxed(flags + (size_t)j * kRadix + t);
-            const uint32_t st = (uint32_t)(v >> 62);
+            const uint32_t st = (uint32_t)(v >> 34) == epoch ? (uint32_t)(v >> 32) & 3u : 0u;
             if (st == 0) {
                 if (++spins > kSpinLimit || ((spins & 255u) == 0 && gaveUp(status))) {
                     atomicOr(status, kStatusLookbackTimeout);
@@ -138,12 +154,12 @@ __global__ void __launch_bounds__(kSortThreads)
                 __nanosleep(32);
                 continue;
             }
-            sum += v & kFlagValue;
+            sum += v & 0xFFFFFFFFull;
             if (st == 2) break;
             --j;
         }
         exclusive = (uint32_t)sum;
-        storeRelaxed(flag, kFlagInclusive | (uint64_t)(exclusive + count));
+        storeRelaxed(flag, tag | (2ull << 32) | (uint64_t)(exclusive + count));
     }
     const uint32_t start = blockExclusiveScan(count, sScan);
     sStart[t] = start;
@@ -158,7 +174,7 @@ __global__ void __launch_bounds__(kSortThreads)
             const uint32_t d = (uint32_t)((key[k] >> shift) & 0xFFu);
             const uint32_t s = sStart[d] + sWarpCnt[warp * kRadix + d] + rank[k];
             sKeys[s] = key[k];
-            sVals[s] = val[k];
+            if constexpr (kValues) sVals[s] = val[k];
         }
     }
     __syncthreads();
@@ -168,7 +184,7 @@ __global__ void __launch_bounds__(kSortThreads)
         const uint32_t dst = sAdjust[(uint32_t)((k >> shift) & 0xFFu)] + s;
         if (dst < n) {
             keysOut[dst] = k;
-            valsOut[dst] = sVals[s];
+            if constexpr (kValues) valsOut[dst] = sVals[s];
         } else {
             atomicOr(status, kStatusIndexRange);
         }
@@ -176,6 +192,7 @@ __global__ void __launch_bounds__(kSortThreads)
 }
 
 constexpr size_t kOnesweepSmem = (size_t)kTileKeys * 8 + (size_t)kTileKeys * 4 + (size_t)kWarps * kRadix * 4;
+constexpr size_t kOnesweepKeysSmem = (size_t)kTileKeys * 8 + (size_t)kWarps * kRadix * 4;
 
 }   // namespace
 
@@ -184,36 +201,62 @@ uint32_t sortTiles(uint32_t n) { return (n + kTileKeys - 1) / kTileKeys; }
 size_t sortFlagWords(uint32_t n, uint32_t bits) { return (size_t)sortTiles(n) * kRadix * sortPasses(bits); }
 
 cudaError_t sortPrepare() {
-    return cudaFuncSetAttribute(onesweepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOnesweepSmem);
+    cudaError_t err =
+        cudaFuncSetAttribute(onesweepKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOnesweepSmem);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(onesweepKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kOnesweepKeysSmem);
+    return err;
 }
 
 // keys/vals[0] hold the input; the sorted result lands in keys/vals[passes & 1]
-// (the caller reads sortResultIndex). hist: kMaxPasses*256 words, flags:
-// sortFlagWords words, tickets: one word a pass; all three are zeroed here.
-cudaError_t launchSort(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_t bits, uint32_t* hist,
-                       uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream) {
-    if (n <= 1) return cudaSuccess;
+// (the caller reads sortResultIndex). vals may be null (keys only). The passes
+// sort bits [firstBit, firstBit + bits) of the keys, eight at a time. hist:
+// kMaxPasses*256 words, flags: sortFlagWords words, tickets: one word a pass;
+// all three are zeroed here.
+cudaError_t launchSortDevice(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, const uint32_t* nDevice,
+                             const uint32_t* epochDevice, uint32_t firstBit, uint32_t bits, uint32_t* hist,
+                             uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream) {
+    if (n <= 1 && !nDevice) return cudaSuccess;
     const uint32_t passes = sortPasses(bits);
-    if (passes > kMaxPasses) return cudaErrorInvalidValue;
+    if (passes > kMaxPasses || firstBit + 8 * passes > 64 + 7) return cudaErrorInvalidValue;
     const uint32_t tiles = sortTiles(n);
     cudaError_t err = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kRadix * passes, stream);
     if (err != cudaSuccess) return err;
-    err = cudaMemsetAsync(flags, 0, sizeof(uint64_t) * (size_t)tiles * kRadix * passes, stream);
-    if (err != cudaSuccess) return err;
+    if (!epochDevice) {
+        err = cudaMemsetAsync(flags, 0, sizeof(uint64_t) * (size_t)tiles * kRadix * passes, stream);
+        if (err != cudaSuccess) return err;
+    }
     err = cudaMemsetAsync(tickets, 0, sizeof(uint32_t) * passes, stream);
     if (err != cudaSuccess) return err;
     int device = 0, sms = 148;
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const uint32_t hblocks = min((n + 255) / 256, (uint32_t)sms * 4);
-    histogramKernel<<<hblocks, 256, 0, stream>>>(keys[0], n, passes, hist);
+    histogramKernel<<<hblocks, 256, 0, stream>>>(keys[0], n, nDevice, firstBit, passes, hist);
+    const bool withValues = vals != nullptr && vals[0] != nullptr;
     for (uint32_t p = 0; p < passes; ++p) {
         const uint32_t in = p & 1u, out = in ^ 1u;
-        onesweepKernel<<<tiles, kSortThreads, kOnesweepSmem, stream>>>(
-            keys[in], vals[in], keys[out], vals[out], n, 8 * p, hist + p * kRadix,
-            flags + (size_t)p * tiles * kRadix, tickets + p, status);
+        if (withValues)
+            onesweepKernel<true><<<tiles, kSortThreads, kOnesweepSmem, stream>>>(
+                keys[in], vals[in], keys[out], vals[out], n, firstBit + 8 * p, hist + p * kRadix,
+                flags + (size_t)p * tiles * kRadix, tickets + p, status, nDevice, epochDevice);
+        else
+            onesweepKernel<false><<<tiles, kSortThreads, kOnesweepKeysSmem, stream>>>(
+                keys[in], nullptr, keys[out], nullptr, n, firstBit + 8 * p, hist + p * kRadix,
+                flags + (size_t)p * tiles * kRadix, tickets + p, status, nDevice, epochDevice);
     }
     return cudaGetLastError();
+}
+
+cudaError_t launchSortBits(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_t firstBit, uint32_t bits,
+                           uint32_t* hist, uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream) {
+    return launchSortDevice(keys, vals, n, nullptr, nullptr, firstBit, bits, hist, flags, tickets, status, stream);
+}
+
+cudaError_t launchSort(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_t bits, uint32_t* hist,
+                       uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream) {
+    return launchSortBits(keys, vals, n, 0, bits, hist, flags, tickets, status, stream);
 }
 
 uint32_t sortResultIndex(uint32_t n, uint32_t bits) { return n <= 1 ? 0u : (sortPasses(bits) & 1u); }

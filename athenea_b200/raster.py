@@ -396,3 +396,119 @@ def l2_loss(colour: torch.Tensor, target: torch.Tensor, dl_dcolour: torch.Tensor
     s = stream if stream is not None else torch.cuda.current_stream(colour.device)
     check(N.lib().ath_l2_loss(_ptr(colour), _ptr(target), int(colour.shape[0]), _ptr(dl_dcolour), _ptr(loss),
                               C.c_void_p(s.cuda_stream)))
+
+
+# ---- the batched, mixed-precision training step ---------------------------------
+@dataclass
+class MixedParams:
+    """ath_mixed_params: geometry FP32 (as Params), SH DC and band 1 in BF16 (N, 12),
+    bands 2-3 in FP8 e4m3 (N, 36) times a per-Gaussian scale (N,)."""
+    means: torch.Tensor
+    scales: torch.Tensor
+    quats: torch.Tensor
+    sh_low: torch.Tensor      # (N, 12) bfloat16
+    sh_high: torch.Tensor     # (N, 36) uint8 (e4m3 bits)
+    sh_scale: torch.Tensor    # (N,) float32
+    sh_degree: int = 3
+    linear: bool = False
+    object_to_world: np.ndarray = field(default_factory=lambda: np.eye(4))
+
+    @property
+    def count(self) -> int:
+        return int(self.means.shape[0])
+
+    @staticmethod
+    def from_params(P: "Params", stream: torch.cuda.Stream | None = None) -> "MixedParams":
+        """ath_params_to_mixed: the SH to BF16 / FP8; the geometry tensors are shared."""
+        n = P.count
+        dev = P.means.device
+        low = torch.empty((n, 12), dtype=torch.bfloat16, device=dev)
+        high = torch.empty((n, 36), dtype=torch.uint8, device=dev)
+        scale = torch.empty(n, dtype=torch.float32, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        check(N.lib().ath_params_to_mixed(C.byref(P._native()), _ptr(low), _ptr(high), _ptr(scale),
+                                          C.c_void_p(s.cuda_stream)))
+        return MixedParams(P.means, P.scales, P.quats, low, high, scale, P.sh_degree, P.linear, P.object_to_world)
+
+    def dequantized_sh(self) -> torch.Tensor:
+        """The SH as the mixed layout holds them, back in FP32 (N, 48)."""
+        n = self.count
+        out = torch.zeros((n, 48), dtype=torch.float32, device=self.means.device)
+        out[:, :12] = self.sh_low.float()
+        e4m3 = self.sh_high.view(torch.float8_e4m3fn).float()
+        out[:, 12:] = e4m3 * self.sh_scale[:, None]
+        return out
+
+    def _native(self) -> N.MixedParams:
+        p = N.MixedParams()
+        p.means, p.scales, p.quats = _ptr(self.means), _ptr(self.scales), _ptr(self.quats)
+        p.sh_low, p.sh_high, p.sh_scale = _ptr(self.sh_low), _ptr(self.sh_high), _ptr(self.sh_scale)
+        p.count = self.count
+        p.sh_degree = self.sh_degree
+        p.linear = 1 if self.linear else 0
+        p.object_to_world[:] = list(_mat(self.object_to_world).reshape(16))
+        return p
+
+
+class BatchTrainer:
+    """ath_batch: many views of one cloud, forward + loss + backward a step, each
+    stage one launch over every view, the step captured in a CUDA graph."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(N.lib().ath_batch_create(C.byref(h)))
+        self._h = h
+        self.pixels = 0
+        self.views = []
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            N.lib().ath_batch_destroy(h)
+            self._h = None
+
+    def set_views(self, views, settings: RenderSettings | None = None) -> None:
+        """views: [(projection, width, height)]; images concatenated in this order."""
+        arr = (N.View * len(views))()
+        for k, (proj, w, h) in enumerate(views):
+            arr[k].projection = proj
+            arr[k].width, arr[k].height = w, h
+        s = (settings or RenderSettings())._native()
+        check(N.lib().ath_batch_set_views(self._h, arr, len(views), C.byref(s)))
+        px = C.c_uint32()
+        check(N.lib().ath_batch_pixels(self._h, C.byref(px)))
+        self.pixels = px.value
+        self.views = [(w, h) for _, w, h in views]
+
+    def set_tuning(self, tile: int, block_batch: int) -> None:
+        check(N.lib().ath_batch_set_tuning(self._h, tile, block_batch))
+
+    def step(self, params: MixedParams, target: torch.Tensor, colour: torch.Tensor, loss: torch.Tensor,
+             grads: "Params", stream: torch.cuda.Stream | None = None) -> None:
+        g = N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
+        s = stream if stream is not None else torch.cuda.current_stream(colour.device)
+        self._keep = (params, target, colour, loss, grads)
+        check(N.lib().ath_batch_train_step(self._h, C.byref(params._native()), _ptr(target), _ptr(colour),
+                                           _ptr(loss), C.byref(g), C.c_void_p(s.cuda_stream)))
+
+    def check(self, stream: torch.cuda.Stream | None = None) -> dict:
+        st = N.BatchStats()
+        s = stream if stream is not None else torch.cuda.current_stream()
+        check(N.lib().ath_batch_check(self._h, C.byref(st), C.c_void_p(s.cuda_stream)))
+        return dict(pairs=st.pairs, capacity=st.capacity, kept=st.kept, tile=st.tile, block_batch=st.block_batch)
+
+    def tune(self, params: MixedParams, target, colour, loss, grads: "Params", repeats: int = 3,
+             stream: torch.cuda.Stream | None = None) -> dict:
+        g = N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
+        st = N.BatchStats()
+        s = stream if stream is not None else torch.cuda.current_stream(colour.device)
+        self._keep = (params, target, colour, loss, grads)
+        check(N.lib().ath_batch_tune(self._h, C.byref(params._native()), _ptr(target), _ptr(colour), _ptr(loss),
+                                     C.byref(g), repeats, C.byref(st), C.c_void_p(s.cuda_stream)))
+        return dict(pairs=st.pairs, tile=st.tile, block_batch=st.block_batch, ms_per_step=st.ms_per_step)
+
+    def buffers(self) -> dict:
+        b = N.BatchBuffers()
+        check(N.lib().ath_batch_buffers_of(self._h, C.byref(b), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        return dict(pairs=b.pairs, key_shift=b.key_shift, slot_bits=b.slot_bits, total_tiles=b.total_tiles,
+                    sorted_pairs=b.sorted_pairs, ranges=b.ranges, tile_bases=[b.tile_bases[k] for k in range(b.views)])

@@ -225,6 +225,90 @@ ath_status ath_raster_backward(ath_raster* r, const float* dl_dcolour, const flo
 ath_status ath_l2_loss(const float* colour, const float* target, uint32_t pixels, float* dl_dcolour, float* loss,
                        void* stream);
 
+/* ---- the batched, mixed-precision training step (no counterpart in the
+ * reference: it renders one camera a call, TileRasterizer.h:316-317) ------ */
+
+/* A cloud in the mixed-precision layout: geometry FP32 as ath_params; the SH
+ * DC and band 1 in BF16 (12 values: DC rgb, then band 1 rgb per basis), bands
+ * 2-3 in FP8 e4m3 (36 values, rgb per basis) times a per-Gaussian FP32 scale. */
+typedef struct {
+    const float* means;     /* float4: x y z, opacity logit */
+    const float* scales;    /* float4: log scales */
+    const float* quats;     /* float4: w x y z */
+    const void* sh_low;     /* 12 bf16 a Gaussian */
+    const void* sh_high;    /* 36 e4m3 a Gaussian */
+    const float* sh_scale;  /* 1 float a Gaussian */
+    uint32_t count;
+    uint32_t sh_degree;
+    int32_t linear;
+    double object_to_world[16];
+} ath_mixed_params;
+
+/* Converts ath_params' FP32 SH to the mixed layout (sh_low 12 x 2 bytes, sh_high
+ * 36 bytes, sh_scale 4 bytes a Gaussian): the bands' scale is their largest
+ * magnitude over e4m3's largest finite value, 448. */
+ath_status ath_params_to_mixed(const ath_params* params, void* sh_low, void* sh_high, float* sh_scale, void* stream);
+
+/* One view of a batch: a projection (ath_projection_for) and its image size. */
+typedef struct {
+    ath_projection projection;
+    uint32_t width, height;
+} ath_view;
+
+typedef struct ath_batch ath_batch;
+
+typedef struct {
+    uint64_t pairs;        /* (tile, Gaussian) pairs of every view, the last step */
+    uint64_t capacity;     /* pairs the buffers hold */
+    uint32_t kept;         /* (view, Gaussian) records drawn */
+    uint32_t tile, block_batch;
+    float ms_per_step;     /* ath_batch_tune: the chosen setting's time */
+} ath_batch_stats;
+
+ath_status ath_batch_create(ath_batch** out);
+void ath_batch_destroy(ath_batch* b);
+/* The views every step draws (at most 256), and the frame settings they share
+ * (background, max_sh_degree, antialias). Images are concatenated in view order:
+ * view v's pixel (x, y) is at v's base + y * width + x; ath_batch_pixels gives the total. */
+ath_status ath_batch_set_views(ath_batch* b, const ath_view* views, uint32_t count, const ath_settings* settings);
+/* Tile size (8, 16 or 32) and records a block stages at once (64, 128 or 256).
+ * Images do not depend on either: a pixel blends the same records in the same
+ * order whatever tile holds it. Default 16 and 256. */
+ath_status ath_batch_set_tuning(ath_batch* b, uint32_t tile, uint32_t block_batch);
+ath_status ath_batch_pixels(ath_batch* b, uint32_t* pixels);
+/* One training step over every view, with nothing read back to the host:
+ * project and emit every view's pairs (one launch), sort them all (one packed
+ * 64-bit sort), blend every view's tiles (one persistent launch), the loss
+ * (each view's mean L2 over its pixels and r g b against `target`, summed over
+ * views, into *loss), and the backward, whose dL/dparameters overwrite `grads`
+ * (FP32, ath_param_grads' layout, sh 48 floats a Gaussian). colour: float4 a
+ * pixel, target: float3 a pixel, both concatenated. The first call sizes the
+ * pair buffers (one host read) and captures the step into a CUDA graph; later
+ * calls with the same pointers replay it. */
+ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
+                                float* loss, ath_param_grads* grads, void* stream);
+/* Waits for `stream` and reports the last step; ATH_E_CAPACITY when its pairs
+ * outgrew the buffers (that step is not valid; the next one grows them). */
+ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* stream);
+/* The autotuner: times `repeats` steps for every tile size in {8, 16, 32} and
+ * block batch in {64, 128, 256}, keeps the fastest and reports it in `best`. */
+ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
+                          float* loss, ath_param_grads* grads, uint32_t repeats, ath_batch_stats* best, void* stream);
+
+/* The last step's sorted pairs and tile ranges, for inspection: device
+ * pointers the batch owns, valid until its next step. A pair is
+ * (global tile << key_shift) | (24-bit depth key << slot_bits) | Gaussian; view
+ * v's tiles start at tile_bases[v] (host array of `views` entries). */
+typedef struct {
+    uint64_t pairs;
+    uint32_t key_shift, slot_bits, total_tiles, views;
+    const uint64_t* sorted_pairs;
+    const uint32_t* ranges;      /* 2 a global tile: [start, end) */
+    const uint32_t* tile_bases;  /* host */
+} ath_batch_buffers;
+
+ath_status ath_batch_buffers_of(ath_batch* b, ath_batch_buffers* out, void* stream);
+
 /* TileRasterizer::latestCounters (TileRasterizer.h:478). ATH_E_NOT_FOUND
  * until a frame drawn with count_splats has finished. */
 ath_status ath_raster_latest_counters(ath_raster* r, ath_splat_counters* out);

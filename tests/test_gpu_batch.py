@@ -1,0 +1,144 @@
+"""The batched, mixed-precision training step (ath_batch_*) against the plain
+per-view path (ath_raster_render_params / ath_raster_backward), on a B200.
+
+With the SH first quantised to the mixed layout (so both paths see the same
+coefficients), the only differences left are the blend's fast exponential and
+fused multiply-adds: pairs, their order and the tile ranges must be identical
+to the bit, images and gradients equal within those roundings. The tile size
+and record batch the autotuner picks between change no image bit.
+"""
+import numpy as np
+import pytest
+import torch
+
+import athenea_b200 as A
+from athenea_b200 import scenes
+from athenea_b200.raster import BatchTrainer, MixedParams
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(320, 180), (640, 360), (480, 270)]
+
+
+def _scene(count=50_000, seed=31):
+    p = scenes.params(count, True, seed, 3)
+    P = A.Params(*[torch.from_numpy(np.ascontiguousarray(p[k])).cuda() for k in ("means", "scales", "quats", "sh")], 3)
+    M = MixedParams.from_params(P)
+    # the plain path sees the same (quantised) coefficients
+    Pq = A.Params(P.means, P.scales, P.quats, M.dequantized_sh().contiguous(), 3)
+    return Pq, M
+
+
+def _views(n=len(SIZES)):
+    out = []
+    for v in range(n):
+        W, H = SIZES[v % len(SIZES)]
+        eye = scenes.circle_eye(v, 8, 3.0, 0.3)
+        cam = A.pinhole_for_vertical_fov(eye, (0, 0, 0), W, H, 60.0)
+        out.append((cam.projection_for(W, H), W, H))
+    return out
+
+
+def _plain(Pq, views, targets):
+    from tests import gpu_helpers as G
+    raster = A.TileRasterizer.create()
+    grads = Pq.zeros_like()
+    loss = torch.zeros(1, device="cuda")
+    images, frames = [], []
+    for (proj, W, H), target in zip(views, targets):
+        t = A.RenderTargets.make(W, H)
+        raster.render_params(proj, Pq, A.RenderSettings(width=W, height=H), t)
+        dl = torch.empty_like(t.colour)
+        A.l2_loss(t.colour, target, dl, loss)
+        frames.append(G.frame_buffers(raster))
+        raster.backward(dl, grads)
+        images.append(t.colour.clone())
+    torch.cuda.synchronize()
+    return images, frames, loss, grads
+
+
+def _batched(M, views, targets, tile=16, block_batch=256, trainer=None):
+    b = trainer or BatchTrainer()
+    b.set_views(views)
+    b.set_tuning(tile, block_batch)
+    colour = torch.empty((b.pixels, 4), device="cuda")
+    target = torch.cat(targets).contiguous()
+    loss = torch.zeros(1, device="cuda")
+    grads = A.Params(torch.zeros_like(M.means), torch.zeros_like(M.scales), torch.zeros_like(M.quats),
+                     torch.zeros((M.count, 48), device="cuda"), 3)
+    b.step(M, target, colour, loss, grads)
+    stats = b.check()
+    torch.cuda.synchronize()
+    return b, colour, loss, grads, stats
+
+
+def test_batched_step_matches_the_plain_path(oracle):
+    from tests import gpu_helpers as G
+    Pq, M = _scene()
+    views = _views()
+    gen = torch.Generator().manual_seed(3)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    images, frames, loss_p, grads_p = _plain(Pq, views, targets)
+    b, colour, loss_b, grads_b, stats = _batched(M, views, targets)
+    buf = b.buffers()
+    assert stats["pairs"] == sum(f["pairs"] for f in frames) == buf["pairs"]
+    sorted_pairs = G.fetch(buf["sorted_pairs"], (buf["pairs"],), np.uint64)
+    ranges = G.fetch(buf["ranges"], (buf["total_tiles"], 2), np.uint32)
+    tiles = (sorted_pairs >> np.uint64(buf["key_shift"])).astype(np.int64)
+    splats = (sorted_pairs & np.uint64((1 << buf["slot_bits"]) - 1)).astype(np.uint32)
+    start = 0
+    for v, f in enumerate(frames):
+        n = f["pairs"]
+        # this view's pairs: its tiles, its Gaussians, in its order
+        np.testing.assert_array_equal(tiles[start:start + n] - buf["tile_bases"][v],
+                                      (f["pair_keys"] >> np.uint64(24)).astype(np.int64))
+        np.testing.assert_array_equal(splats[start:start + n], f["pair_splats"])
+        r = ranges[buf["tile_bases"][v]:buf["tile_bases"][v] + f["tiles"]].astype(np.int64)
+        live = r[:, 1] > r[:, 0]
+        np.testing.assert_array_equal(r[live] - start, f["ranges"].astype(np.int64)[live])
+        start += n
+    # images: the fast exponential, within 1e-4 but for the odd blend decision at its threshold
+    got = colour.cpu().numpy()
+    base = 0
+    for (proj, W, H), img in zip(views, images):
+        d = np.abs(got[base:base + W * H] - img.cpu().numpy()).max(axis=1)
+        assert np.mean(d <= 1e-4) >= 0.9999, float(np.mean(d <= 1e-4))
+        assert d.max() <= 2e-2
+        base += W * H
+    assert abs(loss_b.item() - loss_p.item()) <= 1e-4 * loss_p.item()
+    for name in ("means", "scales", "quats", "sh"):
+        a = getattr(grads_b, name).cpu().numpy().ravel().astype(np.float64)
+        c = getattr(grads_p, name).cpu().numpy().ravel().astype(np.float64)
+        cos = np.dot(a, c) / (np.linalg.norm(a) * np.linalg.norm(c) + 1e-30)
+        assert cos > 0.9999, (name, cos)
+        assert abs(np.linalg.norm(a) / np.linalg.norm(c) - 1.0) < 1e-3, name
+
+
+def test_tile_size_and_block_batch_change_no_image_bit():
+    Pq, M = _scene(30_000, 8)
+    views = _views()
+    gen = torch.Generator().manual_seed(4)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    ref = None
+    for tile in (8, 16, 32):
+        for nb in (64, 256):
+            _, colour, _, _, _ = _batched(M, views, targets, tile, nb)
+            img = colour.cpu().numpy()
+            if ref is None:
+                ref = img
+            else:
+                np.testing.assert_array_equal(img, ref, err_msg=f"tile {tile}, batch {nb}")
+
+
+def test_replayed_step_draws_the_same_image_and_tune_picks_a_setting():
+    Pq, M = _scene(30_000, 9)
+    views = _views()
+    gen = torch.Generator().manual_seed(5)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    b, colour, loss, grads, _ = _batched(M, views, targets)
+    first = colour.cpu().numpy().copy()
+    b.step(M, torch.cat(targets).contiguous(), colour, loss, grads)   # same pointers? a new target tensor: recaptured
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(colour.cpu().numpy(), first)
+    best = b.tune(M, torch.cat(targets).contiguous(), colour, loss, grads, repeats=2)
+    assert best["tile"] in (8, 16, 32) and best["block_batch"] in (64, 128, 256) and best["ms_per_step"] > 0
