@@ -104,7 +104,8 @@ class View(C.Structure):
 
 class BatchStats(C.Structure):
     _fields_ = [("pairs", C.c_uint64), ("capacity", C.c_uint64), ("kept", C.c_uint32), ("tile", C.c_uint32),
-                ("block_batch", C.c_uint32), ("ms_per_step", C.c_float)]
+                ("block_batch", C.c_uint32), ("ms_per_step", C.c_float), ("degenerate", C.c_uint32),
+                ("evaluated", C.c_uint64)]
 
 
 class BatchBuffers(C.Structure):
@@ -145,6 +146,8 @@ SIGNATURES = {
     "ath_batch_train_step": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads), _P]),
     "ath_batch_check": (C.c_int32, [_P, C.POINTER(BatchStats), _P]),
     "ath_batch_buffers_of": (C.c_int32, [_P, C.POINTER(BatchBuffers), _P]),
+    "ath_batch_time_stages": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads),
+                                          C.POINTER(C.c_float), _P]),
     "ath_batch_tune": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads), C.c_uint32,
                                    C.POINTER(BatchStats), _P]),
     "ath_raster_frame_buffers": (C.c_int32, [_P, C.POINTER(FrameBuffers)]),

@@ -96,7 +96,7 @@ template <uint32_t L>
 __device__ __forceinline__ void projectAdjoint(const FrameConst& F, const InstanceConst& I, uint32_t i,
                                                const float gw[kGradWords], ParamGrad& acc) {
     const Gauss g = loadGauss<L>(I, i);
-    const Geometry G = projectGeometry(F, I, g, g.opacity);
+    const Geometry G = projectGeometry<L == kLayoutMixed>(F, I, g, g.opacity);
     const float* m = I.m;
 
     // ---- colour: c = decode(base + rest(dir)) ------------------------------
@@ -173,9 +173,20 @@ __device__ __forceinline__ void projectAdjoint(const FrameConst& F, const Instan
     const float a2 = G.a + 0.3f, c2 = G.c + 0.3f, b = G.b;
     const float det = G.det, det2 = det * det;
     const float gA = gw[kGradA], gB = gw[kGradB2], gC = gw[kGradC];
-    float da2 = gA * (-c2 * c2 / det2) + gB * (b * c2 / det2) + gC * (1.0f / det - a2 * c2 / det2);
-    float db = gA * (2.0f * b * c2 / det2) + gB * (-1.0f / det - 2.0f * b * b / det2) + gC * (2.0f * a2 * b / det2);
-    float dc2 = gA * (1.0f / det - c2 * a2 / det2) + gB * (b * a2 / det2) + gC * (-a2 * a2 / det2);
+    float da2, db, dc2;
+    if (G.wide) {
+        // the mixed path's FP64 conic (gauss.cuh wideCovariance), differentiated in FP64
+        const WideCovariance W = wideCovariance(G.t3, G.u3, G.M);
+        const double d2 = W.det * W.det;
+        da2 = (float)(gA * (-W.c2 * W.c2 / d2) + gB * (W.b * W.c2 / d2) + gC * (1.0 / W.det - W.a2 * W.c2 / d2));
+        db = (float)(gA * (2.0 * W.b * W.c2 / d2) + gB * (-1.0 / W.det - 2.0 * W.b * W.b / d2) +
+                     gC * (2.0 * W.a2 * W.b / d2));
+        dc2 = (float)(gA * (1.0 / W.det - W.c2 * W.a2 / d2) + gB * (W.b * W.a2 / d2) + gC * (-W.a2 * W.a2 / d2));
+    } else {
+        da2 = gA * (-c2 * c2 / det2) + gB * (b * c2 / det2) + gC * (1.0f / det - a2 * c2 / det2);
+        db = gA * (2.0f * b * c2 / det2) + gB * (-1.0f / det - 2.0f * b * b / det2) + gC * (2.0f * a2 * b / det2);
+        dc2 = gA * (1.0f / det - c2 * a2 / det2) + gB * (b * a2 / det2) + gC * (-a2 * a2 / det2);
+    }
     da2 += dDet * c2;
     dc2 += dDet * a2;
     db += dDet * (-2.0f * b);

@@ -23,10 +23,15 @@
 //
 // The geometry that decides footprints, tiles and depth keys is the plain
 // path's to the bit (this file builds with --fmad=false and calls the same
-// projectGeometry): pairs, their order and the tile ranges are the reference's.
-// Colour (SH in BF16/FP8 from the mixed layout), the blend's exponential and
-// its divisions use the fast hardware paths; the image error that costs is
-// measured against an FP64 oracle.
+// projectGeometry): pairs, their order and the tile ranges are the reference's,
+// except for near-degenerate footprints (det < 1e-6 trace^2 of the dilated 2D
+// covariance), whose determinants and inverse come from FP64 (gauss.cuh
+// wideCovariance) and whose tile test evaluates the conic in factored form;
+// ath_batch_stats.degenerate counts them. Records carry the factored conic
+// (ca, fr, fs): power = ca (dx + fr dy)^2 + fs dy^2, which has no cancellation
+// and one operation fewer than the expanded form. Colour (SH in BF16/FP8 from
+// the mixed layout), the blend's exponential and its divisions use the fast
+// hardware paths; the image error that costs is measured against an FP64 oracle.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -57,6 +62,8 @@ __global__ void beginStepKernel(uint32_t* words) {
     words[kBatchBackTicket] = 0;
     words[kBatchKept] = 0;
     for (int p = 0; p < 8; ++p) words[kBatchSortTickets + p] = 0;
+    words[kBatchEvaluated] = words[kBatchEvaluated + 1] = 0;
+    words[kBatchDegenerate] = 0;
 }
 
 // The decoupled look-back of lookbackExclusive with epoch-tagged 32-bit values.
@@ -100,6 +107,29 @@ __device__ uint32_t lookbackEpoch(uint64_t* flags, uint32_t b, uint32_t aggregat
 // the same operations minPowerOverBox performs, so the result is its result.
 __device__ __forceinline__ float quad(float a, float b, float c, float x, float y) {
     return ((a * x) * x + ((2.0f * b) * x) * y) + (c * y) * y;
+}
+
+// minPowerOverBox for a near-degenerate footprint: the same candidate points,
+// each evaluated in the factored form ca (x + fr y)^2 + fs y^2, which does not
+// cancel however thin the footprint is.
+__device__ __forceinline__ float minPowerOverBoxFactored(float a, float b, float c, float fr, float fs, float lox,
+                                                         float loy, float hix, float hiy) {
+    if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) return 0.0f;
+    float best = 3.4e38f;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        float x, y;
+        if (e < 2) {
+            x = e == 0 ? lox : hix;
+            y = c > 1e-12f ? clampf(((-b) * x) / c, loy, hiy) : loy;
+        } else {
+            y = e == 2 ? loy : hiy;
+            x = a > 1e-12f ? clampf(((-b) * y) / a, lox, hix) : lox;
+        }
+        const float t = x + fr * y;
+        best = fminf(best, (a * t) * t + (fs * y) * y);
+    }
+    return best;
 }
 
 template <uint32_t L>
@@ -169,16 +199,25 @@ __global__ void __launch_bounds__(kProjThreads)
     const uint32_t i = gb * kProjThreads + threadIdx.x;
     uint32_t touched = 0, depthKey = 0, rx0 = 0, ry0 = 0, rx1 = 0, ry1 = 0;
     uint64_t mask = 0;
-    float cx = 0, cy = 0, ca = 0, cb = 0, cc = 0, cutoff = 0;
+    float cx = 0, cy = 0, ca = 0, cb = 0, cc = 0, cutoff = 0, fr = 0, fs = 0;
+    bool wide = false;
     if (i < B.count && gb < gaussBlocks) {
         const Gauss g = loadGauss<L>(I, i);
-        const Geometry G = projectGeometry(F, I, g, g.opacity);
+        const Geometry G = projectGeometry<true>(F, I, g, g.opacity);
         if (!G.cull) {
-            // frame.slang:383-402 for tile size T
-            const float det2 = G.ca * G.cc - G.cb * G.cb;
-            const float inv = det2 > 1e-20f ? 1.0f / det2 : 0.0f;
-            const float ex = sqrtf(fmaxf((G.cutoff * G.cc) * inv, 0.0f));
-            const float ey = sqrtf(fmaxf((G.cutoff * G.ca) * inv, 0.0f));
+            // frame.slang:383-402 for tile size T; a near-degenerate footprint's
+            // extents from its covariance's diagonal, which cc / det(conic) and
+            // ca / det(conic) equal, without the cancelling determinant
+            float ex, ey;
+            if (G.wide) {
+                ex = sqrtf(G.cutoff * (G.a + 0.3f));
+                ey = sqrtf(G.cutoff * (G.c + 0.3f));
+            } else {
+                const float det2 = G.ca * G.cc - G.cb * G.cb;
+                const float inv = det2 > 1e-20f ? 1.0f / det2 : 0.0f;
+                ex = sqrtf(fmaxf((G.cutoff * G.cc) * inv, 0.0f));
+                ey = sqrtf(fmaxf((G.cutoff * G.ca) * inv, 0.0f));
+            }
             const float x1 = G.cx - ex, y1 = G.cy - ey, x2 = G.cx + ex, y2 = G.cy + ey;
             if (!(x2 < 0.0f || y2 < 0.0f || x1 >= (float)F.width || y1 >= (float)F.height)) {
                 rx0 = (uint32_t)fmaxf(x1, 0.0f) / T;
@@ -186,45 +225,55 @@ __global__ void __launch_bounds__(kProjThreads)
                 rx1 = (uint32_t)fminf(x2, (float)F.width - 1.0f) / T;
                 ry1 = (uint32_t)fminf(y2, (float)F.height - 1.0f) / T;
                 cx = G.cx; cy = G.cy; ca = G.ca; cb = G.cb; cc = G.cc; cutoff = G.cutoff;
-                const uint32_t cols = rx1 - rx0 + 1;
+                fr = G.fr; fs = G.fs; wide = G.wide;
                 uint32_t bit = 0;
-                for (uint32_t ty = ry0; ty <= ry1; ++ty) {
-                    const float loy = ((float)(ty * T) + 0.5f) - cy;
-                    const float hiy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
-                    // the row's x* = -b y / a at its two y edges
-                    const float xLo = ca > 1e-12f ? ((-cb) * loy) / ca : 0.0f;
-                    const float xHi = ca > 1e-12f ? ((-cb) * hiy) / ca : 0.0f;
-                    for (uint32_t tx = rx0; tx <= rx1; ++tx, ++bit) {
-                        const float lox = ((float)(tx * T) + 0.5f) - cx;
-                        const float hix = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
-                        float best;
-                        if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) {
-                            best = 0.0f;
-                        } else {
-                            best = 3.4e38f;
-                            const float yl = cc > 1e-12f ? clampf(((-cb) * lox) / cc, loy, hiy) : loy;
-                            best = fminf(best, quad(ca, cb, cc, lox, yl));
-                            const float yh = cc > 1e-12f ? clampf(((-cb) * hix) / cc, loy, hiy) : loy;
-                            best = fminf(best, quad(ca, cb, cc, hix, yh));
-                            const float xl = ca > 1e-12f ? clampf(xLo, lox, hix) : lox;
-                            best = fminf(best, quad(ca, cb, cc, xl, loy));
-                            const float xh = ca > 1e-12f ? clampf(xHi, lox, hix) : lox;
-                            best = fminf(best, quad(ca, cb, cc, xh, hiy));
+                if (wide) {
+                    for (uint32_t ty = ry0; ty <= ry1; ++ty)
+                        for (uint32_t tx = rx0; tx <= rx1; ++tx) {
+                            const float lx = ((float)(tx * T) + 0.5f) - cx, ly = ((float)(ty * T) + 0.5f) - cy;
+                            const float hx = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
+                            const float hy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
+                            if (minPowerOverBoxFactored(ca, cb, cc, fr, fs, lx, ly, hx, hy) <= cutoff) touched += 1;
                         }
-                        if (best <= cutoff) {
-                            touched += 1;
-                            if (bit < 64) mask |= 1ull << bit;
+                } else {
+                    for (uint32_t ty = ry0; ty <= ry1; ++ty) {
+                        const float loy = ((float)(ty * T) + 0.5f) - cy;
+                        const float hiy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
+                        // the row's x* = -b y / a at its two y edges
+                        const float xLo = ca > 1e-12f ? ((-cb) * loy) / ca : 0.0f;
+                        const float xHi = ca > 1e-12f ? ((-cb) * hiy) / ca : 0.0f;
+                        for (uint32_t tx = rx0; tx <= rx1; ++tx, ++bit) {
+                            const float lox = ((float)(tx * T) + 0.5f) - cx;
+                            const float hix = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
+                            float best;
+                            if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) {
+                                best = 0.0f;
+                            } else {
+                                best = 3.4e38f;
+                                const float yl = cc > 1e-12f ? clampf(((-cb) * lox) / cc, loy, hiy) : loy;
+                                best = fminf(best, quad(ca, cb, cc, lox, yl));
+                                const float yh = cc > 1e-12f ? clampf(((-cb) * hix) / cc, loy, hiy) : loy;
+                                best = fminf(best, quad(ca, cb, cc, hix, yh));
+                                const float xl = ca > 1e-12f ? clampf(xLo, lox, hix) : lox;
+                                best = fminf(best, quad(ca, cb, cc, xl, loy));
+                                const float xh = ca > 1e-12f ? clampf(xHi, lox, hix) : lox;
+                                best = fminf(best, quad(ca, cb, cc, xh, hiy));
+                            }
+                            if (best <= cutoff) {
+                                touched += 1;
+                                if (bit < 64) mask |= 1ull << bit;
+                            }
                         }
                     }
                 }
-                (void)cols;
                 if (touched) {
                     const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
                     float colour[3];
                     colourFast<L>(I, g, i, degree, g.px - I.eye[0], g.py - I.eye[1], g.pz - I.eye[2], colour);
                     const size_t r = ((size_t)v * B.count + i) * 3;
+                    if (G.wide) atomicAdd(&words[kBatchDegenerate], 1u);
                     recs[r + 0] = make_float4(G.cx, G.cy, G.tz, G.cutoff);
-                    recs[r + 1] = make_float4(G.ca, G.cb, G.cc, G.alpha);
+                    recs[r + 1] = make_float4(G.ca, G.fr, G.fs, G.alpha);
                     recs[r + 2] = make_float4(colour[0], colour[1], colour[2], 0.0f);
                     depthKey = __float_as_uint(G.tz) >> 7;
                 }
@@ -267,7 +316,7 @@ __global__ void __launch_bounds__(kProjThreads)
     const uint64_t head = ((uint64_t)(sView.tileBase) << B.keyShift) | ((uint64_t)depthKey << B.slotBits) | i;
     const uint32_t cols = rx1 - rx0 + 1;
     const uint32_t area = cols * (ry1 - ry0 + 1);
-    if (area <= 64) {
+    if (area <= 64 && !wide) {
         uint64_t m = mask;
         while (m) {
             const uint32_t bit = (uint32_t)__ffsll((long long)m) - 1u;
@@ -282,7 +331,9 @@ __global__ void __launch_bounds__(kProjThreads)
                 const float lx = ((float)(tx * T) + 0.5f) - cx, ly = ((float)(ty * T) + 0.5f) - cy;
                 const float hx = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
                 const float hy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
-                if (minPowerOverBox(ca, cb, cc, lx, ly, hx, hy) <= cutoff) {
+                const float best = wide ? minPowerOverBoxFactored(ca, cb, cc, fr, fs, lx, ly, hx, hy)
+                                        : minPowerOverBox(ca, cb, cc, lx, ly, hx, hy);
+                if (best <= cutoff) {
                     if (at < B.capacity) pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
                     ++at;
                 }
@@ -322,6 +373,7 @@ __global__ void __launch_bounds__(T * T)
     for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
     const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
     const float kL2e = 1.4426950408889634f;
+    uint32_t evaluated = 0;   // (pixel, record) evaluations this thread made
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) sTile = atomicAdd(&words[kBatchBlendTicket], 1u);
@@ -348,20 +400,22 @@ __global__ void __launch_bounds__(T * T)
                     const size_t s = (recBase + (pairs[mine] & slotMask)) * 3;
                     sScreen[k] = recs[s + 0];
                     const float4 c = recs[s + 1];
-                    // the conic pre-scaled by -log2(e)/2: power in base-2 exponent units
-                    const float kx = c.x * (-0.5f * kL2e), ky = c.y * (-kL2e), kz = c.z * (-0.5f * kL2e);
-                    sConic[k] = make_float4(kx, ky, kz, c.w);
+                    // the factored conic's two weights pre-scaled by -log2(e)/2:
+                    // power in base-2 exponent units
+                    sConic[k] = make_float4(c.x * (-0.5f * kL2e), c.y, c.z * (-0.5f * kL2e), c.w);
                     sColour[k] = recs[s + 2];
                 }
             }
             __syncthreads();
             const uint32_t count = min(NB, range.y - first);
-            for (uint32_t j = 0; j < count && !done; ++j) {
+            uint32_t j = 0;
+            for (; j < count && !done; ++j) {
                 const float4 sc = sScreen[j];
                 const float4 k = sConic[j];
                 const float dx = pxc - sc.x, dy = pyc - sc.y;
                 // e = -log2(e)/2 * power; power > cutoff  <=>  e < -log2(e)/2 * cutoff
-                const float e = __fmaf_rn(k.x * dx, dx, __fmaf_rn(k.y * dx, dy, k.z * dy * dy));   // kx ky kz
+                const float t = __fmaf_rn(k.y, dy, dx);
+                const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
                 if (e < (-0.5f * kL2e) * sc.w) continue;
                 const float alpha = fminf(0.99f, k.w * fastExp2(e));
                 if (alpha < kFaint) continue;
@@ -375,6 +429,7 @@ __global__ void __launch_bounds__(T * T)
                 last = first - range.x + j + 1;
                 if (Tr < 1e-4f) done = true;
             }
+            evaluated += j;
         }
         if (inside) {
             const uint32_t at = V.pixelBase + py * V.width + px;
@@ -385,6 +440,11 @@ __global__ void __launch_bounds__(T * T)
             lastContrib[at] = last;
         }
     }
+    uint64_t e = evaluated;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
+    if ((threadIdx.x & 31u) == 0 && e)
+        atomicAdd(reinterpret_cast<unsigned long long*>(words + kBatchEvaluated), (unsigned long long)e);
 }
 
 // ---- the loss: a view's mean L2 over its pixels and r g b, summed over views ----
@@ -504,8 +564,9 @@ __global__ void __launch_bounds__(T * T)
                     const float4 k = sConic[j];
                     const float dx = pxc - sc.x, dy = pyc - sc.y;
                     // the forward's exponent, operation for operation (so the same records pass)
-                    const float kx = k.x * (-0.5f * kL2e), ky = k.y * (-kL2e), kz = k.z * (-0.5f * kL2e);
-                    const float e = __fmaf_rn(kx * dx, dx, __fmaf_rn(ky * dx, dy, kz * dy * dy));
+                    const float kA = k.x * (-0.5f * kL2e), kS = k.z * (-0.5f * kL2e);
+                    const float t = __fmaf_rn(k.y, dy, dx);
+                    const float e = __fmaf_rn(kA * t, t, (kS * dy) * dy);
                     if (e >= (-0.5f * kL2e) * sc.w) {
                         const float G = fastExp2(e);
                         const float raw = k.w * G;
@@ -532,8 +593,11 @@ __global__ void __launch_bounds__(T * T)
                                 gv[2] = dPower * (dx * dx);
                                 gv[3] = dPower * (2.0f * dx * dy);
                                 gv[4] = dPower * (dy * dy);
-                                gv[0] = dPower * (-2.0f * (k.x * dx + k.y * dy));
-                                gv[1] = dPower * (-2.0f * (k.y * dx + k.z * dy));
+                                // d power / d centre: -2 (ca dx + cb dy), -2 (cb dx + cc dy)
+                                // in the factored form (cb = ca fr, cc = fs + ca fr^2)
+                                const float at = k.x * t;
+                                gv[0] = dPower * (-2.0f * at);
+                                gv[1] = dPower * (-2.0f * (k.y * at + k.z * dy));
                             }
                         }
                     }
@@ -773,7 +837,9 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
 
 // One step, enqueued (captured or not). `countOnly`: the projection alone, to size the pairs.
 cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* target, float4* colour, float* loss,
-                        ath_param_grads& g, cudaStream_t stream, bool countOnly) {
+                        ath_param_grads& g, cudaStream_t stream, bool countOnly, cudaEvent_t* marks = nullptr) {
+    auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], stream); };
+    mark(0);
     BatchConst B = batchConst(b, P);
     if (countOnly) B.capacity = 0;
     uint32_t* words = static_cast<uint32_t*>(b->words.ptr);
@@ -787,6 +853,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
             static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint64_t*>(b->projFlags.ptr), words, gaussBlocks);
     if (err == cudaSuccess) err = cudaGetLastError();
     if (countOnly || err != cudaSuccess) return err;
+    mark(1);
     uint64_t* keys[2] = {static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint64_t*>(b->pairs[1].ptr)};
     const uint32_t bits = 24 + b->tileBits;
     err = launchSortDevice(keys, nullptr, (uint32_t)b->capacity, words + kBatchPairsLo, words + kBatchEpoch,
@@ -794,6 +861,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
                            static_cast<uint64_t*>(b->sortFlags.ptr), words + kBatchSortTickets, words + kBatchStatus,
                            stream);
     const uint32_t sorted = sortResultIndex(2, bits);
+    mark(2);
     b->lastSorted = sorted;
     b->lastSlotBits = B.slotBits;
     if (err == cudaSuccess) err = cudaMemsetAsync(b->ranges.ptr, 0, (size_t)b->totalTiles * 8, stream);
@@ -803,7 +871,9 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
                                                     static_cast<uint2*>(b->ranges.ptr), words + kBatchStatus);
         err = cudaGetLastError();
     }
+    mark(3);
     if (err == cudaSuccess) err = launchBlendsFor(b, B, sorted, stream, true, colour, nullptr, nullptr);
+    mark(4);
     if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
     if (err == cudaSuccess) {
         lossBatchKernel<<<(b->totalPixels + 255) / 256, 256, 0, stream>>>(
@@ -812,9 +882,11 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     }
     if (err == cudaSuccess)
         err = cudaMemsetAsync(b->grads.ptr, 0, (size_t)V * P.count * kGradWords * sizeof(float), stream);
+    mark(5);
     if (err == cudaSuccess)
         err = launchBlendsFor(b, B, sorted, stream, false, nullptr, static_cast<float4*>(b->dL.ptr),
                               static_cast<float*>(b->grads.ptr));
+    mark(6);
     if (err == cudaSuccess && P.count) {
         projectAdjointBatchKernel<kLayoutMixed><<<(P.count + 127) / 128, 128, 0, stream>>>(
             B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
@@ -822,6 +894,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
             g.sh, 48);
         err = cudaGetLastError();
     }
+    mark(7);
     return err;
 }
 
@@ -1038,6 +1111,8 @@ extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* 
     if (err != cudaSuccess) return failCuda(err, "ath_batch_check");
     out->pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
     out->kept = w[kBatchKept];
+    out->evaluated = (uint64_t)w[kBatchEvaluated] | ((uint64_t)w[kBatchEvaluated + 1] << 32);
+    out->degenerate = w[kBatchDegenerate];
     out->tile = b->tile;
     out->block_batch = b->blockBatch;
     out->capacity = b->capacity;
@@ -1052,6 +1127,26 @@ extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* 
         return fail(ATH_E_INTERNAL, "a batched step met an index outside its buffers");
     }
     return ATH_OK;
+}
+
+extern "C" ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params* params, const float* target,
+                                            float* colour, float* loss, ath_param_grads* grads, float ms[7],
+                                            void* streamPtr) {
+    // A step as ath_batch_train_step enqueues it, uncaptured, with events between
+    // its stages, waited for: project+emit, sort, ranges, blend, loss, blend
+    // adjoint, projection adjoint.
+    if (!b || !params || !grads || !ms) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_time_stages: null argument");
+    ath_status st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);   // sized and placed
+    if (st != ATH_OK) return st;
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    cudaEvent_t marks[8];
+    for (auto& e : marks) cudaEventCreate(&e);
+    ath_param_grads g = *grads;
+    cudaError_t err = enqueueStep(b, *params, target, reinterpret_cast<float4*>(colour), loss, g, stream, false, marks);
+    if (err == cudaSuccess) err = cudaEventSynchronize(marks[7]);
+    for (int k = 0; k < 7 && err == cudaSuccess; ++k) cudaEventElapsedTime(&ms[k], marks[k], marks[k + 1]);
+    for (auto& e : marks) cudaEventDestroy(e);
+    return err == cudaSuccess ? ATH_OK : failCuda(err, "ath_batch_time_stages");
 }
 
 extern "C" ath_status ath_batch_buffers_of(ath_batch* b, ath_batch_buffers* out, void* streamPtr) {

@@ -48,6 +48,8 @@ enum BatchWord : uint32_t {
     kBatchBackTicket = 6,    // the persistent backward's tile queue
     kBatchKept = 7,          // (view, Gaussian) records kept
     kBatchSortTickets = 8,   // one a sort pass (8)
+    kBatchEvaluated = 16,    // 64-bit (16, 17): (pixel, record) evaluations of the forward blend
+    kBatchDegenerate = 18,   // records whose conic took the FP64 path
     kBatchWords = 32,
 };
 

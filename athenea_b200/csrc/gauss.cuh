@@ -130,8 +130,10 @@ struct Geometry {
     float det, detBefore; // after and before the +0.3 dilation
     float paid, alpha;
     float ca, cb, cc;     // the conic
+    float fr, fs;         // the factored conic's ratio and tail (mixed path only)
     float cutoff;
     bool clampX, clampY;  // the Jacobian's point was clamped to the frustum's 1.3x
+    bool wide;            // determinants and conic from wideCovariance (mixed path only)
     float txc, tyc;
     float jx0, jx2, jy1, jy2;
     float t3[3], u3[3];   // J W rows
@@ -139,12 +141,47 @@ struct Geometry {
     float R[3][3];
 };
 
+// ---- near-degenerate footprints in FP64 ----------------------------------------
+// A footprint whose dilated 2D covariance has det < 1e-6 trace^2 (a long thin
+// needle seen across hundreds of pixels) loses its determinant to cancellation
+// in FP32: a' c' ~ b^2, and the undilated determinant a c - b^2 that sets the
+// paid opacity can come out at zero or below. The mixed-precision path
+// recomputes that covariance from the same FP32 Jacobian rows and R diag(s) in
+// FP64 (the products of FP32 factors are exact there), and takes the
+// determinants, the paid opacity and the inverse from it.
+struct WideCovariance {
+    double a2, b, c2;        // the dilated covariance
+    double det, detBefore;   // its determinant, and the undilated one
+};
+
+__device__ __forceinline__ WideCovariance wideCovariance(const float t3[3], const float u3[3], const float M[3][3]) {
+    double ax[3], ay[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        ax[j] = ((double)t3[0] * M[0][j] + (double)t3[1] * M[1][j]) + (double)t3[2] * M[2][j];
+        ay[j] = ((double)u3[0] * M[0][j] + (double)u3[1] * M[1][j]) + (double)u3[2] * M[2][j];
+    }
+    WideCovariance W;
+    const double a = (ax[0] * ax[0] + ax[1] * ax[1]) + ax[2] * ax[2];
+    W.b = (ax[0] * ay[0] + ax[1] * ay[1]) + ax[2] * ay[2];
+    const double c = (ay[0] * ay[0] + ay[1] * ay[1]) + ay[2] * ay[2];
+    W.a2 = a + 0.3;
+    W.c2 = c + 0.3;
+    W.detBefore = a * c - W.b * W.b;
+    W.det = W.a2 * W.c2 - W.b * W.b;
+    return W;
+}
+
 // splat_project.slang:519-757 for one splat (no lens, no shutter, no catcher or
 // sheet; a surfel is drawn as the thin Gaussian it projects to).
+// kWide: the mixed-precision path, which takes near-degenerate footprints
+// through wideCovariance (G.wide set); the plain path's arithmetic is unchanged.
+template <bool kWide = false>
 __device__ __forceinline__ Geometry projectGeometry(const FrameConst& F, const InstanceConst& I, const Gauss& g,
                                                     float opacity) {
     Geometry G;
     G.cull = 0;
+    G.wide = false;
     const float* m = I.m;
     G.tx = ((m[0] * g.px + m[1] * g.py) + m[2] * g.pz) + m[3];
     G.ty = ((m[4] * g.px + m[5] * g.py) + m[6] * g.pz) + m[7];
@@ -205,21 +242,42 @@ __device__ __forceinline__ Geometry projectGeometry(const FrameConst& F, const I
     G.detBefore = G.a * G.c - G.b * G.b;
     const float a2 = G.a + 0.3f, c2 = G.c + 0.3f;
     G.det = a2 * c2 - G.b * G.b;
+    WideCovariance W{};
+    if (kWide && G.det < 1e-6f * ((a2 + c2) * (a2 + c2))) {
+        W = wideCovariance(G.t3, G.u3, G.M);
+        G.wide = true;
+        G.det = W.det > 1e-12 ? (float)W.det : 0.0f;
+        G.detBefore = (float)W.detBefore;
+    }
     if (!(G.det > 1e-12f)) {
         G.cull = kCullDegenerate;
         return G;
     }
-    const float filtered = sqrtf(fmaxf(G.detBefore, 0.0f) / G.det);
+    const float filtered = G.wide ? (float)sqrt(fmax(W.detBefore, 0.0) / W.det)
+                                  : sqrtf(fmaxf(G.detBefore, 0.0f) / G.det);
     G.paid = I.antialias != 0 ? filtered : I.paidAt > 0.0f ? fminf(filtered / I.paidAt, 1.0f) : 1.0f;
     G.alpha = opacity > 1.0f ? opacity : paidOpacity(opacity, G.paid);
     if (!(G.alpha >= kFaint)) {
         G.cull = kCullFaint;
         return G;
     }
-    const float boundDet = a2 * c2 - G.b * G.b;
-    G.ca = c2 / boundDet;
-    G.cb = (-G.b) / boundDet;
-    G.cc = a2 / boundDet;
+    if (G.wide) {
+        G.ca = (float)(W.c2 / W.det);
+        G.cb = (float)(-W.b / W.det);
+        G.cc = (float)(W.a2 / W.det);
+    } else {
+        const float boundDet = a2 * c2 - G.b * G.b;
+        G.ca = c2 / boundDet;
+        G.cb = (-G.b) / boundDet;
+        G.cc = a2 / boundDet;
+    }
+    if (kWide) {
+        // the factored conic: with D the determinant, the conic (c', -b, a') / D
+        // is ca (x + fr y)^2 + fs y^2 with ca = c'/D, fr = -b/c', fs = 1/c'
+        // (fs = cc - cb^2/ca). D is its only input that cancels.
+        G.fr = G.wide ? (float)(-W.b / W.c2) : (-G.b) / c2;
+        G.fs = G.wide ? (float)(1.0 / W.c2) : 1.0f / c2;
+    }
     G.cutoff = G.alpha > 1.0f ? falloffCutoff(G.alpha) : cutoffPower(G.alpha);
     return G;
 }

@@ -495,7 +495,8 @@ class BatchTrainer:
         st = N.BatchStats()
         s = stream if stream is not None else torch.cuda.current_stream()
         check(N.lib().ath_batch_check(self._h, C.byref(st), C.c_void_p(s.cuda_stream)))
-        return dict(pairs=st.pairs, capacity=st.capacity, kept=st.kept, tile=st.tile, block_batch=st.block_batch)
+        return dict(pairs=st.pairs, capacity=st.capacity, kept=st.kept, tile=st.tile, block_batch=st.block_batch,
+                    degenerate=st.degenerate, evaluated=st.evaluated)
 
     def tune(self, params: MixedParams, target, colour, loss, grads: "Params", repeats: int = 3,
              stream: torch.cuda.Stream | None = None) -> dict:
@@ -506,6 +507,18 @@ class BatchTrainer:
         check(N.lib().ath_batch_tune(self._h, C.byref(params._native()), _ptr(target), _ptr(colour), _ptr(loss),
                                      C.byref(g), repeats, C.byref(st), C.c_void_p(s.cuda_stream)))
         return dict(pairs=st.pairs, tile=st.tile, block_batch=st.block_batch, ms_per_step=st.ms_per_step)
+
+    def time_stages(self, params: MixedParams, target, colour, loss, grads: "Params",
+                    stream: torch.cuda.Stream | None = None) -> dict:
+        """ath_batch_time_stages: one step, not captured, with events between its stages (ms)."""
+        g = N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
+        ms = (C.c_float * 7)()
+        s = stream if stream is not None else torch.cuda.current_stream(colour.device)
+        self._keep = (params, target, colour, loss, grads)
+        check(N.lib().ath_batch_time_stages(self._h, C.byref(params._native()), _ptr(target), _ptr(colour),
+                                            _ptr(loss), C.byref(g), ms, C.c_void_p(s.cuda_stream)))
+        names = ("project_emit", "sort", "ranges", "blend", "loss", "blend_adjoint", "project_adjoint")
+        return {n: float(v) for n, v in zip(names, ms)}
 
     def buffers(self) -> dict:
         b = N.BatchBuffers()

@@ -1,14 +1,20 @@
-"""Benchmark of the splat rasteriser on B200.
+"""Benchmark of the splat rasteriser's training step on B200.
 
-Workload: 1.5M clustered Gaussians (SH degree 3), views at 1920x1080 on a
-circular walk of radius 3 around the cloud (vertical fov 60 degrees), 16x16
-tiles, black background. One step draws every view of the batch.
+Workload: 1.5M clustered Gaussians (SH degree 3), 8 views at 1920x1080 a GPU on
+a circular walk of radius 3 around the cloud (vertical fov 60 degrees), black
+background, mean-L2 loss against targets uniform in [0,1]^3.
+
+The headline `value` is the batched mixed-precision step (forward, loss and
+backward of every view, one launch a stage, replayed from a CUDA graph; SH in
+BF16 / FP8 e4m3) in ms a view. The plain FP32 path (one differentiable frame, the
+loss and the backward a view) runs on the same scene and views and is reported
+beside it with the speed-up.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank draws its own batch of views (weak scaling: the views
-are independent, the Gaussians replicated; no collective on the forward path).
-Rank 0 prints one JSON line.
+Under torchrun each rank draws its own views (weak scaling: views are
+independent, the Gaussians replicated) and the gradients are summed over ranks
+with one all-reduce a step. Rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -29,6 +35,11 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(count=1_500_000, width=1920, height=1080, views=8, clustered=True, sh_degree=3, vfov=60.0)
 METRIC = "fwd+bwd ms/view, 1.5M Gaussians 1080p, batched+BF16 vs plain FP32, err<=1e-4"
+
+
+# DRAM bytes a launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# batched kernels, from an ncu capture of this workload (profiles/).
+NCU_TRAFFIC: dict = {}
 
 
 def peaks() -> dict:
@@ -153,7 +164,33 @@ class PlainTrainer:
         return stats
 
 
+def _timed(fn, steps: int, stream, world: int, dev) -> float:
+    """K calls of `fn` between CUDA events on `stream`, a barrier and a
+    synchronize on both sides; ms per call, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    end.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms / steps
+
+
 def run_ours(args) -> dict | None:
+    """The batched mixed-precision step (ath_batch_train_step: every view of the
+    batch in one launch a stage, the step replayed from a CUDA graph) and, beside
+    it, the plain FP32 path one view at a time, on the same scene and views."""
     import torch
     import torch.distributed as dist
 
@@ -171,77 +208,114 @@ def run_ours(args) -> dict | None:
     params = A.Params(*[torch.from_numpy(p[k]).to(dev) for k in ("means", "scales", "quats", "sh")],
                       sh_degree=p["sh_degree"])
     del p
+    mixed = A.MixedParams.from_params(params)
     projs = view_cameras(V, first=rank * V)
+    views = [(proj, W, H) for proj in projs]
     gen = torch.Generator().manual_seed(20261203 + 7 + rank)
-    host_targets = [torch.rand((W * H, 3), generator=gen).pin_memory() for _ in range(V)]
-    dev_targets = [t.to(dev) for t in host_targets]
+    host_target = torch.rand((V * W * H, 3), generator=gen).pin_memory()
+    target = host_target.to(dev)
     stream = torch.cuda.current_stream(dev)
-    trainer = PlainTrainer(params, projs, dev_targets, W, H, dev)
+
+    # ---- the batched mixed-precision step ----------------------------------
+    bt = A.BatchTrainer()
+    bt.set_views(views)
+    colour = torch.empty((bt.pixels, 4), dtype=torch.float32, device=dev)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    # the gradients in one flat buffer, so that a multi-GPU step sums them over
+    # ranks (every rank's views) with one all-reduce
+    n, stride = params.count, int(params.sh.shape[1])
+    flat = torch.zeros(n * (12 + stride), dtype=torch.float32, device=dev)
+    grads = A.Params(flat[:4 * n].view(n, 4), flat[4 * n:8 * n].view(n, 4), flat[8 * n:12 * n].view(n, 4),
+                     flat[12 * n:].view(n, stride), params.sh_degree)
+    tuned = bt.tune(mixed, target, colour, loss, grads, repeats=2)
+
+    def batched_step():
+        bt.step(mixed, target, colour, loss, grads, stream=stream)
+        if world > 1:
+            dist.all_reduce(flat)
 
     for _ in range(args.warmup):
-        trainer.step(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        batched_step()
+    bt.check()
     with ClockSampler(local) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            trainer.step(stream)
-        end.record(stream)
-        torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
+        ms_batched = _timed(batched_step, args.steps, stream, world, dev)
+    stats = bt.check()   # raises if a timed step overflowed its buffers or a wait gave up
+    stages = bt.time_stages(mixed, target, colour, loss, grads, stream=stream)
+    stats = bt.check()
+
+    # e2e through the public API: each step's target images copied in from pinned
+    # host memory (into one of two staging buffers on a copy stream, overlapping
+    # the step before) and moved to the step's target on the compute stream; the
+    # loss read back to pinned host memory.
+    copy = torch.cuda.Stream(dev)
+    staging = [torch.empty_like(target), torch.empty_like(target)]
+    h2d_done = [torch.cuda.Event(), torch.cuda.Event()]
+    moved = [torch.cuda.Event(), torch.cuda.Event()]
+    loss_host = torch.empty(1, dtype=torch.float32, pin_memory=True)
+
+    def upload(k):
+        copy.wait_event(moved[k % 2])
+        with torch.cuda.stream(copy):
+            staging[k % 2].copy_(host_target, non_blocking=True)
+            h2d_done[k % 2].record(copy)
+
+    for e in moved:
+        e.record(stream)
+    torch.cuda.synchronize()
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     torch.cuda.synchronize()
-    ms_per_step = ms / args.steps
-
-    # e2e: through the public API, each step's target images copied in from pinned
-    # host memory (on a copy stream, each view's copy overlapping the views before
-    # it) and the loss read back to the host.
-    copy = torch.cuda.Stream(dev)
-    staged = [torch.empty_like(t) for t in dev_targets]
-    loss_host = torch.empty(1, dtype=torch.float32, pin_memory=True)
     e2e_start, e2e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
     e2e_start.record(stream)
-    for _ in range(args.steps):
-        copy.wait_stream(stream)
-        ready = []
-        for v in range(V):
-            with torch.cuda.stream(copy):
-                staged[v].copy_(host_targets[v], non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(copy)
-            ready.append(ev)
-        trainer.step(stream, targets=staged, ready=ready)
-        loss_host.copy_(trainer.loss, non_blocking=True)
+    copy.wait_stream(stream)
+    upload(0)
+    for k in range(args.steps):
+        if k + 1 < args.steps:
+            upload(k + 1)
+        stream.wait_event(h2d_done[k % 2])
+        target.copy_(staging[k % 2], non_blocking=True)
+        moved[k % 2].record(stream)
+        batched_step()
+        loss_host.copy_(loss, non_blocking=True)
     e2e_end.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e2e_start.elapsed_time(e2e_end) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    loss_batched = float(loss_host.item())
+    del bt, staging
 
-    # per-stage times of one forward (events between the stages, waited for)
+    # ---- the plain FP32 path, one view at a time, same scene and views --------
+    dev_targets = [target[v * W * H:(v + 1) * W * H] for v in range(V)]
+    plain = PlainTrainer(params, projs, dev_targets, W, H, dev)
+    for _ in range(args.warmup):
+        plain.step(stream)
+    ms_plain = _timed(lambda: plain.step(stream), args.steps, stream, world, dev)
     timed = A.RenderSettings(width=W, height=H, time_stages=True)
-    st = trainer.raster.render_params(projs[0], params, timed, trainer.frames, stream=stream)
+    st = plain.raster.render_params(projs[0], params, timed, plain.frames, stream=stream)
     bw0, bw1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    A.l2_loss(trainer.frames.colour, dev_targets[0], trainer.dl, trainer.loss, stream=stream)
+    A.l2_loss(plain.frames.colour, dev_targets[0], plain.dl, plain.loss, stream=stream)
     bw0.record(stream)
-    trainer.raster.backward(trainer.dl, trainer.grads, stream=stream)
+    plain.raster.backward(plain.dl, plain.grads, stream=stream)
     bw1.record(stream)
     torch.cuda.synchronize()
-    stages = {"project_ms": st.project_ms, "emit_ms": st.emit_ms, "sort_and_ranges_ms": st.tile_sort_ms,
-              "blend_ms": st.blend_ms, "backward_ms": bw0.elapsed_time(bw1)}
-    passes = math.ceil((24 + max(1, math.ceil(math.log2(max(2, ((W + 15) // 16) * ((H + 15) // 16)))))) / 8)
-    launches_per_view = 5 + passes + 3   # project, emit, histogram, passes, ranges, blend; loss, 2 backward
-    out = dict(ms_per_step=ms_per_step, views=V * world, stats=st, stages=stages, e2e_ms=e2e_ms,
-               clocks=clocks.summary(), launches=launches_per_view * V * args.steps,
-               sh_words=23, count=params.count, passes=passes, loss=float(loss_host.item()),
-               h2d=sum(t.numel() * 4 for t in host_targets), d2h=4)
+    plain_stages = {"project_ms": st.project_ms, "emit_ms": st.emit_ms, "sort_and_ranges_ms": st.tile_sort_ms,
+                    "blend_ms": st.blend_ms, "backward_ms": bw0.elapsed_time(bw1)}
+
+    T = tuned["tile"]
+    total_tiles = V * ((W + T - 1) // T) * ((H + T - 1) // T)
+    passes = math.ceil((24 + max(1, math.ceil(math.log2(max(2, total_tiles))))) / 8)
+    # the step's launches: begin, projectEmit, histogram, the sort's passes, ranges,
+    # blend, loss, blend adjoint, projection adjoint (and 3 memsets, not kernels)
+    launches = (2 + 1 + passes + 1 + 1 + 1 + 1 + 1) * args.steps
+    out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
+               stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
+               count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4,
+               plain_visible=st.visible, plain_pairs=st.pairs)
     if world > 1:
+        dist.barrier()
         dist.destroy_process_group()
     return out if rank == 0 else None
 
@@ -316,47 +390,62 @@ def main():
     if rank != 0 or res is None:
         return
     P = peaks()
-    st = res["stats"]
-    stages = res["stages"]
+    W, H, V = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["views"]
+    stats, stages = res["stats"], res["stages"]
     dominant = max(stages, key=stages.get)
-    W, H = WORKLOAD["width"], WORKLOAD["height"]
-    # algorithmic bytes a launch, per stage (DESIGN.md states each figure)
-    per_slot_read = 16 + 16 + 16 + 4 * 48      # FP32 training parameters a Gaussian
-    bytes_ = {
-        "project_ms": res["count"] * (per_slot_read + 4 + 4) + st.visible * (48 + 8),
-        "emit_ms": st.visible * (48 + 8 + 8) + st.pairs * 12,
-        "sort_and_ranges_ms": st.pairs * (8 + 24 * res["passes"] + 8 + 8),
+    fp32_peak = 148 * 128 * 2 * P.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    # algorithmic work a launch, per stage (per-unit figures stated in DESIGN.md)
+    mixed_bytes = 16 + 16 + 16 + 24 + 36 + 4          # a Gaussian in the mixed layout
+    work = {
+        "project_emit": ("hbm", res["count"] * mixed_bytes + stats["kept"] * 48 + stats["pairs"] * 8),
+        "sort": ("hbm", stats["pairs"] * (8 + 16 * res["passes"])),
+        "ranges": ("hbm", stats["pairs"] * 8 + stats["pairs"] // 16 * 8),
+        "blend": ("fp32", stats["evaluated"] * 20),
+        "loss": ("hbm", (V * W * H) * (16 + 12 + 16)),
+        "blend_adjoint": ("fp32", stats["evaluated"] * 60),
+        "project_adjoint": ("hbm", res["count"] * (mixed_bytes + 60 * 4) + stats["kept"] * 40),
     }
-    cpu = None if args.no_cpu else cpu_baseline()
-    if dominant in ("blend_ms", "backward_ms"):
-        flops = (cpu["evaluated"] if cpu else st.pairs * 256) * 20
-        achieved = flops / (stages[dominant] * 1e-3) / 1e12
-        fp32_peak = 148 * 128 * 2 * (P.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
-        roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                    "frac": achieved / fp32_peak, "traffic": None,
-                    "kernel": "blendKernel" if dominant == "blend_ms" else "blendBackwardKernel",
-                    "peak_source": "nominal FP32 FMA rate at the measured max SM clock (no FP32 peak is measured)"}
-    else:
-        achieved = bytes_[dominant] / (stages[dominant] * 1e-3) / 1e9
+    bound, amount = work[dominant]
+    secs = stages[dominant] * 1e-3
+    kernel_names = {"project_emit": "projectEmitKernel", "sort": "onesweepKernel", "ranges": "rangesBatchKernel",
+                    "blend": "blendBatchKernel", "loss": "lossBatchKernel", "blend_adjoint": "blendAdjointBatchKernel",
+                    "project_adjoint": "projectAdjointBatchKernel"}
+    if bound == "hbm":
+        achieved = amount / secs / 1e9
         roofline = {"bound": "hbm", "achieved": achieved, "peak": P["hbm_gbs"], "unit": "GB/s",
-                    "frac": achieved / P["hbm_gbs"], "traffic": None, "kernel": dominant,
-                    "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
-    ms_view = res["ms_per_step"] / WORKLOAD["views"]
+                    "frac": achieved / P["hbm_gbs"], "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)"}
+    else:
+        achieved = amount / secs / 1e12
+        roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp32_peak,
+                    "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2) at the measured max SM clock; "
+                                   "no FP32 peak is measured"}
+    roofline["kernel"] = kernel_names[dominant]
+    roofline["traffic"] = NCU_TRAFFIC.get(kernel_names[dominant])
+    roofline["stage_share"] = stages[dominant] / sum(stages.values())
+    cpu = None if args.no_cpu else cpu_baseline()
+    ms_view = res["ms_batched"] / V
     line = {
         "metric": METRIC, "value": ms_view, "unit": "ms/view", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset)",
+        "warmup": args.warmup, "ms_per_step": res["ms_batched"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (SH bf16/e4m3)", "data": "synthetic (seeded; no dataset)",
         "config": {"workload": "clustered-1.5M-1920x1080", "gaussians": WORKLOAD["count"], "width": W, "height": H,
-                   "views_per_gpu": WORKLOAD["views"], "sh_degree": 3, "tile": 16,
-                   "path": "plain FP32, one view at a time: forward, mean-L2 loss, backward",
-                   "loss": "mean L2 against a target uniform in [0,1]^3",
-                   "parallelism": f"views sharded over {world} GPU(s)",
-                   "l2": "inputs larger than L2 (FP32 parameters 360 MB > 126 MB)",
-                   "note": "the batched/mixed-precision path is not in this measurement yet"},
-        "stages_ms": stages, "visible": st.visible, "pairs": st.pairs,
+                   "views_per_gpu": V, "sh_degree": 3, "tile": res["tuned"]["tile"],
+                   "block_batch": res["tuned"]["block_batch"],
+                   "path": "batched mixed-precision step: every view in one launch a stage, replayed from a CUDA "
+                           "graph; forward, mean-L2 loss, backward to FP32 gradients",
+                   "loss": "mean L2 a view against a target uniform in [0,1]^3, summed over views",
+                   "parallelism": f"views sharded over {world} GPU(s), gradients all-reduced"
+                                  if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (records 576 MB, pairs > 100 MB, targets 199 MB > 126 MB)"},
+        "plain_fp32": {"ms_per_view": res["ms_plain"] / V, "speedup": res["ms_plain"] / res["ms_batched"],
+                       "stages_ms": res["plain_stages"],
+                       "path": "ath_raster_render_params + ath_l2_loss + ath_raster_backward a view"},
+        "stages_ms": stages, "pairs": stats["pairs"], "kept": stats["kept"], "evaluated": stats["evaluated"],
+        "degenerate_fp64": stats["degenerate"], "loss": res["loss"],
         "roofline": roofline,
-        "e2e": {"value": res["e2e_ms"] / WORKLOAD["views"], "unit": "ms/view",
-                "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
+        "e2e": {"value": res["e2e_ms"] / V, "unit": "ms/view", "h2d_bytes_per_step": res["h2d"],
+                "d2h_bytes_per_step": res["d2h"]},
         "gpu_launches": res["launches"],
         "clocks": res["clocks"],
     }

@@ -263,6 +263,8 @@ typedef struct {
     uint32_t kept;         /* (view, Gaussian) records drawn */
     uint32_t tile, block_batch;
     float ms_per_step;     /* ath_batch_tune: the chosen setting's time */
+    uint32_t degenerate;   /* records whose 2D conic was inverted in FP64 (det < 1e-6 trace^2) */
+    uint64_t evaluated;    /* (pixel, record) evaluations of the forward blend */
 } ath_batch_stats;
 
 ath_status ath_batch_create(ath_batch** out);
@@ -294,6 +296,12 @@ ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* stream);
  * block batch in {64, 128, 256}, keeps the fastest and reports it in `best`. */
 ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
                           float* loss, ath_param_grads* grads, uint32_t repeats, ath_batch_stats* best, void* stream);
+
+/* One step as ath_batch_train_step runs it, not captured, with events between
+ * its stages, waited for: ms[] = project+emit, sort, ranges, blend, loss, blend
+ * adjoint, projection adjoint. For measurement. */
+ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
+                                 float* loss, ath_param_grads* grads, float ms[7], void* stream);
 
 /* The last step's sorted pairs and tile ranges, for inspection: device
  * pointers the batch owns, valid until its next step. A pair is

@@ -190,6 +190,15 @@ void orc_render_params_f64(const orc_frame64* f, uint32_t count, const double* m
                            const double* quats, const double* logits, const double* shs, uint32_t shDegree,
                            double* colour, double* depth, int threads);
 
+/* orc_render_params_f64 from the FP32 training layout as the GPU holds it
+ * (means x y z logit, log scales, quaternion w x y z, each 4 floats a splat; SH
+ * rows of `shStride` floats), with orc_render_f64's near-decision flags and
+ * tile sampling: the image-error check of the mixed-precision path at scale. */
+void orc_render_params_sampled_f64(const orc_frame64* f, uint32_t count, const float* means, const float* scales,
+                                   const float* quats, const float* sh, uint32_t shStride, uint32_t shDegree,
+                                   double* colour, double* depth, uint8_t* nearDecision, double margin,
+                                   uint32_t tileStride, uint32_t tileOffset, int threads);
+
 /* Central finite differences (step eps) of L = mean over pixels and r g b of
  * (colour - target)^2, in double, for the Gaussians `which`: out[k*59 + j] for
  * parameter j of which[k] in the order means x y z, logit, log scales x y z,

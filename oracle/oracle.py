@@ -116,6 +116,9 @@ def lib():
                                      C.c_uint32, C.c_uint32, C.c_int]
         L.orc_render_params_f64.argtypes = [C.POINTER(Frame64), C.c_uint32, _P, _P, _P, _P, _P, C.c_uint32,
                                             _P, _P, C.c_int]
+        L.orc_render_params_sampled_f64.argtypes = [C.POINTER(Frame64), C.c_uint32, _P, _P, _P, _P, C.c_uint32,
+                                                    C.c_uint32, _P, _P, _P, C.c_double, C.c_uint32, C.c_uint32,
+                                                    C.c_int]
         _lib = L
     return _lib
 
@@ -378,4 +381,20 @@ def render_f64(f: Frame64, positions, shape, sh, *, margin=1e-5, tile_stride=1, 
     lib().orc_render_f64(C.byref(f), n, _ptr(np.ascontiguousarray(positions, np.float32)),
                          _ptr(np.ascontiguousarray(shape, np.uint32)), _ptr(np.ascontiguousarray(sh, np.uint32)),
                          _ptr(colour), _ptr(depth), _ptr(near), margin, tile_stride, tile_offset, threads)
+    return dict(colour=colour, depth=depth, near=near)
+
+
+def render_params_sampled_f64(f: Frame64, means, scales, quats, sh, sh_degree, *, margin=1e-5, tile_stride=1,
+                              tile_offset=0, threads=0):
+    """FP32 training parameters ((N,4) means+logit, (N,4) log scales, (N,4) wxyz,
+    (N,stride) SH) rendered in FP64; pixels of unsampled tiles stay NaN."""
+    w, h = f.width, f.height
+    colour = np.full((h * w, 4), np.nan, np.float64)
+    depth = np.full(h * w, np.nan, np.float64)
+    near = np.zeros(h * w, np.uint8)
+    sh = np.ascontiguousarray(sh, np.float32)
+    lib().orc_render_params_sampled_f64(
+        C.byref(f), means.shape[0], _ptr(np.ascontiguousarray(means, np.float32)),
+        _ptr(np.ascontiguousarray(scales, np.float32)), _ptr(np.ascontiguousarray(quats, np.float32)), _ptr(sh),
+        sh.shape[1], sh_degree, _ptr(colour), _ptr(depth), _ptr(near), margin, tile_stride, tile_offset, threads)
     return dict(colour=colour, depth=depth, near=near)

@@ -382,6 +382,41 @@ void orc_render_params_f64(const orc_frame64* f, uint32_t count, const double* m
     blend64(*f, fr, colour, depth, nullptr, 0.0, 1, 0, threads);
 }
 
+void orc_render_params_sampled_f64(const orc_frame64* f, uint32_t count, const float* means, const float* scales,
+                                   const float* quats, const float* sh, uint32_t shStride, uint32_t shDegree,
+                                   double* colour, double* depth, uint8_t* nearDecision, double margin,
+                                   uint32_t tileStride, uint32_t tileOffset, int threads) {
+    Frame64 fr;
+    fr.recs.resize(count);
+#pragma omp parallel for schedule(static, 4096) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (int64_t ii = 0; ii < (int64_t)count; ++ii) {
+        const uint32_t i = (uint32_t)ii;
+        Gauss64 g{};
+        for (int k = 0; k < 3; ++k) {
+            g.p[k] = means[(size_t)i * 4 + k];
+            g.scale[k] = std::exp((double)scales[(size_t)i * 4 + k]);
+        }
+        g.opacity = sigmoid(means[(size_t)i * 4 + 3]);
+        const float* q = quats + (size_t)i * 4;   // w x y z
+        const double qw = q[0], qx = q[1], qy = q[2], qz = q[3];
+        const double n = std::sqrt(qw * qw + qx * qx + qy * qy + qz * qz);
+        g.q[0] = qx / n;
+        g.q[1] = qy / n;
+        g.q[2] = qz / n;
+        g.q[3] = qw / n;
+        const float* c = sh + (size_t)i * shStride;
+        for (int k = 0; k < 3; ++k) g.base[k] = 0.5 + kSH0 * (double)c[k];
+        const uint32_t bases = shDegree >= 3 ? 15 : shDegree == 2 ? 8 : shDegree == 1 ? 3 : 0;
+        for (uint32_t b = 0; b < bases && 3 + b * 3 + 2 < shStride; ++b)
+            for (int ch = 0; ch < 3; ++ch) g.rest[b][ch] = c[3 + b * 3 + ch];
+        g.degree = shDegree;
+        fr.recs[i] = project64(*f, g, margin);
+        fr.recs[i].slot = i;
+    }
+    bin64(*f, fr, margin, tileStride == 0 ? 1 : tileStride, tileOffset);
+    blend64(*f, fr, colour, depth, nearDecision, margin, tileStride == 0 ? 1 : tileStride, tileOffset, threads);
+}
+
 }   // extern "C"
 
 // ---------------------------------------------------------------------------
