@@ -2,14 +2,15 @@
 
 The kernels live in libathenea_b200.so (csrc/, built by _build.py); this
 package is the Python mirror of the reference's rasteriser interface over its
-C ABI (include/athenea_raster.h).
+C ABI (include/athenea_raster.h), plus the training path the reference does
+not have: differentiable frames (Params, TileRasterizer.render_params /
+backward) and the batched mixed-precision step (MixedParams, BatchTrainer).
 """
 from ._native import AtheneaError  # noqa: F401
-from .raster import (Camera, CloudLoader, FrameStats, GpuSplats, Lens, Params, RenderSettings,  # noqa: F401
-                     RenderTargets, SplatCounters, SplatEdit, SplatInstance, TileRasterizer, encoding_3dgs, l2_loss,
-                     pinhole_for_vertical_fov)
+from .raster import (BatchTrainer, Camera, CloudLoader, FrameStats, GpuSplats, Lens, MixedParams,  # noqa: F401
+                     Params, RenderSettings, RenderTargets, SplatCounters, SplatEdit, SplatInstance, TileRasterizer,
+                     encoding_3dgs, l2_loss, pinhole_for_vertical_fov)
 
-__all__ = ["AtheneaError", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "Params", "l2_loss",
-           "RenderSettings",
-           "RenderTargets", "SplatCounters", "SplatEdit", "SplatInstance", "TileRasterizer", "encoding_3dgs",
-           "pinhole_for_vertical_fov"]
+__all__ = ["AtheneaError", "BatchTrainer", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "MixedParams",
+           "Params", "RenderSettings", "RenderTargets", "SplatCounters", "SplatEdit", "SplatInstance",
+           "TileRasterizer", "encoding_3dgs", "l2_loss", "pinhole_for_vertical_fov"]

@@ -76,3 +76,11 @@ def test_without_a_device_create_fails_loudly(native):
     status = native.lib().ath_raster_create(C.byref(h))
     assert status == 6 and not h.value   # DeviceFailure, no handle
     assert len(native.lib().ath_last_error_message()) > 0
+
+
+def test_the_package_exports_what_bench_and_tests_use():
+    import athenea_b200 as A
+    for name in A.__all__:
+        assert hasattr(A, name), name
+    for name in ("BatchTrainer", "MixedParams", "Params", "TileRasterizer", "l2_loss", "pinhole_for_vertical_fov"):
+        assert name in A.__all__, name
