@@ -227,7 +227,11 @@ def run_ours(args) -> dict | None:
     flat = torch.zeros(n * (12 + stride), dtype=torch.float32, device=dev)
     grads = A.Params(flat[:4 * n].view(n, 4), flat[4 * n:8 * n].view(n, 4), flat[8 * n:12 * n].view(n, 4),
                      flat[12 * n:].view(n, stride), params.sh_degree)
-    tuned = bt.tune(mixed, target, colour, loss, grads, repeats=2)
+    if args.tile:
+        bt.set_tuning(args.tile, args.block_batch)
+        tuned = {"tile": args.tile, "block_batch": args.block_batch}
+    else:
+        tuned = bt.tune(mixed, target, colour, loss, grads, repeats=2)
 
     def batched_step():
         bt.step(mixed, target, colour, loss, grads, stream=stream)
@@ -288,21 +292,23 @@ def run_ours(args) -> dict | None:
     del bt, staging
 
     # ---- the plain FP32 path, one view at a time, same scene and views --------
-    dev_targets = [target[v * W * H:(v + 1) * W * H] for v in range(V)]
-    plain = PlainTrainer(params, projs, dev_targets, W, H, dev)
-    for _ in range(args.warmup):
-        plain.step(stream)
-    ms_plain = _timed(lambda: plain.step(stream), args.steps, stream, world, dev)
-    timed = A.RenderSettings(width=W, height=H, time_stages=True)
-    st = plain.raster.render_params(projs[0], params, timed, plain.frames, stream=stream)
-    bw0, bw1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    A.l2_loss(plain.frames.colour, dev_targets[0], plain.dl, plain.loss, stream=stream)
-    bw0.record(stream)
-    plain.raster.backward(plain.dl, plain.grads, stream=stream)
-    bw1.record(stream)
-    torch.cuda.synchronize()
-    plain_stages = {"project_ms": st.project_ms, "emit_ms": st.emit_ms, "sort_and_ranges_ms": st.tile_sort_ms,
-                    "blend_ms": st.blend_ms, "backward_ms": bw0.elapsed_time(bw1)}
+    ms_plain, plain_stages = None, None
+    if not args.no_plain:
+        dev_targets = [target[v * W * H:(v + 1) * W * H] for v in range(V)]
+        plain = PlainTrainer(params, projs, dev_targets, W, H, dev)
+        for _ in range(args.warmup):
+            plain.step(stream)
+        ms_plain = _timed(lambda: plain.step(stream), args.steps, stream, world, dev)
+        timed = A.RenderSettings(width=W, height=H, time_stages=True)
+        st = plain.raster.render_params(projs[0], params, timed, plain.frames, stream=stream)
+        bw0, bw1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        A.l2_loss(plain.frames.colour, dev_targets[0], plain.dl, plain.loss, stream=stream)
+        bw0.record(stream)
+        plain.raster.backward(plain.dl, plain.grads, stream=stream)
+        bw1.record(stream)
+        torch.cuda.synchronize()
+        plain_stages = {"project_ms": st.project_ms, "emit_ms": st.emit_ms, "sort_and_ranges_ms": st.tile_sort_ms,
+                        "blend_ms": st.blend_ms, "backward_ms": bw0.elapsed_time(bw1)}
 
     T = tuned["tile"]
     total_tiles = V * ((W + T - 1) // T) * ((H + T - 1) // T)
@@ -312,8 +318,7 @@ def run_ours(args) -> dict | None:
     launches = (2 + 1 + passes + 1 + 1 + 1 + 1 + 1) * args.steps
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
                stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
-               count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4,
-               plain_visible=st.visible, plain_pairs=st.pairs)
+               count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -359,6 +364,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--views", type=int, default=WORKLOAD["views"], help="views a GPU draws a step")
     ap.add_argument("--gaussians", type=int, default=WORKLOAD["count"], help="Gaussians in the scene")
+    ap.add_argument("--tile", type=int, choices=[8, 16, 32], default=0,
+                    help="fix the batched step's tile size instead of autotuning")
+    ap.add_argument("--block-batch", type=int, choices=[64, 128, 256], default=256,
+                    help="records a block stages at once, with --tile")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     args = ap.parse_args()
     WORKLOAD["views"] = args.views
     WORKLOAD["count"] = args.gaussians
@@ -438,9 +448,10 @@ def main():
                    "parallelism": f"views sharded over {world} GPU(s), gradients all-reduced"
                                   if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (records 576 MB, pairs > 100 MB, targets 199 MB > 126 MB)"},
-        "plain_fp32": {"ms_per_view": res["ms_plain"] / V, "speedup": res["ms_plain"] / res["ms_batched"],
-                       "stages_ms": res["plain_stages"],
-                       "path": "ath_raster_render_params + ath_l2_loss + ath_raster_backward a view"},
+        "plain_fp32": None if res["ms_plain"] is None else {
+            "ms_per_view": res["ms_plain"] / V, "speedup": res["ms_plain"] / res["ms_batched"],
+            "stages_ms": res["plain_stages"],
+            "path": "ath_raster_render_params + ath_l2_loss + ath_raster_backward a view, same scene and views"},
         "stages_ms": stages, "pairs": stats["pairs"], "kept": stats["kept"], "evaluated": stats["evaluated"],
         "degenerate_fp64": stats["degenerate"], "loss": res["loss"],
         "roofline": roofline,

@@ -248,7 +248,10 @@ void blend64(const orc_frame64& f, const Frame64& fr, double* colour, double* de
                     for (int k = 0; k < 3; ++k) rgb[k] += weight * r.colour[k];
                     depthSum += weight * r.z;
                     T *= 1.0 - alpha;
-                    if (std::fabs(T - 1e-4) <= margin * 1e-4) nearD = true;
+                    // T is a product of as many factors as the walk has blended, each
+                    // rounded in FP32 on the GPU: its relative error grows with their
+                    // count, so the stop at T = 1e-4 is flagged within a relative 1e-3
+                    if (margin > 0.0 && std::fabs(T - 1e-4) <= std::max(margin, 1e-3) * 1e-4) nearD = true;
                     if (T < 1e-4) break;
                 }
                 const size_t at = (size_t)py * f.width + px;

@@ -5,9 +5,11 @@ the SH as the mixed layout holds them (BF16 DC and band 1, FP8 e4m3 bands 2-3
 times a per-Gaussian scale), dequantised to FP32, then taken to double. So the
 error below is the arithmetic's: the fast exponential, FMA contraction, FP32
 accumulation and the factored conic. It is the largest absolute difference over
-r g b a of every sampled pixel whose FP64 walk takes no decision within a
-relative 1e-5 of its threshold (the cutoff, alpha = 1/255 and 0.99, T = 1e-4),
-where a rounding can move a whole splat in or out of the pixel. PSNR (peak 1)
+r g b a of every sampled pixel whose FP64 walk takes no decision near its
+threshold (the cutoff, alpha = 1/255 and 0.99 within a relative 1e-5; the stop
+at T = 1e-4 within a relative 1e-3, T being a product of as many FP32 factors
+as the walk blends), where a rounding can move a whole splat in or out of the
+pixel. PSNR (peak 1)
 is over all sampled pixels, near decisions included. What the quantisation
 itself does to the image (FP64 of the FP32 coefficients against FP64 of the
 stored ones) is printed beside it.
@@ -88,8 +90,10 @@ def _errors(img, ref):
     clear = sampled & (ref["near"] == 0)
     diff = np.abs(img.astype(np.float64) - ref["colour"])
     mse = float(np.mean(diff[sampled] ** 2))
+    worst = np.where(clear)[0][np.argmax(diff[clear].max(axis=1))]
     return dict(max_abs=float(diff[clear].max()), psnr=10 * math.log10(1.0 / max(mse, 1e-30)),
-                sampled=int(sampled.sum()), near=float(1.0 - clear.sum() / max(sampled.sum(), 1)))
+                sampled=int(sampled.sum()), near=float(1.0 - clear.sum() / max(sampled.sum(), 1)),
+                worst_pixel=int(worst), worst_fp64_T=float(1.0 - ref["colour"][worst, 3]))
 
 
 @pytest.mark.parametrize("name", list(CASES))
