@@ -1,8 +1,10 @@
 """Builds libathenea_b200.so in-tree: every .cu under csrc/ for sm_100a.
 
-The kernels of the plain path build with --fmad=false (no a*b+c is fused
-unless the source says fmaf), which is what lets them match the CPU
-restatement bit for bit.
+The kernels build with --fmad=false (no a*b+c is fused unless the source says
+fmaf), which is what lets the plain path and the batched path's geometry match
+the CPU restatement bit for bit. The files in CONTRACTED hold only arithmetic
+that has no bit-exact counterpart (the batched path's blends) and build with
+FMA contraction.
 """
 from __future__ import annotations
 
@@ -17,7 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libathenea_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--fmad=false", "-I", os.path.join(HERE, "..", "include")]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-I", os.path.join(HERE, "..", "include")]
+CONTRACTED = {"batch_blend.cu"}
 
 
 def nvcc() -> str:
@@ -37,7 +40,8 @@ def _compile(src: str, extra: list[str]) -> str:
     deps.append(os.path.join(HERE, "..", "include", "athenea_raster.h"))
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
         return obj
-    cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", src, "-o", obj]
+    fmad = "--fmad=true" if os.path.basename(src) in CONTRACTED else "--fmad=false"
+    cmd = [nvcc(), *ARCH, *COMMON, fmad, *extra, "-c", src, "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n{res.stdout}\n{res.stderr}")

@@ -1,0 +1,417 @@
+// The batched path's blends: the persistent forward over every view's tiles and
+// its adjoint. This file builds with FMA contraction (the other kernels of the
+// plain and batched paths do not): nothing here has to match the reference's
+// FP32 to the bit, only the forward and the adjoint each other, and both are
+// compiled alike. Which records a pixel blends is decided per pixel, the same
+// way in both, whatever the tile size.
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "batch_kernels.cuh"
+
+namespace ath {
+namespace {
+
+// ---- the persistent blend ------------------------------------------------------
+// One block of T*T/2 threads takes tiles off a queue. Warp w owns an 8x8 box of
+// the tile and each lane two pixels of it, (x, y) and (x, y + 4). Staging a
+// batch of records, the block marks for each record the boxes its footprint can
+// reach (a conservative test: the box's least power against the cutoff, with a
+// margin); a warp then walks only the records marked for its box, found 32 at a
+// time by a ballot, in list order. A pixel blends exactly the records it would
+// blend walking the whole list: the per-pixel test decides, the box test only
+// skips records no pixel of the box can pass. So the image does not depend on
+// the tile size.
+constexpr uint32_t kBox = 8;
+
+// The footprint's half extents from the factored conic: the covariance's
+// diagonal a' = cutoff (1/ca + fr^2/fs) and c' = cutoff / fs.
+__device__ __forceinline__ void footprintExtent(float ca, float fr, float fs, float cutoff, float& ex, float& ey) {
+    ex = ca > 0.0f && fs > 0.0f ? sqrtf(cutoff * (1.0f / ca + (fr * fr) / fs)) * 1.0001f + 1e-3f : 3.4e38f;
+    ey = fs > 0.0f ? sqrtf(cutoff / fs) * 1.0001f + 1e-3f : 3.4e38f;
+}
+
+// Bit b set when box b of the tile (boxes row-major, T/8 a row) meets the
+// footprint's bounding box: the boxes whose pixel-centre columns and rows
+// overlap [cx - ex, cx + ex] x [cy - ey, cy + ey]. Conservative: the extents
+// carry a margin over the per-pixel test's rounding.
+template <uint32_t T>
+__device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 screen, float ca, float fr, float fs) {
+    constexpr int kAcross = (int)(T / kBox);
+    float ex, ey;
+    footprintExtent(ca, fr, fs, screen.w, ex, ey);
+    // box column b holds pixel centres tileX0 + 8 b + 0.5 .. tileX0 + 8 b + 7.5
+    const float x0 = (screen.x - ex) - (tileX0 + 0.5f), x1 = (screen.x + ex) - (tileX0 + 0.5f);
+    const float y0 = (screen.y - ey) - (tileY0 + 0.5f), y1 = (screen.y + ey) - (tileY0 + 0.5f);
+    const float lim = (float)kAcross;
+    const int bx0 = (int)ceilf(clampf((x0 - 7.0f) * 0.125f, -1.0f, lim));
+    const int bx1 = (int)floorf(clampf(x1 * 0.125f, -1.0f, lim));
+    const int by0 = (int)ceilf(clampf((y0 - 7.0f) * 0.125f, -1.0f, lim));
+    const int by1 = (int)floorf(clampf(y1 * 0.125f, -1.0f, lim));
+    const int cx0 = max(bx0, 0), cx1 = min(bx1, kAcross - 1), cy0 = max(by0, 0), cy1 = min(by1, kAcross - 1);
+    if (cx0 > cx1 || cy0 > cy1) return 0u;
+    const uint32_t row = ((1u << (cx1 - cx0 + 1)) - 1u) << cx0;
+    uint32_t mask = 0;
+#pragma unroll
+    for (int r = 0; r < kAcross; ++r)
+        if (r >= cy0 && r <= cy1) mask |= row << (r * kAcross);
+    return mask;
+}
+
+template <uint32_t T, uint32_t NB>
+__global__ void __launch_bounds__(T * T / 2)
+    blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
+                     const uint64_t* __restrict__ pairs, const float4* __restrict__ recs,
+                     float4* __restrict__ colour, float* __restrict__ depth, float* __restrict__ finalT,
+                     uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ words) {
+    constexpr uint32_t kThreads = T * T / 2;
+    constexpr uint32_t kAcross = T / kBox;
+    __shared__ float4 sScreen[NB];
+    __shared__ float4 sConic[NB];
+    __shared__ float4 sColour[NB];
+    __shared__ uint32_t sMask[NB];
+    __shared__ uint32_t sTileBase[kMaxBatchViews];
+    __shared__ uint32_t sTile;
+    for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
+    const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
+    const float kL2e = 1.4426950408889634f;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
+    uint32_t evaluated = 0;   // (pixel, record) evaluations this thread made
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) sTile = atomicAdd(&words[kBatchBlendTicket], 1u);
+        __syncthreads();
+        const uint32_t tile = sTile;
+        if (tile >= B.totalTiles) break;
+        const uint32_t v = viewOf(sTileBase, B.views, tile);
+        const BatchView& V = views[v];
+        const uint32_t local = tile - V.tileBase;
+        const uint32_t tx = local % V.tilesX, ty = local / V.tilesX;
+        const float tileX0 = (float)(tx * T), tileY0 = (float)(ty * T);
+        const uint32_t px = tx * T + lx, py[2] = {ty * T + ly, ty * T + ly + 4};
+        const uint2 range = ranges[tile];
+        const float pxc = (float)px + 0.5f;
+        const size_t recBase = (size_t)v * B.count;
+        float r[2] = {0.0f, 0.0f}, g[2] = {0.0f, 0.0f}, bl[2] = {0.0f, 0.0f}, Tr[2] = {1.0f, 1.0f};
+        float depthSum[2] = {0.0f, 0.0f};
+        uint32_t last[2] = {0, 0};
+        bool done[2];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) done[p] = !(px < V.width && py[p] < V.height);
+        for (uint32_t first = range.x; first < range.y; first += NB) {
+            if (__syncthreads_count(done[0] && done[1]) == kThreads) break;
+            const uint32_t count = min(NB, range.y - first);
+            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
+                const size_t s = (recBase + (pairs[first + k] & slotMask)) * 3;
+                const float4 sc = recs[s + 0];
+                const float4 c = recs[s + 1];
+                sScreen[k] = sc;
+                // the factored conic's two weights pre-scaled by -log2(e)/2:
+                // power in base-2 exponent units
+                sConic[k] = make_float4(c.x * (-0.5f * kL2e), c.y, c.z * (-0.5f * kL2e), c.w);
+                sColour[k] = recs[s + 2];
+                sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
+            }
+            __syncthreads();
+            if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) continue;
+            for (uint32_t base = 0; base < count; base += 32) {
+                const uint32_t m = base + lane < count ? sMask[base + lane] : 0u;
+                uint32_t todo = __ballot_sync(0xFFFFFFFFu, (m >> warp) & 1u);
+                while (todo) {
+                    const uint32_t j = base + (uint32_t)__ffs(todo) - 1u;
+                    todo &= todo - 1u;
+                    const float4 sc = sScreen[j];
+                    const float4 k = sConic[j];
+                    const float dx = pxc - sc.x;
+#pragma unroll
+                    for (int p = 0; p < 2; ++p) {
+                        if (done[p]) continue;
+                        ++evaluated;
+                        const float dy = ((float)py[p] + 0.5f) - sc.y;
+                        // e = -log2(e)/2 * power; power > cutoff  <=>  e < -log2(e)/2 * cutoff
+                        const float t = __fmaf_rn(k.y, dy, dx);
+                        const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
+                        if (e < (-0.5f * kL2e) * sc.w) continue;
+                        const float alpha = fminf(0.99f, k.w * fastExp2(e));
+                        if (alpha < kFaint) continue;
+                        const float w = Tr[p] * alpha;
+                        const float4 c = sColour[j];
+                        r[p] = __fmaf_rn(w, c.x, r[p]);
+                        g[p] = __fmaf_rn(w, c.y, g[p]);
+                        bl[p] = __fmaf_rn(w, c.z, bl[p]);
+                        depthSum[p] = __fmaf_rn(w, sc.z, depthSum[p]);
+                        Tr[p] = Tr[p] * (1.0f - alpha);
+                        last[p] = first - range.x + j + 1;
+                        if (Tr[p] < 1e-4f) done[p] = true;
+                    }
+                }
+                if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            if (!(px < V.width && py[p] < V.height)) continue;
+            const uint32_t at = V.pixelBase + py[p] * V.width + px;
+            const float coverage = 1.0f - Tr[p];
+            colour[at] = make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1], bl[p] + Tr[p] * B.bg[2],
+                                     coverage + Tr[p] * B.bg[3]);
+            if (depth) depth[at] = coverage > 1e-6f ? depthSum[p] / coverage : 0.0f;
+            finalT[at] = Tr[p];
+            lastContrib[at] = last[p];
+        }
+    }
+    uint64_t e = evaluated;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
+    if (lane == 0 && e)
+        atomicAdd(reinterpret_cast<unsigned long long*>(words + kBatchEvaluated), (unsigned long long)e);
+}
+
+// Nine values summed over a warp: the first eight by a transposed reduction
+// (each level sends half of the values still held and keeps the other half,
+// so three levels leave value (lane >> 2) spread over lanes differing in their
+// two low bits), the ninth by a butterfly. Lanes with lane % 4 == 0 hold value
+// lane >> 2; every lane holds the ninth.
+__device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int half = 4, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
+        const bool upper = (lane & (uint32_t)bit) != 0;
+#pragma unroll
+        for (int k = 0; k < half; ++k) {
+            const float send = upper ? v[k] : v[k + half];
+            const float keep = upper ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, bit);
+        }
+    }
+    float s = v[0];
+    s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
+    s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
+    float n = v[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
+    ninth = n;
+    return s;
+}
+
+// ---- the blend's adjoint, over the same tile queue ------------------------------
+// The forward's warp boxes and masks, walked in reverse: a warp takes the records
+// marked for its box from its pixels' last contributor down, each lane its two
+// pixels' terms summed before the warp reduction.
+template <uint32_t T, uint32_t NB>
+__global__ void __launch_bounds__(T * T / 2)
+    blendAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
+                            const uint64_t* __restrict__ pairs, const float4* __restrict__ recs,
+                            const float* __restrict__ finalT, const uint32_t* __restrict__ lastContrib,
+                            const float4* __restrict__ dLdColour, float* __restrict__ grads,
+                            uint32_t* __restrict__ words) {
+    constexpr uint32_t kThreads = T * T / 2;
+    constexpr uint32_t kAcross = T / kBox;
+    constexpr uint32_t kWords = 9;   // centre x y, conic a b c, alpha, colour r g b (no depth loss)
+    __shared__ float4 sScreen[NB];
+    __shared__ float4 sConic[NB];
+    __shared__ float4 sColour[NB];
+    __shared__ uint32_t sRec[NB];
+    __shared__ uint32_t sMask[NB];
+    __shared__ float sAcc[NB * kWords];
+    __shared__ uint32_t sTileBase[kMaxBatchViews];
+    __shared__ uint32_t sTile, sMaxLast;
+    for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
+    const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
+    const float kL2e = 1.4426950408889634f;
+    const float kUnscale = -2.0f / kL2e;   // undoes the -log2(e)/2 pre-scale (for the gradients only)
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sTile = atomicAdd(&words[kBatchBackTicket], 1u);
+            sMaxLast = 0;
+        }
+        __syncthreads();
+        const uint32_t tile = sTile;
+        if (tile >= B.totalTiles) break;
+        const uint32_t v = viewOf(sTileBase, B.views, tile);
+        const BatchView& V = views[v];
+        const uint32_t local = tile - V.tileBase;
+        const uint32_t tx = local % V.tilesX, ty = local / V.tilesX;
+        const float tileX0 = (float)(tx * T), tileY0 = (float)(ty * T);
+        const uint32_t px = tx * T + lx, py[2] = {ty * T + ly, ty * T + ly + 4};
+        const uint2 range = ranges[tile];
+        const float pxc = (float)px + 0.5f;
+        float Tr[2], S[2][3], dC[2][3], dAlphaOut[2];
+        uint32_t last[2];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const bool inside = px < V.width && py[p] < V.height;
+            const uint32_t at = inside ? V.pixelBase + py[p] * V.width + px : 0u;
+            Tr[p] = inside ? finalT[at] : 1.0f;
+            last[p] = inside ? min(lastContrib[at], range.y - range.x) : 0u;
+            const float4 d = inside ? dLdColour[at] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            dC[p][0] = d.x; dC[p][1] = d.y; dC[p][2] = d.z;
+            dAlphaOut[p] = d.w * Tr[p] * (1.0f - B.bg[3]);
+            S[p][0] = B.bg[0]; S[p][1] = B.bg[1]; S[p][2] = B.bg[2];
+        }
+        const uint32_t warpLast = __reduce_max_sync(0xFFFFFFFFu, max(last[0], last[1]));
+        if (lane == 0 && warpLast) atomicMax(&sMaxLast, warpLast);
+        __syncthreads();
+        const uint32_t end = range.x + sMaxLast;
+        const size_t recBase = (size_t)v * B.count;
+        for (uint32_t batchEnd = end; batchEnd > range.x;) {
+            const uint32_t batchStart = batchEnd - range.x > NB ? batchEnd - NB : range.x;
+            const uint32_t count = batchEnd - batchStart;
+            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
+                const uint32_t s = (uint32_t)(pairs[batchStart + k] & slotMask);
+                sRec[k] = s;
+                const size_t q = (recBase + s) * 3;
+                const float4 sc = recs[q + 0];
+                const float4 c = recs[q + 1];
+                sScreen[k] = sc;
+                // the forward's pre-scale, operation for operation (so the same records pass)
+                sConic[k] = make_float4(c.x * (-0.5f * kL2e), c.y, c.z * (-0.5f * kL2e), c.w);
+                sColour[k] = recs[q + 2];
+                sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
+            }
+            for (uint32_t k = threadIdx.x; k < count * kWords; k += kThreads) sAcc[k] = 0.0f;
+            __syncthreads();
+            const uint32_t relStart = batchStart - range.x;
+            if (relStart < warpLast) {
+                for (int base = (int)((count - 1) & ~31u); base >= 0; base -= 32) {
+                    if (relStart + (uint32_t)base >= warpLast) continue;
+                    const uint32_t m = (uint32_t)base + lane < count ? sMask[base + lane] : 0u;
+                    uint32_t todo = __ballot_sync(0xFFFFFFFFu, (m >> warp) & 1u);
+                    while (todo) {
+                        const uint32_t hb = 31u - (uint32_t)__clz(todo);
+                        todo &= ~(1u << hb);
+                        const uint32_t j = (uint32_t)base + hb;
+                        const uint32_t rel = relStart + j;
+                        if (rel >= warpLast) continue;
+                        const float4 sc = sScreen[j];
+                        const float4 k = sConic[j];
+                        const float4 c = sColour[j];
+                        const float dx = pxc - sc.x;
+                        float gv[kWords];
+#pragma unroll
+                        for (int q = 0; q < (int)kWords; ++q) gv[q] = 0.0f;
+                        bool live = false;
+#pragma unroll
+                        for (int p = 0; p < 2; ++p) {
+                            if (rel >= last[p]) continue;
+                            const float dy = ((float)py[p] + 0.5f) - sc.y;
+                            const float t = __fmaf_rn(k.y, dy, dx);
+                            const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
+                            if (e < (-0.5f * kL2e) * sc.w) continue;
+                            const float G = fastExp2(e);
+                            const float raw = k.w * G;
+                            const float alpha = fminf(0.99f, raw);
+                            if (alpha < kFaint) continue;
+                            live = true;
+                            const float oneMinus = 1.0f - alpha;
+                            const float inv = fastRcp(oneMinus);
+                            const float Tb = Tr[p] * inv;
+                            const float w = Tb * alpha;
+                            gv[6] = __fmaf_rn(w, dC[p][0], gv[6]);
+                            gv[7] = __fmaf_rn(w, dC[p][1], gv[7]);
+                            gv[8] = __fmaf_rn(w, dC[p][2], gv[8]);
+                            const float dAlpha = Tb * ((c.x - S[p][0]) * dC[p][0] + (c.y - S[p][1]) * dC[p][1] +
+                                                       (c.z - S[p][2]) * dC[p][2]) +
+                                                 dAlphaOut[p] * inv;
+                            S[p][0] = __fmaf_rn(alpha, c.x - S[p][0], S[p][0]);
+                            S[p][1] = __fmaf_rn(alpha, c.y - S[p][1], S[p][1]);
+                            S[p][2] = __fmaf_rn(alpha, c.z - S[p][2], S[p][2]);
+                            Tr[p] = Tb;
+                            if (raw < 0.99f && k.w <= 1.0f) {
+                                gv[5] = __fmaf_rn(dAlpha, G, gv[5]);
+                                const float dPower = -0.5f * alpha * dAlpha;
+                                gv[2] = __fmaf_rn(dPower, dx * dx, gv[2]);
+                                gv[3] = __fmaf_rn(dPower, 2.0f * dx * dy, gv[3]);
+                                gv[4] = __fmaf_rn(dPower, dy * dy, gv[4]);
+                                // d power / d centre: -2 (ca dx + cb dy), -2 (cb dx + cc dy)
+                                // in the factored form (cb = ca fr, cc = fs + ca fr^2)
+                                const float at = (k.x * kUnscale) * t;
+                                gv[0] = __fmaf_rn(dPower, -2.0f * at, gv[0]);
+                                gv[1] = __fmaf_rn(dPower, -2.0f * (k.y * at + (k.z * kUnscale) * dy), gv[1]);
+                            }
+                        }
+                        const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, live);
+                        if (!lanes) continue;
+                        float* acc = sAcc + j * kWords;
+                        if ((lanes & (lanes - 1u)) == 0u) {
+                            // one lane live: its terms are the warp's
+                            if (live) {
+#pragma unroll
+                                for (int q = 0; q < (int)kWords; ++q)
+                                    if (gv[q] != 0.0f) atomicAdd(acc + q, gv[q]);
+                            }
+                        } else {
+                            float ninth;
+                            const float s = warpSum9(gv, ninth);
+                            if ((lane & 3u) == 0u && s != 0.0f) atomicAdd(acc + (lane >> 2), s);
+                            if (lane == 0 && ninth != 0.0f) atomicAdd(acc + 8, ninth);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < count * kWords; k += kThreads) {
+                const float s = sAcc[k];
+                if (s != 0.0f) atomicAdd(&grads[(recBase + sRec[k / kWords]) * kGradWords + k % kWords], s);
+            }
+            __syncthreads();   // the next batch's loads overwrite what the flush reads
+            batchEnd = batchStart;
+        }
+    }
+}
+
+
+
+template <typename K>
+int residentGrid(K kernel, int threads, int sms) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0);
+    return (n > 0 ? n : 1) * sms;
+}
+
+template <uint32_t T, uint32_t NB>
+cudaError_t blendWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour) {
+    const int grid = residentGrid(blendBatchKernel<T, NB>, T * T / 2, L.sms);
+    blendBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.recs, colour, nullptr,
+                                                                L.finalT, L.lastContrib, L.words);
+    return cudaGetLastError();
+}
+
+template <uint32_t T, uint32_t NB>
+cudaError_t adjointWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, const float4* dL,
+                        float* grads) {
+    const int grid = residentGrid(blendAdjointBatchKernel<T, NB>, T * T / 2, L.sms);
+    blendAdjointBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.recs, L.finalT,
+                                                                       L.lastContrib, dL, grads, L.words);
+    return cudaGetLastError();
+}
+
+}   // namespace
+
+#define ATH_BLEND_CASES(CALL)                                                                              \
+    CALL(8, 64) CALL(8, 128) CALL(8, 256) CALL(16, 64) CALL(16, 128) CALL(16, 256) CALL(32, 64) CALL(32, 128) \
+    CALL(32, 256)
+
+cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour) {
+#define ATH_CASE(T_, NB_) \
+    if (L.tile == T_ && L.blockBatch == NB_) return blendWith<T_, NB_>(B, L, stream, colour);
+    ATH_BLEND_CASES(ATH_CASE)
+#undef ATH_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launchBatchBlendAdjoint(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream,
+                                    const float4* dLdColour, float* grads) {
+#define ATH_CASE(T_, NB_) \
+    if (L.tile == T_ && L.blockBatch == NB_) return adjointWith<T_, NB_>(B, L, stream, dLdColour, grads);
+    ATH_BLEND_CASES(ATH_CASE)
+#undef ATH_CASE
+    return cudaErrorInvalidValue;
+}
+
+}   // namespace ath

@@ -3,6 +3,8 @@
 
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 #include "gauss.cuh"
 #include "raster_types.cuh"
 #include "splat_math.cuh"
@@ -71,6 +73,29 @@ __device__ __forceinline__ float fastRcp(float x) {
     return y;
 }
 
+// minPowerOverBox for a near-degenerate footprint: the same candidate points,
+// each evaluated in the factored form ca (x + fr y)^2 + fs y^2, which does not
+// cancel however thin the footprint is.
+__device__ __forceinline__ float minPowerOverBoxFactored(float a, float b, float c, float fr, float fs, float lox,
+                                                         float loy, float hix, float hiy) {
+    if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) return 0.0f;
+    float best = 3.4e38f;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        float x, y;
+        if (e < 2) {
+            x = e == 0 ? lox : hix;
+            y = c > 1e-12f ? clampf(((-b) * x) / c, loy, hiy) : loy;
+        } else {
+            y = e == 2 ? loy : hiy;
+            x = a > 1e-12f ? clampf(((-b) * y) / a, lox, hix) : lox;
+        }
+        const float t = x + fr * y;
+        best = fminf(best, (a * t) * t + (fs * y) * y);
+    }
+    return best;
+}
+
 // The view of a global tile or pixel: the last view whose base is at most `x`.
 __device__ __forceinline__ uint32_t viewOf(const uint32_t* bases, uint32_t views, uint32_t x) {
     uint32_t lo = 0, hi = views;
@@ -80,5 +105,24 @@ __device__ __forceinline__ uint32_t viewOf(const uint32_t* bases, uint32_t views
     }
     return lo;
 }
+
+// What the persistent blends of batch_blend.cu need from a batch.
+struct BlendLaunch {
+    const BatchView* views;
+    const uint2* ranges;
+    const uint64_t* pairs;   // sorted
+    const float4* recs;
+    uint32_t* words;
+    float* finalT;
+    uint32_t* lastContrib;
+    int sms;
+    uint32_t tile, blockBatch;
+};
+
+// The forward blend of every view's tiles (colour, final T, last contributor).
+cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour);
+// Its adjoint: dL/d(record) for every (view, Gaussian) record, added into `grads`.
+cudaError_t launchBatchBlendAdjoint(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream,
+                                    const float4* dLdColour, float* grads);
 
 }   // namespace ath

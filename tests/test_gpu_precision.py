@@ -6,10 +6,12 @@ times a per-Gaussian scale), dequantised to FP32, then taken to double. So the
 error below is the arithmetic's: the fast exponential, FMA contraction, FP32
 accumulation and the factored conic. It is the largest absolute difference over
 r g b a of every sampled pixel whose FP64 walk takes no decision near its
-threshold (the cutoff, alpha = 1/255 and 0.99 within a relative 1e-5; the stop
-at T = 1e-4 within a relative 1e-3, T being a product of as many FP32 factors
-as the walk blends), where a rounding can move a whole splat in or out of the
-pixel. PSNR (peak 1)
+threshold, where a rounding can move a whole splat in or out of the pixel: the
+cutoff, alpha = 1/255 and 0.99 within a relative 1e-4 (a footprint's FP32
+centre is a rounding of a pixel coordinate, up to 1.2e-4 px at x = 1920,
+which moves its power at the cutoff by up to about 1e-4 relative); the stop at
+T = 1e-4 within a relative 1e-3 (T is a product of as many FP32 factors as
+the walk blends). PSNR (peak 1)
 is over all sampled pixels, near decisions included. What the quantisation
 itself does to the image (FP64 of the FP32 coefficients against FP64 of the
 stored ones) is printed beside it.
@@ -26,6 +28,7 @@ from athenea_b200 import scenes
 pytestmark = pytest.mark.gpu
 
 TOLERANCE = 1e-4   # max-abs against FP64, pixels clear of a decision
+MARGIN = 1e-4      # the relative window of a decision
 
 # name: (Gaussians, clustered, seed, view sizes, tile stride of the FP64 sample)
 CASES = {
@@ -81,7 +84,7 @@ def _plain_image(P, proj, W, H):
 def _f64(O, proj, W, H, p, sh, stride, offset):
     from tests import gpu_helpers as G
     f64 = O.frame64(G.oracle_projection(O, proj), np.eye(4), W, H, rest_per_colour=15, sh_words=23)
-    return O.render_params_sampled_f64(f64, p["means"], p["scales"], p["quats"], sh, p["sh_degree"], margin=1e-5,
+    return O.render_params_sampled_f64(f64, p["means"], p["scales"], p["quats"], sh, p["sh_degree"], margin=MARGIN,
                                        tile_stride=stride, tile_offset=offset)
 
 
@@ -114,7 +117,7 @@ def test_mixed_precision_image_error_against_fp64(oracle, name):
               f"PSNR {e['psnr']:.1f} dB over {e['sampled']} sampled pixels ({100 * e['near']:.3f}% near a decision); "
               f"quantisation alone: PSNR {q['psnr']:.1f} dB, max-abs {q['max_abs']:.3g}")
         assert e["max_abs"] <= TOLERANCE, (name, v, e)
-        assert e["near"] < 0.01, (name, v, e)
+        assert e["near"] < 0.03, (name, v, e)
     assert stats["degenerate"] == 0   # these scenes hold no near-degenerate footprint
 
 
@@ -158,4 +161,4 @@ def test_near_degenerate_footprints_take_fp64_and_stay_within_tolerance(oracle):
           f"PSNR {e['psnr']:.1f} dB; plain FP32 path on the same footprints: max-abs {plain['max_abs']:.3g}, "
           f"PSNR {plain['psnr']:.1f} dB")
     assert e["max_abs"] <= TOLERANCE, e
-    assert e["near"] < 0.02, e
+    assert e["near"] < 0.05, e
