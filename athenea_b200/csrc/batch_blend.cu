@@ -32,10 +32,12 @@ __device__ __forceinline__ void footprintExtent(float ca, float fr, float fs, fl
     ey = fs > 0.0f ? sqrtf(cutoff / fs) * 1.0001f + 1e-3f : 3.4e38f;
 }
 
-// Bit b set when box b of the tile (boxes row-major, T/8 a row) meets the
-// footprint's bounding box: the boxes whose pixel-centre columns and rows
-// overlap [cx - ex, cx + ex] x [cy - ey, cy + ey]. Conservative: the extents
-// carry a margin over the per-pixel test's rounding.
+// Bit b set when box b of the tile (boxes row-major, T/8 a row) may hold a pixel
+// centre inside the footprint: among the boxes whose pixel-centre columns and
+// rows overlap the footprint's bounding box [cx - ex, cx + ex] x [cy - ey, cy + ey],
+// those whose least power (minPowerOverBoxFactored) is within the cutoff.
+// Conservative: extents and cutoff carry a margin over the per-pixel test's
+// rounding.
 template <uint32_t T>
 __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 screen, float ca, float fr, float fs) {
     constexpr int kAcross = (int)(T / kBox);
@@ -51,11 +53,18 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
     const int by1 = (int)floorf(clampf(y1 * 0.125f, -1.0f, lim));
     const int cx0 = max(bx0, 0), cx1 = min(bx1, kAcross - 1), cy0 = max(by0, 0), cy1 = min(by1, kAcross - 1);
     if (cx0 > cx1 || cy0 > cy1) return 0u;
-    const uint32_t row = ((1u << (cx1 - cx0 + 1)) - 1u) << cx0;
+    const float cb = ca * fr, cc = fs + ca * fr * fr;
+    const float limit = screen.w * 1.0001f + 1e-4f;
     uint32_t mask = 0;
-#pragma unroll
-    for (int r = 0; r < kAcross; ++r)
-        if (r >= cy0 && r <= cy1) mask |= row << (r * kAcross);
+    for (int r = cy0; r <= cy1; ++r) {
+        const float loy = (tileY0 + (float)(r * (int)kBox) + 0.5f) - screen.y;
+        for (int c = cx0; c <= cx1; ++c) {
+            const float lox = (tileX0 + (float)(c * (int)kBox) + 0.5f) - screen.x;
+            const float least = minPowerOverBoxFactored(ca, cb, cc, fr, fs, lox, loy, lox + (float)(kBox - 1),
+                                                        loy + (float)(kBox - 1));
+            if (least <= limit) mask |= 1u << (r * kAcross + c);
+        }
+    }
     return mask;
 }
 
