@@ -165,7 +165,12 @@ Rec64 project64(const orc_frame64& f, const Gauss64& g, double margin) {
         const double v = g.base[k] + rest[k];
         r.colour[k] = f.linearCloud ? std::max(v, 0.0) : srgbToLinear(v);
     }
-    const float zf = (float)tz;
+    // The blend order is the method's, a discrete choice the arithmetic does not
+    // refine: the 24-bit key of the FP32 depth, from the FP32 rows of the object ->
+    // view transform, as the rasteriser computes it (splat_project.slang:519-523,
+    // frame.slang:17-20), then the slot.
+    const float zf = (((float)f.m[8] * (float)g.p[0] + (float)f.m[9] * (float)g.p[1]) + (float)f.m[10] * (float)g.p[2]) +
+                     (float)f.m[11];
     uint32_t bits;
     std::memcpy(&bits, &zf, 4);
     r.key = bits >> 7;
@@ -229,6 +234,7 @@ void blend64(const orc_frame64& f, const Frame64& fr, double* colour, double* de
                 const double pxc = px + 0.5, pyc = py + 0.5;
                 double rgb[3] = {0, 0, 0}, T = 1.0, depthSum = 0.0;
                 bool nearD = false;
+
                 for (uint32_t s : fr.lists[t]) {
                     const Rec64& r = fr.recs[s];
                     const double dx = pxc - r.cx, dy = pyc - r.cy;

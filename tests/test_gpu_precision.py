@@ -11,7 +11,8 @@ cutoff, alpha = 1/255 and 0.99 within a relative 1e-4 (a footprint's FP32
 centre is a rounding of a pixel coordinate, up to 1.2e-4 px at x = 1920,
 which moves its power at the cutoff by up to about 1e-4 relative); the stop at
 T = 1e-4 within a relative 1e-3 (T is a product of as many FP32 factors as
-the walk blends). PSNR (peak 1)
+the walk blends). The blend order is not an arithmetic result but the method's
+choice: both orders follow the FP32 depth key, as the reference computes it. PSNR (peak 1)
 is over all sampled pixels, near decisions included. What the quantisation
 itself does to the image (FP64 of the FP32 coefficients against FP64 of the
 stored ones) is printed beside it.
