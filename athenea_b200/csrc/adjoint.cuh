@@ -90,57 +90,15 @@ struct ParamGrad {
     }
 };
 
-// The projection's adjoint for one Gaussian and one view: dL/d(record) `gw`
-// (gradient words of raster_types.cuh) -> dL/dparameters, added into `acc`.
+// The projection's adjoint past the colour, for one Gaussian and one view:
+// dL/d(record) `gw` -> dL/d(position, opacity logit, log scales, quaternion).
+// `G` is projectGeometry's result for (F, I, g); `dp` holds what the colour's
+// adjoint gave the position and ends, with the geometry's share, in `acc`.
 template <uint32_t L>
-__device__ __forceinline__ void projectAdjoint(const FrameConst& F, const InstanceConst& I, uint32_t i,
-                                               const float gw[kGradWords], ParamGrad& acc) {
-    const Gauss g = loadGauss<L>(I, i);
-    const Geometry G = projectGeometry<L == kLayoutMixed>(F, I, g, g.opacity);
+__device__ __forceinline__ void geometryAdjoint(const FrameConst& F, const InstanceConst& I, uint32_t i, const Gauss& g,
+                                                const Geometry& G, const float gw[kGradWords], float dp[3],
+                                                ParamGrad& acc) {
     const float* m = I.m;
-
-    // ---- colour: c = decode(base + rest(dir)) ------------------------------
-    float dp[3] = {0.0f, 0.0f, 0.0f};
-    const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
-    const float ex = g.px - I.eye[0], ey = g.py - I.eye[1], ez = g.pz - I.eye[2];
-    const float len = sqrtf((ex * ex + ey * ey) + ez * ez);
-    const float dir[3] = {ex / len, ey / len, ez / len};
-    float Y[15], dY[15][3];
-    shBasis(degree, dir[0], dir[1], dir[2], Y, dY);
-    const uint32_t bases = degree == 3 ? 15 : degree == 2 ? 8 : degree == 1 ? 3 : 0;
-    float dDir[3] = {0.0f, 0.0f, 0.0f};
-    const float gc[3] = {gw[kGradR], gw[kGradG], gw[kGradB]};
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch) {
-        float v = g.base[ch];
-#pragma unroll
-        for (uint32_t k = 0; k < 15; ++k)
-            if (k < bases) v += Y[k] * restAt<L>(I, i, k * 3 + (uint32_t)ch);
-        float dcdv;
-        if (I.linear != 0) {
-            dcdv = v > 0.0f ? 1.0f : 0.0f;
-        } else {
-            dcdv = v <= 0.0f ? 0.0f : v <= 0.04045f ? 1.0f / 12.92f : (2.4f / 1.055f) * pow_f((v + 0.055f) / 1.055f, 1.4f);
-        }
-        const float dv = gc[ch] * dcdv;
-        acc.dSh[ch] += kSH0 * dv;
-#pragma unroll
-        for (uint32_t k = 0; k < 15; ++k) {
-            if (k >= bases) continue;
-            acc.dSh[3 + k * 3 + ch] += Y[k] * dv;
-            const float coef = restAt<L>(I, i, k * 3 + (uint32_t)ch) * dv;
-            dDir[0] += dY[k][0] * coef;
-            dDir[1] += dY[k][1] * coef;
-            dDir[2] += dY[k][2] * coef;
-        }
-    }
-    {
-        // dir = e / |e|
-        const float dd = dDir[0] * dir[0] + dDir[1] * dir[1] + dDir[2] * dir[2];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) dp[k] += (dDir[k] - dir[k] * dd) / len;
-    }
-
     // ---- opacity and the payback: alpha = paidOpacity(sigmoid(logit), paid) ----
     const float o = g.opacity;
     float dAlphaDo, dAlphaDpaid;
@@ -271,6 +229,59 @@ __device__ __forceinline__ void projectAdjoint(const FrameConst& F, const Instan
 #pragma unroll
     for (int k = 0; k < 3; ++k) acc.dLogScale[k] += dScale[k] * g.scale[k];
     acc.dQuat[0] += dQuat.x; acc.dQuat[1] += dQuat.y; acc.dQuat[2] += dQuat.z; acc.dQuat[3] += dQuat.w;
+}
+
+// The projection's adjoint for one Gaussian and one view: dL/d(record) `gw`
+// (gradient words of raster_types.cuh) -> dL/dparameters, added into `acc`.
+template <uint32_t L>
+__device__ __forceinline__ void projectAdjoint(const FrameConst& F, const InstanceConst& I, uint32_t i,
+                                               const float gw[kGradWords], ParamGrad& acc) {
+    const Gauss g = loadGauss<L>(I, i);
+    const Geometry G = projectGeometry<L == kLayoutMixed>(F, I, g, g.opacity);
+
+    // ---- colour: c = decode(base + rest(dir)) ------------------------------
+    float dp[3] = {0.0f, 0.0f, 0.0f};
+    const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
+    const float ex = g.px - I.eye[0], ey = g.py - I.eye[1], ez = g.pz - I.eye[2];
+    const float len = sqrtf((ex * ex + ey * ey) + ez * ez);
+    const float dir[3] = {ex / len, ey / len, ez / len};
+    float Y[15], dY[15][3];
+    shBasis(degree, dir[0], dir[1], dir[2], Y, dY);
+    const uint32_t bases = degree == 3 ? 15 : degree == 2 ? 8 : degree == 1 ? 3 : 0;
+    float dDir[3] = {0.0f, 0.0f, 0.0f};
+    const float gc[3] = {gw[kGradR], gw[kGradG], gw[kGradB]};
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        float v = g.base[ch];
+#pragma unroll
+        for (uint32_t k = 0; k < 15; ++k)
+            if (k < bases) v += Y[k] * restAt<L>(I, i, k * 3 + (uint32_t)ch);
+        float dcdv;
+        if (I.linear != 0) {
+            dcdv = v > 0.0f ? 1.0f : 0.0f;
+        } else {
+            dcdv = v <= 0.0f ? 0.0f : v <= 0.04045f ? 1.0f / 12.92f : (2.4f / 1.055f) * pow_f((v + 0.055f) / 1.055f, 1.4f);
+        }
+        const float dv = gc[ch] * dcdv;
+        acc.dSh[ch] += kSH0 * dv;
+#pragma unroll
+        for (uint32_t k = 0; k < 15; ++k) {
+            if (k >= bases) continue;
+            acc.dSh[3 + k * 3 + ch] += Y[k] * dv;
+            const float coef = restAt<L>(I, i, k * 3 + (uint32_t)ch) * dv;
+            dDir[0] += dY[k][0] * coef;
+            dDir[1] += dY[k][1] * coef;
+            dDir[2] += dY[k][2] * coef;
+        }
+    }
+    {
+        // dir = e / |e|
+        const float dd = dDir[0] * dir[0] + dDir[1] * dir[1] + dDir[2] * dir[2];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) dp[k] += (dDir[k] - dir[k] * dd) / len;
+    }
+
+    geometryAdjoint<L>(F, I, i, g, G, gw, dp, acc);
 }
 
 

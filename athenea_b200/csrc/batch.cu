@@ -109,13 +109,8 @@ __device__ __forceinline__ float quad(float a, float b, float c, float x, float 
     return ((a * x) * x + ((2.0f * b) * x) * y) + (c * y) * y;
 }
 
-template <uint32_t L>
-__device__ void colourFast(const InstanceConst& I, const Gauss& g, uint32_t i, uint32_t degree, float dx, float dy,
-                           float dz, float colour[3]) {
-    const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
-    const float inv = fastRcp(len);
-    const float x = dx * inv, y = dy * inv, z = dz * inv;
-    float Y[15];
+// The SH basis after the constant term (common/sh.slang:25-51) at direction (x, y, z).
+__device__ __forceinline__ void shBasisFast(float x, float y, float z, float Y[15]) {
     const float C1 = 0.4886025119029199f;
     Y[0] = -C1 * y; Y[1] = C1 * z; Y[2] = -C1 * x;
     const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
@@ -127,20 +122,112 @@ __device__ void colourFast(const InstanceConst& I, const Gauss& g, uint32_t i, u
     Y[11] = 0.3731763325901154f * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
     Y[12] = -0.4570457994644658f * x * (4.0f * zz - xx - yy); Y[13] = 1.445305721320277f * z * (xx - yy);
     Y[14] = -0.5900435899266435f * x * (xx - 3.0f * yy);
-    const uint32_t bases = degree == 3 ? 15 : degree == 2 ? 8 : degree == 1 ? 3 : 0;
+}
+
+// The gradient of basis function k of shBasisFast with respect to (x, y, z).
+__device__ __forceinline__ void shBasisGrad(uint32_t k, float x, float y, float z, float g[3]) {
+    const float C1 = 0.4886025119029199f, C20 = 1.0925484305920792f, C22 = 0.31539156525252005f,
+                C24 = 0.5462742152960396f, C30 = -0.5900435899266435f, C31 = 2.890611442640554f,
+                C32 = -0.4570457994644658f, C33 = 0.3731763325901154f, C35 = 1.445305721320277f;
+    const float xx = x * x, yy = y * y, zz = z * z;
+    g[0] = g[1] = g[2] = 0.0f;
+    switch (k) {
+        case 0: g[1] = -C1; break;
+        case 1: g[2] = C1; break;
+        case 2: g[0] = -C1; break;
+        case 3: g[0] = C20 * y; g[1] = C20 * x; break;
+        case 4: g[1] = -C20 * z; g[2] = -C20 * y; break;
+        case 5: g[0] = -2.0f * C22 * x; g[1] = -2.0f * C22 * y; g[2] = 4.0f * C22 * z; break;
+        case 6: g[0] = -C20 * z; g[2] = -C20 * x; break;
+        case 7: g[0] = 2.0f * C24 * x; g[1] = -2.0f * C24 * y; break;
+        case 8: g[0] = C30 * 6.0f * x * y; g[1] = C30 * (3.0f * xx - 3.0f * yy); break;
+        case 9: g[0] = C31 * y * z; g[1] = C31 * x * z; g[2] = C31 * x * y; break;
+        case 10: g[0] = C32 * (-2.0f * x * y); g[1] = C32 * (4.0f * zz - xx - 3.0f * yy); g[2] = C32 * 8.0f * y * z; break;
+        case 11: g[0] = C33 * (-6.0f * x * z); g[1] = C33 * (-6.0f * y * z); g[2] = C33 * (6.0f * zz - 3.0f * xx - 3.0f * yy); break;
+        case 12: g[0] = C32 * (4.0f * zz - 3.0f * xx - yy); g[1] = C32 * (-2.0f * x * y); g[2] = C32 * 8.0f * x * z; break;
+        case 13: g[0] = C35 * 2.0f * x * z; g[1] = C35 * (-2.0f * y * z); g[2] = C35 * (xx - yy); break;
+        default: g[0] = C30 * (3.0f * xx - 3.0f * yy); g[1] = C30 * (-6.0f * x * y); break;
+    }
+}
+
+__device__ __forceinline__ uint32_t basesOf(uint32_t degree) {
+    return degree == 3 ? 15 : degree == 2 ? 8 : degree == 1 ? 3 : 0;
+}
+
+// The colour (linear, clamped at 0) of a Gaussian seen along (dx, dy, dz) from
+// the eye, from the mixed layout's SH held in registers.
+__device__ __forceinline__ void colourFast(const MixedSh& sh, const Gauss& g, uint32_t degree, uint32_t linear,
+                                           float dx, float dy, float dz, float colour[3]) {
+    const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
+    const float inv = fastRcp(len);
+    float Y[15];
+    shBasisFast(dx * inv, dy * inv, dz * inv, Y);
+    const uint32_t bases = basesOf(degree);
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
         float v = g.base[ch];
 #pragma unroll
         for (uint32_t k = 0; k < 15; ++k)
-            if (k < bases) v = __fmaf_rn(Y[k], restAt<L>(I, i, k * 3 + (uint32_t)ch), v);
-        if (I.linear) {
+            if (k < bases) v = __fmaf_rn(Y[k], sh.rest(k * 3 + (uint32_t)ch), v);
+        if (linear) {
             colour[ch] = fmaxf(v, 0.0f);
         } else {
             const float c = fmaxf(v, 0.0f);
             colour[ch] = c <= 0.04045f ? c * (1.0f / 12.92f) : __powf((c + 0.055f) * (1.0f / 1.055f), 2.4f);
         }
     }
+}
+
+// colourFast's adjoint: dL/dcolour `gc` -> dL/dSH (added into dSh, the DC
+// first) and dL/dposition through the view direction (added into dp).
+__device__ __forceinline__ void colourAdjointFast(const MixedSh& sh, const Gauss& g, uint32_t degree, uint32_t linear,
+                                                  const float eye[3], const float gc[3], float dSh[48], float dp[3]) {
+    const float ex = g.px - eye[0], ey = g.py - eye[1], ez = g.pz - eye[2];
+    const float len = sqrtf((ex * ex + ey * ey) + ez * ez);
+    const float inv = fastRcp(len);
+    const float x = ex * inv, y = ey * inv, z = ez * inv;
+    float Y[15];
+    shBasisFast(x, y, z, Y);
+    const uint32_t bases = basesOf(degree);
+    float dv[3];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        float v = g.base[ch];
+#pragma unroll
+        for (uint32_t k = 0; k < 15; ++k)
+            if (k < bases) v = __fmaf_rn(Y[k], sh.rest(k * 3 + (uint32_t)ch), v);
+        float dcdv;
+        if (linear) {
+            dcdv = v > 0.0f ? 1.0f : 0.0f;
+        } else {
+            dcdv = v <= 0.0f      ? 0.0f
+                   : v <= 0.04045f ? 1.0f / 12.92f
+                                   : (2.4f / 1.055f) * __powf((v + 0.055f) * (1.0f / 1.055f), 1.4f);
+        }
+        dv[ch] = gc[ch] * dcdv;
+        dSh[ch] += kSH0 * dv[ch];
+    }
+    float dDir[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (uint32_t k = 0; k < 15; ++k) {
+        if (k >= bases) continue;
+        float w = 0.0f;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            dSh[3 + k * 3 + ch] += Y[k] * dv[ch];
+            w = __fmaf_rn(sh.rest(k * 3 + (uint32_t)ch), dv[ch], w);
+        }
+        float gk[3];
+        shBasisGrad(k, x, y, z, gk);
+        dDir[0] = __fmaf_rn(gk[0], w, dDir[0]);
+        dDir[1] = __fmaf_rn(gk[1], w, dDir[1]);
+        dDir[2] = __fmaf_rn(gk[2], w, dDir[2]);
+    }
+    // dir = e / |e|
+    const float dd = (dDir[0] * x + dDir[1] * y) + dDir[2] * z;
+    dp[0] += (dDir[0] - x * dd) * inv;
+    dp[1] += (dDir[1] - y * dd) * inv;
+    dp[2] += (dDir[2] - z * dd) * inv;
 }
 
 template <uint32_t L>
@@ -246,7 +333,8 @@ __global__ void __launch_bounds__(kProjThreads)
                 if (touched) {
                     const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
                     float colour[3];
-                    colourFast<L>(I, g, i, degree, g.px - I.eye[0], g.py - I.eye[1], g.pz - I.eye[2], colour);
+                    colourFast(loadMixedSh(I, i), g, degree, I.linear, g.px - I.eye[0], g.py - I.eye[1],
+                               g.pz - I.eye[2], colour);
                     const size_t r = ((size_t)v * B.count + i) * 3;
                     if (G.wide) atomicAdd(&words[kBatchDegenerate], 1u);
                     recs[r + 0] = make_float4(G.cx, G.cy, G.tz, G.cutoff);
@@ -363,15 +451,41 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---- the projection's adjoint over every view: one thread a Gaussian ---------
-template <uint32_t L>
+// Two passes over the views, so that what is live across them stays small: the
+// colour's adjoint (the SH gradient, 48 values, and the position's share through
+// the view direction), then the geometry's (position, opacity, scales,
+// rotation). The cloud's loads and the SH (packed in registers) are read once.
 __global__ void __launch_bounds__(128)
     projectAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float* __restrict__ grads,
                               float4* __restrict__ gMeans, float4* __restrict__ gScales, float4* __restrict__ gQuats,
                               float* __restrict__ gSh, uint32_t shStride) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.count) return;
+    InstanceConst I = B.inst;
+    const Gauss g = loadGauss<kLayoutMixed>(I, i);
+    const uint32_t degree = min(degreeOf(I.restPerColour), B.shLimit);
+    float dp[3] = {0.0f, 0.0f, 0.0f};
+    {
+        const MixedSh sh = loadMixedSh(I, i);
+        float dSh[48];
+#pragma unroll
+        for (int k = 0; k < 48; ++k) dSh[k] = 0.0f;
+        for (uint32_t v = 0; v < B.views; ++v) {
+            const float* gr = grads + ((size_t)v * B.count + i) * kGradWords;
+            const float gc[3] = {gr[kGradR], gr[kGradG], gr[kGradB]};
+            if (gc[0] == 0.0f && gc[1] == 0.0f && gc[2] == 0.0f) continue;
+            colourAdjointFast(sh, g, degree, I.linear, views[v].eye, gc, dSh, dp);
+        }
+        float* row = gSh + (size_t)i * shStride;
+#pragma unroll
+        for (uint32_t k = 0; k < 48; ++k)
+            if (k < shStride) row[k] = dSh[k];
+    }
     ParamGrad acc;
-    acc.clear();
+    acc.dp[0] = acc.dp[1] = acc.dp[2] = 0.0f;
+    acc.dLogit = 0.0f;
+    acc.dLogScale[0] = acc.dLogScale[1] = acc.dLogScale[2] = 0.0f;
+    acc.dQuat[0] = acc.dQuat[1] = acc.dQuat[2] = acc.dQuat[3] = 0.0f;
     for (uint32_t v = 0; v < B.views; ++v) {
         const float* gr = grads + ((size_t)v * B.count + i) * kGradWords;
         float gw[kGradWords];
@@ -387,13 +501,16 @@ __global__ void __launch_bounds__(128)
         F.width = V.width; F.height = V.height; F.tilesX = V.tilesX; F.tilesY = V.tilesY;
         F.focalX = V.focalX; F.focalY = V.focalY; F.centreX = V.centreX; F.centreY = V.centreY;
         F.nearZ = V.nearZ; F.farZ = V.farZ; F.orthographic = V.orthographic; F.shLimit = B.shLimit;
-        InstanceConst I = B.inst;
 #pragma unroll
         for (int k = 0; k < 12; ++k) I.m[k] = V.m[k];
         I.eye[0] = V.eye[0]; I.eye[1] = V.eye[1]; I.eye[2] = V.eye[2];
-        projectAdjoint<L>(F, I, i, gw, acc);
+        const Geometry G = projectGeometry<true>(F, I, g, g.opacity);
+        float dpv[3] = {0.0f, 0.0f, 0.0f};
+        geometryAdjoint<kLayoutMixed>(F, I, i, g, G, gw, dpv, acc);
     }
-    acc.addTo(i, shStride, gMeans, gScales, gQuats, gSh, true);
+    gMeans[i] = make_float4(acc.dp[0] + dp[0], acc.dp[1] + dp[1], acc.dp[2] + dp[2], acc.dLogit);
+    gScales[i] = make_float4(acc.dLogScale[0], acc.dLogScale[1], acc.dLogScale[2], 0.0f);
+    gQuats[i] = make_float4(acc.dQuat[0], acc.dQuat[1], acc.dQuat[2], acc.dQuat[3]);
 }
 
 // ---- FP32 SH -> the mixed layout ------------------------------------------------
@@ -612,7 +729,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
                               static_cast<float*>(b->grads.ptr));
     mark(6);
     if (err == cudaSuccess && P.count) {
-        projectAdjointBatchKernel<kLayoutMixed><<<(P.count + 127) / 128, 128, 0, stream>>>(
+        projectAdjointBatchKernel<<<(P.count + 127) / 128, 128, 0, stream>>>(
             B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
             reinterpret_cast<float4*>(g.means), reinterpret_cast<float4*>(g.scales), reinterpret_cast<float4*>(g.quats),
             g.sh, 48);
@@ -772,6 +889,10 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
     if (P.count && (!P.means || !P.scales || !P.quats || !P.sh_low || !P.sh_high || !P.sh_scale))
         return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: a cloud needs every array of the mixed layout");
     if (P.sh_degree > 3) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: sh_degree must be 0..3");
+    if ((reinterpret_cast<uintptr_t>(P.sh_low) & 7u) || (reinterpret_cast<uintptr_t>(P.sh_high) & 3u) ||
+        (reinterpret_cast<uintptr_t>(P.means) & 15u) || (reinterpret_cast<uintptr_t>(P.scales) & 15u) ||
+        (reinterpret_cast<uintptr_t>(P.quats) & 15u))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: a cloud array is not aligned to its element");
     const uint32_t slotBits = bitsForValues(std::max<uint64_t>(P.count, 2));
     if (24 + slotBits + b->tileBits > 64)
         return fail(ATH_E_UNSUPPORTED, "ath_batch_train_step: tiles, depth key and Gaussian index exceed 64 bits");

@@ -92,6 +92,45 @@ __device__ __forceinline__ float restAt(const InstanceConst& I, uint32_t i, uint
     }
 }
 
+// ---- the mixed layout's SH of one Gaussian, held packed in 16 registers -------
+// Loaded with 13 word loads instead of one load a coefficient; rest(index) is
+// restAt<kLayoutMixed>'s value to the bit (a BF16's bits are a float's top
+// half; an e4m3 widens exactly and takes the same FP32 product with the scale).
+struct MixedSh {
+    uint32_t low[6];    // 12 BF16: DC r g b, then band 1's 9
+    uint32_t high[9];   // 36 e4m3: bands 2 and 3
+    float scale;
+
+    __device__ __forceinline__ float bf16At(uint32_t k) const {
+        const uint32_t word = low[k >> 1];
+        return __uint_as_float((k & 1u) ? (word & 0xFFFF0000u) : (word << 16));
+    }
+    // coefficient `index` = basis * 3 + channel of the rest (after the DC)
+    __device__ __forceinline__ float rest(uint32_t index) const {
+        if (index < 9) return bf16At(3 + index);
+        const uint32_t k = index - 9;
+        __nv_fp8_e4m3 e;
+        e.__x = (__nv_fp8_storage_t)((high[k >> 2] >> (8 * (k & 3u))) & 0xFFu);
+        return float(e) * scale;
+    }
+};
+
+__device__ __forceinline__ MixedSh loadMixedSh(const InstanceConst& I, uint32_t i) {
+    MixedSh s;
+    const uint2* low = reinterpret_cast<const uint2*>(reinterpret_cast<const uint8_t*>(I.shLow) + (size_t)i * 24);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const uint2 w = __ldg(low + k);
+        s.low[2 * k] = w.x;
+        s.low[2 * k + 1] = w.y;
+    }
+    const uint32_t* high = reinterpret_cast<const uint32_t*>(reinterpret_cast<const uint8_t*>(I.shHigh) + (size_t)i * 36);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s.high[k] = __ldg(high + k);
+    s.scale = __ldg(I.shScale + i);
+    return s;
+}
+
 template <uint32_t L>
 __device__ __forceinline__ Gauss loadGauss(const InstanceConst& I, uint32_t i) {
     if constexpr (L == kLayoutPacked) {

@@ -235,8 +235,8 @@ typedef struct {
     const float* means;     /* float4: x y z, opacity logit */
     const float* scales;    /* float4: log scales */
     const float* quats;     /* float4: w x y z */
-    const void* sh_low;     /* 12 bf16 a Gaussian */
-    const void* sh_high;    /* 36 e4m3 a Gaussian */
+    const void* sh_low;     /* 12 bf16 a Gaussian; 8-byte aligned */
+    const void* sh_high;    /* 36 e4m3 a Gaussian; 4-byte aligned */
     const float* sh_scale;  /* 1 float a Gaussian */
     uint32_t count;
     uint32_t sh_degree;
