@@ -72,19 +72,19 @@ template <uint32_t T, uint32_t NB>
 __global__ void __launch_bounds__(T * T / 2)
     blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                      const uint64_t* __restrict__ pairs, const float4* __restrict__ recs,
-                     float4* __restrict__ colour, float* __restrict__ depth, float* __restrict__ finalT,
-                     uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ words) {
+                     float4* __restrict__ colour, float* __restrict__ finalT, uint32_t* __restrict__ lastContrib,
+                     uint32_t* __restrict__ words) {
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
-    __shared__ float4 sScreen[NB];
-    __shared__ float4 sConic[NB];
-    __shared__ float4 sColour[NB];
+    __shared__ float2 sCentre[NB];
+    __shared__ float4 sConic[NB];    // ca, fr, fs pre-scaled; alpha
+    __shared__ float4 sColour[NB];   // r g b; the cutoff pre-scaled
     __shared__ uint32_t sMask[NB];
     __shared__ uint32_t sTileBase[kMaxBatchViews];
     __shared__ uint32_t sTile;
     for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
     const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
-    const float kL2e = 1.4426950408889634f;
+    const float kScale = -0.5f * 1.4426950408889634f;   // power -> base-2 exponent
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
     uint32_t evaluated = 0;   // (pixel, record) evaluations this thread made
@@ -101,10 +101,9 @@ __global__ void __launch_bounds__(T * T / 2)
         const float tileX0 = (float)(tx * T), tileY0 = (float)(ty * T);
         const uint32_t px = tx * T + lx, py[2] = {ty * T + ly, ty * T + ly + 4};
         const uint2 range = ranges[tile];
-        const float pxc = (float)px + 0.5f;
+        const float pxc = (float)px + 0.5f, pyc[2] = {(float)py[0] + 0.5f, (float)py[1] + 0.5f};
         const size_t recBase = (size_t)v * B.count;
         float r[2] = {0.0f, 0.0f}, g[2] = {0.0f, 0.0f}, bl[2] = {0.0f, 0.0f}, Tr[2] = {1.0f, 1.0f};
-        float depthSum[2] = {0.0f, 0.0f};
         uint32_t last[2] = {0, 0};
         bool done[2];
 #pragma unroll
@@ -116,11 +115,11 @@ __global__ void __launch_bounds__(T * T / 2)
                 const size_t s = (recBase + (pairs[first + k] & slotMask)) * 3;
                 const float4 sc = recs[s + 0];
                 const float4 c = recs[s + 1];
-                sScreen[k] = sc;
-                // the factored conic's two weights pre-scaled by -log2(e)/2:
-                // power in base-2 exponent units
-                sConic[k] = make_float4(c.x * (-0.5f * kL2e), c.y, c.z * (-0.5f * kL2e), c.w);
-                sColour[k] = recs[s + 2];
+                const float4 rgb = recs[s + 2];
+                sCentre[k] = make_float2(sc.x, sc.y);
+                // the factored conic's two weights pre-scaled to base-2 exponent units
+                sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
+                sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
                 sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
             }
             __syncthreads();
@@ -131,18 +130,19 @@ __global__ void __launch_bounds__(T * T / 2)
                 while (todo) {
                     const uint32_t j = base + (uint32_t)__ffs(todo) - 1u;
                     todo &= todo - 1u;
-                    const float4 sc = sScreen[j];
+                    const float2 ce = sCentre[j];
                     const float4 k = sConic[j];
-                    const float dx = pxc - sc.x;
+                    const float limit = sColour[j].w;
+                    const float dx = pxc - ce.x;
 #pragma unroll
                     for (int p = 0; p < 2; ++p) {
                         if (done[p]) continue;
                         ++evaluated;
-                        const float dy = ((float)py[p] + 0.5f) - sc.y;
+                        const float dy = pyc[p] - ce.y;
                         // e = -log2(e)/2 * power; power > cutoff  <=>  e < -log2(e)/2 * cutoff
                         const float t = __fmaf_rn(k.y, dy, dx);
                         const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
-                        if (e < (-0.5f * kL2e) * sc.w) continue;
+                        if (e < limit) continue;
                         const float alpha = fminf(0.99f, k.w * fastExp2(e));
                         if (alpha < kFaint) continue;
                         const float w = Tr[p] * alpha;
@@ -150,7 +150,6 @@ __global__ void __launch_bounds__(T * T / 2)
                         r[p] = __fmaf_rn(w, c.x, r[p]);
                         g[p] = __fmaf_rn(w, c.y, g[p]);
                         bl[p] = __fmaf_rn(w, c.z, bl[p]);
-                        depthSum[p] = __fmaf_rn(w, sc.z, depthSum[p]);
                         Tr[p] = Tr[p] * (1.0f - alpha);
                         last[p] = first - range.x + j + 1;
                         if (Tr[p] < 1e-4f) done[p] = true;
@@ -166,7 +165,6 @@ __global__ void __launch_bounds__(T * T / 2)
             const float coverage = 1.0f - Tr[p];
             colour[at] = make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1], bl[p] + Tr[p] * B.bg[2],
                                      coverage + Tr[p] * B.bg[3]);
-            if (depth) depth[at] = coverage > 1e-6f ? depthSum[p] / coverage : 0.0f;
             finalT[at] = Tr[p];
             lastContrib[at] = last[p];
         }
@@ -207,8 +205,13 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
 
 // ---- the blend's adjoint, over the same tile queue ------------------------------
 // The forward's warp boxes and masks, walked in reverse: a warp takes the records
-// marked for its box from its pixels' last contributor down, each lane its two
-// pixels' terms summed before the warp reduction.
+// marked for its box from its pixels' last contributor down. What a lane sums
+// over its two pixels, and the warp over its 64, are moments of dL/dpower over
+// the pixel offsets in the factored frame (t = dx + fr dy, dy): sum dP t,
+// sum dP dy, sum dP t^2, sum dP t dy, sum dP dy^2; the record's centre and conic
+// gradients follow from them once a record, when the block flushes. The batched
+// loss has no alpha term, so dL/d(alpha out) is 0 and the colour behind a
+// record enters only through S.dC, one value a pixel.
 template <uint32_t T, uint32_t NB>
 __global__ void __launch_bounds__(T * T / 2)
     blendAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
@@ -218,8 +221,8 @@ __global__ void __launch_bounds__(T * T / 2)
                             uint32_t* __restrict__ words) {
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
-    constexpr uint32_t kWords = 9;   // centre x y, conic a b c, alpha, colour r g b (no depth loss)
-    __shared__ float4 sScreen[NB];
+    constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
+    __shared__ float2 sCentre[NB];
     __shared__ float4 sConic[NB];
     __shared__ float4 sColour[NB];
     __shared__ uint32_t sRec[NB];
@@ -229,8 +232,8 @@ __global__ void __launch_bounds__(T * T / 2)
     __shared__ uint32_t sTile, sMaxLast;
     for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
     const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
-    const float kL2e = 1.4426950408889634f;
-    const float kUnscale = -2.0f / kL2e;   // undoes the -log2(e)/2 pre-scale (for the gradients only)
+    const float kScale = -0.5f * 1.4426950408889634f;
+    const float kUnscale = 1.0f / kScale;   // for the gradients only
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
     while (true) {
@@ -249,8 +252,8 @@ __global__ void __launch_bounds__(T * T / 2)
         const float tileX0 = (float)(tx * T), tileY0 = (float)(ty * T);
         const uint32_t px = tx * T + lx, py[2] = {ty * T + ly, ty * T + ly + 4};
         const uint2 range = ranges[tile];
-        const float pxc = (float)px + 0.5f;
-        float Tr[2], S[2][3], dC[2][3], dAlphaOut[2];
+        const float pxc = (float)px + 0.5f, pyc[2] = {(float)py[0] + 0.5f, (float)py[1] + 0.5f};
+        float Tr[2], sd[2], dC[2][3];
         uint32_t last[2];
 #pragma unroll
         for (int p = 0; p < 2; ++p) {
@@ -260,8 +263,7 @@ __global__ void __launch_bounds__(T * T / 2)
             last[p] = inside ? min(lastContrib[at], range.y - range.x) : 0u;
             const float4 d = inside ? dLdColour[at] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             dC[p][0] = d.x; dC[p][1] = d.y; dC[p][2] = d.z;
-            dAlphaOut[p] = d.w * Tr[p] * (1.0f - B.bg[3]);
-            S[p][0] = B.bg[0]; S[p][1] = B.bg[1]; S[p][2] = B.bg[2];
+            sd[p] = (B.bg[0] * d.x + B.bg[1] * d.y) + B.bg[2] * d.z;   // S.dC, S the colour behind
         }
         const uint32_t warpLast = __reduce_max_sync(0xFFFFFFFFu, max(last[0], last[1]));
         if (lane == 0 && warpLast) atomicMax(&sMaxLast, warpLast);
@@ -277,10 +279,11 @@ __global__ void __launch_bounds__(T * T / 2)
                 const size_t q = (recBase + s) * 3;
                 const float4 sc = recs[q + 0];
                 const float4 c = recs[q + 1];
-                sScreen[k] = sc;
+                const float4 rgb = recs[q + 2];
+                sCentre[k] = make_float2(sc.x, sc.y);
                 // the forward's pre-scale, operation for operation (so the same records pass)
-                sConic[k] = make_float4(c.x * (-0.5f * kL2e), c.y, c.z * (-0.5f * kL2e), c.w);
-                sColour[k] = recs[q + 2];
+                sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
+                sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
                 sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
             }
             for (uint32_t k = threadIdx.x; k < count * kWords; k += kThreads) sAcc[k] = 0.0f;
@@ -297,10 +300,10 @@ __global__ void __launch_bounds__(T * T / 2)
                         const uint32_t j = (uint32_t)base + hb;
                         const uint32_t rel = relStart + j;
                         if (rel >= warpLast) continue;
-                        const float4 sc = sScreen[j];
+                        const float2 ce = sCentre[j];
                         const float4 k = sConic[j];
                         const float4 c = sColour[j];
-                        const float dx = pxc - sc.x;
+                        const float dx = pxc - ce.x;
                         float gv[kWords];
 #pragma unroll
                         for (int q = 0; q < (int)kWords; ++q) gv[q] = 0.0f;
@@ -308,47 +311,41 @@ __global__ void __launch_bounds__(T * T / 2)
 #pragma unroll
                         for (int p = 0; p < 2; ++p) {
                             if (rel >= last[p]) continue;
-                            const float dy = ((float)py[p] + 0.5f) - sc.y;
+                            const float dy = pyc[p] - ce.y;
                             const float t = __fmaf_rn(k.y, dy, dx);
                             const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
-                            if (e < (-0.5f * kL2e) * sc.w) continue;
+                            if (e < c.w) continue;
                             const float G = fastExp2(e);
                             const float raw = k.w * G;
                             const float alpha = fminf(0.99f, raw);
                             if (alpha < kFaint) continue;
                             live = true;
-                            const float oneMinus = 1.0f - alpha;
-                            const float inv = fastRcp(oneMinus);
+                            const float inv = fastRcp(1.0f - alpha);
                             const float Tb = Tr[p] * inv;
                             const float w = Tb * alpha;
                             gv[6] = __fmaf_rn(w, dC[p][0], gv[6]);
                             gv[7] = __fmaf_rn(w, dC[p][1], gv[7]);
                             gv[8] = __fmaf_rn(w, dC[p][2], gv[8]);
-                            const float dAlpha = Tb * ((c.x - S[p][0]) * dC[p][0] + (c.y - S[p][1]) * dC[p][1] +
-                                                       (c.z - S[p][2]) * dC[p][2]) +
-                                                 dAlphaOut[p] * inv;
-                            S[p][0] = __fmaf_rn(alpha, c.x - S[p][0], S[p][0]);
-                            S[p][1] = __fmaf_rn(alpha, c.y - S[p][1], S[p][1]);
-                            S[p][2] = __fmaf_rn(alpha, c.z - S[p][2], S[p][2]);
+                            const float cd = (c.x * dC[p][0] + c.y * dC[p][1]) + c.z * dC[p][2];
+                            const float dAlpha = Tb * (cd - sd[p]);
+                            sd[p] = __fmaf_rn(alpha, cd - sd[p], sd[p]);
                             Tr[p] = Tb;
                             if (raw < 0.99f && k.w <= 1.0f) {
                                 gv[5] = __fmaf_rn(dAlpha, G, gv[5]);
-                                const float dPower = -0.5f * alpha * dAlpha;
-                                gv[2] = __fmaf_rn(dPower, dx * dx, gv[2]);
-                                gv[3] = __fmaf_rn(dPower, 2.0f * dx * dy, gv[3]);
-                                gv[4] = __fmaf_rn(dPower, dy * dy, gv[4]);
-                                // d power / d centre: -2 (ca dx + cb dy), -2 (cb dx + cc dy)
-                                // in the factored form (cb = ca fr, cc = fs + ca fr^2)
-                                const float at = (k.x * kUnscale) * t;
-                                gv[0] = __fmaf_rn(dPower, -2.0f * at, gv[0]);
-                                gv[1] = __fmaf_rn(dPower, -2.0f * (k.y * at + (k.z * kUnscale) * dy), gv[1]);
+                                const float dP = -0.5f * alpha * dAlpha;
+                                const float dPt = dP * t, dPy = dP * dy;
+                                gv[0] += dPt;
+                                gv[1] += dPy;
+                                gv[2] = __fmaf_rn(dPt, t, gv[2]);
+                                gv[3] = __fmaf_rn(dPt, dy, gv[3]);
+                                gv[4] = __fmaf_rn(dPy, dy, gv[4]);
                             }
                         }
                         const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, live);
                         if (!lanes) continue;
                         float* acc = sAcc + j * kWords;
-                        if ((lanes & (lanes - 1u)) == 0u) {
-                            // one lane live: its terms are the warp's
+                        if (__popc(lanes) <= 3) {
+                            // few lanes live: their terms straight into the record's sums
                             if (live) {
 #pragma unroll
                                 for (int q = 0; q < (int)kWords; ++q)
@@ -364,17 +361,32 @@ __global__ void __launch_bounds__(T * T / 2)
                 }
             }
             __syncthreads();
-            for (uint32_t k = threadIdx.x; k < count * kWords; k += kThreads) {
-                const float s = sAcc[k];
-                if (s != 0.0f) atomicAdd(&grads[(recBase + sRec[k / kWords]) * kGradWords + k % kWords], s);
+            // the moments -> dL/d(centre, conic) in the record's terms, then to the record
+            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
+                const float* a = sAcc + k * kWords;
+                float out[kWords];
+                const float4 cn = sConic[k];
+                const float ca = cn.x * kUnscale, fr = cn.y, fs = cn.z * kUnscale;
+                const float mt = a[0], my = a[1], mtt = a[2], mty = a[3], myy = a[4];
+                out[kGradCx] = -2.0f * ca * mt;
+                out[kGradCy] = -2.0f * (fr * ca * mt + fs * my);
+                out[kGradA] = mtt - 2.0f * fr * mty + fr * fr * myy;   // sum dP dx^2, dx = t - fr dy
+                out[kGradB2] = 2.0f * (mty - fr * myy);                 // sum dP 2 dx dy
+                out[kGradC] = myy;                                      // sum dP dy^2
+                out[kGradAlpha] = a[5];
+                out[kGradR] = a[6];
+                out[kGradG] = a[7];
+                out[kGradB] = a[8];
+                float* dst = grads + (recBase + sRec[k]) * kGradWords;
+#pragma unroll
+                for (int q = 0; q < (int)kWords; ++q)
+                    if (out[q] != 0.0f) atomicAdd(dst + q, out[q]);
             }
             __syncthreads();   // the next batch's loads overwrite what the flush reads
             batchEnd = batchStart;
         }
     }
 }
-
-
 
 template <typename K>
 int residentGrid(K kernel, int threads, int sms) {
@@ -386,8 +398,8 @@ int residentGrid(K kernel, int threads, int sms) {
 template <uint32_t T, uint32_t NB>
 cudaError_t blendWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour) {
     const int grid = residentGrid(blendBatchKernel<T, NB>, T * T / 2, L.sms);
-    blendBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.recs, colour, nullptr,
-                                                                L.finalT, L.lastContrib, L.words);
+    blendBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.recs, colour, L.finalT,
+                                                                L.lastContrib, L.words);
     return cudaGetLastError();
 }
 
