@@ -66,7 +66,7 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* sWa
 }
 
 template <bool kValues>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
     onesweepKernel(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
                    uint64_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, uint32_t n, uint32_t shift,
                    const uint32_t* __restrict__ globalHist, uint64_t* __restrict__ flags, uint32_t* __restrict__ ticket,
