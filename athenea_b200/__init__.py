@@ -7,10 +7,11 @@ not have: differentiable frames (Params, TileRasterizer.render_params /
 backward) and the batched mixed-precision step (MixedParams, BatchTrainer).
 """
 from ._native import AtheneaError  # noqa: F401
+from .parallel import GradientBuffer, shard_views  # noqa: F401
 from .raster import (BatchTrainer, Camera, CloudLoader, FrameStats, GpuSplats, Lens, MixedParams,  # noqa: F401
                      Params, RenderSettings, RenderTargets, SplatCounters, SplatEdit, SplatInstance, TileRasterizer,
                      encoding_3dgs, l2_loss, pinhole_for_vertical_fov)
 
-__all__ = ["AtheneaError", "BatchTrainer", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "MixedParams",
+__all__ = ["AtheneaError", "BatchTrainer", "GradientBuffer", "shard_views", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "MixedParams",
            "Params", "RenderSettings", "RenderTargets", "SplatCounters", "SplatEdit", "SplatInstance",
            "TileRasterizer", "encoding_3dgs", "l2_loss", "pinhole_for_vertical_fov"]

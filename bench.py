@@ -209,7 +209,9 @@ def run_ours(args) -> dict | None:
                       sh_degree=p["sh_degree"])
     del p
     mixed = A.MixedParams.from_params(params)
-    projs = view_cameras(V, first=rank * V)
+    # weak scaling: every rank draws V views of its own, views rank*V .. rank*V + V - 1
+    shard = A.shard_views(V * world, rank, world)
+    projs = view_cameras(len(shard), first=shard.start)
     views = [(proj, W, H) for proj in projs]
     gen = torch.Generator().manual_seed(20261203 + 7 + rank)
     host_target = torch.rand((V * W * H, 3), generator=gen).pin_memory()
@@ -223,10 +225,8 @@ def run_ours(args) -> dict | None:
     loss = torch.zeros(1, dtype=torch.float32, device=dev)
     # the gradients in one flat buffer, so that a multi-GPU step sums them over
     # ranks (every rank's views) with one all-reduce
-    n, stride = params.count, int(params.sh.shape[1])
-    flat = torch.zeros(n * (12 + stride), dtype=torch.float32, device=dev)
-    grads = A.Params(flat[:4 * n].view(n, 4), flat[4 * n:8 * n].view(n, 4), flat[8 * n:12 * n].view(n, 4),
-                     flat[12 * n:].view(n, stride), params.sh_degree)
+    exchange = A.GradientBuffer(params.count, int(params.sh.shape[1]), params.sh_degree, device=dev)
+    grads = exchange.params
     if args.tile:
         bt.set_tuning(args.tile, args.block_batch)
         tuned = {"tile": args.tile, "block_batch": args.block_batch}
@@ -235,8 +235,7 @@ def run_ours(args) -> dict | None:
 
     def batched_step():
         bt.step(mixed, target, colour, loss, grads, stream=stream)
-        if world > 1:
-            dist.all_reduce(flat)
+        exchange.allreduce()
 
     for _ in range(args.warmup):
         batched_step()
