@@ -421,34 +421,6 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// ---- the loss: a view's mean L2 over its pixels and r g b, summed over views ----
-__global__ void __launch_bounds__(256)
-    lossBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float4* __restrict__ colour,
-                    const float* __restrict__ target, float4* __restrict__ dL, float* __restrict__ loss) {
-    __shared__ uint32_t sPixelBase[kMaxBatchViews];
-    __shared__ float sPart[8];
-    for (uint32_t k = threadIdx.x; k < B.views; k += blockDim.x) sPixelBase[k] = views[k].pixelBase;
-    __syncthreads();
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    float l = 0.0f;
-    if (p < B.totalPixels) {
-        const float scale = views[viewOf(sPixelBase, B.views, p)].lossScale;
-        const float4 c = colour[p];
-        const float er = c.x - target[(size_t)p * 3 + 0], eg = c.y - target[(size_t)p * 3 + 1],
-                    eb = c.z - target[(size_t)p * 3 + 2];
-        l = (er * er + eg * eg + eb * eb) * scale;
-        dL[p] = make_float4(2.0f * scale * er, 2.0f * scale * eg, 2.0f * scale * eb, 0.0f);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xFFFFFFFFu, l, o);
-    if ((threadIdx.x & 31u) == 0) sPart[threadIdx.x >> 5] = l;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float b = 0.0f;
-        for (uint32_t w = 0; w < blockDim.x / 32; ++w) b += sPart[w];
-        if (b != 0.0f) atomicAdd(loss, b);
-    }
-}
 
 // ---- the projection's adjoint over every view: one thread a Gaussian ---------
 // Two passes over the views, so that what is live across them stays small: the
@@ -661,7 +633,8 @@ int residentBlocks(K kernel, int threads, int sms) {
 }
 
 cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t sorted, cudaStream_t stream, bool forward,
-                            float4* colour, float4* dL, float* grads) {
+                            float4* colour, float4* dL, float* grads, const float* target = nullptr,
+                            float* loss = nullptr) {
     BlendLaunch L{};
     L.views = static_cast<const BatchView*>(b->viewsDev.ptr);
     L.ranges = static_cast<const uint2*>(b->ranges.ptr);
@@ -673,7 +646,8 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
     L.sms = b->sms;
     L.tile = b->tile;
     L.blockBatch = b->blockBatch;
-    return forward ? launchBatchBlend(B, L, stream, colour) : launchBatchBlendAdjoint(B, L, stream, dL, grads);
+    return forward ? launchBatchBlend(B, L, stream, colour, target, dL, loss)
+                   : launchBatchBlendAdjoint(B, L, stream, dL, grads);
 }
 
 // One step, enqueued (captured or not). `countOnly`: the projection alone, to size the pairs.
@@ -713,14 +687,11 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
         err = cudaGetLastError();
     }
     mark(3);
-    if (err == cudaSuccess) err = launchBlendsFor(b, B, sorted, stream, true, colour, nullptr, nullptr);
-    mark(4);
     if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
-    if (err == cudaSuccess) {
-        lossBatchKernel<<<(b->totalPixels + 255) / 256, 256, 0, stream>>>(
-            B, static_cast<const BatchView*>(b->viewsDev.ptr), colour, target, static_cast<float4*>(b->dL.ptr), loss);
-        err = cudaGetLastError();
-    }
+    if (err == cudaSuccess)
+        err = launchBlendsFor(b, B, sorted, stream, true, colour, static_cast<float4*>(b->dL.ptr), nullptr, target,
+                              loss);
+    mark(4);
     if (err == cudaSuccess)
         err = cudaMemsetAsync(b->grads.ptr, 0, (size_t)V * P.count * kGradWords * sizeof(float), stream);
     mark(5);

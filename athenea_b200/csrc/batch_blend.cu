@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(T * T / 2)
     blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                      const uint64_t* __restrict__ pairs, const float4* __restrict__ recs,
                      float4* __restrict__ colour, float* __restrict__ finalT, uint32_t* __restrict__ lastContrib,
+                     const float* __restrict__ target, float4* __restrict__ dL, float* __restrict__ loss,
                      uint32_t* __restrict__ words) {
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
@@ -88,6 +89,7 @@ __global__ void __launch_bounds__(T * T / 2)
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
     uint32_t evaluated = 0;   // (pixel, record) evaluations this thread made
+    float lossSum = 0.0f;     // this thread's pixels' share of the loss
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) sTile = atomicAdd(&words[kBatchBlendTicket], 1u);
@@ -163,12 +165,22 @@ __global__ void __launch_bounds__(T * T / 2)
             if (!(px < V.width && py[p] < V.height)) continue;
             const uint32_t at = V.pixelBase + py[p] * V.width + px;
             const float coverage = 1.0f - Tr[p];
-            colour[at] = make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1], bl[p] + Tr[p] * B.bg[2],
-                                     coverage + Tr[p] * B.bg[3]);
+            const float4 c = make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1], bl[p] + Tr[p] * B.bg[2],
+                                         coverage + Tr[p] * B.bg[3]);
+            colour[at] = c;
             finalT[at] = Tr[p];
             lastContrib[at] = last[p];
+            // the loss: the view's mean L2 over its pixels and r g b, and its gradient
+            const float er = c.x - target[(size_t)at * 3 + 0], eg = c.y - target[(size_t)at * 3 + 1],
+                        eb = c.z - target[(size_t)at * 3 + 2];
+            lossSum += (er * er + eg * eg + eb * eb) * V.lossScale;
+            const float k2 = 2.0f * V.lossScale;
+            dL[at] = make_float4(k2 * er, k2 * eg, k2 * eb, 0.0f);
         }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lossSum += __shfl_xor_sync(0xFFFFFFFFu, lossSum, o);
+    if (lane == 0 && lossSum != 0.0f) atomicAdd(loss, lossSum);
     uint64_t e = evaluated;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
@@ -396,10 +408,11 @@ int residentGrid(K kernel, int threads, int sms) {
 }
 
 template <uint32_t T, uint32_t NB>
-cudaError_t blendWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour) {
+cudaError_t blendWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
+                      const float* target, float4* dL, float* loss) {
     const int grid = residentGrid(blendBatchKernel<T, NB>, T * T / 2, L.sms);
     blendBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.recs, colour, L.finalT,
-                                                                L.lastContrib, L.words);
+                                                                L.lastContrib, target, dL, loss, L.words);
     return cudaGetLastError();
 }
 
@@ -418,9 +431,10 @@ cudaError_t adjointWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t 
     CALL(8, 64) CALL(8, 128) CALL(8, 256) CALL(16, 64) CALL(16, 128) CALL(16, 256) CALL(32, 64) CALL(32, 128) \
     CALL(32, 256)
 
-cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour) {
+cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
+                             const float* target, float4* dL, float* loss) {
 #define ATH_CASE(T_, NB_) \
-    if (L.tile == T_ && L.blockBatch == NB_) return blendWith<T_, NB_>(B, L, stream, colour);
+    if (L.tile == T_ && L.blockBatch == NB_) return blendWith<T_, NB_>(B, L, stream, colour, target, dL, loss);
     ATH_BLEND_CASES(ATH_CASE)
 #undef ATH_CASE
     return cudaErrorInvalidValue;

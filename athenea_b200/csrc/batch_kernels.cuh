@@ -119,8 +119,12 @@ struct BlendLaunch {
     uint32_t tile, blockBatch;
 };
 
-// The forward blend of every view's tiles (colour, final T, last contributor).
-cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour);
+// The forward blend of every view's tiles (colour, final T, last contributor)
+// with the loss in its epilogue: each view's mean L2 against `target` (float3 a
+// pixel) over its pixels and r g b, summed over views into *loss (which the
+// caller zeroes), and dL/dcolour into `dL`.
+cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
+                             const float* target, float4* dL, float* loss);
 // Its adjoint: dL/d(record) for every (view, Gaussian) record, added into `grads`.
 cudaError_t launchBatchBlendAdjoint(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream,
                                     const float4* dLdColour, float* grads);

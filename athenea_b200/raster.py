@@ -517,7 +517,7 @@ class BatchTrainer:
         self._keep = (params, target, colour, loss, grads)
         check(N.lib().ath_batch_time_stages(self._h, C.byref(params._native()), _ptr(target), _ptr(colour),
                                             _ptr(loss), C.byref(g), ms, C.c_void_p(s.cuda_stream)))
-        names = ("project_emit", "sort", "ranges", "blend", "loss", "blend_adjoint", "project_adjoint")
+        names = ("project_emit", "sort", "ranges", "blend_and_loss", "clear_grads", "blend_adjoint", "project_adjoint")
         return {n: float(v) for n, v in zip(names, ms)}
 
     def buffers(self) -> dict:

@@ -312,9 +312,9 @@ def run_ours(args) -> dict | None:
     T = tuned["tile"]
     total_tiles = V * ((W + T - 1) // T) * ((H + T - 1) // T)
     passes = math.ceil((24 + max(1, math.ceil(math.log2(max(2, total_tiles))))) / 8)
-    # the step's launches: begin, projectEmit, histogram, the sort's passes, ranges,
-    # blend, loss, blend adjoint, projection adjoint (and 3 memsets, not kernels)
-    launches = (2 + 1 + passes + 1 + 1 + 1 + 1 + 1) * args.steps
+    # the step's kernels: begin, projectEmit, histogram, the sort's passes, ranges,
+    # blend (with the loss), blend adjoint, projection adjoint (memsets are not counted)
+    launches = (2 + 1 + passes + 1 + 1 + 1 + 1) * args.steps
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
                stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
                count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4)
@@ -409,15 +409,16 @@ def main():
         "project_emit": ("hbm", res["count"] * mixed_bytes + stats["kept"] * 48 + stats["pairs"] * 8),
         "sort": ("hbm", stats["pairs"] * (8 + 16 * res["passes"])),
         "ranges": ("hbm", stats["pairs"] * 8 + stats["pairs"] // 16 * 8),
-        "blend": ("fp32", stats["evaluated"] * 20),
-        "loss": ("hbm", (V * W * H) * (16 + 12 + 16)),
+        "blend_and_loss": ("fp32", stats["evaluated"] * 20),
+        "clear_grads": ("hbm", V * res["count"] * 40),
         "blend_adjoint": ("fp32", stats["evaluated"] * 60),
         "project_adjoint": ("hbm", res["count"] * (mixed_bytes + 60 * 4) + stats["kept"] * 40),
     }
     bound, amount = work[dominant]
     secs = stages[dominant] * 1e-3
     kernel_names = {"project_emit": "projectEmitKernel", "sort": "onesweepKernel", "ranges": "rangesBatchKernel",
-                    "blend": "blendBatchKernel", "loss": "lossBatchKernel", "blend_adjoint": "blendAdjointBatchKernel",
+                    "blend_and_loss": "blendBatchKernel", "clear_grads": "cudaMemsetAsync",
+                    "blend_adjoint": "blendAdjointBatchKernel",
                     "project_adjoint": "projectAdjointBatchKernel"}
     if bound == "hbm":
         achieved = amount / secs / 1e9
