@@ -111,7 +111,7 @@ class BatchStats(C.Structure):
 class BatchBuffers(C.Structure):
     _fields_ = [("pairs", C.c_uint64), ("key_shift", C.c_uint32), ("slot_bits", C.c_uint32),
                 ("total_tiles", C.c_uint32), ("views", C.c_uint32), ("sorted_pairs", C.c_void_p),
-                ("ranges", C.c_void_p), ("tile_bases", C.POINTER(C.c_uint32))]
+                ("ranges", C.c_void_p), ("sorted_values", C.c_void_p), ("tile_bases", C.POINTER(C.c_uint32))]
 
 
 class Encoding(C.Structure):
@@ -146,6 +146,7 @@ SIGNATURES = {
     "ath_batch_train_step": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads), _P]),
     "ath_batch_check": (C.c_int32, [_P, C.POINTER(BatchStats), _P]),
     "ath_batch_buffers_of": (C.c_int32, [_P, C.POINTER(BatchBuffers), _P]),
+    "ath_batch_set_key_mode": (C.c_int32, [_P, C.c_uint32]),
     "ath_batch_time_stages": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads),
                                           C.POINTER(C.c_float), _P]),
     "ath_batch_tune": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads), C.c_uint32,

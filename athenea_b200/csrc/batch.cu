@@ -233,8 +233,8 @@ __device__ __forceinline__ void colourAdjointFast(const MixedSh& sh, const Gauss
 template <uint32_t L>
 __global__ void __launch_bounds__(kProjThreads)
     projectEmitKernel(const BatchConst B, const BatchView* __restrict__ views, float4* __restrict__ recs,
-                      uint64_t* __restrict__ pairs, uint64_t* __restrict__ flags, uint32_t* __restrict__ words,
-                      uint32_t gaussBlocks) {
+                      uint64_t* __restrict__ pairs, uint32_t* __restrict__ values, uint64_t* __restrict__ flags,
+                      uint32_t* __restrict__ words, uint32_t gaussBlocks) {
     __shared__ uint32_t sTicket;
     __shared__ uint32_t sWarp[kProjThreads / 32];
     __shared__ uint32_t sPrefix;
@@ -378,7 +378,10 @@ __global__ void __launch_bounds__(kProjThreads)
     if (!touched) return;
     // the pairs, in the rect's row-major order (splat_emit.slang:37-49)
     uint64_t at = (uint64_t)sPrefix + warpBase + (incl - touched);
-    const uint64_t head = ((uint64_t)(sView.tileBase) << B.keyShift) | ((uint64_t)depthKey << B.slotBits) | i;
+    // packed: (global tile << keyShift) | (depth << slotBits) | Gaussian; wide: (global tile << 24) | depth,
+    // the Gaussian beside it in `values`
+    const uint64_t head = ((uint64_t)(sView.tileBase) << B.keyShift) | ((uint64_t)depthKey << B.slotBits) |
+                          (B.wide ? 0u : i);
     const uint32_t cols = rx1 - rx0 + 1;
     const uint32_t area = cols * (ry1 - ry0 + 1);
     if (area <= 64 && !wide) {
@@ -387,7 +390,10 @@ __global__ void __launch_bounds__(kProjThreads)
             const uint32_t bit = (uint32_t)__ffsll((long long)m) - 1u;
             m &= m - 1;
             const uint32_t tx = rx0 + bit % cols, ty = ry0 + bit / cols;
-            if (at < B.capacity) pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
+            if (at < B.capacity) {
+                pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
+                if (B.wide) values[at] = i;
+            }
             ++at;
         }
     } else {
@@ -399,7 +405,10 @@ __global__ void __launch_bounds__(kProjThreads)
                 const float best = wide ? minPowerOverBoxFactored(ca, cb, cc, fr, fs, lx, ly, hx, hy)
                                         : minPowerOverBox(ca, cb, cc, lx, ly, hx, hy);
                 if (best <= cutoff) {
-                    if (at < B.capacity) pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
+                    if (at < B.capacity) {
+                        pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
+                        if (B.wide) values[at] = i;
+                    }
                     ++at;
                 }
             }
@@ -526,7 +535,9 @@ struct ath_batch {
     std::vector<uint32_t> widths, heights, tileBases;
     uint32_t lastSorted = 0, lastSlotBits = 0;
     // scratch
-    DeviceBuffer words, recs, grads, projFlags, pairs[2], sortHist, sortFlags, ranges, finalT, lastContrib, dL;
+    DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges, finalT, lastContrib, dL;
+    uint32_t keyMode = 0;      // 0 packed when it fits in 64 bits, else wide; 1 packed; 2 wide
+    bool lastWide = false;
     uint32_t count = 0;
     uint64_t capacity = 0;
     bool resize = true;
@@ -595,12 +606,22 @@ void placeCloud(ath_batch* b, const double objectToWorld[16]) {
     }
 }
 
+// Whether a step's pairs take the wide form: a 64-bit (tile << 24 | depth) key
+// and a 32-bit Gaussian index, sorted as key and value. The packed form (one
+// 64-bit word) is used while tile, depth and Gaussian bits fit in 64.
+bool wideKeys(const ath_batch* b, uint32_t count) {
+    if (b->keyMode == 2) return true;
+    if (b->keyMode == 1) return false;
+    return 24 + bitsForValues(std::max<uint64_t>(count, 2)) + b->tileBits > 64;
+}
+
 BatchConst batchConst(const ath_batch* b, const ath_mixed_params& P) {
     BatchConst B{};
     B.views = (uint32_t)b->views.size();
     B.count = P.count;
     B.tile = b->tile;
-    B.slotBits = bitsForValues(std::max<uint64_t>(P.count, 2));
+    B.wide = wideKeys(b, P.count) ? 1u : 0u;
+    B.slotBits = B.wide ? 0u : bitsForValues(std::max<uint64_t>(P.count, 2));
     B.keyShift = 24 + B.slotBits;
     B.totalTiles = b->totalTiles;
     B.totalPixels = b->totalPixels;
@@ -639,6 +660,7 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
     L.views = static_cast<const BatchView*>(b->viewsDev.ptr);
     L.ranges = static_cast<const uint2*>(b->ranges.ptr);
     L.pairs = static_cast<const uint64_t*>(b->pairs[sorted].ptr);
+    L.values = B.wide ? static_cast<const uint32_t*>(b->values[sorted].ptr) : nullptr;
     L.recs = static_cast<const float4*>(b->recs.ptr);
     L.words = static_cast<uint32_t*>(b->words.ptr);
     L.finalT = static_cast<float*>(b->finalT.ptr);
@@ -665,20 +687,23 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     if (err == cudaSuccess && P.count)
         projectEmitKernel<kLayoutMixed><<<gaussBlocks * V, kProjThreads, 0, stream>>>(
             B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<float4*>(b->recs.ptr),
-            static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint64_t*>(b->projFlags.ptr), words, gaussBlocks);
+            static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint32_t*>(b->values[0].ptr),
+            static_cast<uint64_t*>(b->projFlags.ptr), words, gaussBlocks);
     if (err == cudaSuccess) err = cudaGetLastError();
     if (countOnly || err != cudaSuccess) return err;
     mark(1);
     uint64_t* keys[2] = {static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint64_t*>(b->pairs[1].ptr)};
+    uint32_t* vals[2] = {static_cast<uint32_t*>(b->values[0].ptr), static_cast<uint32_t*>(b->values[1].ptr)};
     const uint32_t bits = 24 + b->tileBits;
-    err = launchSortDevice(keys, nullptr, (uint32_t)b->capacity, words + kBatchPairsLo, words + kBatchEpoch,
-                           B.slotBits, bits, static_cast<uint32_t*>(b->sortHist.ptr),
+    err = launchSortDevice(keys, B.wide ? vals : nullptr, (uint32_t)b->capacity, words + kBatchPairsLo,
+                           words + kBatchEpoch, B.slotBits, bits, static_cast<uint32_t*>(b->sortHist.ptr),
                            static_cast<uint64_t*>(b->sortFlags.ptr), words + kBatchSortTickets, words + kBatchStatus,
                            stream);
     const uint32_t sorted = sortResultIndex(2, bits);
     mark(2);
     b->lastSorted = sorted;
     b->lastSlotBits = B.slotBits;
+    b->lastWide = B.wide != 0;
     if (err == cudaSuccess) err = cudaMemsetAsync(b->ranges.ptr, 0, (size_t)b->totalTiles * 8, stream);
     if (err == cudaSuccess) {
         const uint32_t grid = std::max<uint32_t>(1, std::min<uint64_t>((b->capacity + 255) / 256, (uint64_t)b->sms * 8));
@@ -742,10 +767,15 @@ ath_status sizePairs(ath_batch* b, const ath_mixed_params& P, cudaStream_t strea
     const uint64_t pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
     const uint64_t want = pairs + pairs / 7 + 65536;
     if (want > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 pairs in one batched step");
-    if (want > b->capacity || !b->pairs[0].ptr) {
-        for (int k = 0; k < 2; ++k)
-            if ((err = b->pairs[k].reserve((size_t)want * 8)) != cudaSuccess) return failCuda(err, "reserving the pairs");
-        b->capacity = want;
+    const bool wide = wideKeys(b, b->count);
+    if (want > b->capacity || !b->pairs[0].ptr || (wide && !b->values[0].ptr)) {
+        const uint64_t room = std::max<uint64_t>(want, b->capacity);
+        for (int k = 0; k < 2; ++k) {
+            if ((err = b->pairs[k].reserve((size_t)room * 8)) != cudaSuccess) return failCuda(err, "reserving the pairs");
+            if (wide && (err = b->values[k].reserve((size_t)room * 4)) != cudaSuccess)
+                return failCuda(err, "reserving the pairs' Gaussians");
+        }
+        b->capacity = room;
     }
     const uint32_t bits = 24 + b->tileBits;
     err = b->sortFlags.reserve(sortFlagWords((uint32_t)b->capacity, bits) * 8);
@@ -830,6 +860,17 @@ extern "C" ath_status ath_batch_set_views(ath_batch* b, const ath_view* views, u
     return ATH_OK;
 }
 
+extern "C" ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode) {
+    if (!b) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_key_mode: null batch");
+    if (mode > 2) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_key_mode: mode must be 0, 1 or 2");
+    if (mode != b->keyMode) {
+        b->keyMode = mode;
+        b->resize = true;   // the next step sizes (and, for wide pairs, allocates) again
+        dropGraph(b);
+    }
+    return ATH_OK;
+}
+
 extern "C" ath_status ath_batch_set_tuning(ath_batch* b, uint32_t tile, uint32_t blockBatch) {
     if (!b) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_tuning: null handle");
     if ((tile != 8 && tile != 16 && tile != 32) || (blockBatch != 64 && blockBatch != 128 && blockBatch != 256))
@@ -865,8 +906,11 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
         (reinterpret_cast<uintptr_t>(P.quats) & 15u))
         return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: a cloud array is not aligned to its element");
     const uint32_t slotBits = bitsForValues(std::max<uint64_t>(P.count, 2));
-    if (24 + slotBits + b->tileBits > 64)
-        return fail(ATH_E_UNSUPPORTED, "ath_batch_train_step: tiles, depth key and Gaussian index exceed 64 bits");
+    if (b->keyMode == 1 && 24 + slotBits + b->tileBits > 64)
+        return fail(ATH_E_UNSUPPORTED, "ath_batch_train_step: tiles, depth key and Gaussian index exceed 64 bits "
+                                       "(packed keys asked for; the wide form has no such limit)");
+    if (24 + b->tileBits > 64)
+        return fail(ATH_E_UNSUPPORTED, "ath_batch_train_step: more than 2^40 tiles");
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
     ath_status st = ATH_OK;
     if (P.count != b->count) {
@@ -975,6 +1019,7 @@ extern "C" ath_status ath_batch_buffers_of(ath_batch* b, ath_batch_buffers* out,
     out->pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
     out->key_shift = 24 + b->lastSlotBits;
     out->slot_bits = b->lastSlotBits;
+    out->sorted_values = b->lastWide ? static_cast<const uint32_t*>(b->values[b->lastSorted].ptr) : nullptr;
     out->total_tiles = b->totalTiles;
     out->views = (uint32_t)b->views.size();
     out->sorted_pairs = static_cast<const uint64_t*>(b->pairs[b->lastSorted].ptr);

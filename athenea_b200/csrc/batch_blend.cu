@@ -71,7 +71,8 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
 template <uint32_t T, uint32_t NB>
 __global__ void __launch_bounds__(T * T / 2)
     blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
-                     const uint64_t* __restrict__ pairs, const float4* __restrict__ recs,
+                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
+                     const float4* __restrict__ recs,
                      float4* __restrict__ colour, float* __restrict__ finalT, uint32_t* __restrict__ lastContrib,
                      const float* __restrict__ target, float4* __restrict__ dL, float* __restrict__ loss,
                      uint32_t* __restrict__ words) {
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(T * T / 2)
             if (__syncthreads_count(done[0] && done[1]) == kThreads) break;
             const uint32_t count = min(NB, range.y - first);
             for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
-                const size_t s = (recBase + (pairs[first + k] & slotMask)) * 3;
+                const size_t s = (recBase + gaussianOf(pairs, values, slotMask, first + k)) * 3;
                 const float4 sc = recs[s + 0];
                 const float4 c = recs[s + 1];
                 const float4 rgb = recs[s + 2];
@@ -227,7 +228,8 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
 template <uint32_t T, uint32_t NB>
 __global__ void __launch_bounds__(T * T / 2)
     blendAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
-                            const uint64_t* __restrict__ pairs, const float4* __restrict__ recs,
+                            const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
+                            const float4* __restrict__ recs,
                             const float* __restrict__ finalT, const uint32_t* __restrict__ lastContrib,
                             const float4* __restrict__ dLdColour, float* __restrict__ grads,
                             uint32_t* __restrict__ words) {
@@ -286,7 +288,7 @@ __global__ void __launch_bounds__(T * T / 2)
             const uint32_t batchStart = batchEnd - range.x > NB ? batchEnd - NB : range.x;
             const uint32_t count = batchEnd - batchStart;
             for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
-                const uint32_t s = (uint32_t)(pairs[batchStart + k] & slotMask);
+                const uint32_t s = gaussianOf(pairs, values, slotMask, batchStart + k);
                 sRec[k] = s;
                 const size_t q = (recBase + s) * 3;
                 const float4 sc = recs[q + 0];
@@ -411,8 +413,8 @@ template <uint32_t T, uint32_t NB>
 cudaError_t blendWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
                       const float* target, float4* dL, float* loss) {
     const int grid = residentGrid(blendBatchKernel<T, NB>, T * T / 2, L.sms);
-    blendBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.recs, colour, L.finalT,
-                                                                L.lastContrib, target, dL, loss, L.words);
+    blendBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs, colour,
+                                                                L.finalT, L.lastContrib, target, dL, loss, L.words);
     return cudaGetLastError();
 }
 
@@ -420,8 +422,8 @@ template <uint32_t T, uint32_t NB>
 cudaError_t adjointWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, const float4* dL,
                         float* grads) {
     const int grid = residentGrid(blendAdjointBatchKernel<T, NB>, T * T / 2, L.sms);
-    blendAdjointBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.recs, L.finalT,
-                                                                       L.lastContrib, dL, grads, L.words);
+    blendAdjointBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs,
+                                                                       L.finalT, L.lastContrib, dL, grads, L.words);
     return cudaGetLastError();
 }
 

@@ -30,8 +30,9 @@ struct BatchConst {
     uint32_t views;
     uint32_t count;          // Gaussians
     uint32_t tile;           // 8, 16 or 32
-    uint32_t slotBits;       // bits of a Gaussian index in a packed pair
-    uint32_t keyShift;       // 24 + slotBits: where the global tile starts in a packed pair
+    uint32_t slotBits;       // bits of a Gaussian index in a packed pair (0 when wide)
+    uint32_t keyShift;       // where the global tile starts in a pair's key: 24 + slotBits, or 24 when wide
+    uint32_t wide;           // 1: key (tile << 24 | depth) and a separate u32 Gaussian index a pair
     uint32_t totalTiles, totalPixels;
     uint32_t shLimit, antialias, linear, restPerColour;
     float bg[4];
@@ -96,6 +97,12 @@ __device__ __forceinline__ float minPowerOverBoxFactored(float a, float b, float
     return best;
 }
 
+// The Gaussian of sorted pair i: in the packed key's low bits, or the wide form's value.
+__device__ __forceinline__ uint32_t gaussianOf(const uint64_t* pairs, const uint32_t* values, uint64_t slotMask,
+                                              uint32_t i) {
+    return values ? values[i] : (uint32_t)(pairs[i] & slotMask);
+}
+
 // The view of a global tile or pixel: the last view whose base is at most `x`.
 __device__ __forceinline__ uint32_t viewOf(const uint32_t* bases, uint32_t views, uint32_t x) {
     uint32_t lo = 0, hi = views;
@@ -111,6 +118,7 @@ struct BlendLaunch {
     const BatchView* views;
     const uint2* ranges;
     const uint64_t* pairs;   // sorted
+    const uint32_t* values;  // wide pairs: the Gaussian of each sorted pair; null when packed
     const float4* recs;
     uint32_t* words;
     float* finalT;

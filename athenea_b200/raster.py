@@ -483,6 +483,10 @@ class BatchTrainer:
     def set_tuning(self, tile: int, block_batch: int) -> None:
         check(N.lib().ath_batch_set_tuning(self._h, tile, block_batch))
 
+    def set_key_mode(self, mode: int) -> None:
+        """ath_batch_set_key_mode: 0 packed while it fits in 64 bits, 1 packed, 2 wide."""
+        check(N.lib().ath_batch_set_key_mode(self._h, mode))
+
     def step(self, params: MixedParams, target: torch.Tensor, colour: torch.Tensor, loss: torch.Tensor,
              grads: "Params", stream: torch.cuda.Stream | None = None) -> None:
         g = N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
@@ -524,4 +528,5 @@ class BatchTrainer:
         b = N.BatchBuffers()
         check(N.lib().ath_batch_buffers_of(self._h, C.byref(b), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
         return dict(pairs=b.pairs, key_shift=b.key_shift, slot_bits=b.slot_bits, total_tiles=b.total_tiles,
-                    sorted_pairs=b.sorted_pairs, ranges=b.ranges, tile_bases=[b.tile_bases[k] for k in range(b.views)])
+                    sorted_pairs=b.sorted_pairs, ranges=b.ranges, sorted_values=b.sorted_values,
+                    tile_bases=[b.tile_bases[k] for k in range(b.views)])

@@ -33,7 +33,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(count=1_500_000, width=1920, height=1080, views=8, clustered=True, sh_degree=3, vfov=60.0)
+WORKLOAD = dict(count=1_500_000, width=1920, height=1080, views=8, clustered=True, sh_degree=3, vfov=60.0,
+                name="clustered-1.5M-1920x1080", mixed_sizes=False)
 METRIC = "fwd+bwd ms/view, 1.5M Gaussians 1080p, batched+BF16 vs plain FP32, err<=1e-4"
 
 
@@ -121,15 +122,19 @@ def make_scene(seed: int):
     return recs, enc
 
 
-def view_cameras(views: int, first: int = 0):
+def view_specs(views: int, first: int = 0):
+    """[(projection, width, height)] of views first .. first + views - 1 of the workload's walk."""
     import athenea_b200 as A
     from athenea_b200 import scenes
-    W, H = WORKLOAD["width"], WORKLOAD["height"]
+    total = max(first + views, 1)
+    sizes = (scenes.view_sizes(total, scenes.SEED) if WORKLOAD["mixed_sizes"]
+             else [(WORKLOAD["width"], WORKLOAD["height"])] * total)
     out = []
     for v in range(first, first + views):
+        W, H = sizes[v]
         eye = scenes.circle_eye(v, max(views, 1) * 4, 3.0, 0.3)
         cam = A.pinhole_for_vertical_fov(eye, (0, 0, 0), W, H, WORKLOAD["vfov"])
-        out.append(cam.projection_for(W, H))
+        out.append((cam.projection_for(W, H), W, H))
     return out
 
 
@@ -139,33 +144,34 @@ class PlainTrainer:
     the mean-L2 loss's gradient (ath_l2_loss) and the backward (ath_raster_backward), one
     view after another, gradients added into one set."""
 
-    def __init__(self, params, projs, targets_dev, W, H, dev):
+    def __init__(self, params, views, targets_dev, dev):
         import torch
         import athenea_b200 as A
         self.A = A
         self.P = params
-        self.projs = projs
+        self.views = views
         self.targets = targets_dev
-        self.W, self.H = W, H
         self.raster = A.TileRasterizer.create()
-        self.settings = A.RenderSettings(width=W, height=H)
-        self.frames = A.RenderTargets.make(W, H, device=dev)
-        self.dl = torch.empty((W * H, 4), dtype=torch.float32, device=dev)
+        self.frames, self.dl = {}, {}
+        for _, W, H in views:
+            if (W, H) not in self.frames:
+                self.frames[(W, H)] = A.RenderTargets.make(W, H, device=dev)
+                self.dl[(W, H)] = torch.empty((W * H, 4), dtype=torch.float32, device=dev)
         self.loss = torch.zeros(1, dtype=torch.float32, device=dev)
         self.grads = params.zeros_like()
 
-    def step(self, stream, targets=None, ready=None):
+    def step(self, stream, targets=None):
         targets = targets if targets is not None else self.targets
         self.loss.zero_()
         for g in (self.grads.means, self.grads.scales, self.grads.quats, self.grads.sh):
             g.zero_()
         stats = None
-        for v, proj in enumerate(self.projs):
-            if ready is not None:
-                stream.wait_event(ready[v])
-            stats = self.raster.render_params(proj, self.P, self.settings, self.frames, stream=stream)
-            self.A.l2_loss(self.frames.colour, targets[v], self.dl, self.loss, stream=stream)
-            self.raster.backward(self.dl, self.grads, stream=stream)
+        for v, (proj, W, H) in enumerate(self.views):
+            frames, dl = self.frames[(W, H)], self.dl[(W, H)]
+            stats = self.raster.render_params(proj, self.P, self.A.RenderSettings(width=W, height=H), frames,
+                                              stream=stream)
+            self.A.l2_loss(frames.colour, targets[v], dl, self.loss, stream=stream)
+            self.raster.backward(dl, self.grads, stream=stream)
         return stats
 
 
@@ -208,7 +214,6 @@ def run_ours(args) -> dict | None:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device("cuda", local)
     V = WORKLOAD["views"]
-    W, H = WORKLOAD["width"], WORKLOAD["height"]
     p = scenes.params(WORKLOAD["count"], WORKLOAD["clustered"], 20261203 + 1, WORKLOAD["sh_degree"])
     params = A.Params(*[torch.from_numpy(p[k]).to(dev) for k in ("means", "scales", "quats", "sh")],
                       sh_degree=p["sh_degree"])
@@ -216,10 +221,10 @@ def run_ours(args) -> dict | None:
     mixed = A.MixedParams.from_params(params)
     # weak scaling: every rank draws V views of its own, views rank*V .. rank*V + V - 1
     shard = A.shard_views(V * world, rank, world)
-    projs = view_cameras(len(shard), first=shard.start)
-    views = [(proj, W, H) for proj in projs]
+    views = view_specs(len(shard), first=shard.start)
+    pixel_base = np.cumsum([0] + [W * H for _, W, H in views])
     gen = torch.Generator().manual_seed(20261203 + 7 + rank)
-    host_target = torch.rand((V * W * H, 3), generator=gen).pin_memory()
+    host_target = torch.rand((int(pixel_base[-1]), 3), generator=gen).pin_memory()
     target = host_target.to(dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -298,31 +303,34 @@ def run_ours(args) -> dict | None:
     # ---- the plain FP32 path, one view at a time, same scene and views --------
     ms_plain, plain_stages = None, None
     if not args.no_plain:
-        dev_targets = [target[v * W * H:(v + 1) * W * H] for v in range(V)]
-        plain = PlainTrainer(params, projs, dev_targets, W, H, dev)
+        dev_targets = [target[int(pixel_base[v]):int(pixel_base[v + 1])] for v in range(len(views))]
+        plain = PlainTrainer(params, views, dev_targets, dev)
         for _ in range(args.warmup):
             plain.step(stream)
         ms_plain = _timed(lambda: plain.step(stream), args.steps, stream, world, dev)
-        timed = A.RenderSettings(width=W, height=H, time_stages=True)
-        st = plain.raster.render_params(projs[0], params, timed, plain.frames, stream=stream)
+        proj0, W0, H0 = views[0]
+        timed = A.RenderSettings(width=W0, height=H0, time_stages=True)
+        frames0, dl0 = plain.frames[(W0, H0)], plain.dl[(W0, H0)]
+        st = plain.raster.render_params(proj0, params, timed, frames0, stream=stream)
         bw0, bw1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        A.l2_loss(plain.frames.colour, dev_targets[0], plain.dl, plain.loss, stream=stream)
+        A.l2_loss(frames0.colour, dev_targets[0], dl0, plain.loss, stream=stream)
         bw0.record(stream)
-        plain.raster.backward(plain.dl, plain.grads, stream=stream)
+        plain.raster.backward(dl0, plain.grads, stream=stream)
         bw1.record(stream)
         torch.cuda.synchronize()
         plain_stages = {"project_ms": st.project_ms, "emit_ms": st.emit_ms, "sort_and_ranges_ms": st.tile_sort_ms,
                         "blend_ms": st.blend_ms, "backward_ms": bw0.elapsed_time(bw1)}
 
     T = tuned["tile"]
-    total_tiles = V * ((W + T - 1) // T) * ((H + T - 1) // T)
+    total_tiles = sum(((W + T - 1) // T) * ((H + T - 1) // T) for _, W, H in views)
     passes = math.ceil((24 + max(1, math.ceil(math.log2(max(2, total_tiles))))) / 8)
     # the step's kernels: begin, projectEmit, histogram, the sort's passes, ranges,
     # blend (with the loss), blend adjoint, projection adjoint (memsets are not counted)
     launches = (2 + 1 + passes + 1 + 1 + 1 + 1) * args.steps
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
                stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
-               count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4)
+               count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4,
+               pixels=int(pixel_base[-1]), sizes=sorted({(W, H) for _, W, H in views}))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -373,9 +381,18 @@ def main():
     ap.add_argument("--block-batch", type=int, choices=[64, 128, 256], default=256,
                     help="records a block stages at once, with --tile")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
+    ap.add_argument("--workload", type=int, choices=[1, 3, 4], default=1,
+                    help="1: 1.5M clustered, 8 views of 1920x1080 (the headline); 3: 2.36M clustered, 64 views of "
+                         "mixed sizes; 4: 50M clustered, 8 views of 3840x2160")
     args = ap.parse_args()
-    WORKLOAD["views"] = args.views
-    WORKLOAD["count"] = args.gaussians
+    if args.workload != 1:
+        from athenea_b200 import scenes
+        w = scenes.WORKLOADS[args.workload]
+        WORKLOAD.update(count=w.count, width=w.width, height=w.height, views=w.views, clustered=w.clustered,
+                        name=w.name, mixed_sizes=args.workload == 3)
+    else:
+        WORKLOAD["views"] = args.views
+        WORKLOAD["count"] = args.gaussians
     args.warmup = max(args.warmup, 3)
     rank, world, _ = dist_env()
 
@@ -405,6 +422,7 @@ def main():
         return
     P = peaks()
     W, H, V = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["views"]
+    headline = args.workload == 1 and WORKLOAD["count"] == 1_500_000 and V == 8
     stats, stages = res["stats"], res["stages"]
     dominant = max(stages, key=stages.get)
     fp32_peak = 148 * 128 * 2 * P.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
@@ -436,7 +454,7 @@ def main():
                     "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2) at the measured max SM clock; "
                                    "no FP32 peak is measured"}
     roofline["kernel"] = kernel_names[dominant]
-    roofline["traffic"] = NCU_TRAFFIC.get(kernel_names[dominant])
+    roofline["traffic"] = NCU_TRAFFIC.get(kernel_names[dominant]) if headline else None
     roofline["stage_share"] = stages[dominant] / sum(stages.values())
     cpu = None if args.no_cpu else cpu_baseline()
     ms_view = res["ms_batched"] / V
@@ -444,7 +462,8 @@ def main():
         "metric": METRIC, "value": ms_view, "unit": "ms/view", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["ms_batched"], "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (SH bf16/e4m3)", "data": "synthetic (seeded; no dataset)",
-        "config": {"workload": "clustered-1.5M-1920x1080", "gaussians": WORKLOAD["count"], "width": W, "height": H,
+        "config": {"workload": WORKLOAD["name"], "gaussians": WORKLOAD["count"],
+                   "sizes": [f"{w}x{h}" for w, h in res["sizes"]], "pixels_per_gpu": res["pixels"],
                    "views_per_gpu": V, "sh_degree": 3, "tile": res["tuned"]["tile"],
                    "block_batch": res["tuned"]["block_batch"],
                    "path": "batched mixed-precision step: every view in one launch a stage, replayed from a CUDA "
@@ -452,7 +471,8 @@ def main():
                    "loss": "mean L2 a view against a target uniform in [0,1]^3, summed over views",
                    "parallelism": f"views sharded over {world} GPU(s), gradients all-reduced"
                                   if world > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (records 576 MB, pairs > 100 MB, targets 199 MB > 126 MB)"},
+                   "l2": f"inputs larger than L2 (records {V * WORKLOAD['count'] * 48 / 1e6:.0f} MB, pairs "
+                         f"{stats['pairs'] * 8 / 1e6:.0f} MB, targets {res['pixels'] * 12 / 1e6:.0f} MB > 126 MB)"},
         "plain_fp32": None if res["ms_plain"] is None else {
             "ms_per_view": res["ms_plain"] / V, "speedup": res["ms_plain"] / res["ms_batched"],
             "stages_ms": res["plain_stages"],

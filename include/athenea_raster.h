@@ -278,6 +278,14 @@ ath_status ath_batch_set_views(ath_batch* b, const ath_view* views, uint32_t cou
  * order whatever tile holds it. Default 16 and 256. */
 ath_status ath_batch_set_tuning(ath_batch* b, uint32_t tile, uint32_t block_batch);
 ath_status ath_batch_pixels(ath_batch* b, uint32_t* pixels);
+/* How a step's (tile, Gaussian) pairs are keyed. 0 (default): one 64-bit word
+ * (global tile | 24-bit depth key | Gaussian index), sorted keys-only, while
+ * those bits fit in 64, else 1 the wide form; 1: always the packed word (a step
+ * whose bits do not fit fails with ATH_E_UNSUPPORTED); 2: the wide form, a
+ * 64-bit (global tile << 24 | depth key) key and a 32-bit Gaussian index,
+ * sorted as key and value (50M Gaussians in 8 views of 3840x2160 need it). The
+ * pairs' order, and so the image, is the same either way. */
+ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode);
 /* One training step over every view, with nothing read back to the host:
  * project and emit every view's pairs (one launch), sort them all (one packed
  * 64-bit sort), blend every view's tiles (one persistent launch), the loss
@@ -305,14 +313,17 @@ ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params* params, c
                                  float* loss, ath_param_grads* grads, float ms[7], void* stream);
 
 /* The last step's sorted pairs and tile ranges, for inspection: device
- * pointers the batch owns, valid until its next step. A pair is
- * (global tile << key_shift) | (24-bit depth key << slot_bits) | Gaussian; view
- * v's tiles start at tile_bases[v] (host array of `views` entries). */
+ * pointers the batch owns, valid until its next step. A packed pair is
+ * (global tile << key_shift) | (24-bit depth key << slot_bits) | Gaussian; a
+ * wide pair's key is (global tile << 24) | depth key (slot_bits 0, key_shift 24)
+ * with its Gaussian in sorted_values. View v's tiles start at tile_bases[v]
+ * (host array of `views` entries). */
 typedef struct {
     uint64_t pairs;
     uint32_t key_shift, slot_bits, total_tiles, views;
     const uint64_t* sorted_pairs;
     const uint32_t* ranges;      /* 2 a global tile: [start, end) */
+    const uint32_t* sorted_values; /* wide pairs: the Gaussian of each sorted pair; NULL when packed */
     const uint32_t* tile_bases;  /* host */
 } ath_batch_buffers;
 

@@ -142,3 +142,39 @@ def test_replayed_step_draws_the_same_image_and_tune_picks_a_setting():
     np.testing.assert_array_equal(colour.cpu().numpy(), first)
     best = b.tune(M, torch.cat(targets).contiguous(), colour, loss, grads, repeats=2)
     assert best["tile"] in (8, 16, 32) and best["block_batch"] in (64, 128, 256) and best["ms_per_step"] > 0
+
+
+def test_wide_pairs_sort_and_draw_as_the_packed_ones():
+    """ath_batch_set_key_mode: the wide (key, Gaussian) pairs come out in the
+    packed pairs' order and draw the same image; the gradients agree."""
+    from tests import gpu_helpers as G
+    Pq, M = _scene(40_000, 12)
+    views = _views()
+    gen = torch.Generator().manual_seed(6)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    out = {}
+    for mode in (1, 2):
+        b = BatchTrainer()
+        b.set_key_mode(mode)
+        b, colour, loss, grads, stats = _batched(M, views, targets, trainer=b)
+        buf = b.buffers()
+        n = buf["pairs"]
+        keys = G.fetch(buf["sorted_pairs"], (n,), np.uint64)
+        if mode == 1:
+            assert buf["sorted_values"] is None
+            gauss = (keys & np.uint64((1 << buf["slot_bits"]) - 1)).astype(np.uint32)
+            tile_depth = keys >> np.uint64(buf["slot_bits"])
+        else:
+            assert buf["slot_bits"] == 0 and buf["key_shift"] == 24
+            gauss = G.fetch(buf["sorted_values"], (n,), np.uint32)
+            tile_depth = keys
+        out[mode] = (tile_depth, gauss, G.fetch(buf["ranges"], (buf["total_tiles"], 2), np.uint32),
+                     colour.cpu().numpy(), grads)
+    np.testing.assert_array_equal(out[1][0], out[2][0])
+    np.testing.assert_array_equal(out[1][1], out[2][1])
+    np.testing.assert_array_equal(out[1][2], out[2][2])
+    np.testing.assert_array_equal(out[1][3], out[2][3])
+    for name in ("means", "scales", "quats", "sh"):
+        a = getattr(out[1][4], name).cpu().numpy().ravel().astype(np.float64)
+        c = getattr(out[2][4], name).cpu().numpy().ravel().astype(np.float64)
+        assert np.abs(a - c).max() <= 1e-6 * (np.abs(c).max() + 1e-30) + 1e-12, name
