@@ -285,6 +285,7 @@ class TileRasterizer:
 
     def __init__(self, handle):
         self._h = handle
+        self._destroy = N.lib().ath_raster_destroy
 
     @staticmethod
     def create() -> "TileRasterizer":
@@ -293,9 +294,12 @@ class TileRasterizer:
         return TileRasterizer(h)
 
     def __del__(self):
+        # the destroy function is held by the instance: at interpreter exit the
+        # module's globals may already be gone
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            N.lib().ath_raster_destroy(h)
+        destroy = getattr(self, "_destroy", None)
+        if h is not None and h.value and destroy is not None:
+            destroy(h)
             self._h = None
 
     def render(self, camera, instances, settings: RenderSettings, targets: RenderTargets,
@@ -458,13 +462,17 @@ class BatchTrainer:
         h = C.c_void_p()
         check(N.lib().ath_batch_create(C.byref(h)))
         self._h = h
+        self._destroy = N.lib().ath_batch_destroy
         self.pixels = 0
         self.views = []
 
     def __del__(self):
+        # the destroy function is held by the instance: at interpreter exit the
+        # module's globals may already be gone
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            N.lib().ath_batch_destroy(h)
+        destroy = getattr(self, "_destroy", None)
+        if h is not None and h.value and destroy is not None:
+            destroy(h)
             self._h = None
 
     def set_views(self, views, settings: RenderSettings | None = None) -> None:
