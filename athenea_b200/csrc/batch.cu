@@ -300,44 +300,15 @@ __global__ void __launch_bounds__(kProjThreads)
                             if (minPowerOverBoxFactored(ca, cb, cc, fr, fs, lx, ly, hx, hy) <= cutoff) touched += 1;
                         }
                 } else {
-                    // Conservative pre-tests ahead of the exact least-power test
-                    // (frame.slang:354-379), which costs four divisions a tile: the
-                    // least power over a box is at most q at the box point nearest
-                    // the centre, and at least lambdaMin(conic) = 1 / lambdaMax(cov)
-                    // times that point's squared distance. Clear of the cutoff by a
-                    // relative 2e-4 either bound decides as the exact test would (the
-                    // expanded form's rounding is under 1e-5 relative when
-                    // det >= 1e-2 trace^2); nearer the cutoff, or for a footprint less
-                    // well conditioned, the exact test runs. The tiles touched are the
-                    // exact test's, bit for bit.
-                    const float a2 = G.a + 0.3f, c2 = G.c + 0.3f, tr = a2 + c2;
-                    const bool pretest = G.det >= 1e-2f * (tr * tr);
-                    const float half = 0.5f * (a2 - c2);
-                    const float lamMin = 1.0f / (0.5f * tr + sqrtf(half * half + G.b * G.b));
-                    const float sure = cutoff * (1.0f - 2e-4f), never = cutoff * (1.0f + 2e-4f);
                     for (uint32_t ty = ry0; ty <= ry1; ++ty) {
                         const float loy = ((float)(ty * T) + 0.5f) - cy;
                         const float hiy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
-                        // the row's x* = -b y / a at its two y edges, when the exact test needs them
-                        bool rowDone = false;
-                        float xLo = 0.0f, xHi = 0.0f;
+                        // the row's x* = -b y / a at its two y edges
+                        const float xLo = ca > 1e-12f ? ((-cb) * loy) / ca : 0.0f;
+                        const float xHi = ca > 1e-12f ? ((-cb) * hiy) / ca : 0.0f;
                         for (uint32_t tx = rx0; tx <= rx1; ++tx, ++bit) {
                             const float lox = ((float)(tx * T) + 0.5f) - cx;
                             const float hix = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
-                            if (pretest) {
-                                const float nx = clampf(0.0f, lox, hix), ny = clampf(0.0f, loy, hiy);
-                                if (quad(ca, cb, cc, nx, ny) <= sure) {
-                                    touched += 1;
-                                    if (bit < 64) mask |= 1ull << bit;
-                                    continue;
-                                }
-                                if (lamMin * (nx * nx + ny * ny) > never) continue;
-                            }
-                            if (!rowDone) {
-                                xLo = ca > 1e-12f ? ((-cb) * loy) / ca : 0.0f;
-                                xHi = ca > 1e-12f ? ((-cb) * hiy) / ca : 0.0f;
-                                rowDone = true;
-                            }
                             float best;
                             if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) {
                                 best = 0.0f;
