@@ -395,35 +395,66 @@ void orc_render_params_sampled_f64(const orc_frame64* f, uint32_t count, const f
                                    const float* quats, const float* sh, uint32_t shStride, uint32_t shDegree,
                                    double* colour, double* depth, uint8_t* nearDecision, double margin,
                                    uint32_t tileStride, uint32_t tileOffset, int threads) {
-    Frame64 fr;
-    fr.recs.resize(count);
-#pragma omp parallel for schedule(static, 4096) num_threads(threads > 0 ? threads : omp_get_max_threads())
-    for (int64_t ii = 0; ii < (int64_t)count; ++ii) {
-        const uint32_t i = (uint32_t)ii;
-        Gauss64 g{};
-        for (int k = 0; k < 3; ++k) {
-            g.p[k] = means[(size_t)i * 4 + k];
-            g.scale[k] = std::exp((double)scales[(size_t)i * 4 + k]);
+    // Only the records whose rect reaches a sampled tile are kept (a cloud of
+    // tens of millions fits this way), in slot order, each with its slot.
+    const uint32_t stride = tileStride == 0 ? 1 : tileStride;
+    const uint32_t tilesX = (f->width + kTile - 1) / kTile;
+    const auto reachesSample = [&](const Rec64& r) {
+        if (!r.live && !r.faintNear) return false;
+        const double x1 = r.cx - r.ex, x2 = r.cx + r.ex, y1 = r.cy - r.ey, y2 = r.cy + r.ey;
+        if (x2 < 0 || y2 < 0 || x1 >= f->width || y1 >= f->height) return false;
+        if (stride == 1) return true;
+        const uint32_t tx0 = (uint32_t)std::max(x1, 0.0) / kTile, ty0 = (uint32_t)std::max(y1, 0.0) / kTile;
+        const uint32_t tx1 = (uint32_t)std::min(x2, f->width - 1.0) / kTile,
+                       ty1 = (uint32_t)std::min(y2, f->height - 1.0) / kTile;
+        for (uint32_t ty = ty0; ty <= ty1; ++ty) {
+            const uint32_t first = ty * tilesX + tx0;
+            const uint32_t gap = (tileOffset + stride - first % stride) % stride;   // to the next sampled tile
+            if (gap <= tx1 - tx0) return true;
         }
-        g.opacity = sigmoid(means[(size_t)i * 4 + 3]);
-        const float* q = quats + (size_t)i * 4;   // w x y z
-        const double qw = q[0], qx = q[1], qy = q[2], qz = q[3];
-        const double n = std::sqrt(qw * qw + qx * qx + qy * qy + qz * qz);
-        g.q[0] = qx / n;
-        g.q[1] = qy / n;
-        g.q[2] = qz / n;
-        g.q[3] = qw / n;
-        const float* c = sh + (size_t)i * shStride;
-        for (int k = 0; k < 3; ++k) g.base[k] = 0.5 + kSH0 * (double)c[k];
-        const uint32_t bases = shDegree >= 3 ? 15 : shDegree == 2 ? 8 : shDegree == 1 ? 3 : 0;
-        for (uint32_t b = 0; b < bases && 3 + b * 3 + 2 < shStride; ++b)
-            for (int ch = 0; ch < 3; ++ch) g.rest[b][ch] = c[3 + b * 3 + ch];
-        g.degree = shDegree;
-        fr.recs[i] = project64(*f, g, margin);
-        fr.recs[i].slot = i;
+        return false;
+    };
+    constexpr uint32_t kChunk = 1u << 16;
+    const uint32_t chunks = (count + kChunk - 1) / kChunk;
+    std::vector<std::vector<Rec64>> kept(chunks);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (int64_t cc = 0; cc < (int64_t)chunks; ++cc) {
+        const uint32_t end = std::min<uint32_t>(count, (uint32_t)(cc + 1) * kChunk);
+        for (uint32_t i = (uint32_t)cc * kChunk; i < end; ++i) {
+            Gauss64 g{};
+            for (int k = 0; k < 3; ++k) {
+                g.p[k] = means[(size_t)i * 4 + k];
+                g.scale[k] = std::exp((double)scales[(size_t)i * 4 + k]);
+            }
+            g.opacity = sigmoid(means[(size_t)i * 4 + 3]);
+            const float* q = quats + (size_t)i * 4;   // w x y z
+            const double qw = q[0], qx = q[1], qy = q[2], qz = q[3];
+            const double n = std::sqrt(qw * qw + qx * qx + qy * qy + qz * qz);
+            g.q[0] = qx / n;
+            g.q[1] = qy / n;
+            g.q[2] = qz / n;
+            g.q[3] = qw / n;
+            const float* c = sh + (size_t)i * shStride;
+            for (int k = 0; k < 3; ++k) g.base[k] = 0.5 + kSH0 * (double)c[k];
+            const uint32_t bases = shDegree >= 3 ? 15 : shDegree == 2 ? 8 : shDegree == 1 ? 3 : 0;
+            for (uint32_t b = 0; b < bases && 3 + b * 3 + 2 < shStride; ++b)
+                for (int ch = 0; ch < 3; ++ch) g.rest[b][ch] = c[3 + b * 3 + ch];
+            g.degree = shDegree;
+            Rec64 r = project64(*f, g, margin);
+            r.slot = i;
+            if (reachesSample(r)) kept[cc].push_back(r);
+        }
     }
-    bin64(*f, fr, margin, tileStride == 0 ? 1 : tileStride, tileOffset);
-    blend64(*f, fr, colour, depth, nearDecision, margin, tileStride == 0 ? 1 : tileStride, tileOffset, threads);
+    Frame64 fr;
+    size_t total = 0;
+    for (const auto& v : kept) total += v.size();
+    fr.recs.reserve(total);
+    for (auto& v : kept) {
+        fr.recs.insert(fr.recs.end(), v.begin(), v.end());
+        std::vector<Rec64>().swap(v);
+    }
+    bin64(*f, fr, margin, stride, tileOffset);
+    blend64(*f, fr, colour, depth, nearDecision, margin, stride, tileOffset, threads);
 }
 
 }   // extern "C"

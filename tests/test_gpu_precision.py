@@ -163,3 +163,25 @@ def test_near_degenerate_footprints_take_fp64_and_stay_within_tolerance(oracle):
           f"PSNR {plain['psnr']:.1f} dB")
     assert e["max_abs"] <= TOLERANCE, e
     assert e["near"] < 0.05, e
+
+
+def test_50m_gaussians_at_4k_against_fp64(oracle):
+    """The precision-at-scale workload: 50M clustered Gaussians, a 3840x2160
+    view (pairs take the wide key form: 26 Gaussian bits + 24 + 15 tile bits),
+    every 97th tile checked against FP64."""
+    count, W, H, stride = 50_000_000, 3840, 2160, 97
+    p = scenes.params(count, True, 20261203 + 4, 3)
+    P = _gpu_params(p)
+    M = A.MixedParams.from_params(P)
+    stored_sh = M.dequantized_sh().cpu().numpy()
+    P.sh = None   # the mixed layout holds the SH now; free the FP32 copy
+    torch.cuda.empty_cache()
+    views = _views([(W, H)])
+    images, stats = _batched_images(M, views)
+    assert stats["degenerate"] == 0
+    ref = _f64(oracle, views[0][0], W, H, p, stored_sh, stride, 0)
+    e = _errors(images[0], ref)
+    print(f"50M at 3840x2160: {stats['pairs']} pairs; max-abs {e['max_abs']:.3g} (pixels clear of a decision), "
+          f"PSNR {e['psnr']:.1f} dB over {e['sampled']} sampled pixels ({100 * e['near']:.3f}% near a decision)")
+    assert e["max_abs"] <= TOLERANCE, e
+    assert e["near"] < 0.05, e
