@@ -10,8 +10,8 @@ from ._native import AtheneaError  # noqa: F401
 from .parallel import GradientBuffer, shard_views  # noqa: F401
 from .raster import (BatchTrainer, Camera, CloudLoader, FrameStats, GpuSplats, Lens, MixedParams,  # noqa: F401
                      Params, RenderSettings, RenderTargets, SplatCounters, SplatEdit, SplatInstance, TileRasterizer,
-                     encoding_3dgs, l2_loss, pinhole_for_vertical_fov)
+                     encoding_3dgs, l2_loss, pinhole_for_vertical_fov, read_splat_ply)
 
 __all__ = ["AtheneaError", "BatchTrainer", "GradientBuffer", "shard_views", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "MixedParams",
            "Params", "RenderSettings", "RenderTargets", "SplatCounters", "SplatEdit", "SplatInstance",
-           "TileRasterizer", "encoding_3dgs", "l2_loss", "pinhole_for_vertical_fov"]
+           "TileRasterizer", "encoding_3dgs", "l2_loss", "pinhole_for_vertical_fov", "read_splat_ply"]

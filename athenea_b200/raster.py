@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -124,6 +125,20 @@ def encoding_3dgs(rest_per_colour: int, stride: int | None = None, **fields) -> 
 
 
 PER_DEGREE = (0, 3, 8, 15)
+
+
+def read_splat_ply(path: str) -> tuple[np.ndarray, dict]:
+    """ath_ply_read (readSplatPly, modules/io/src/SplatReaders.cpp:50-200): a 3DGS
+    PLY's vertex records as an (N, stride) float32 array and their encoding, for
+    CloudLoader.upload(torch.from_numpy(records).cuda(), encoding)."""
+    count = C.c_uint32()
+    e = N.Encoding()
+    raw = os.fsencode(path)
+    check(N.lib().ath_ply_read_header(raw, C.byref(count), C.byref(e)))
+    records = np.zeros((count.value, e.stride), np.float32)
+    check(N.lib().ath_ply_read(raw, records.ctypes.data_as(C.c_void_p), records.size, C.byref(count), C.byref(e)))
+    encoding = {k: int(getattr(e, k)) for k, _ in N.Encoding._fields_}
+    return records, encoding
 
 
 class CloudLoader:

@@ -408,6 +408,22 @@ typedef struct {
 ath_status ath_decode_records(const float* records, uint32_t count, const ath_encoding* encoding, float* positions,
                               uint32_t* shape, uint32_t* sh, uint32_t* kept, void* stream);
 
+/* ---- 3DGS PLY files (modules/io/src/SplatReaders.cpp:50-200, readSplatPly) --- */
+
+/* A trained splat cloud's header: its vertex count and the encoding of its
+ * records (stride = floats a record, one a vertex property in file order). Only
+ * binary little-endian files are read, as by the reference: another format, a
+ * list property, an unknown property type or harmonics that are not a whole
+ * degree are ATH_E_UNSUPPORTED; a missing x y z / opacity / scale_0..2 /
+ * rot_0..3 / f_dc_0..2 is ATH_E_INVALID_ARGUMENT; no file is ATH_E_NOT_FOUND. */
+ath_status ath_ply_read_header(const char* path, uint32_t* count, ath_encoding* encoding);
+/* The vertex element as count x stride floats into host memory `records`
+ * (`capacity` floats), every property widened to float; then
+ * ath_decode_records on a device copy gives the packed cloud. A file shorter
+ * than its header says is ATH_E_IO_FAILURE. */
+ath_status ath_ply_read(const char* path, float* records, uint64_t capacity, uint32_t* count,
+                        ath_encoding* encoding);
+
 /* ---- diagnostics --------------------------------------------------------- */
 
 /* The message of the last failure on this thread ("" when none). */

@@ -6,7 +6,9 @@ itself: the reference's own comparison scene (randomCloud(3000, 7) at 250x190,
 tests/render/test_splat_render.cpp:77-128, perspective section, with the
 partial last tile row and column), its depth keys, cull reasons, pairs and
 tile ranges in full, and the image and depth as SHA-256 of their FP32 bytes
-plus every 23rd pixel. The scene's 3DGS records come from tests/fixtures.py
+plus every 23rd pixel; and the reference's two splat files
+(tests/data/splats/tiny.ply and sh3.ply, read where the reference is checked
+out) as their vertex records and property names. The scene's 3DGS records come from tests/fixtures.py
 (SplatFixtures.h restated); their SHA-256 is kept to catch a drift there.
 
     python tests/golden/make_golden.py
@@ -49,6 +51,40 @@ def digest(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()
 
 
+REFERENCE_SPLATS = "/root/reference/tests/data/splats"
+
+
+def read_ply_numpy(path):
+    """An independent reader for the fixture files (binary little-endian, float
+    properties only): (records (N, properties) float32, property names)."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    end = raw.index(b"end_header\n") + len(b"end_header\n")
+    names, count = [], 0
+    for line in raw[:end].decode().splitlines():
+        w = line.split()
+        if w[:2] == ["element", "vertex"]:
+            count = int(w[2])
+        elif w and w[0] == "property":
+            assert w[1] == "float", line
+            names.append(w[2])
+    records = np.frombuffer(raw, np.float32, count * len(names), end).reshape(count, len(names)).copy()
+    return records, names, hashlib.sha256(raw).hexdigest()
+
+
+def ply_fixtures():
+    """tiny.ply (64 splats, degree 0) and sh3.ply (64 splats, degree 3) of the
+    reference's tests/data/splats, as their records and property names."""
+    out = {}
+    for name in ("tiny", "sh3"):
+        records, names, sha = read_ply_numpy(os.path.join(REFERENCE_SPLATS, name + ".ply"))
+        out[name + "_records"] = records
+        out[name + "_names"] = np.array(names)
+        out[name + "_sha256"] = sha
+    np.savez_compressed(os.path.join(HERE, "splats_tiny_sh3.npz"), **out)
+    print("wrote splats_tiny_sh3.npz:", {k: v.shape for k, v in out.items() if hasattr(v, "shape")})
+
+
 def main():
     from oracle import oracle as O
     O.build()
@@ -62,6 +98,8 @@ def main():
         ranges=b["ranges"], colour_sha256=digest(out["colour"]), depth_sha256=digest(out["depth"]),
         colour_sample=out["colour"][::STRIDE], depth_sample=out["depth"][::STRIDE])
     print("wrote raster_random3000_250x190.npz:", b["pairs"], "pairs,", int(out["proj"]["visible"].sum()), "visible")
+    if os.path.isdir(REFERENCE_SPLATS):
+        ply_fixtures()
 
 
 if __name__ == "__main__":
