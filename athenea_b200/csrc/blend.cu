@@ -18,15 +18,20 @@ namespace ath {
 namespace {
 
 constexpr uint32_t kBlendThreads = kTile * kTile;
+constexpr float kColourGradScale = 256.0f;   // frame.slang:36
 
+// kContribution: the contributionMode hooks of splat_blend.slang:364-398 (modes
+// 1 and 4); the plain frame builds without them.
+template <bool kContribution>
 __global__ void __launch_bounds__(kBlendThreads)
     blendKernel(const FrameConst F, uint32_t pairs, uint32_t slots, const uint2* __restrict__ ranges,
                 const uint32_t* __restrict__ pairValues, const float4* __restrict__ recs, float4* __restrict__ colour,
                 float* __restrict__ depth, float4* __restrict__ position, float* __restrict__ finalT,
-                uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ status) {
+                uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ status, Contribution contrib) {
     __shared__ float4 sScreen[kBlendThreads];
     __shared__ float4 sConic[kBlendThreads];
     __shared__ float4 sColour[kBlendThreads];
+    __shared__ uint32_t sSlot[kContribution ? kBlendThreads : 1];
 
     const uint32_t tile = blockIdx.x;
     const uint32_t tx = tile % F.tilesX, ty = tile / F.tilesX;
@@ -53,6 +58,7 @@ __global__ void __launch_bounds__(kBlendThreads)
                 atomicOr(status, kStatusIndexRange);
                 s = 0;
             }
+            if (kContribution) sSlot[threadIdx.x] = s;
             sScreen[threadIdx.x] = recs[(size_t)s * 3 + 0];
             sConic[threadIdx.x] = recs[(size_t)s * 3 + 1];
             sColour[threadIdx.x] = recs[(size_t)s * 3 + 2];
@@ -69,6 +75,22 @@ __global__ void __launch_bounds__(kBlendThreads)
             const float alpha = fminf(0.99f, falloffAlpha(fabsf(k.w), exp_f((-0.5f) * power)));
             if (alpha < kFaint) continue;
             const float weight = T * alpha;
+            if (kContribution) {
+                const uint32_t slot = sSlot[j];
+                if (contrib.mode == 1u) {
+                    atomicAdd(&contrib.words[slot], (uint32_t)(weight * 4096.0f + 0.5f));
+                } else {
+                    const uint32_t at = py * F.width + px;
+                    const float4 dl = reinterpret_cast<const float4*>(contrib.finalColour)[at];
+                    const float dls[3] = {dl.x, dl.y, dl.z};
+                    for (uint32_t ch = 0; ch < 3; ++ch) {
+                        const float gc = (weight * dls[ch]) * kColourGradScale;
+                        const int step = (int)floorf(gc + hash01((at * 3u + ch) ^ (slot * 2654435761u)));
+                        if (step != 0) atomicAdd(&contrib.words[slot * 4 + ch], (uint32_t)step);
+                    }
+                    atomicAdd(&contrib.words[slot * 4 + 3], (uint32_t)(weight * kColourGradScale + 0.5f));
+                }
+            }
             const float4 c = sColour[j];
             r = r + weight * c.x;
             g = g + weight * c.y;
@@ -108,11 +130,16 @@ __global__ void __launch_bounds__(kBlendThreads)
 
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
                         const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
-                        float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream) {
+                        float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream,
+                        const Contribution& contrib) {
     const uint32_t tiles = F.tilesX * F.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blendKernel<<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, depth,
-                                                    position, finalT, lastContrib, status);
+    if (contrib.mode != 0u)
+        blendKernel<true><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, depth,
+                                                              position, finalT, lastContrib, status, contrib);
+    else
+        blendKernel<false><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour,
+                                                               depth, position, finalT, lastContrib, status, contrib);
     return cudaGetLastError();
 }
 

@@ -372,6 +372,12 @@ ath_status checkFrame(const ath_settings& s, const ath_targets& targets) {
     if (targets.width != s.width || targets.height != s.height)
         return fail(ATH_E_INVALID_ARGUMENT, "the targets are not the frame's size");
     if (!targets.colour || !targets.depth) return fail(ATH_E_INVALID_ARGUMENT, "the targets need colour and depth");
+    if (s.contribution_mode != 0 && s.contribution_mode != 1 && s.contribution_mode != 4)
+        return fail(ATH_E_UNSUPPORTED, "contribution modes 2 and 3 are not built; 1 and 4 are");
+    if (s.contribution_mode != 0 && !s.contribution)
+        return fail(ATH_E_INVALID_ARGUMENT, "a contribution mode needs its contribution buffer");
+    if (s.contribution_mode == 4 && !s.final_colour)
+        return fail(ATH_E_INVALID_ARGUMENT, "contribution mode 4 needs final_colour (dL/dpixel)");
     return ATH_OK;
 }
 
@@ -463,7 +469,8 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
                           static_cast<const float4*>(r->recs.ptr), reinterpret_cast<float4*>(targets->colour),
                           targets->depth, reinterpret_cast<float4*>(targets->position),
                           training ? static_cast<float*>(r->finalT.ptr) : nullptr,
-                          training ? static_cast<uint32_t*>(r->lastContrib.ptr) : nullptr, words + kWordSticky, stream);
+                          training ? static_cast<uint32_t*>(r->lastContrib.ptr) : nullptr, words + kWordSticky, stream,
+                          Contribution{s.contribution_mode, s.contribution, s.final_colour});
     mark(5);
     if (err != cudaSuccess) return failCuda(err, "drawing the frame");
     r->lastSlots = slots;

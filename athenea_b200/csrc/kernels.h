@@ -45,9 +45,17 @@ cudaError_t launchSortDevice(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, c
                              uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream);
 
 // blend.cu
+// The reference's contributionMode hooks of the blend (modes 1 and 4).
+struct Contribution {
+    uint32_t mode = 0;                   // 0 none, 1 weights, 4 colour gradients
+    uint32_t* words = nullptr;
+    const float* finalColour = nullptr;  // mode 4: dL/dpixel, float4 a pixel
+};
+
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
                         const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
-                        float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream);
+                        float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream,
+                        const Contribution& contrib = Contribution{});
 
 // backward.cu
 cudaError_t launchBlendBackward(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,

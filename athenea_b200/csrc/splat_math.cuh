@@ -161,6 +161,14 @@ __device__ __forceinline__ float srgbToLinear(float c) {
     return c <= 0.04045f ? c / 12.92f : pow_f((c + 0.055f) / 1.055f, 2.4f);
 }
 
+// common/color.slang:43-47: a hash of v to [0, 1] (PCG-style), the dither of
+// the colour gradient's rounding (splat_blend.slang:393-394).
+__host__ __device__ __forceinline__ float hash01(uint32_t v) {
+    const uint32_t state = v * 747796405u + 2891336453u;
+    const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (float)((word >> 22u) ^ word) / 4294967295.0f;
+}
+
 // common/sh.slang:94-96
 __device__ __forceinline__ uint32_t degreeOf(uint32_t restPerColour) {
     return restPerColour >= 15 ? 3 : restPerColour >= 8 ? 2 : restPerColour >= 3 ? 1 : 0;

@@ -210,6 +210,9 @@ class RenderSettings:
     time_stages: bool = False
     count_splats: bool = False
     counters_tag: int = 0
+    contribution_mode: int = 0    # 1 weights, 4 colour gradients (TileRasterizer.h:351-367)
+    contribution: torch.Tensor | None = None    # int32: a word a slot (mode 1) or four (mode 4)
+    final_colour: torch.Tensor | None = None    # float4 a pixel: dL/dpixel for mode 4
 
     def _native(self) -> N.Settings:
         s = N.Settings()
@@ -225,6 +228,9 @@ class RenderSettings:
         s.time_stages = 1 if self.time_stages else 0
         s.count_splats = 1 if self.count_splats else 0
         s.counters_tag = self.counters_tag
+        s.contribution_mode = self.contribution_mode
+        s.contribution = _ptr(self.contribution) if self.contribution is not None else None
+        s.final_colour = _ptr(self.final_colour) if self.final_colour is not None else None
         return s
 
 

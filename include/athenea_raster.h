@@ -120,6 +120,18 @@ typedef struct {
     int32_t time_stages;        /* wait after each stage and fill the *_ms stats */
     int32_t count_splats;       /* count culls by reason (ath_raster_latest_counters) */
     uint64_t counters_tag;
+    /* What each splat gave the frame, added into `contribution` (device memory,
+     * never cleared here, so frames from many cameras sum into it), in the
+     * reference's contributionMode (TileRasterizer.h:351-367,
+     * splat_blend.slang:364-398): 0 nothing; 1 a uint a slot, the transmittance
+     * times alpha it blended with summed over its pixels, in 1/4096; 4 four
+     * words a slot, three signed (the weight times `final_colour`, here a
+     * loss's derivative at each pixel, float4 a pixel, summed in 1/256 with
+     * hash-dithered rounding) and the weight in 1/256. Slots are the instances'
+     * splats one after another. Modes 2 and 3 are ATH_E_UNSUPPORTED. */
+    uint32_t contribution_mode;
+    uint32_t* contribution;
+    const float* final_colour;
 } ath_settings;
 
 /* RenderTargets (TileRasterizer.h:421-450) plus the P layer

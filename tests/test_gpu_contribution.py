@@ -1,0 +1,70 @@
+"""The blend's contribution hooks (TileRasterizer.h:351-367, splat_blend.slang:
+364-398) on a B200, against the CPU restatement: mode 1 (each splat's summed
+weight in 1/4096) and mode 4 (each splat's colour gradient in 1/256 with the
+hash-dithered rounding, and its weight) are integer sums of the same FP32
+weights, so they must match word for word; frames add into the buffer."""
+import numpy as np
+import pytest
+import torch
+
+import athenea_b200 as A
+from tests.fixtures import random_cloud
+
+pytestmark = pytest.mark.gpu
+
+
+def _frame(oracle, W=250, H=190):
+    from tests import gpu_helpers as G
+    from tests.test_gpu_parity import _decode
+    packed = _decode(oracle, random_cloud(3000, 7))
+    cam = A.Camera.looking_at((1.5, 1.0, 6.0), (0, 0, 0))
+    cam.lens.focal = 30.0
+    proj = cam.projection_for(W, H)
+    splats = G.upload(packed)
+    want = oracle.render([(packed[0], packed[1], packed[2], packed[3], packed[4], np.eye(4), 0)],
+                         G.oracle_projection(oracle, proj), W, H)
+    return proj, splats, want
+
+
+def test_mode_1_weights_are_the_references(oracle):
+    W, H = 250, 190
+    proj, splats, want = _frame(oracle, W, H)
+    words = torch.zeros(splats.count, dtype=torch.int32, device="cuda")
+    raster = A.TileRasterizer.create()
+    t = A.RenderTargets.make(W, H)
+    s = A.RenderSettings(width=W, height=H, contribution_mode=1, contribution=words)
+    raster.render(proj, [A.SplatInstance(splats)], s, t)
+    raster.render(proj, [A.SplatInstance(splats)], s, t)   # frames add in
+    torch.cuda.synchronize()
+    ref = oracle.contribution_weight(want["frame"], want["binned"], want["proj"]).astype(np.uint64)
+    got = words.cpu().numpy().view(np.uint32).astype(np.uint64)
+    np.testing.assert_array_equal(got, 2 * ref)
+    assert ref.sum() > 0
+
+
+def test_mode_4_colour_gradients_are_the_references(oracle):
+    W, H = 250, 190
+    proj, splats, want = _frame(oracle, W, H)
+    dl = torch.randn((W * H, 4), generator=torch.Generator().manual_seed(9)) * 1e-3
+    words = torch.zeros((splats.count, 4), dtype=torch.int32, device="cuda")
+    raster = A.TileRasterizer.create()
+    t = A.RenderTargets.make(W, H)
+    s = A.RenderSettings(width=W, height=H, contribution_mode=4, contribution=words, final_colour=dl.cuda())
+    raster.render(proj, [A.SplatInstance(splats)], s, t)
+    torch.cuda.synchronize()
+    ref = oracle.colour_gradient(want["frame"], want["binned"], want["proj"], dl.numpy())
+    np.testing.assert_array_equal(words.cpu().numpy(), ref)
+    assert np.abs(ref[:, :3]).sum() > 0
+
+
+def test_modes_2_and_3_are_refused(oracle):
+    W, H = 64, 48
+    proj, splats, _ = _frame(oracle, W, H)
+    words = torch.zeros((splats.count, 2), dtype=torch.int32, device="cuda")
+    raster = A.TileRasterizer.create()
+    t = A.RenderTargets.make(W, H)
+    for mode in (2, 3):
+        with pytest.raises(A.AtheneaError) as e:
+            raster.render(proj, [A.SplatInstance(splats)],
+                          A.RenderSettings(width=W, height=H, contribution_mode=mode, contribution=words), t)
+        assert e.value.code == 4
