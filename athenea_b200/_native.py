@@ -134,6 +134,8 @@ SIGNATURES = {
     "ath_raster_render": (C.c_int32, [_P, C.POINTER(Projection), _P, C.c_uint32, C.POINTER(Settings),
                                       C.POINTER(Targets), C.POINTER(FrameStats), _P]),
     "ath_raster_latest_counters": (C.c_int32, [_P, C.POINTER(SplatCounters)]),
+    "ath_raster_render_over": (C.c_int32, [_P, C.POINTER(Projection), _P, C.c_uint32, C.POINTER(Settings),
+                                           C.POINTER(Targets), C.POINTER(Targets), C.POINTER(FrameStats), _P]),
     "ath_raster_render_params": (C.c_int32, [_P, C.POINTER(Projection), C.POINTER(Params), C.POINTER(Settings),
                                              C.POINTER(Targets), C.POINTER(FrameStats), _P]),
     "ath_raster_backward": (C.c_int32, [_P, _P, _P, C.POINTER(ParamGrads), _P]),

@@ -21,13 +21,17 @@ constexpr uint32_t kBlendThreads = kTile * kTile;
 constexpr float kColourGradScale = 256.0f;   // frame.slang:36
 
 // kContribution: the contributionMode hooks of splat_blend.slang:364-398 (modes
-// 1 and 4); the plain frame builds without them.
-template <bool kContribution>
+// 1 and 4). kUnder: the composite over an opaque layer under the splats
+// (:249-251,329-333,516-523,555-575): a pixel's walk stops at the first record
+// at or behind the layer's depth, and the layer takes the rest of the pixel.
+// The plain frame builds without either.
+template <bool kContribution, bool kUnder>
 __global__ void __launch_bounds__(kBlendThreads)
     blendKernel(const FrameConst F, uint32_t pairs, uint32_t slots, const uint2* __restrict__ ranges,
                 const uint32_t* __restrict__ pairValues, const float4* __restrict__ recs, float4* __restrict__ colour,
                 float* __restrict__ depth, float4* __restrict__ position, float* __restrict__ finalT,
-                uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ status, Contribution contrib) {
+                uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ status, Contribution contrib,
+                Under under) {
     __shared__ float4 sScreen[kBlendThreads];
     __shared__ float4 sConic[kBlendThreads];
     __shared__ float4 sColour[kBlendThreads];
@@ -44,6 +48,8 @@ __global__ void __launch_bounds__(kBlendThreads)
         range = make_uint2(0, 0);
     }
     const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+    const float underZ = kUnder && inside ? under.depth[py * F.width + px] : 0.0f;
+    const bool underHit = kUnder && underZ > 0.0f;
 
     float r = 0.0f, g = 0.0f, bl = 0.0f;
     float T = 1.0f, depthSum = 0.0f, depthAt = -1.0f;
@@ -67,6 +73,10 @@ __global__ void __launch_bounds__(kBlendThreads)
         const uint32_t count = min(kBlendThreads, range.y - first);
         for (uint32_t j = 0; j < count && !done; ++j) {
             const float4 sc = sScreen[j];
+            if (kUnder && underHit && sc.z >= underZ) {
+                done = true;
+                break;
+            }
             const float4 k = sConic[j];
             const float dx = pxc - sc.x;
             const float dy = pyc - sc.y;
@@ -105,8 +115,15 @@ __global__ void __launch_bounds__(kBlendThreads)
     if (!inside) return;
     const uint32_t at = py * F.width + px;
     const float coverage = 1.0f - T;
-    colour[at] = make_float4(r + T * F.bg[0], g + T * F.bg[1], bl + T * F.bg[2], coverage + T * F.bg[3]);
-    const float z = F.depthMode == 0 ? (coverage > 1e-6f ? depthSum / coverage : 0.0f) : fmaxf(depthAt, 0.0f);
+    float4 behind = make_float4(F.bg[0], F.bg[1], F.bg[2], F.bg[3]);
+    if (kUnder && underHit) {
+        behind = reinterpret_cast<const float4*>(under.colour)[at];
+        depthSum = depthSum + T * underZ;
+        if (depthAt < 0.0f) depthAt = underZ;
+    }
+    const float total = kUnder && underHit ? 1.0f : coverage;
+    colour[at] = make_float4(r + T * behind.x, g + T * behind.y, bl + T * behind.z, coverage + T * behind.w);
+    const float z = F.depthMode == 0 ? (total > 1e-6f ? depthSum / total : 0.0f) : fmaxf(depthAt, 0.0f);
     depth[at] = z;
     if (finalT) finalT[at] = T;
     if (lastContrib) lastContrib[at] = last;
@@ -131,15 +148,18 @@ __global__ void __launch_bounds__(kBlendThreads)
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
                         const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
                         float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream,
-                        const Contribution& contrib) {
+                        const Contribution& contrib, const Under& under) {
     const uint32_t tiles = F.tilesX * F.tilesY;
     if (tiles == 0) return cudaSuccess;
-    if (contrib.mode != 0u)
-        blendKernel<true><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, depth,
-                                                              position, finalT, lastContrib, status, contrib);
-    else
-        blendKernel<false><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour,
-                                                               depth, position, finalT, lastContrib, status, contrib);
+#define ATH_BLEND(C_, U_)                                                                                          \
+    blendKernel<C_, U_><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, depth, \
+                                                            position, finalT, lastContrib, status, contrib, under)
+    const bool c = contrib.mode != 0u, u = under.depth != nullptr;
+    if (c && u) ATH_BLEND(true, true);
+    else if (c) ATH_BLEND(true, false);
+    else if (u) ATH_BLEND(false, true);
+    else ATH_BLEND(false, false);
+#undef ATH_BLEND
     return cudaGetLastError();
 }
 

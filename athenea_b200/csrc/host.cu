@@ -387,7 +387,7 @@ ath_status checkFrame(const ath_settings& s, const ath_targets& targets) {
 // record blended, for the backward.
 ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, uint32_t instanceCount,
                      uint32_t slots, uint32_t layout, const ath_settings& s, ath_targets* targets,
-                     ath_frame_stats* stats, cudaStream_t stream, bool training) {
+                     ath_frame_stats* stats, cudaStream_t stream, bool training, const ath_targets* under = nullptr) {
     const auto frameStart = std::chrono::steady_clock::now();
     const uint32_t tiles = F.tilesX * F.tilesY;
     const uint32_t bits = 24 + F.tileBits;
@@ -470,7 +470,8 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
                           targets->depth, reinterpret_cast<float4*>(targets->position),
                           training ? static_cast<float*>(r->finalT.ptr) : nullptr,
                           training ? static_cast<uint32_t*>(r->lastContrib.ptr) : nullptr, words + kWordSticky, stream,
-                          Contribution{s.contribution_mode, s.contribution, s.final_colour});
+                          Contribution{s.contribution_mode, s.contribution, s.final_colour},
+                          under ? Under{under->colour, under->depth} : Under{});
     mark(5);
     if (err != cudaSuccess) return failCuda(err, "drawing the frame");
     r->lastSlots = slots;
@@ -537,14 +538,21 @@ ath_status reserveInstances(ath_raster* r, uint32_t instanceCount) {
 
 }   // namespace
 
-extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* projection, const ath_instance* instances,
-                                        uint32_t instanceCount, const ath_settings* settings, ath_targets* targets,
-                                        ath_frame_stats* stats, void* streamPtr) {
+namespace {
+
+ath_status renderPacked(ath_raster* r, const ath_projection* projection, const ath_instance* instances,
+                        uint32_t instanceCount, const ath_settings* settings, ath_targets* targets,
+                        const ath_targets* under, ath_frame_stats* stats, void* streamPtr) {
     if (!r || !projection || !settings || !targets || (instanceCount && !instances))
         return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render: null argument");
     const ath_settings& s = *settings;
     ath_status st = checkFrame(s, *targets);
     if (st != ATH_OK) return st;
+    // TileRasterizer.cpp:320-322
+    if (under && (under->width != s.width || under->height != s.height))
+        return fail(ATH_E_INVALID_ARGUMENT, "the under-layer is not the frame's size");
+    if (under && (!under->colour || !under->depth))
+        return fail(ATH_E_INVALID_ARGUMENT, "the under-layer needs colour and depth");
     uint64_t total = 0;
     for (uint32_t k = 0; k < instanceCount; ++k) {
         const ath_status v = validInstance(instances[k], k);
@@ -562,7 +570,23 @@ extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* pro
     }
     r->trainingValid = false;
     return drawFrame(r, frameConstFor(*projection, s), staged, instanceCount, (uint32_t)total, kLayoutPacked, s,
-                     targets, stats, static_cast<cudaStream_t>(streamPtr), false);
+                     targets, stats, static_cast<cudaStream_t>(streamPtr), false, under);
+}
+
+}   // namespace
+
+extern "C" ath_status ath_raster_render(ath_raster* r, const ath_projection* projection, const ath_instance* instances,
+                                        uint32_t instanceCount, const ath_settings* settings, ath_targets* targets,
+                                        ath_frame_stats* stats, void* streamPtr) {
+    return renderPacked(r, projection, instances, instanceCount, settings, targets, nullptr, stats, streamPtr);
+}
+
+extern "C" ath_status ath_raster_render_over(ath_raster* r, const ath_projection* projection,
+                                             const ath_instance* instances, uint32_t instanceCount,
+                                             const ath_settings* settings, ath_targets* targets,
+                                             const ath_targets* under, ath_frame_stats* stats, void* streamPtr) {
+    if (!under) return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_render_over: null under-layer");
+    return renderPacked(r, projection, instances, instanceCount, settings, targets, under, stats, streamPtr);
 }
 
 namespace ath {

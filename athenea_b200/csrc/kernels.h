@@ -52,10 +52,17 @@ struct Contribution {
     const float* finalColour = nullptr;  // mode 4: dL/dpixel, float4 a pixel
 };
 
+// An opaque layer under the splats (TileRasterizer::render's `under`): its
+// colour (float4) and depth (float, 0 where it has nothing) a pixel.
+struct Under {
+    const float* colour = nullptr;
+    const float* depth = nullptr;
+};
+
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
                         const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
                         float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream,
-                        const Contribution& contrib = Contribution{});
+                        const Contribution& contrib = Contribution{}, const Under& under = Under{});
 
 // backward.cu
 cudaError_t launchBlendBackward(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,

@@ -324,8 +324,10 @@ class TileRasterizer:
             self._h = None
 
     def render(self, camera, instances, settings: RenderSettings, targets: RenderTargets,
-               stream: torch.cuda.Stream | None = None) -> FrameStats:
-        """render(const Camera&/const Projection&, ...) -> FrameStats (TileRasterizer.cpp:287-1295)."""
+               stream: torch.cuda.Stream | None = None, under: "RenderTargets | None" = None) -> FrameStats:
+        """render(const Camera&/const Projection&, ..., const RenderTargets* under) -> FrameStats
+        (TileRasterizer.cpp:287-1295); `under`, when given, is an opaque layer the splats are
+        composited over (ath_raster_render_over)."""
         proj = camera.projection_for(settings.width, settings.height) if isinstance(camera, Camera) else camera
         arr, n = _instances(instances)
         t = N.Targets(targets.width, targets.height, _ptr(targets.colour), _ptr(targets.depth),
@@ -333,8 +335,13 @@ class TileRasterizer:
         stats = N.FrameStats()
         dev = targets.colour.device if targets.colour is not None else torch.device("cuda")
         s = stream if stream is not None else torch.cuda.current_stream(dev)
-        check(N.lib().ath_raster_render(self._h, C.byref(proj), arr, n, C.byref(settings._native()), C.byref(t),
-                                        C.byref(stats), C.c_void_p(s.cuda_stream)))
+        if under is None:
+            check(N.lib().ath_raster_render(self._h, C.byref(proj), arr, n, C.byref(settings._native()), C.byref(t),
+                                            C.byref(stats), C.c_void_p(s.cuda_stream)))
+        else:
+            u = N.Targets(under.width, under.height, _ptr(under.colour), _ptr(under.depth), None)
+            check(N.lib().ath_raster_render_over(self._h, C.byref(proj), arr, n, C.byref(settings._native()),
+                                                 C.byref(t), C.byref(u), C.byref(stats), C.c_void_p(s.cuda_stream)))
         return FrameStats(*[getattr(stats, f) for f, _ in N.FrameStats._fields_])
 
     def latest_counters(self) -> SplatCounters | None:

@@ -187,6 +187,16 @@ ath_status ath_raster_render(ath_raster* r, const ath_projection* projection, co
                              uint32_t instance_count, const ath_settings* settings, ath_targets* targets,
                              ath_frame_stats* stats, void* stream);
 
+/* TileRasterizer::render with its `under` layer (TileRasterizer.h:468-474;
+ * splat_blend.slang:249-251,329-333,516-523,555-575): the splats composited
+ * over an opaque layer of the frame's size (colour float4, depth float a pixel,
+ * depth 0 where it has nothing). A pixel's walk stops at the first splat at or
+ * behind the layer; the layer takes what light is left, and the pixel's depth
+ * and coverage count it. A layer of another size is ATH_E_INVALID_ARGUMENT. */
+ath_status ath_raster_render_over(ath_raster* r, const ath_projection* projection, const ath_instance* instances,
+                                  uint32_t instance_count, const ath_settings* settings, ath_targets* targets,
+                                  const ath_targets* under, ath_frame_stats* stats, void* stream);
+
 /* ---- differentiation (no counterpart in the reference's API: it only has
  * the colour gradient of splat_blend.slang:381-398, contributionMode 4) ------ */
 

@@ -571,13 +571,16 @@ struct Walk {
     uint32_t evaluated = 0;
 };
 
+// underZ > 0: an opaque layer under the splats at that depth ends the walk at
+// the first record at or behind it (splat_blend.slang:249-251,329-333).
 template <typename Visit>
 Walk walkPixel(const orc_frame& f, uint32_t start, uint32_t end, const uint32_t* pairSplats, const float* records,
-               float pxc, float pyc, Visit visit) {
+               float pxc, float pyc, Visit visit, float underZ = 0.0f) {
     Walk wk;
     for (uint32_t j = start; j < end; ++j) {
         const uint32_t s = pairSplats[j];
         const float* rec = records + s * 12;
+        if (underZ > 0.0f && rec[2] >= underZ) break;
         wk.evaluated += 1;
         const float dx = pxc - rec[0];
         const float dy = pyc - rec[1];
@@ -947,6 +950,45 @@ uint64_t orc_blend(const orc_frame* f, const uint32_t* ranges, const uint32_t* p
         }
     }
     return evaluated;
+}
+
+void orc_blend_over(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
+                    const float* underColour, const float* underDepth, float* colour, float* depth, int threads) {
+    // splat_blend.slang:236-578 with composite = true and only the under layer
+    // (no points, catchers or media): the walk stops at the layer, which then
+    // takes the rest of the pixel (:516-523,555-575).
+    const uint32_t tiles = f->tilesX * f->tilesY;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threadsOr(threads))
+    for (int64_t ti = 0; ti < (int64_t)tiles; ++ti) {
+        const uint32_t t = (uint32_t)ti;
+        const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
+        const uint32_t start = ranges[t * 2], end = ranges[t * 2 + 1];
+        for (uint32_t ly = 0; ly < kTile; ++ly) {
+            for (uint32_t lx = 0; lx < kTile; ++lx) {
+                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+                if (px >= f->width || py >= f->height) continue;
+                const uint32_t at = py * f->width + px;
+                const float underZ = underDepth[at];
+                const bool hit = underZ > 0.0f;
+                Walk wk = walkPixel(*f, start, end, pairSplats, records, (float)px + 0.5f, (float)py + 0.5f,
+                                    [](uint32_t, float) {}, hit ? underZ : 0.0f);
+                const float coverage = 1.0f - wk.t;
+                float behind[4] = {f->bg[0], f->bg[1], f->bg[2], f->bg[3]};
+                if (hit) {
+                    for (int k = 0; k < 4; ++k) behind[k] = underColour[at * 4 + k];
+                    wk.depthSum = wk.depthSum + wk.t * underZ;
+                    if (wk.depthAt < 0.0f) wk.depthAt = underZ;
+                }
+                const float total = hit ? 1.0f : coverage;
+                colour[at * 4 + 0] = wk.rgb[0] + wk.t * behind[0];
+                colour[at * 4 + 1] = wk.rgb[1] + wk.t * behind[1];
+                colour[at * 4 + 2] = wk.rgb[2] + wk.t * behind[2];
+                colour[at * 4 + 3] = coverage + wk.t * behind[3];
+                depth[at] = f->depthMode == 0 ? (total > 1e-6f ? wk.depthSum / total : 0.0f)
+                                              : std::max(wk.depthAt, 0.0f);
+            }
+        }
+    }
 }
 
 void orc_colour_gradient(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,

@@ -136,6 +136,14 @@ uint64_t orc_blend(const orc_frame* f, const uint32_t* ranges, const uint32_t* p
                    const float* records, float* colour, float* depth, float* finalT, uint32_t* lastContrib,
                    int threads);
 
+/* orc_blend over an opaque layer under the splats (TileRasterizer::render's
+ * `under`, splat_blend.slang's composite path without points): underColour
+ * float4 and underDepth float a pixel; a pixel whose underDepth > 0 stops its
+ * walk at the first record at or behind that depth and takes the layer's
+ * colour and depth behind what it blended. */
+void orc_blend_over(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
+                    const float* underColour, const float* underDepth, float* colour, float* depth, int threads);
+
 /* contributionMode 4 (splat_blend.slang:381-398): per slot four signed words,
  * weight * dLdPixel.rgb in 1/256 with hash-dithered rounding, and the weight. */
 void orc_colour_gradient(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,

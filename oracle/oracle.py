@@ -116,6 +116,7 @@ def lib():
                                      C.c_uint32, C.c_uint32, C.c_int]
         L.orc_render_params_f64.argtypes = [C.POINTER(Frame64), C.c_uint32, _P, _P, _P, _P, _P, C.c_uint32,
                                             _P, _P, C.c_int]
+        L.orc_blend_over.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P, _P, _P, C.c_int]
         L.orc_render_params_sampled_f64.argtypes = [C.POINTER(Frame64), C.c_uint32, _P, _P, _P, _P, C.c_uint32,
                                                     C.c_uint32, _P, _P, _P, C.c_double, C.c_uint32, C.c_uint32,
                                                     C.c_int]
@@ -305,6 +306,18 @@ def blend(f: Frame, binned: dict, proj: dict, threads=0):
     ev = lib().orc_blend(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]), _ptr(colour),
                          _ptr(depth), _ptr(final_t), _ptr(last), threads)
     return dict(colour=colour, depth=depth, final_t=final_t, last=last, evaluated=int(ev))
+
+
+def blend_over(f: Frame, binned: dict, proj: dict, under_colour: np.ndarray, under_depth: np.ndarray, threads=0):
+    """The blend over an opaque under layer (float4 colour, float depth a pixel; depth 0 = none)."""
+    w, h = f.width, f.height
+    colour = np.zeros((h * w, 4), np.float32)
+    depth = np.zeros(h * w, np.float32)
+    ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
+    lib().orc_blend_over(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]),
+                         _ptr(np.ascontiguousarray(under_colour, np.float32)),
+                         _ptr(np.ascontiguousarray(under_depth, np.float32)), _ptr(colour), _ptr(depth), threads)
+    return dict(colour=colour, depth=depth)
 
 
 def colour_gradient(f: Frame, binned: dict, proj: dict, dl_dpixel: np.ndarray) -> np.ndarray:

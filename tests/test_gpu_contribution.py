@@ -13,7 +13,7 @@ from tests.fixtures import random_cloud
 pytestmark = pytest.mark.gpu
 
 
-def _frame(oracle, W=250, H=190):
+def _frame(oracle, W=250, H=190, **settings):
     from tests import gpu_helpers as G
     from tests.test_gpu_parity import _decode
     packed = _decode(oracle, random_cloud(3000, 7))
@@ -22,7 +22,7 @@ def _frame(oracle, W=250, H=190):
     proj = cam.projection_for(W, H)
     splats = G.upload(packed)
     want = oracle.render([(packed[0], packed[1], packed[2], packed[3], packed[4], np.eye(4), 0)],
-                         G.oracle_projection(oracle, proj), W, H)
+                         G.oracle_projection(oracle, proj), W, H, **settings)
     return proj, splats, want
 
 
@@ -68,3 +68,33 @@ def test_modes_2_and_3_are_refused(oracle):
             raster.render(proj, [A.SplatInstance(splats)],
                           A.RenderSettings(width=W, height=H, contribution_mode=mode, contribution=words), t)
         assert e.value.code == 4
+
+
+def test_composite_over_an_under_layer_is_the_references(oracle):
+    """TileRasterizer::render's `under` (splat_blend.slang's composite path): the
+    walk stops at the layer, which takes the rest of the pixel; a pixel whose
+    layer depth is 0 has nothing under it."""
+    W, H = 250, 190
+    gen = torch.Generator().manual_seed(21)
+    under = A.RenderTargets.make(W, H)
+    under.colour.copy_(torch.rand((W * H, 4), generator=gen).cuda())
+    depth = 5.0 + torch.rand(W * H, generator=gen) * 3.0   # the cloud spans about 5 to 7.5 from this camera
+    depth[torch.rand(W * H, generator=gen) < 0.2] = 0.0
+    under.depth.copy_(depth.cuda())
+    for mode in (0, 1):
+        proj, splats, want = _frame(oracle, W, H, depth_mode=mode)
+        raster = A.TileRasterizer.create()
+        t = A.RenderTargets.make(W, H)
+        raster.render(proj, [A.SplatInstance(splats)], A.RenderSettings(width=W, height=H, depth_mode=mode), t,
+                      under=under)
+        torch.cuda.synchronize()
+        ref = oracle.blend_over(want["frame"], want["binned"], want["proj"], under.colour.cpu().numpy(),
+                                depth.numpy())
+        assert np.abs(t.colour.cpu().numpy() - ref["colour"]).max() <= 1e-5, mode
+        assert np.abs(t.depth.cpu().numpy() - ref["depth"]).max() <= 1e-4, mode
+        # the layer shows where it is nearer than the splats
+        assert np.abs(t.colour.cpu().numpy() - want["colour"]).max() > 0.1
+    with pytest.raises(A.AtheneaError) as e:
+        A.TileRasterizer.create().render(proj, [A.SplatInstance(splats)], A.RenderSettings(width=W, height=H),
+                                         A.RenderTargets.make(W, H), under=A.RenderTargets.make(W - 1, H))
+    assert e.value.code == 3
