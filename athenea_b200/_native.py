@@ -57,7 +57,8 @@ class Settings(C.Structure):
                 ("max_sh_degree", C.c_uint32), ("background", C.c_float * 4), ("depth_mode", C.c_uint32),
                 ("depth_threshold", C.c_float), ("time_stages", C.c_int32), ("count_splats", C.c_int32),
                 ("counters_tag", C.c_uint64), ("contribution_mode", C.c_uint32), ("contribution", C.c_void_p),
-                ("final_colour", C.c_void_p)]
+                ("final_colour", C.c_void_p), ("crypto_ids", C.c_void_p), ("crypto", C.c_void_p),
+                ("under_crypto", C.c_void_p)]
 
 
 class Targets(C.Structure):

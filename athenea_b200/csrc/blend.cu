@@ -19,23 +19,86 @@ namespace {
 
 constexpr uint32_t kBlendThreads = kTile * kTile;
 constexpr float kColourGradScale = 256.0f;   // frame.slang:36
+constexpr uint32_t kCryptoSlots = 6;         // splat_blend.slang:82
+
+// A pixel's Cryptomatte ranks (splat_blend.slang:88-143): the ids that covered
+// it most and their summed weights. Id 0 names nothing and is never kept; a full
+// list gives its lightest slot up to a heavier id. Written ranked by weight,
+// descending (a stable insertion sort), as 3 float4 (id bits, weight, id bits,
+// weight).
+struct CryptoList {
+    uint32_t ids[kCryptoSlots];
+    float weights[kCryptoSlots];
+
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (uint32_t k = 0; k < kCryptoSlots; ++k) {
+            ids[k] = 0;
+            weights[k] = 0.0f;
+        }
+    }
+    __device__ __forceinline__ void add(uint32_t id, float weight) {
+        if (weight <= 0.0f || id == 0) return;
+        uint32_t lightest = 0;
+        float lightestWeight = weights[0];
+#pragma unroll
+        for (uint32_t k = 0; k < kCryptoSlots; ++k) {
+            if (ids[k] == id && weights[k] > 0.0f) {
+                weights[k] += weight;
+                return;
+            }
+            if (weights[k] < lightestWeight) {
+                lightest = k;
+                lightestWeight = weights[k];
+            }
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kCryptoSlots; ++k)
+            if (k == lightest && weight > weights[k]) {
+                ids[k] = id;
+                weights[k] = weight;
+            }
+    }
+    __device__ __forceinline__ void write(float4* out, uint32_t at, uint32_t pixels) const {
+        uint32_t order[kCryptoSlots];
+#pragma unroll
+        for (uint32_t k = 0; k < kCryptoSlots; ++k) order[k] = k;
+        for (uint32_t i = 1; i < kCryptoSlots; ++i) {
+            const uint32_t pick = order[i];
+            uint32_t j = i;
+            while (j > 0 && weights[order[j - 1]] < weights[pick]) {
+                order[j] = order[j - 1];
+                --j;
+            }
+            order[j] = pick;
+        }
+        for (uint32_t layer = 0; layer < kCryptoSlots / 2; ++layer) {
+            const uint32_t a = order[layer * 2], b = order[layer * 2 + 1];
+            out[(size_t)layer * pixels + at] =
+                make_float4(weights[a] > 0.0f ? __uint_as_float(ids[a]) : 0.0f, fmaxf(weights[a], 0.0f),
+                            weights[b] > 0.0f ? __uint_as_float(ids[b]) : 0.0f, fmaxf(weights[b], 0.0f));
+        }
+    }
+};
 
 // kContribution: the contributionMode hooks of splat_blend.slang:364-398 (modes
 // 1 and 4). kUnder: the composite over an opaque layer under the splats
 // (:249-251,329-333,516-523,555-575): a pixel's walk stops at the first record
 // at or behind the layer's depth, and the layer takes the rest of the pixel.
 // The plain frame builds without either.
-template <bool kContribution, bool kUnder>
+template <bool kContribution, bool kUnder, bool kMatte>
 __global__ void __launch_bounds__(kBlendThreads)
     blendKernel(const FrameConst F, uint32_t pairs, uint32_t slots, const uint2* __restrict__ ranges,
                 const uint32_t* __restrict__ pairValues, const float4* __restrict__ recs, float4* __restrict__ colour,
                 float* __restrict__ depth, float4* __restrict__ position, float* __restrict__ finalT,
                 uint32_t* __restrict__ lastContrib, uint32_t* __restrict__ status, Contribution contrib,
-                Under under) {
+                Under under, Matte matte) {
     __shared__ float4 sScreen[kBlendThreads];
     __shared__ float4 sConic[kBlendThreads];
     __shared__ float4 sColour[kBlendThreads];
-    __shared__ uint32_t sSlot[kContribution ? kBlendThreads : 1];
+    __shared__ uint32_t sSlot[kContribution || kMatte ? kBlendThreads : 1];
+    CryptoList list;
+    if (kMatte) list.clear();
 
     const uint32_t tile = blockIdx.x;
     const uint32_t tx = tile % F.tilesX, ty = tile / F.tilesX;
@@ -64,7 +127,7 @@ __global__ void __launch_bounds__(kBlendThreads)
                 atomicOr(status, kStatusIndexRange);
                 s = 0;
             }
-            if (kContribution) sSlot[threadIdx.x] = s;
+            if (kContribution || kMatte) sSlot[threadIdx.x] = s;
             sScreen[threadIdx.x] = recs[(size_t)s * 3 + 0];
             sConic[threadIdx.x] = recs[(size_t)s * 3 + 1];
             sColour[threadIdx.x] = recs[(size_t)s * 3 + 2];
@@ -101,6 +164,7 @@ __global__ void __launch_bounds__(kBlendThreads)
                     atomicAdd(&contrib.words[slot * 4 + 3], (uint32_t)(weight * kColourGradScale + 0.5f));
                 }
             }
+            if (kMatte) list.add(matte.ids[sSlot[j]], weight);
             const float4 c = sColour[j];
             r = r + weight * c.x;
             g = g + weight * c.y;
@@ -122,6 +186,11 @@ __global__ void __launch_bounds__(kBlendThreads)
         if (depthAt < 0.0f) depthAt = underZ;
     }
     const float total = kUnder && underHit ? 1.0f : coverage;
+    if (kMatte) {
+        // what closed the walk takes the rest of the pixel (splat_blend.slang:525-534)
+        list.add(kUnder && underHit && matte.underIds ? matte.underIds[at] : 0u, kUnder && underHit ? T : 0.0f);
+        list.write(reinterpret_cast<float4*>(matte.out), at, F.width * F.height);
+    }
     colour[at] = make_float4(r + T * behind.x, g + T * behind.y, bl + T * behind.z, coverage + T * behind.w);
     const float z = F.depthMode == 0 ? (total > 1e-6f ? depthSum / total : 0.0f) : fmaxf(depthAt, 0.0f);
     depth[at] = z;
@@ -148,17 +217,25 @@ __global__ void __launch_bounds__(kBlendThreads)
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
                         const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
                         float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream,
-                        const Contribution& contrib, const Under& under) {
+                        const Contribution& contrib, const Under& under, const Matte& matte) {
     const uint32_t tiles = F.tilesX * F.tilesY;
     if (tiles == 0) return cudaSuccess;
-#define ATH_BLEND(C_, U_)                                                                                          \
-    blendKernel<C_, U_><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, depth, \
-                                                            position, finalT, lastContrib, status, contrib, under)
-    const bool c = contrib.mode != 0u, u = under.depth != nullptr;
-    if (c && u) ATH_BLEND(true, true);
-    else if (c) ATH_BLEND(true, false);
-    else if (u) ATH_BLEND(false, true);
-    else ATH_BLEND(false, false);
+#define ATH_BLEND(C_, U_, M_)                                                                          \
+    blendKernel<C_, U_, M_><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, \
+                                                                depth, position, finalT, lastContrib, status,     \
+                                                                contrib, under, matte)
+    const bool c = contrib.mode != 0u, u = under.depth != nullptr, m = matte.out != nullptr;
+    if (m) {
+        if (c && u) ATH_BLEND(true, true, true);
+        else if (c) ATH_BLEND(true, false, true);
+        else if (u) ATH_BLEND(false, true, true);
+        else ATH_BLEND(false, false, true);
+    } else {
+        if (c && u) ATH_BLEND(true, true, false);
+        else if (c) ATH_BLEND(true, false, false);
+        else if (u) ATH_BLEND(false, true, false);
+        else ATH_BLEND(false, false, false);
+    }
 #undef ATH_BLEND
     return cudaGetLastError();
 }

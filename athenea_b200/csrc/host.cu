@@ -378,6 +378,8 @@ ath_status checkFrame(const ath_settings& s, const ath_targets& targets) {
         return fail(ATH_E_INVALID_ARGUMENT, "a contribution mode needs its contribution buffer");
     if (s.contribution_mode == 4 && !s.final_colour)
         return fail(ATH_E_INVALID_ARGUMENT, "contribution mode 4 needs final_colour (dL/dpixel)");
+    if ((s.crypto != nullptr) != (s.crypto_ids != nullptr))
+        return fail(ATH_E_INVALID_ARGUMENT, "a Cryptomatte needs both its ids and its layers");
     return ATH_OK;
 }
 
@@ -471,7 +473,8 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
                           training ? static_cast<float*>(r->finalT.ptr) : nullptr,
                           training ? static_cast<uint32_t*>(r->lastContrib.ptr) : nullptr, words + kWordSticky, stream,
                           Contribution{s.contribution_mode, s.contribution, s.final_colour},
-                          under ? Under{under->colour, under->depth} : Under{});
+                          under ? Under{under->colour, under->depth} : Under{},
+                          Matte{s.crypto_ids, s.crypto, under ? s.under_crypto : nullptr});
     mark(5);
     if (err != cudaSuccess) return failCuda(err, "drawing the frame");
     r->lastSlots = slots;

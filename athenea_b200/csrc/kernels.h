@@ -59,10 +59,18 @@ struct Under {
     const float* depth = nullptr;
 };
 
+// Cryptomatte: a uint id a slot in, 3 float4 layers a pixel out.
+struct Matte {
+    const uint32_t* ids = nullptr;
+    float* out = nullptr;
+    const uint32_t* underIds = nullptr;
+};
+
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,
                         const uint32_t* pairValues, const float4* recs, float4* colour, float* depth, float4* position,
                         float* finalT, uint32_t* lastContrib, uint32_t* status, cudaStream_t stream,
-                        const Contribution& contrib = Contribution{}, const Under& under = Under{});
+                        const Contribution& contrib = Contribution{}, const Under& under = Under{},
+                        const Matte& matte = Matte{});
 
 // backward.cu
 cudaError_t launchBlendBackward(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,

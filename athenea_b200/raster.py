@@ -213,6 +213,9 @@ class RenderSettings:
     contribution_mode: int = 0    # 1 weights, 4 colour gradients (TileRasterizer.h:351-367)
     contribution: torch.Tensor | None = None    # int32: a word a slot (mode 1) or four (mode 4)
     final_colour: torch.Tensor | None = None    # float4 a pixel: dL/dpixel for mode 4
+    crypto_ids: torch.Tensor | None = None      # int32 a slot: the Cryptomatte id (0 names nothing)
+    crypto: torch.Tensor | None = None          # (3, height * width, 4) float32: the matte's layers
+    under_crypto: torch.Tensor | None = None    # int32 a pixel: the under layer's id
 
     def _native(self) -> N.Settings:
         s = N.Settings()
@@ -231,6 +234,9 @@ class RenderSettings:
         s.contribution_mode = self.contribution_mode
         s.contribution = _ptr(self.contribution) if self.contribution is not None else None
         s.final_colour = _ptr(self.final_colour) if self.final_colour is not None else None
+        s.crypto_ids = _ptr(self.crypto_ids) if self.crypto_ids is not None else None
+        s.crypto = _ptr(self.crypto) if self.crypto is not None else None
+        s.under_crypto = _ptr(self.under_crypto) if self.under_crypto is not None else None
         return s
 
 

@@ -132,6 +132,15 @@ typedef struct {
     uint32_t contribution_mode;
     uint32_t* contribution;
     const float* final_colour;
+    /* Cryptomatte (splat_blend.slang:29-35,88-143,420-421,525-534): with
+     * crypto_ids (a uint id a slot; 0 names nothing) and crypto (3 x width x
+     * height float4, layer-major), each pixel keeps the 6 ids that covered it
+     * most, ranked by coverage (weight summed a id) and written as (id bits as
+     * float, coverage, id, coverage). under_crypto, optional, is the under
+     * layer's id a pixel (ath_raster_render_over). */
+    const uint32_t* crypto_ids;
+    float* crypto;
+    const uint32_t* under_crypto;
 } ath_settings;
 
 /* RenderTargets (TileRasterizer.h:421-450) plus the P layer

@@ -991,6 +991,74 @@ void orc_blend_over(const orc_frame* f, const uint32_t* ranges, const uint32_t* 
     }
 }
 
+void orc_blend_matte(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
+                     const uint32_t* cryptoIds, const float* underDepth, const uint32_t* underCrypto, float* crypto,
+                     int threads) {
+    // splat_blend.slang:88-143 (CryptoList), :420-421 (each splat's weight under its
+    // id), :525-534 (the under layer's id takes the light left): 6 ids a pixel,
+    // written ranked as 3 float4 layers. underDepth may be null (no layer).
+    constexpr uint32_t kSlots = 6;
+    const uint32_t tiles = f->tilesX * f->tilesY;
+    const uint32_t pixels = f->width * f->height;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threadsOr(threads))
+    for (int64_t ti = 0; ti < (int64_t)tiles; ++ti) {
+        const uint32_t t = (uint32_t)ti;
+        const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
+        for (uint32_t ly = 0; ly < kTile; ++ly) {
+            for (uint32_t lx = 0; lx < kTile; ++lx) {
+                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+                if (px >= f->width || py >= f->height) continue;
+                const uint32_t at = py * f->width + px;
+                uint32_t ids[kSlots] = {0, 0, 0, 0, 0, 0};
+                float weights[kSlots] = {0, 0, 0, 0, 0, 0};
+                const auto add = [&](uint32_t id, float w) {
+                    if (w <= 0.0f || id == 0) return;
+                    uint32_t lightest = 0;
+                    for (uint32_t k = 0; k < kSlots; ++k) {
+                        if (ids[k] == id && weights[k] > 0.0f) {
+                            weights[k] += w;
+                            return;
+                        }
+                        if (weights[k] < weights[lightest]) lightest = k;
+                    }
+                    if (w > weights[lightest]) {
+                        ids[lightest] = id;
+                        weights[lightest] = w;
+                    }
+                };
+                const float underZ = underDepth ? underDepth[at] : 0.0f;
+                const bool hit = underZ > 0.0f;
+                const Walk wk = walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
+                                          (float)py + 0.5f, [&](uint32_t s, float w) { add(cryptoIds[s], w); },
+                                          hit ? underZ : 0.0f);
+                add(hit && underCrypto ? underCrypto[at] : 0u, hit ? wk.t : 0.0f);
+                uint32_t order[kSlots];
+                for (uint32_t k = 0; k < kSlots; ++k) order[k] = k;
+                for (uint32_t i = 1; i < kSlots; ++i) {
+                    const uint32_t pick = order[i];
+                    uint32_t j = i;
+                    while (j > 0 && weights[order[j - 1]] < weights[pick]) {
+                        order[j] = order[j - 1];
+                        --j;
+                    }
+                    order[j] = pick;
+                }
+                for (uint32_t layer = 0; layer < kSlots / 2; ++layer) {
+                    const uint32_t a = order[layer * 2], b = order[layer * 2 + 1];
+                    float* out = crypto + ((size_t)layer * pixels + at) * 4;
+                    float idA = 0.0f, idB = 0.0f;
+                    if (weights[a] > 0.0f) std::memcpy(&idA, &ids[a], 4);
+                    if (weights[b] > 0.0f) std::memcpy(&idB, &ids[b], 4);
+                    out[0] = idA;
+                    out[1] = std::max(weights[a], 0.0f);
+                    out[2] = idB;
+                    out[3] = std::max(weights[b], 0.0f);
+                }
+            }
+        }
+    }
+}
+
 void orc_colour_gradient(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
                          const float* records, const float* dLdPixel, int32_t* contribution) {
     const uint32_t tiles = f->tilesX * f->tilesY;

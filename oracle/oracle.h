@@ -141,6 +141,13 @@ uint64_t orc_blend(const orc_frame* f, const uint32_t* ranges, const uint32_t* p
  * float4 and underDepth float a pixel; a pixel whose underDepth > 0 stops its
  * walk at the first record at or behind that depth and takes the layer's
  * colour and depth behind what it blended. */
+/* The Cryptomatte of a frame (splat_blend.slang's matte path): cryptoIds a
+ * uint a slot; crypto 3 x pixels float4 out. underDepth / underCrypto may be
+ * null (no under layer). */
+void orc_blend_matte(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
+                     const uint32_t* cryptoIds, const float* underDepth, const uint32_t* underCrypto, float* crypto,
+                     int threads);
+
 void orc_blend_over(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
                     const float* underColour, const float* underDepth, float* colour, float* depth, int threads);
 

@@ -117,6 +117,7 @@ def lib():
         L.orc_render_params_f64.argtypes = [C.POINTER(Frame64), C.c_uint32, _P, _P, _P, _P, _P, C.c_uint32,
                                             _P, _P, C.c_int]
         L.orc_blend_over.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P, _P, _P, C.c_int]
+        L.orc_blend_matte.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P, _P, _P, C.c_int]
         L.orc_render_params_sampled_f64.argtypes = [C.POINTER(Frame64), C.c_uint32, _P, _P, _P, _P, C.c_uint32,
                                                     C.c_uint32, _P, _P, _P, C.c_double, C.c_uint32, C.c_uint32,
                                                     C.c_int]
@@ -318,6 +319,20 @@ def blend_over(f: Frame, binned: dict, proj: dict, under_colour: np.ndarray, und
                          _ptr(np.ascontiguousarray(under_colour, np.float32)),
                          _ptr(np.ascontiguousarray(under_depth, np.float32)), _ptr(colour), _ptr(depth), threads)
     return dict(colour=colour, depth=depth)
+
+
+def blend_matte(f: Frame, binned: dict, proj: dict, crypto_ids: np.ndarray, under_depth=None, under_crypto=None,
+                threads=0) -> np.ndarray:
+    """The Cryptomatte layers: (3, pixels, 4) float32 (id bits, coverage, id bits, coverage)."""
+    pixels = f.width * f.height
+    out = np.zeros((3, pixels, 4), np.float32)
+    ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
+    ud = None if under_depth is None else np.ascontiguousarray(under_depth, np.float32)
+    uc = None if under_crypto is None else np.ascontiguousarray(under_crypto, np.uint32)
+    lib().orc_blend_matte(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]),
+                          _ptr(np.ascontiguousarray(crypto_ids, np.uint32)), _ptr(ud) if ud is not None else None,
+                          _ptr(uc) if uc is not None else None, _ptr(out), threads)
+    return out
 
 
 def colour_gradient(f: Frame, binned: dict, proj: dict, dl_dpixel: np.ndarray) -> np.ndarray:

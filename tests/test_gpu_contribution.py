@@ -98,3 +98,32 @@ def test_composite_over_an_under_layer_is_the_references(oracle):
         A.TileRasterizer.create().render(proj, [A.SplatInstance(splats)], A.RenderSettings(width=W, height=H),
                                          A.RenderTargets.make(W, H), under=A.RenderTargets.make(W - 1, H))
     assert e.value.code == 3
+
+
+def test_cryptomatte_layers_are_the_references(oracle):
+    """The matte path (splat_blend.slang:88-143,420-421,525-534): 6 ids a pixel by
+    summed weight, alone and over an under layer with ids of its own."""
+    W, H = 250, 190
+    proj, splats, want = _frame(oracle, W, H)
+    rng = np.random.default_rng(5)
+    ids = rng.integers(0, 40, size=splats.count).astype(np.uint32)   # few ids, so they share pixels; 0 names nothing
+    gen = torch.Generator().manual_seed(8)
+    under = A.RenderTargets.make(W, H)
+    under.colour.copy_(torch.rand((W * H, 4), generator=gen).cuda())
+    depth = 5.0 + torch.rand(W * H, generator=gen) * 3.0
+    depth[torch.rand(W * H, generator=gen) < 0.3] = 0.0
+    under.depth.copy_(depth.cuda())
+    under_ids = rng.integers(1, 1000, size=W * H).astype(np.uint32)
+    for with_under in (False, True):
+        crypto = torch.zeros((3, W * H, 4), dtype=torch.float32, device="cuda")
+        s = A.RenderSettings(width=W, height=H, crypto_ids=torch.from_numpy(ids.view(np.int32)).cuda(), crypto=crypto,
+                             under_crypto=torch.from_numpy(under_ids.view(np.int32)).cuda())
+        t = A.RenderTargets.make(W, H)
+        A.TileRasterizer.create().render(proj, [A.SplatInstance(splats)], s, t,
+                                         under=under if with_under else None)
+        torch.cuda.synchronize()
+        ref = oracle.blend_matte(want["frame"], want["binned"], want["proj"], ids,
+                                 depth.numpy() if with_under else None, under_ids if with_under else None)
+        got = crypto.cpu().numpy()
+        np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32))
+        assert (got[0, :, 1] > 0).mean() > 0.3
