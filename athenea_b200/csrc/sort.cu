@@ -140,45 +140,23 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
         storeRelaxed(flag, tag | (2ull << 32) | (uint64_t)(exclusive + count));
     } else {
         storeRelaxed(flag, tag | (1ull << 32) | (uint64_t)count);
-        // The look-back reads kLookAhead predecessors' words at once (their loads
-        // overlap), then takes them in order: aggregates are added until an
-        // inclusive prefix ends the walk; a word not yet written stops the
-        // batch there and is read again. When a wave of tiles starts together
-        // most predecessors hold only aggregates, and the walk back to an
-        // inclusive prefix is long: reading them kLookAhead at a time shortens
-        // its chain of dependent loads by that factor.
-        constexpr int kLookAhead = 4;
         uint64_t sum = 0;
         int64_t j = (int64_t)tile - 1;
         uint32_t spins = 0;
-        bool ended = false;
-        while (j >= 0 && !ended) {
-            uint64_t v[kLookAhead];
-#pragma unroll
-            for (int k = 0; k < kLookAhead; ++k)
-                v[k] = j - k >= 0 ? loadRelaxed(flags + (size_t)(j - k) * kRadix + t) : 0ull;
-            int taken = 0;
-            bool waiting = false;
-#pragma unroll
-            for (int k = 0; k < kLookAhead; ++k) {
-                if (ended || waiting || j - k < 0) continue;
-                const uint32_t st = (uint32_t)(v[k] >> 34) == epoch ? (uint32_t)(v[k] >> 32) & 3u : 0u;
-                if (st == 0) {
-                    waiting = true;
-                    continue;
-                }
-                sum += v[k] & 0xFFFFFFFFull;
-                ++taken;
-                if (st == 2) ended = true;
-            }
-            j -= taken;
-            if (waiting && !ended) {
+        while (j >= 0) {
+            const uint64_t v = loadRelaxed(flags + (size_t)j * kRadix + t);
+            const uint32_t st = (uint32_t)(v >> 34) == epoch ? (uint32_t)(v >> 32) & 3u : 0u;
+            if (st == 0) {
                 if (++spins > kSpinLimit || ((spins & 255u) == 0 && gaveUp(status))) {
                     atomicOr(status, kStatusLookbackTimeout);
                     break;
                 }
                 __nanosleep(32);
+                continue;
             }
+            sum += v & 0xFFFFFFFFull;
+            if (st == 2) break;
+            --j;
         }
         exclusive = (uint32_t)sum;
         storeRelaxed(flag, tag | (2ull << 32) | (uint64_t)(exclusive + count));
