@@ -23,6 +23,13 @@ constexpr uint32_t kSortThreads = 256;
 constexpr uint32_t kWarps = kSortThreads / 32;
 constexpr uint32_t kItems = 16;
 constexpr uint32_t kTileKeys = kSortThreads * kItems;   // 4096
+// A warp ranks its items in kChains independent chains (items 0-7 and 8-15),
+// each with its own digit counters, so the two chains' shared-memory round
+// trips overlap instead of queueing behind each other; the chains are ordered
+// after each other like warps.
+constexpr uint32_t kChains = 2;
+constexpr uint32_t kChainItems = kItems / kChains;
+constexpr uint32_t kCounters = kWarps * kChains;
 constexpr uint32_t kMaxPasses = 8;
 
 // `nDevice`, when given, holds the key count (a count only the device knows, as
@@ -75,7 +82,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(sKeys + kTileKeys);
-    uint32_t* sWarpCnt = kValues ? sVals + kTileKeys : sVals;   // kWarps x kRadix
+    uint32_t* sWarpCnt = kValues ? sVals + kTileKeys : sVals;   // kCounters x kRadix
     __shared__ uint32_t sTile;
     __shared__ uint32_t sStart[kRadix];
     __shared__ uint32_t sAdjust[kRadix];
@@ -87,7 +94,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
     // epoch reads as not ready. Without an epoch (0) the caller clears them.
     const uint32_t epoch = epochDevice ? (*epochDevice & 0x3FFFFFFFu) : 0u;
     if (tid == 0) sTile = atomicAdd(ticket, 1u);
-    for (uint32_t j = tid; j < kWarps * kRadix; j += kSortThreads) sWarpCnt[j] = 0;
+    for (uint32_t j = tid; j < kCounters * kRadix; j += kSortThreads) sWarpCnt[j] = 0;
     __syncthreads();
     const uint32_t tile = sTile;
     const uint32_t base = tile * kTileKeys;
@@ -108,17 +115,27 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
         if constexpr (kValues) val[k] = valid ? valsIn[idx] : 0u;
     }
 #pragma unroll
-    for (uint32_t k = 0; k < kItems; ++k) {
-        const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
-        const bool valid = idx < n;
-        const uint32_t d = valid ? (uint32_t)((key[k] >> shift) & 0xFFu) : kRadix + lane;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        uint32_t before = 0;
-        if (valid) before = sWarpCnt[warp * kRadix + d];
+    for (uint32_t i = 0; i < kChainItems; ++i) {
+        uint32_t d[kChains], peers[kChains], before[kChains];
+        bool valid[kChains];
+#pragma unroll
+        for (uint32_t c = 0; c < kChains; ++c) {
+            const uint32_t k = c * kChainItems + i;
+            valid[c] = base + warp * 32 * kItems + k * 32 + lane < n;
+            d[c] = valid[c] ? (uint32_t)((key[k] >> shift) & 0xFFu) : kRadix + lane;
+            peers[c] = __match_any_sync(0xFFFFFFFFu, d[c]);
+        }
+#pragma unroll
+        for (uint32_t c = 0; c < kChains; ++c)
+            before[c] = valid[c] ? sWarpCnt[(warp * kChains + c) * kRadix + d[c]] : 0u;
         __syncwarp();
-        if (valid && lane == (uint32_t)(__ffs(peers) - 1)) sWarpCnt[warp * kRadix + d] = before + __popc(peers);
+#pragma unroll
+        for (uint32_t c = 0; c < kChains; ++c)
+            if (valid[c] && lane == (uint32_t)(__ffs(peers[c]) - 1))
+                sWarpCnt[(warp * kChains + c) * kRadix + d[c]] = before[c] + __popc(peers[c]);
         __syncwarp();
-        rank[k] = before + __popc(peers & ltMask);
+#pragma unroll
+        for (uint32_t c = 0; c < kChains; ++c) rank[c * kChainItems + i] = before[c] + __popc(peers[c] & ltMask);
     }
     __syncthreads();
 
@@ -126,7 +143,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
     const uint32_t t = tid;
     uint32_t count = 0;
 #pragma unroll
-    for (uint32_t w = 0; w < kWarps; ++w) {
+    for (uint32_t w = 0; w < kCounters; ++w) {
         const uint32_t c = sWarpCnt[w * kRadix + t];
         sWarpCnt[w * kRadix + t] = count;
         count += c;
@@ -172,7 +189,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
         const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
         if (idx < n) {
             const uint32_t d = (uint32_t)((key[k] >> shift) & 0xFFu);
-            const uint32_t s = sStart[d] + sWarpCnt[warp * kRadix + d] + rank[k];
+            const uint32_t s = sStart[d] + sWarpCnt[(warp * kChains + k / kChainItems) * kRadix + d] + rank[k];
             sKeys[s] = key[k];
             if constexpr (kValues) sVals[s] = val[k];
         }
@@ -191,8 +208,8 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
     }
 }
 
-constexpr size_t kOnesweepSmem = (size_t)kTileKeys * 8 + (size_t)kTileKeys * 4 + (size_t)kWarps * kRadix * 4;
-constexpr size_t kOnesweepKeysSmem = (size_t)kTileKeys * 8 + (size_t)kWarps * kRadix * 4;
+constexpr size_t kOnesweepSmem = (size_t)kTileKeys * 8 + (size_t)kTileKeys * 4 + (size_t)kCounters * kRadix * 4;
+constexpr size_t kOnesweepKeysSmem = (size_t)kTileKeys * 8 + (size_t)kCounters * kRadix * 4;
 
 }   // namespace
 
