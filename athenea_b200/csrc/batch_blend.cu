@@ -68,18 +68,6 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
     return mask;
 }
 
-// cp.async: 16 bytes global -> shared, not through registers.
-__device__ __forceinline__ void copyAsync16(void* dst, const void* src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void copyAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void copyAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// The batches of a tile's records are double-buffered: while the block blends
-// batch b from one stage, the records of batch b + 1 are copied into the other
-// by cp.async (their pair indices read a batch earlier still), so the gather's
-// latency hides behind the blending instead of opening every batch.
 template <uint32_t T, uint32_t NB>
 __global__ void __launch_bounds__(T * T / 2)
     blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
@@ -90,11 +78,10 @@ __global__ void __launch_bounds__(T * T / 2)
                      uint32_t* __restrict__ words) {
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
-    constexpr uint32_t kPer = (NB + kThreads - 1) / kThreads;   // records a thread stages a batch
-    // stage s: [0] screen (cx, cy, z, cutoff -> the cutoff pre-scaled), [1] the factored
-    // conic (ca, fr, fs pre-scaled; alpha), [2] colour
-    __shared__ float4 sRec[2][3][NB];
-    __shared__ uint32_t sMask[2][NB];
+    __shared__ float2 sCentre[NB];
+    __shared__ float4 sConic[NB];    // ca, fr, fs pre-scaled; alpha
+    __shared__ float4 sColour[NB];   // r g b; the cutoff pre-scaled
+    __shared__ uint32_t sMask[NB];
     __shared__ uint32_t sTileBase[kMaxBatchViews];
     __shared__ uint32_t sTile;
     for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
@@ -124,94 +111,55 @@ __global__ void __launch_bounds__(T * T / 2)
         bool done[2];
 #pragma unroll
         for (int p = 0; p < 2; ++p) done[p] = !(px < V.width && py[p] < V.height);
-        const uint32_t batches = (range.y - range.x + NB - 1) / NB;
-        // the Gaussians of this thread's records in the next batch to copy
-        uint32_t nextG[kPer];
-        const auto fetch = [&](uint32_t batch) {
-#pragma unroll
-            for (uint32_t q = 0; q < kPer; ++q) {
-                const uint32_t k = threadIdx.x + q * kThreads;
-                const uint32_t at = range.x + batch * NB + k;
-                nextG[q] = batch < batches && k < NB && at < range.y ? gaussianOf(pairs, values, slotMask, at) : 0u;
-            }
-        };
-        const auto issue = [&](uint32_t batch) {
-            const uint32_t st = batch & 1u, first = range.x + batch * NB, count = min(NB, range.y - first);
-#pragma unroll
-            for (uint32_t q = 0; q < kPer; ++q) {
-                const uint32_t k = threadIdx.x + q * kThreads;
-                if (k < count) {
-                    const float4* src = recs + (recBase + nextG[q]) * 3;
-                    copyAsync16(&sRec[st][0][k], src + 0);
-                    copyAsync16(&sRec[st][1][k], src + 1);
-                    copyAsync16(&sRec[st][2][k], src + 2);
-                }
-            }
-            copyAsyncCommit();
-        };
-        const auto prepare = [&](uint32_t batch) {
-            const uint32_t st = batch & 1u, first = range.x + batch * NB, count = min(NB, range.y - first);
-            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
-                const float4 sc = sRec[st][0][k];
-                const float4 c = sRec[st][1][k];
-                sMask[st][k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
-                // the factored conic's two weights and the cutoff pre-scaled to base-2 exponent units
-                sRec[st][1][k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
-                sRec[st][0][k].w = kScale * sc.w;
-            }
-        };
-        if (batches) {
-            fetch(0);
-            issue(0);
-            fetch(1);
-            copyAsyncWaitAll();
-            __syncthreads();
-            prepare(0);
-        }
-        for (uint32_t b = 0; b < batches; ++b) {
+        for (uint32_t first = range.x; first < range.y; first += NB) {
             if (__syncthreads_count(done[0] && done[1]) == kThreads) break;
-            const uint32_t st = b & 1u, first = range.x + b * NB, count = min(NB, range.y - first);
-            if (b + 1 < batches) {
-                issue(b + 1);
-                fetch(b + 2);
+            const uint32_t count = min(NB, range.y - first);
+            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
+                const size_t s = (recBase + gaussianOf(pairs, values, slotMask, first + k)) * 3;
+                const float4 sc = recs[s + 0];
+                const float4 c = recs[s + 1];
+                const float4 rgb = recs[s + 2];
+                sCentre[k] = make_float2(sc.x, sc.y);
+                // the factored conic's two weights pre-scaled to base-2 exponent units
+                sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
+                sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
+                sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
             }
-            if (!__all_sync(0xFFFFFFFFu, done[0] && done[1])) {
-                for (uint32_t base = 0; base < count; base += 32) {
-                    const uint32_t m = base + lane < count ? sMask[st][base + lane] : 0u;
-                    uint32_t todo = __ballot_sync(0xFFFFFFFFu, (m >> warp) & 1u);
-                    while (todo) {
-                        const uint32_t j = base + (uint32_t)__ffs(todo) - 1u;
-                        todo &= todo - 1u;
-                        const float4 sc = sRec[st][0][j];
-                        const float4 k = sRec[st][1][j];
-                        const float dx = pxc - sc.x;
+            __syncthreads();
+            if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) continue;
+            for (uint32_t base = 0; base < count; base += 32) {
+                const uint32_t m = base + lane < count ? sMask[base + lane] : 0u;
+                uint32_t todo = __ballot_sync(0xFFFFFFFFu, (m >> warp) & 1u);
+                while (todo) {
+                    const uint32_t j = base + (uint32_t)__ffs(todo) - 1u;
+                    todo &= todo - 1u;
+                    const float2 ce = sCentre[j];
+                    const float4 k = sConic[j];
+                    const float limit = sColour[j].w;
+                    const float dx = pxc - ce.x;
 #pragma unroll
-                        for (int p = 0; p < 2; ++p) {
-                            if (done[p]) continue;
-                            ++evaluated;
-                            const float dy = pyc[p] - sc.y;
-                            // e = -log2(e)/2 * power; power > cutoff  <=>  e < -log2(e)/2 * cutoff
-                            const float t = __fmaf_rn(k.y, dy, dx);
-                            const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
-                            if (e < sc.w) continue;
-                            const float alpha = fminf(0.99f, k.w * fastExp2(e));
-                            if (alpha < kFaint) continue;
-                            const float w = Tr[p] * alpha;
-                            const float4 c = sRec[st][2][j];
-                            r[p] = __fmaf_rn(w, c.x, r[p]);
-                            g[p] = __fmaf_rn(w, c.y, g[p]);
-                            bl[p] = __fmaf_rn(w, c.z, bl[p]);
-                            Tr[p] = Tr[p] * (1.0f - alpha);
-                            last[p] = first - range.x + j + 1;
-                            if (Tr[p] < 1e-4f) done[p] = true;
-                        }
+                    for (int p = 0; p < 2; ++p) {
+                        if (done[p]) continue;
+                        ++evaluated;
+                        const float dy = pyc[p] - ce.y;
+                        // e = -log2(e)/2 * power; power > cutoff  <=>  e < -log2(e)/2 * cutoff
+                        const float t = __fmaf_rn(k.y, dy, dx);
+                        const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
+                        if (e < limit) continue;
+                        const float alpha = fminf(0.99f, k.w * fastExp2(e));
+                        if (alpha < kFaint) continue;
+                        const float w = Tr[p] * alpha;
+                        const float4 c = sColour[j];
+                        r[p] = __fmaf_rn(w, c.x, r[p]);
+                        g[p] = __fmaf_rn(w, c.y, g[p]);
+                        bl[p] = __fmaf_rn(w, c.z, bl[p]);
+                        Tr[p] = Tr[p] * (1.0f - alpha);
+                        last[p] = first - range.x + j + 1;
+                        if (Tr[p] < 1e-4f) done[p] = true;
                     }
-                    if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
                 }
+                if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
             }
-            copyAsyncWaitAll();   // batch b + 1 has landed (this thread's copies) ...
-            __syncthreads();      // ... everyone's, and nobody reads stage st any more
-            if (b + 1 < batches) prepare(b + 1);
         }
 #pragma unroll
         for (int p = 0; p < 2; ++p) {
