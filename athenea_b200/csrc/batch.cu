@@ -50,7 +50,7 @@
 namespace ath {
 namespace {
 
-constexpr uint32_t kProjThreads = 128;
+constexpr uint32_t kProjThreads = 256;
 
 // ---- the step's first kernel: a new epoch, the step's counters cleared ------
 __global__ void beginStepKernel(uint32_t* words) {
