@@ -10,8 +10,10 @@ from ._native import AtheneaError  # noqa: F401
 from .parallel import GradientBuffer, shard_views  # noqa: F401
 from .raster import (BatchTrainer, Camera, CloudLoader, FrameStats, GpuSplats, Lens, MixedParams,  # noqa: F401
                      Params, RenderSettings, RenderTargets, SplatCounters, SplatEdit, SplatInstance, TileRasterizer,
-                     encoding_3dgs, l2_loss, pinhole_for_vertical_fov, read_splat_ply)
+                     check_bounded_wait, encoding_3dgs, l2_loss, memory_held, pinhole_for_vertical_fov,
+                     read_splat_ply, set_memory_budget)
 
 __all__ = ["AtheneaError", "BatchTrainer", "GradientBuffer", "shard_views", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "MixedParams",
            "Params", "RenderSettings", "RenderTargets", "SplatCounters", "SplatEdit", "SplatInstance",
-           "TileRasterizer", "encoding_3dgs", "l2_loss", "pinhole_for_vertical_fov", "read_splat_ply"]
+           "TileRasterizer", "check_bounded_wait", "encoding_3dgs", "l2_loss", "memory_held",
+           "pinhole_for_vertical_fov", "read_splat_ply", "set_memory_budget"]

@@ -364,6 +364,31 @@ class TileRasterizer:
         check(N.lib().ath_raster_release_scratch(self._h))
 
 
+def set_memory_budget(nbytes: int) -> None:
+    """A cap on this library's device memory, in bytes (0: none), as the reference's
+    ATHENEA_GPU_BUDGET (modules/gpu/src/Device.cpp:434-449): a frame whose scratch would
+    pass it raises AtheneaError OutOfMemory (9); release_scratch gives memory back."""
+    check(N.lib().ath_set_memory_budget(C.c_uint64(int(nbytes))))
+
+
+def memory_held() -> tuple[int, int]:
+    """(bytes this library's device buffers hold now, the budget; 0 = none)."""
+    held, budget = C.c_uint64(), C.c_uint64()
+    check(N.lib().ath_memory_held(C.byref(held), C.byref(budget)))
+    return held.value, budget.value
+
+
+def check_bounded_wait(preset: int, limit: int, stream: torch.cuda.Stream | None = None) -> int:
+    """Run the library's bounded device-side wait on a flag set to `preset` (0: never set),
+    giving up after `limit` spins; returns the spins taken, or raises AtheneaError Timeout (12)
+    when it gave up. The context stays usable either way."""
+    spins = C.c_uint32()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    check(N.lib().ath_check_bounded_wait(C.c_uint32(preset), C.c_uint32(limit), C.byref(spins),
+                                         C.c_void_p(s.cuda_stream)))
+    return spins.value
+
+
 # ---- differentiation -----------------------------------------------------------
 @dataclass
 class Params:

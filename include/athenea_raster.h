@@ -457,6 +457,21 @@ ath_status ath_ply_read(const char* path, float* records, uint64_t capacity, uin
 
 /* ---- diagnostics --------------------------------------------------------- */
 
+/* A device-memory budget for this library's scratch, in bytes (0: none), as
+ * the reference's ATHENEA_GPU_BUDGET (modules/gpu/src/Device.cpp:434-449; the
+ * same environment variable, in MiB, sets it at load): a frame whose scratch
+ * would pass it fails with ATH_E_OUT_OF_MEMORY, and ath_raster_release_scratch
+ * gives memory back (TileRasterizer.cpp:178-191). ath_memory_held reports the
+ * bytes this library's buffers hold now and the budget. */
+ath_status ath_set_memory_budget(uint64_t bytes);
+ath_status ath_memory_held(uint64_t* bytes, uint64_t* budget);
+/* Every device-side wait of this library spins a bounded number of times, then
+ * sets a status bit and returns (ATH_E_TIMEOUT to the caller, the context
+ * usable). This runs that wait on a flag set to `preset` (0: never set) with
+ * at most `limit` spins, and reports how many it took: ATH_E_TIMEOUT when the
+ * flag was never set. For failure-detection tests; no counterpart in the reference. */
+ath_status ath_check_bounded_wait(uint32_t preset, uint32_t limit, uint32_t* spins, void* stream);
+
 /* The message of the last failure on this thread ("" when none). */
 const char* ath_last_error_message(void);
 /* Version of this library, "major.minor.patch". */
