@@ -102,13 +102,6 @@ __device__ uint32_t lookbackEpoch(uint64_t* flags, uint32_t b, uint32_t aggregat
     return (uint32_t)exclusive;
 }
 
-// frame.slang:354-379 for tile size T, its divisions shared: x* = -b x / c of a
-// column's two x edges are computed once a rect row... the per-edge values are
-// the same operations minPowerOverBox performs, so the result is its result.
-__device__ __forceinline__ float quad(float a, float b, float c, float x, float y) {
-    return ((a * x) * x + ((2.0f * b) * x) * y) + (c * y) * y;
-}
-
 // The SH basis after the constant term (common/sh.slang:25-51) at direction (x, y, z).
 __device__ __forceinline__ void shBasisFast(float x, float y, float z, float Y[15]) {
     const float C1 = 0.4886025119029199f;
@@ -230,16 +223,66 @@ __device__ __forceinline__ void colourAdjointFast(const MixedSh& sh, const Gauss
     dp[2] += (dDir[2] - z * dd) * inv;
 }
 
+// A tile of the rect (rx0, ry0, cols) at row-major index `local`: the row from a
+// float quotient corrected to the exact one.
+__device__ __forceinline__ void rectTile(uint32_t local, uint32_t cols, float invCols, uint32_t& c, uint32_t& r) {
+    r = (uint32_t)(((float)local + 0.5f) * invCols);
+    if (r * cols > local) --r;
+    else if ((r + 1) * cols <= local) ++r;
+    c = local - r * cols;
+}
+
+// frame.slang:374-379 for tile size T: does tile (tx, ty) hold a pixel centre
+// inside the footprint? The factored form for a near-degenerate footprint.
+__device__ __forceinline__ bool footprintTouches(float4 fa, float4 fb, bool wide, uint32_t tx, uint32_t ty,
+                                                 uint32_t T, uint32_t width, uint32_t height) {
+    const float lx = ((float)(tx * T) + 0.5f) - fa.x, ly = ((float)(ty * T) + 0.5f) - fa.y;
+    const float hx = ((float)(min((tx + 1) * T, width) - 1) + 0.5f) - fa.x;
+    const float hy = ((float)(min((ty + 1) * T, height) - 1) + 0.5f) - fa.y;
+    const float best = wide ? minPowerOverBoxFactored(fa.z, fa.w, fb.x, fb.z, fb.w, lx, ly, hx, hy)
+                            : minPowerOverBox(fa.z, fa.w, fb.x, lx, ly, hx, hy);
+    return best <= fb.y;
+}
+
+// The least lane k whose inclusive sum `incl` passes q (q below the warp's total).
+__device__ __forceinline__ uint32_t ownerOf(uint32_t incl, uint32_t q) {
+    uint32_t lo = 0;
+#pragma unroll
+    for (uint32_t step = 16; step >= 1; step >>= 1) {
+        const uint32_t probe = __shfl_sync(0xFFFFFFFFu, incl, lo + step - 1u);
+        if (probe <= q) lo += step;
+    }
+    return lo;
+}
+
+// ---- the batched projection and pair emission: one thread a (view, Gaussian) ----
+// A block projects kProjThreads Gaussians for one view and writes their records.
+// The tiles are tested and the pairs written by warps: the candidate tiles of a
+// warp's 32 footprints (each footprint's screen rect, row-major) are one list,
+// lane l taking entry 32 c + l, so a warp's work is the sum of its rects, not 32
+// times the largest. A first walk counts the pairs (its ballots kept in shared
+// memory), the block's total is scanned across blocks by the epoch look-back, and
+// a second walk writes the pairs in list order: a footprint's pairs in its rect's
+// row-major order, footprints in thread order (splat_emit.slang:37-49).
+constexpr uint32_t kBallotCache = 16;   // chunks of 32 candidates whose ballots a warp keeps
+
 template <uint32_t L>
 __global__ void __launch_bounds__(kProjThreads)
     projectEmitKernel(const BatchConst B, const BatchView* __restrict__ views, float4* __restrict__ recs,
                       uint64_t* __restrict__ pairs, uint32_t* __restrict__ values, uint64_t* __restrict__ flags,
                       uint32_t* __restrict__ words, uint32_t gaussBlocks) {
+    constexpr uint32_t kWarps = kProjThreads / 32;
     __shared__ uint32_t sTicket;
-    __shared__ uint32_t sWarp[kProjThreads / 32];
+    __shared__ uint32_t sWarp[kWarps];
     __shared__ uint32_t sPrefix;
     __shared__ BatchView sView;
     __shared__ FrameConst sF;
+    __shared__ float4 sFa[kProjThreads];   // cx cy ca cb
+    __shared__ float4 sFb[kProjThreads];   // cc cutoff fr fs
+    __shared__ uint4 sRect[kProjThreads];  // rx0 ry0 cols, (depth key, 1 << 31 if wide)
+    __shared__ float sInvCols[kProjThreads];
+    __shared__ uint32_t sHit[kProjThreads];
+    __shared__ uint32_t sBallot[kWarps][kBallotCache];
     if (threadIdx.x == 0) sTicket = atomicAdd(&words[kBatchTicket], 1u);
     __syncthreads();
     const uint32_t t = sTicket;
@@ -255,17 +298,16 @@ __global__ void __launch_bounds__(kProjThreads)
     __syncthreads();
     const uint32_t epoch = words[kBatchEpoch];
     const FrameConst& F = sF;
-    InstanceConst I = B.inst;
-#pragma unroll
-    for (int k = 0; k < 12; ++k) I.m[k] = sView.m[k];
-    I.eye[0] = sView.eye[0]; I.eye[1] = sView.eye[1]; I.eye[2] = sView.eye[2];
     const uint32_t T = B.tile;
     const uint32_t i = gb * kProjThreads + threadIdx.x;
-    uint32_t touched = 0, depthKey = 0, rx0 = 0, ry0 = 0, rx1 = 0, ry1 = 0;
-    uint64_t mask = 0;
-    float cx = 0, cy = 0, ca = 0, cb = 0, cc = 0, cutoff = 0, fr = 0, fs = 0;
-    bool wide = false;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t area = 0;
+    sHit[threadIdx.x] = 0u;
     if (i < B.count && gb < gaussBlocks) {
+        InstanceConst I = B.inst;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) I.m[k] = sView.m[k];
+        I.eye[0] = sView.eye[0]; I.eye[1] = sView.eye[1]; I.eye[2] = sView.eye[2];
         const Gauss g = loadGauss<L>(I, i);
         const Geometry G = projectGeometry<true>(F, I, g, g.opacity);
         if (!G.cull) {
@@ -284,80 +326,66 @@ __global__ void __launch_bounds__(kProjThreads)
             }
             const float x1 = G.cx - ex, y1 = G.cy - ey, x2 = G.cx + ex, y2 = G.cy + ey;
             if (!(x2 < 0.0f || y2 < 0.0f || x1 >= (float)F.width || y1 >= (float)F.height)) {
-                rx0 = (uint32_t)fmaxf(x1, 0.0f) / T;
-                ry0 = (uint32_t)fmaxf(y1, 0.0f) / T;
-                rx1 = (uint32_t)fminf(x2, (float)F.width - 1.0f) / T;
-                ry1 = (uint32_t)fminf(y2, (float)F.height - 1.0f) / T;
-                cx = G.cx; cy = G.cy; ca = G.ca; cb = G.cb; cc = G.cc; cutoff = G.cutoff;
-                fr = G.fr; fs = G.fs; wide = G.wide;
-                uint32_t bit = 0;
-                if (wide) {
-                    for (uint32_t ty = ry0; ty <= ry1; ++ty)
-                        for (uint32_t tx = rx0; tx <= rx1; ++tx) {
-                            const float lx = ((float)(tx * T) + 0.5f) - cx, ly = ((float)(ty * T) + 0.5f) - cy;
-                            const float hx = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
-                            const float hy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
-                            if (minPowerOverBoxFactored(ca, cb, cc, fr, fs, lx, ly, hx, hy) <= cutoff) touched += 1;
-                        }
-                } else {
-                    for (uint32_t ty = ry0; ty <= ry1; ++ty) {
-                        const float loy = ((float)(ty * T) + 0.5f) - cy;
-                        const float hiy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
-                        // the row's x* = -b y / a at its two y edges
-                        const float xLo = ca > 1e-12f ? ((-cb) * loy) / ca : 0.0f;
-                        const float xHi = ca > 1e-12f ? ((-cb) * hiy) / ca : 0.0f;
-                        for (uint32_t tx = rx0; tx <= rx1; ++tx, ++bit) {
-                            const float lox = ((float)(tx * T) + 0.5f) - cx;
-                            const float hix = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
-                            float best;
-                            if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) {
-                                best = 0.0f;
-                            } else {
-                                best = 3.4e38f;
-                                const float yl = cc > 1e-12f ? clampf(((-cb) * lox) / cc, loy, hiy) : loy;
-                                best = fminf(best, quad(ca, cb, cc, lox, yl));
-                                const float yh = cc > 1e-12f ? clampf(((-cb) * hix) / cc, loy, hiy) : loy;
-                                best = fminf(best, quad(ca, cb, cc, hix, yh));
-                                const float xl = ca > 1e-12f ? clampf(xLo, lox, hix) : lox;
-                                best = fminf(best, quad(ca, cb, cc, xl, loy));
-                                const float xh = ca > 1e-12f ? clampf(xHi, lox, hix) : lox;
-                                best = fminf(best, quad(ca, cb, cc, xh, hiy));
-                            }
-                            if (best <= cutoff) {
-                                touched += 1;
-                                if (bit < 64) mask |= 1ull << bit;
-                            }
-                        }
-                    }
-                }
-                if (touched) {
-                    const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
-                    float colour[3];
-                    colourFast(loadMixedSh(I, i), g, degree, I.linear, g.px - I.eye[0], g.py - I.eye[1],
-                               g.pz - I.eye[2], colour);
-                    const size_t r = ((size_t)v * B.count + i) * 3;
-                    if (G.wide) atomicAdd(&words[kBatchDegenerate], 1u);
-                    recs[r + 0] = make_float4(G.cx, G.cy, G.tz, G.cutoff);
-                    recs[r + 1] = make_float4(G.ca, G.fr, G.fs, G.alpha);
-                    recs[r + 2] = make_float4(colour[0], colour[1], colour[2], 0.0f);
-                    depthKey = __float_as_uint(G.tz) >> 7;
-                }
+                const uint32_t rx0 = (uint32_t)fmaxf(x1, 0.0f) / T;
+                const uint32_t ry0 = (uint32_t)fmaxf(y1, 0.0f) / T;
+                const uint32_t rx1 = (uint32_t)fminf(x2, (float)F.width - 1.0f) / T;
+                const uint32_t ry1 = (uint32_t)fminf(y2, (float)F.height - 1.0f) / T;
+                const uint32_t cols = rx1 - rx0 + 1;
+                area = cols * (ry1 - ry0 + 1);
+                sFa[threadIdx.x] = make_float4(G.cx, G.cy, G.ca, G.cb);
+                sFb[threadIdx.x] = make_float4(G.cc, G.cutoff, G.fr, G.fs);
+                sRect[threadIdx.x] = make_uint4(rx0, ry0, cols, (__float_as_uint(G.tz) >> 7) | (G.wide ? 1u << 31 : 0u));
+                sInvCols[threadIdx.x] = 1.0f / (float)cols;
+                // the record (read only through the pairs, so written for any rect on screen)
+                const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
+                float colour[3];
+                colourFast(loadMixedSh(I, i), g, degree, I.linear, g.px - I.eye[0], g.py - I.eye[1], g.pz - I.eye[2],
+                           colour);
+                const size_t r = ((size_t)v * B.count + i) * 3;
+                recs[r + 0] = make_float4(G.cx, G.cy, G.tz, G.cutoff);
+                recs[r + 1] = make_float4(G.ca, G.fr, G.fs, G.alpha);
+                recs[r + 2] = make_float4(colour[0], colour[1], colour[2], 0.0f);
             }
         }
     }
-    // the scan of every view's pairs, in (Gaussian block, view, thread) order
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t incl = touched;
+    // the warp's candidate list: lane k's rect at [incl - area, incl)
+    uint32_t incl = area;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
         if (lane >= (uint32_t)o) incl += u;
     }
-    if (lane == 31) sWarp[warp] = incl;
-    const uint32_t kept = __syncthreads_count(touched > 0);
+    const uint32_t excl = incl - area;
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    const uint32_t base = warp * 32;
+    __syncwarp();
+    uint32_t warpPairs = 0;
+    for (uint32_t ch = 0, q0 = 0; q0 < total; ++ch, q0 += 32) {
+        const uint32_t q = q0 + lane;
+        const uint32_t owner = ownerOf(incl, min(q, total - 1u));
+        const uint32_t start = __shfl_sync(0xFFFFFFFFu, excl, owner);
+        bool hit = false;
+        if (q < total) {
+            const uint4 rect = sRect[base + owner];
+            uint32_t c, r;
+            rectTile(q - start, rect.z, sInvCols[base + owner], c, r);
+            hit = footprintTouches(sFa[base + owner], sFb[base + owner], (rect.w >> 31) != 0u, rect.x + c, rect.y + r,
+                                   T, F.width, F.height);
+        }
+        const uint32_t hits = __ballot_sync(0xFFFFFFFFu, hit);
+        if (ch < kBallotCache && lane == 0) sBallot[warp][ch] = hits;
+        warpPairs += __popc(hits);
+        if (hit) sHit[base + owner] = 1u;
+    }
+    __syncwarp();
+    const bool touched = sHit[threadIdx.x] != 0u;
+    if (touched && (sRect[threadIdx.x].w >> 31)) atomicAdd(&words[kBatchDegenerate], 1u);
+    // the scan of every view's pairs, in (Gaussian block, view, warp) order
+    if (lane == 0) sWarp[warp] = warpPairs;
+    const uint32_t kept = __syncthreads_count(touched);
     uint32_t warpBase = 0, blockTotal = 0;
 #pragma unroll
-    for (uint32_t w = 0; w < kProjThreads / 32; ++w) {
+    for (uint32_t w = 0; w < kWarps; ++w) {
         warpBase += w < warp ? sWarp[w] : 0u;
         blockTotal += sWarp[w];
     }
@@ -367,51 +395,47 @@ __global__ void __launch_bounds__(kProjThreads)
             sPrefix = prefix;
             if (kept) atomicAdd(&words[kBatchKept], kept);
             if (t == gridDim.x - 1) {
-                const uint64_t total = (uint64_t)prefix + blockTotal;
-                words[kBatchPairsLo] = (uint32_t)total;
-                words[kBatchPairsHi] = (uint32_t)(total >> 32);
-                if (total > B.capacity) atomicOr(&words[kBatchStatus], kStatusPairOverflow);
+                const uint64_t all = (uint64_t)prefix + blockTotal;
+                words[kBatchPairsLo] = (uint32_t)all;
+                words[kBatchPairsHi] = (uint32_t)(all >> 32);
+                if (all > B.capacity) atomicOr(&words[kBatchStatus], kStatusPairOverflow);
             }
         }
     }
     __syncthreads();
-    if (!touched) return;
-    // the pairs, in the rect's row-major order (splat_emit.slang:37-49)
-    uint64_t at = (uint64_t)sPrefix + warpBase + (incl - touched);
-    // packed: (global tile << keyShift) | (depth << slotBits) | Gaussian; wide: (global tile << 24) | depth,
-    // the Gaussian beside it in `values`
-    const uint64_t head = ((uint64_t)(sView.tileBase) << B.keyShift) | ((uint64_t)depthKey << B.slotBits) |
-                          (B.wide ? 0u : i);
-    const uint32_t cols = rx1 - rx0 + 1;
-    const uint32_t area = cols * (ry1 - ry0 + 1);
-    if (area <= 64 && !wide) {
-        uint64_t m = mask;
-        while (m) {
-            const uint32_t bit = (uint32_t)__ffsll((long long)m) - 1u;
-            m &= m - 1;
-            const uint32_t tx = rx0 + bit % cols, ty = ry0 + bit / cols;
-            if (at < B.capacity) {
-                pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
-                if (B.wide) values[at] = i;
-            }
-            ++at;
+    if (warpPairs == 0) return;
+    // the pairs, in list order. packed: (global tile << keyShift) | (depth << slotBits) | Gaussian;
+    // wide: (global tile << 24) | depth, the Gaussian beside it in `values`
+    const uint32_t tileBase = sView.tileBase;
+    const uint32_t below = (1u << lane) - 1u;
+    uint64_t at = (uint64_t)sPrefix + warpBase;
+    for (uint32_t ch = 0, q0 = 0; q0 < total; ++ch, q0 += 32) {
+        const uint32_t q = q0 + lane;
+        const uint32_t owner = ownerOf(incl, min(q, total - 1u));
+        const uint32_t start = __shfl_sync(0xFFFFFFFFu, excl, owner);
+        const uint4 rect = sRect[base + owner];
+        uint32_t c = 0, r = 0;
+        if (q < total) rectTile(q - start, rect.z, sInvCols[base + owner], c, r);
+        const uint32_t tx = rect.x + c, ty = rect.y + r;
+        uint32_t hits;
+        if (ch < kBallotCache) {
+            hits = sBallot[warp][ch];
+        } else {
+            const bool hit = q < total && footprintTouches(sFa[base + owner], sFb[base + owner], (rect.w >> 31) != 0u,
+                                                           tx, ty, T, F.width, F.height);
+            hits = __ballot_sync(0xFFFFFFFFu, hit);
         }
-    } else {
-        for (uint32_t ty = ry0; ty <= ry1; ++ty)
-            for (uint32_t tx = rx0; tx <= rx1; ++tx) {
-                const float lx = ((float)(tx * T) + 0.5f) - cx, ly = ((float)(ty * T) + 0.5f) - cy;
-                const float hx = ((float)(min((tx + 1) * T, F.width) - 1) + 0.5f) - cx;
-                const float hy = ((float)(min((ty + 1) * T, F.height) - 1) + 0.5f) - cy;
-                const float best = wide ? minPowerOverBoxFactored(ca, cb, cc, fr, fs, lx, ly, hx, hy)
-                                        : minPowerOverBox(ca, cb, cc, lx, ly, hx, hy);
-                if (best <= cutoff) {
-                    if (at < B.capacity) {
-                        pairs[at] = head + ((uint64_t)(ty * sView.tilesX + tx) << B.keyShift);
-                        if (B.wide) values[at] = i;
-                    }
-                    ++at;
-                }
+        if ((hits >> lane) & 1u) {
+            const uint64_t pos = at + __popc(hits & below);
+            const uint32_t gi = gb * kProjThreads + base + owner;
+            if (pos < B.capacity) {
+                const uint32_t tile = tileBase + ty * sView.tilesX + tx;
+                pairs[pos] = ((uint64_t)tile << B.keyShift) | ((uint64_t)(rect.w & 0x7FFFFFFFu) << B.slotBits) |
+                             (B.wide ? 0u : gi);
+                if (B.wide) values[pos] = gi;
             }
+        }
+        at += __popc(hits);
     }
 }
 
@@ -993,8 +1017,8 @@ extern "C" ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params
                                             float* colour, float* loss, ath_param_grads* grads, float ms[7],
                                             void* streamPtr) {
     // A step as ath_batch_train_step enqueues it, uncaptured, with events between
-    // its stages, waited for: project+emit, sort, ranges, blend, loss, blend
-    // adjoint, projection adjoint.
+    // its stages, waited for: project+emit, sort, ranges, blend and loss,
+    // clearing the record gradients, blend adjoint, projection adjoint.
     if (!b || !params || !grads || !ms) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_time_stages: null argument");
     ath_status st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);   // sized and placed
     if (st != ATH_OK) return st;

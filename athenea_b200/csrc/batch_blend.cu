@@ -358,19 +358,12 @@ __global__ void __launch_bounds__(T * T / 2)
                         const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, live);
                         if (!lanes) continue;
                         float* acc = sAcc + j * kWords;
-                        if (__popc(lanes) <= 3) {
-                            // few lanes live: their terms straight into the record's sums
-                            if (live) {
-#pragma unroll
-                                for (int q = 0; q < (int)kWords; ++q)
-                                    if (gv[q] != 0.0f) atomicAdd(acc + q, gv[q]);
-                            }
-                        } else {
-                            float ninth;
-                            const float s = warpSum9(gv, ninth);
-                            if ((lane & 3u) == 0u && s != 0.0f) atomicAdd(acc + (lane >> 2), s);
-                            if (lane == 0 && ninth != 0.0f) atomicAdd(acc + 8, ninth);
-                        }
+                        // the warp's sums, however few lanes are live (shared-memory atomics from
+                        // each live lane were slower: they serialise on the record's nine words)
+                        float ninth;
+                        const float s = warpSum9(gv, ninth);
+                        if ((lane & 3u) == 0u && s != 0.0f) atomicAdd(acc + (lane >> 2), s);
+                        if (lane == 0 && ninth != 0.0f) atomicAdd(acc + 8, ninth);
                     }
                 }
             }
