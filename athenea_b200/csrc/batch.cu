@@ -15,7 +15,7 @@
 //                 the tile and depth bits only: stability keeps each tile's
 //                 ties in Gaussian order, the reference's (frame.slang:17-20).
 //   blend         a persistent kernel over every view's tiles (a tile queue),
-//                 tile size 8, 16 or 32 and a record batch of 64, 128 or 256.
+//                 tile size 8, 16 or 32 and a record batch of 64, 128, 256 or 512.
 //   loss          mean L2 a view against its target, summed over views.
 //   blendAdjoint  the same queue, reverse order, as backward.cu.
 //   projectAdjoint one thread a Gaussian over every view, its gradient kept in
@@ -897,8 +897,9 @@ extern "C" ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode) {
 
 extern "C" ath_status ath_batch_set_tuning(ath_batch* b, uint32_t tile, uint32_t blockBatch) {
     if (!b) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_tuning: null handle");
-    if ((tile != 8 && tile != 16 && tile != 32) || (blockBatch != 64 && blockBatch != 128 && blockBatch != 256))
-        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_tuning: tile 8, 16 or 32; block batch 64, 128 or 256");
+    if ((tile != 8 && tile != 16 && tile != 32) ||
+        (blockBatch != 64 && blockBatch != 128 && blockBatch != 256 && blockBatch != 512))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_tuning: tile 8, 16 or 32; block batch 64, 128, 256 or 512");
     if (tile != b->tile || blockBatch != b->blockBatch) {
         b->tile = tile;
         b->blockBatch = blockBatch;
@@ -1057,7 +1058,7 @@ extern "C" ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* param
                                      ath_batch_stats* best, void* streamPtr) {
     if (!b || !params) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_tune: null argument");
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
-    const uint32_t tiles[3] = {8, 16, 32}, batches[3] = {64, 128, 256};
+    const uint32_t tiles[3] = {32, 16, 8}, batches[4] = {64, 128, 256, 512};
     float bestMs = 1e30f;
     uint32_t bestTile = b->tile, bestBatch = b->blockBatch;
     cudaEvent_t e0, e1;
@@ -1085,6 +1086,16 @@ extern "C" ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* param
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    // the pair buffers grew to the setting with the most pairs; size them again for the one kept
+    // (the sort's grid follows their capacity)
+    cudaStreamSynchronize(stream);
+    dropGraph(b);
+    for (int k = 0; k < 2; ++k) {
+        b->pairs[k].release();
+        b->values[k].release();
+    }
+    b->capacity = 0;
+    b->resize = true;
     ath_status st = ath_batch_set_tuning(b, bestTile, bestBatch);
     if (st == ATH_OK) st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);
     if (st == ATH_OK && best) st = ath_batch_check(b, best, streamPtr);

@@ -423,8 +423,8 @@ cudaError_t adjointWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t 
 }   // namespace
 
 #define ATH_BLEND_CASES(CALL)                                                                              \
-    CALL(8, 64) CALL(8, 128) CALL(8, 256) CALL(16, 64) CALL(16, 128) CALL(16, 256) CALL(32, 64) CALL(32, 128) \
-    CALL(32, 256)
+    CALL(8, 64) CALL(8, 128) CALL(8, 256) CALL(8, 512) CALL(16, 64) CALL(16, 128) CALL(16, 256) CALL(16, 512)     \
+    CALL(32, 64) CALL(32, 128) CALL(32, 256) CALL(32, 512)
 
 cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
                              const float* target, float4* dL, float* loss) {

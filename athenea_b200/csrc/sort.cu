@@ -94,11 +94,12 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
     // epoch reads as not ready. Without an epoch (0) the caller clears them.
     const uint32_t epoch = epochDevice ? (*epochDevice & 0x3FFFFFFFu) : 0u;
     if (tid == 0) sTile = atomicAdd(ticket, 1u);
-    for (uint32_t j = tid; j < kCounters * kRadix; j += kSortThreads) sWarpCnt[j] = 0;
     __syncthreads();
     const uint32_t tile = sTile;
     const uint32_t base = tile * kTileKeys;
-    if (base >= n) return;   // a tile past the keys (the grid was sized for a bound)
+    if (base >= n) return;   // a tile past the keys (the grid was sized for a bound): out before any work
+    for (uint32_t j = tid; j < kCounters * kRadix; j += kSortThreads) sWarpCnt[j] = 0;
+    __syncthreads();
     const uint32_t ltMask = (1u << lane) - 1u;
 
     // Rank: warp `warp` owns keys [base + warp*32*kItems, +32*kItems), item k of

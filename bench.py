@@ -378,7 +378,7 @@ def main():
     ap.add_argument("--gaussians", type=int, default=WORKLOAD["count"], help="Gaussians in the scene")
     ap.add_argument("--tile", type=int, choices=[8, 16, 32], default=0,
                     help="fix the batched step's tile size instead of autotuning")
-    ap.add_argument("--block-batch", type=int, choices=[64, 128, 256], default=256,
+    ap.add_argument("--block-batch", type=int, choices=[64, 128, 256, 512], default=256,
                     help="records a block stages at once, with --tile")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--workload", type=int, choices=[1, 3, 4], default=1,

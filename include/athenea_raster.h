@@ -304,7 +304,7 @@ void ath_batch_destroy(ath_batch* b);
  * (background, max_sh_degree, antialias). Images are concatenated in view order:
  * view v's pixel (x, y) is at v's base + y * width + x; ath_batch_pixels gives the total. */
 ath_status ath_batch_set_views(ath_batch* b, const ath_view* views, uint32_t count, const ath_settings* settings);
-/* Tile size (8, 16 or 32) and records a block stages at once (64, 128 or 256).
+/* Tile size (8, 16 or 32) and records a block stages at once (64, 128, 256 or 512).
  * Images do not depend on either: a pixel blends the same records in the same
  * order whatever tile holds it. Default 16 and 256. */
 ath_status ath_batch_set_tuning(ath_batch* b, uint32_t tile, uint32_t block_batch);
@@ -332,7 +332,8 @@ ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, co
  * outgrew the buffers (that step is not valid; the next one grows them). */
 ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* stream);
 /* The autotuner: times `repeats` steps for every tile size in {8, 16, 32} and
- * block batch in {64, 128, 256}, keeps the fastest and reports it in `best`. */
+ * block batch in {64, 128, 256, 512}, keeps the fastest and reports it in `best`.
+ * The pair buffers are then sized again for the setting kept. */
 ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
                           float* loss, ath_param_grads* grads, uint32_t repeats, ath_batch_stats* best, void* stream);
 

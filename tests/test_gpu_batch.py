@@ -157,7 +157,7 @@ def test_replayed_step_draws_the_same_image_and_tune_picks_a_setting():
     torch.cuda.synchronize()
     np.testing.assert_array_equal(colour.cpu().numpy(), first)
     best = b.tune(M, torch.cat(targets).contiguous(), colour, loss, grads, repeats=2)
-    assert best["tile"] in (8, 16, 32) and best["block_batch"] in (64, 128, 256) and best["ms_per_step"] > 0
+    assert best["tile"] in (8, 16, 32) and best["block_batch"] in (64, 128, 256, 512) and best["ms_per_step"] > 0
 
 
 def test_wide_pairs_sort_and_draw_as_the_packed_ones():
