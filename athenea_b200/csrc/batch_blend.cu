@@ -69,7 +69,7 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
 }
 
 template <uint32_t T, uint32_t NB>
-__global__ void __launch_bounds__(T * T / 2)
+__global__ void __launch_bounds__(T * T / 2, 2)
     blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                      const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
                      const float4* __restrict__ recs,
@@ -306,14 +306,15 @@ __global__ void __launch_bounds__(T * T / 2)
             if (relStart < warpLast) {
                 for (int base = (int)((count - 1) & ~31u); base >= 0; base -= 32) {
                     if (relStart + (uint32_t)base >= warpLast) continue;
-                    const uint32_t m = (uint32_t)base + lane < count ? sMask[base + lane] : 0u;
+                    // the records marked for this warp's box, up to its pixels' last contributor
+                    const uint32_t m = (uint32_t)base + lane < count && relStart + (uint32_t)base + lane < warpLast
+                                           ? sMask[base + lane] : 0u;
                     uint32_t todo = __ballot_sync(0xFFFFFFFFu, (m >> warp) & 1u);
                     while (todo) {
                         const uint32_t hb = 31u - (uint32_t)__clz(todo);
                         todo &= ~(1u << hb);
                         const uint32_t j = (uint32_t)base + hb;
                         const uint32_t rel = relStart + j;
-                        if (rel >= warpLast) continue;
                         const float2 ce = sCentre[j];
                         const float4 k = sConic[j];
                         const float4 c = sColour[j];
