@@ -475,9 +475,17 @@ __global__ void __launch_bounds__(128)
         float dSh[48];
 #pragma unroll
         for (int k = 0; k < 48; ++k) dSh[k] = 0.0f;
+        // each view's colour gradient loaded a view ahead, so its latency overlaps the work
+        const float* gr0 = grads + (size_t)i * kGradWords;
+        float next[3] = {gr0[kGradR], gr0[kGradG], gr0[kGradB]};
         for (uint32_t v = 0; v < B.views; ++v) {
-            const float* gr = grads + ((size_t)v * B.count + i) * kGradWords;
-            const float gc[3] = {gr[kGradR], gr[kGradG], gr[kGradB]};
+            const float gc[3] = {next[0], next[1], next[2]};
+            if (v + 1 < B.views) {
+                const float* gr = grads + ((size_t)(v + 1) * B.count + i) * kGradWords;
+                next[0] = gr[kGradR];
+                next[1] = gr[kGradG];
+                next[2] = gr[kGradB];
+            }
             if (gc[0] == 0.0f && gc[1] == 0.0f && gc[2] == 0.0f) continue;
             colourAdjointFast(sh, g, degree, I.linear, views[v].eye, gc, dSh, dp);
         }
@@ -491,14 +499,21 @@ __global__ void __launch_bounds__(128)
     acc.dLogit = 0.0f;
     acc.dLogScale[0] = acc.dLogScale[1] = acc.dLogScale[2] = 0.0f;
     acc.dQuat[0] = acc.dQuat[1] = acc.dQuat[2] = acc.dQuat[3] = 0.0f;
+    float next[kGradWords];
+#pragma unroll
+    for (int k = 0; k < (int)kGradWords; ++k) next[k] = grads[(size_t)i * kGradWords + k];
     for (uint32_t v = 0; v < B.views; ++v) {
-        const float* gr = grads + ((size_t)v * B.count + i) * kGradWords;
         float gw[kGradWords];
         bool any = false;
 #pragma unroll
         for (int k = 0; k < (int)kGradWords; ++k) {
-            gw[k] = gr[k];
+            gw[k] = next[k];
             any |= gw[k] != 0.0f;
+        }
+        if (v + 1 < B.views) {
+            const float* gr = grads + ((size_t)(v + 1) * B.count + i) * kGradWords;
+#pragma unroll
+            for (int k = 0; k < (int)kGradWords; ++k) next[k] = gr[k];
         }
         if (!any) continue;
         const BatchView& V = views[v];
