@@ -68,6 +68,18 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
     return mask;
 }
 
+// The Gaussian indices of pairs [first, end) that this thread stages (k = thread + q threads,
+// k < NB), for a load issued ahead of their use; 0 past the end.
+template <uint32_t kThreads, uint32_t NB, uint32_t kPer>
+__device__ __forceinline__ void prefetchIndices(const uint64_t* pairs, const uint32_t* values, uint64_t slotMask,
+                                                uint32_t first, uint32_t end, uint32_t (&out)[kPer]) {
+#pragma unroll
+    for (uint32_t q = 0; q < kPer; ++q) {
+        const uint32_t k = threadIdx.x + q * kThreads;
+        out[q] = k < NB && first + k < end ? gaussianOf(pairs, values, slotMask, first + k) : 0u;
+    }
+}
+
 template <uint32_t T, uint32_t NB>
 __global__ void __launch_bounds__(T * T / 2, 2)
     blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
@@ -236,6 +248,7 @@ __global__ void __launch_bounds__(T * T / 2)
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
     constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
+    constexpr uint32_t kPer = (NB + kThreads - 1) / kThreads;   // records a thread stages a batch
     __shared__ float2 sCentre[NB];
     __shared__ float4 sConic[NB];
     __shared__ float4 sColour[NB];
@@ -284,16 +297,31 @@ __global__ void __launch_bounds__(T * T / 2)
         __syncthreads();
         const uint32_t end = range.x + sMaxLast;
         const size_t recBase = (size_t)v * B.count;
+        uint32_t ahead[kPer];   // the batch's Gaussian indices, loaded a batch ahead
+        {
+            const uint32_t start = end - range.x > NB ? end - NB : range.x;
+            prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, start, end, ahead);
+        }
         for (uint32_t batchEnd = end; batchEnd > range.x;) {
             const uint32_t batchStart = batchEnd - range.x > NB ? batchEnd - NB : range.x;
             const uint32_t count = batchEnd - batchStart;
-            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
-                const uint32_t s = gaussianOf(pairs, values, slotMask, batchStart + k);
+            uint32_t gauss[kPer];
+#pragma unroll
+            for (uint32_t q = 0; q < kPer; ++q) gauss[q] = ahead[q];
+            if (batchStart > range.x) {
+                const uint32_t prevStart = batchStart - range.x > NB ? batchStart - NB : range.x;
+                prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, prevStart, batchStart, ahead);
+            }
+#pragma unroll
+            for (uint32_t q = 0; q < kPer; ++q) {
+                const uint32_t k = threadIdx.x + q * kThreads;
+                if (k >= count) break;
+                const uint32_t s = gauss[q];
                 sRec[k] = s;
-                const size_t q = (recBase + s) * 3;
-                const float4 sc = recs[q + 0];
-                const float4 c = recs[q + 1];
-                const float4 rgb = recs[q + 2];
+                const size_t at = (recBase + s) * 3;
+                const float4 sc = recs[at + 0];
+                const float4 c = recs[at + 1];
+                const float4 rgb = recs[at + 2];
                 sCentre[k] = make_float2(sc.x, sc.y);
                 // the forward's pre-scale, operation for operation (so the same records pass)
                 sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
