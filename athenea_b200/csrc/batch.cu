@@ -439,18 +439,48 @@ __global__ void __launch_bounds__(kProjThreads, 4)   // four blocks an SM: the k
     }
 }
 
+// Each tile's range in the sorted pairs: a thread takes a run of eight keys (four
+// 16-byte loads) and the key before it, and writes a range's start and the
+// previous range's end where the tile changes.
+constexpr uint32_t kRangeRun = 8;
+
 __global__ void __launch_bounds__(256)
     rangesBatchKernel(uint64_t capacity, const uint32_t* __restrict__ words, uint32_t keyShift, uint32_t totalTiles,
                       const uint64_t* __restrict__ pairs, uint2* __restrict__ ranges, uint32_t* __restrict__ status) {
     const uint64_t n = min((uint64_t)words[kBatchPairsLo] | ((uint64_t)words[kBatchPairsHi] << 32), capacity);
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t t = (uint32_t)(pairs[i] >> keyShift);
-        if (t >= totalTiles) {
-            atomicOr(status, kStatusIndexRange);
-            continue;
+    for (uint64_t run = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; run * kRangeRun < n;
+         run += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i0 = run * kRangeRun;
+        uint64_t key[kRangeRun];
+        if (i0 + kRangeRun <= n) {
+            const ulonglong2* at = reinterpret_cast<const ulonglong2*>(pairs + i0);
+#pragma unroll
+            for (uint32_t k = 0; k < kRangeRun / 2; ++k) {
+                const ulonglong2 two = at[k];
+                key[2 * k] = two.x;
+                key[2 * k + 1] = two.y;
+            }
+        } else {
+#pragma unroll
+            for (uint32_t k = 0; k < kRangeRun; ++k) key[k] = i0 + k < n ? pairs[i0 + k] : 0ull;
         }
-        if (i == 0 || (uint32_t)(pairs[i - 1] >> keyShift) != t) ranges[t].x = (uint32_t)i;
-        if (i + 1 == n || (uint32_t)(pairs[i + 1] >> keyShift) != t) ranges[t].y = (uint32_t)(i + 1);
+        uint32_t prev = i0 == 0 ? 0xFFFFFFFFu : (uint32_t)(pairs[i0 - 1] >> keyShift);
+#pragma unroll
+        for (uint32_t k = 0; k < kRangeRun; ++k) {
+            const uint64_t i = i0 + k;
+            if (i >= n) break;
+            uint32_t t = (uint32_t)(key[k] >> keyShift);
+            if (t >= totalTiles) {
+                atomicOr(status, kStatusIndexRange);
+                t = 0xFFFFFFFFu;
+            }
+            if (t != prev) {
+                if (t != 0xFFFFFFFFu) ranges[t].x = (uint32_t)i;
+                if (prev < totalTiles) ranges[prev].y = (uint32_t)i;
+            }
+            if (i + 1 == n && t != 0xFFFFFFFFu) ranges[t].y = (uint32_t)n;
+            prev = t;
+        }
     }
 }
 
@@ -745,7 +775,8 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     b->lastWide = B.wide != 0;
     if (err == cudaSuccess) err = cudaMemsetAsync(b->ranges.ptr, 0, (size_t)b->totalTiles * 8, stream);
     if (err == cudaSuccess) {
-        const uint32_t grid = std::max<uint32_t>(1, std::min<uint64_t>((b->capacity + 255) / 256, (uint64_t)b->sms * 8));
+        const uint32_t grid = std::max<uint32_t>(
+            1, std::min<uint64_t>((b->capacity + 256 * kRangeRun - 1) / (256 * kRangeRun), (uint64_t)b->sms * 8));
         rangesBatchKernel<<<grid, 256, 0, stream>>>(b->capacity, words, B.keyShift, b->totalTiles, keys[sorted],
                                                     static_cast<uint2*>(b->ranges.ptr), words + kBatchStatus);
         err = cudaGetLastError();
