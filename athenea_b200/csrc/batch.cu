@@ -270,7 +270,7 @@ template <uint32_t L>
 __global__ void __launch_bounds__(kProjThreads, 4)   // four blocks an SM: the kernel is latency-bound
     projectEmitKernel(const BatchConst B, const BatchView* __restrict__ views, float4* __restrict__ recs,
                       uint64_t* __restrict__ pairs, uint32_t* __restrict__ values, uint64_t* __restrict__ flags,
-                      uint32_t* __restrict__ words, uint32_t gaussBlocks) {
+                      uint32_t* __restrict__ words, float* __restrict__ grads, uint32_t gaussBlocks) {
     constexpr uint32_t kWarps = kProjThreads / 32;
     __shared__ uint32_t sTicket;
     __shared__ uint32_t sWarp[kWarps];
@@ -304,6 +304,10 @@ __global__ void __launch_bounds__(kProjThreads, 4)   // four blocks an SM: the k
     uint32_t area = 0;
     sHit[threadIdx.x] = 0u;
     if (i < B.count && gb < gaussBlocks) {
+        // the record's gradient words, which the blend adjoint sums into, start at zero
+        float2* zero = reinterpret_cast<float2*>(grads + ((size_t)v * B.count + i) * kGradWords);
+#pragma unroll
+        for (uint32_t k = 0; k < kGradWords / 2; ++k) zero[k] = make_float2(0.0f, 0.0f);
         InstanceConst I = B.inst;
 #pragma unroll
         for (int k = 0; k < 12; ++k) I.m[k] = sView.m[k];
@@ -757,7 +761,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
         projectEmitKernel<kLayoutMixed><<<gaussBlocks * V, kProjThreads, 0, stream>>>(
             B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<float4*>(b->recs.ptr),
             static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint32_t*>(b->values[0].ptr),
-            static_cast<uint64_t*>(b->projFlags.ptr), words, gaussBlocks);
+            static_cast<uint64_t*>(b->projFlags.ptr), words, static_cast<float*>(b->grads.ptr), gaussBlocks);
     if (err == cudaSuccess) err = cudaGetLastError();
     if (countOnly || err != cudaSuccess) return err;
     mark(1);
@@ -786,9 +790,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     if (err == cudaSuccess)
         err = launchBlendsFor(b, B, sorted, stream, true, colour, static_cast<float4*>(b->dL.ptr), nullptr, target,
                               loss);
-    mark(4);
-    if (err == cudaSuccess)
-        err = cudaMemsetAsync(b->grads.ptr, 0, (size_t)V * P.count * kGradWords * sizeof(float), stream);
+    mark(4);   // (the record gradients were cleared by the projection)
     mark(5);
     if (err == cudaSuccess)
         err = launchBlendsFor(b, B, sorted, stream, false, nullptr, static_cast<float4*>(b->dL.ptr),
