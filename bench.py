@@ -41,10 +41,10 @@ METRIC = "fwd+bwd ms/view, 1.5M Gaussians 1080p, batched+BF16 vs plain FP32, err
 # DRAM bytes a launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # batched kernels, from an ncu capture of this workload (profiles/).
 NCU_TRAFFIC: dict = {
-    # profiles/batched_kernels_1.5M_2x1080p_tile32.md: 157.0 MB on 2 views, scaled to 8
-    "blendAdjointBatchKernel": 4 * 156.92e6,
-    "blendBatchKernel": 4 * 213.04e6,
-    "projectEmitKernel": 4 * 346.23e6,
+    # profiles/batched_kernels_1.5M_2x1080p_tile32.md: 158.9 MB on 2 views, scaled to 8
+    "blendAdjointBatchKernel": 4 * 158.95e6,
+    "blendBatchKernel": 4 * 212.91e6,
+    "projectEmitKernel": 4 * 459.14e6,
 }
 
 
