@@ -608,7 +608,7 @@ struct ath_batch {
     std::vector<uint32_t> widths, heights, tileBases;
     uint32_t lastSorted = 0, lastSlotBits = 0;
     // scratch
-    DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges, finalT, lastContrib, dL;
+    DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges;
     uint32_t keyMode = 0;      // 0 packed when it fits in 64 bits, else wide; 1 packed; 2 wide
     bool lastWide = false;
     uint32_t count = 0;
@@ -726,9 +726,8 @@ int residentBlocks(K kernel, int threads, int sms) {
     return std::max(n, 1) * sms;
 }
 
-cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t sorted, cudaStream_t stream, bool forward,
-                            float4* colour, float4* dL, float* grads, const float* target = nullptr,
-                            float* loss = nullptr) {
+cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t sorted, cudaStream_t stream,
+                            float4* colour, const float* target, float* loss, float* grads) {
     BlendLaunch L{};
     L.views = static_cast<const BatchView*>(b->viewsDev.ptr);
     L.ranges = static_cast<const uint2*>(b->ranges.ptr);
@@ -736,13 +735,10 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
     L.values = B.wide ? static_cast<const uint32_t*>(b->values[sorted].ptr) : nullptr;
     L.recs = static_cast<const float4*>(b->recs.ptr);
     L.words = static_cast<uint32_t*>(b->words.ptr);
-    L.finalT = static_cast<float*>(b->finalT.ptr);
-    L.lastContrib = static_cast<uint32_t*>(b->lastContrib.ptr);
     L.sms = b->sms;
     L.tile = b->tile;
     L.blockBatch = b->blockBatch;
-    return forward ? launchBatchBlend(B, L, stream, colour, target, dL, loss)
-                   : launchBatchBlendAdjoint(B, L, stream, dL, grads);
+    return launchBatchBlendStep(B, L, stream, colour, target, loss, grads);
 }
 
 // One step, enqueued (captured or not). `countOnly`: the projection alone, to size the pairs.
@@ -787,15 +783,10 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     }
     mark(3);
     if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
+    // the forward blend, the loss and the blend adjoint (the record gradients were cleared by the projection)
     if (err == cudaSuccess)
-        err = launchBlendsFor(b, B, sorted, stream, true, colour, static_cast<float4*>(b->dL.ptr), nullptr, target,
-                              loss);
-    mark(4);   // (the record gradients were cleared by the projection)
-    mark(5);
-    if (err == cudaSuccess)
-        err = launchBlendsFor(b, B, sorted, stream, false, nullptr, static_cast<float4*>(b->dL.ptr),
-                              static_cast<float*>(b->grads.ptr));
-    mark(6);
+        err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr));
+    mark(4);
     if (err == cudaSuccess && P.count) {
         projectAdjointBatchKernel<<<(P.count + 127) / 128, 128, 0, stream>>>(
             B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
@@ -803,7 +794,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
             g.sh, 48);
         err = cudaGetLastError();
     }
-    mark(7);
+    mark(5);
     return err;
 }
 
@@ -816,9 +807,6 @@ ath_status reserveBatch(ath_batch* b, uint32_t count) {
     if (err == cudaSuccess) err = b->grads.reserve((size_t)V * count * kGradWords * sizeof(float));
     if (err == cudaSuccess) err = b->projFlags.reserve((size_t)std::max(1u, gaussBlocks * V) * 8);
     if (err == cudaSuccess) err = b->ranges.reserve((size_t)std::max(1u, b->totalTiles) * 8);
-    if (err == cudaSuccess) err = b->finalT.reserve((size_t)std::max(1u, b->totalPixels) * 4);
-    if (err == cudaSuccess) err = b->lastContrib.reserve((size_t)std::max(1u, b->totalPixels) * 4);
-    if (err == cudaSuccess) err = b->dL.reserve((size_t)std::max(1u, b->totalPixels) * 16);
     if (err == cudaSuccess) err = b->sortHist.reserve(8 * 256 * sizeof(uint32_t));
     if (err == cudaSuccess) err = b->viewsDev.reserve(std::max<size_t>(1, b->views.size()) * sizeof(BatchView));
     if (err != cudaSuccess) return failCuda(err, "reserving the batch's scratch");
@@ -1063,21 +1051,21 @@ extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* 
 }
 
 extern "C" ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params* params, const float* target,
-                                            float* colour, float* loss, ath_param_grads* grads, float ms[7],
+                                            float* colour, float* loss, ath_param_grads* grads, float ms[5],
                                             void* streamPtr) {
     // A step as ath_batch_train_step enqueues it, uncaptured, with events between
-    // its stages, waited for: project+emit, sort, ranges, blend and loss,
-    // clearing the record gradients, blend adjoint, projection adjoint.
+    // its stages, waited for: project+emit, sort, ranges, blends (forward, loss and
+    // adjoint in one kernel), projection adjoint.
     if (!b || !params || !grads || !ms) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_time_stages: null argument");
     ath_status st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);   // sized and placed
     if (st != ATH_OK) return st;
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
-    cudaEvent_t marks[8];
+    cudaEvent_t marks[6];
     for (auto& e : marks) cudaEventCreate(&e);
     ath_param_grads g = *grads;
     cudaError_t err = enqueueStep(b, *params, target, reinterpret_cast<float4*>(colour), loss, g, stream, false, marks);
-    if (err == cudaSuccess) err = cudaEventSynchronize(marks[7]);
-    for (int k = 0; k < 7 && err == cudaSuccess; ++k) cudaEventElapsedTime(&ms[k], marks[k], marks[k + 1]);
+    if (err == cudaSuccess) err = cudaEventSynchronize(marks[5]);
+    for (int k = 0; k < 5 && err == cudaSuccess; ++k) cudaEventElapsedTime(&ms[k], marks[k], marks[k + 1]);
     for (auto& e : marks) cudaEventDestroy(e);
     return err == cudaSuccess ? ATH_OK : failCuda(err, "ath_batch_time_stages");
 }

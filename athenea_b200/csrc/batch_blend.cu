@@ -1,9 +1,10 @@
-// The batched path's blends: the persistent forward over every view's tiles and
-// its adjoint. This file builds with FMA contraction (the other kernels of the
-// plain and batched paths do not): nothing here has to match the reference's
-// FP32 to the bit, only the forward and the adjoint each other, and both are
-// compiled alike. Which records a pixel blends is decided per pixel, the same
-// way in both, whatever the tile size.
+// The batched path's blends: a training step's forward blend, loss and blend
+// adjoint in one persistent kernel over every view's tiles. This file builds
+// with FMA contraction (the other kernels of the plain and batched paths do
+// not): nothing here has to match the reference's FP32 to the bit, only the
+// forward and the adjoint each other, and both are compiled alike. Which records
+// a pixel blends is decided per pixel, the same way in both, whatever the tile
+// size.
 #include <cstdint>
 
 #include <cuda_runtime.h>
@@ -13,16 +14,7 @@
 namespace ath {
 namespace {
 
-// ---- the persistent blend ------------------------------------------------------
-// One block of T*T/2 threads takes tiles off a queue. Warp w owns an 8x8 box of
-// the tile and each lane two pixels of it, (x, y) and (x, y + 4). Staging a
-// batch of records, the block marks for each record the boxes its footprint can
-// reach (a conservative test: the box's least power against the cutoff, with a
-// margin); a warp then walks only the records marked for its box, found 32 at a
-// time by a ballot, in list order. A pixel blends exactly the records it would
-// blend walking the whole list: the per-pixel test decides, the box test only
-// skips records no pixel of the box can pass. So the image does not depend on
-// the tile size.
+// A warp's box of pixels: 8x8, two pixels a lane.
 constexpr uint32_t kBox = 8;
 
 // The footprint's half extents from the factored conic: the covariance's
@@ -80,32 +72,90 @@ __device__ __forceinline__ void prefetchIndices(const uint64_t* pairs, const uin
     }
 }
 
+// Nine values summed over a warp: the first eight by a transposed reduction
+// (each level sends half of the values still held and keeps the other half,
+// so three levels leave value (lane >> 2) spread over lanes differing in their
+// two low bits), the ninth by a butterfly. Lanes with lane % 4 == 0 hold value
+// lane >> 2; every lane holds the ninth.
+__device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int half = 4, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
+        const bool upper = (lane & (uint32_t)bit) != 0;
+#pragma unroll
+        for (int k = 0; k < half; ++k) {
+            const float send = upper ? v[k] : v[k + half];
+            const float keep = upper ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, bit);
+        }
+    }
+    float s = v[0];
+    s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
+    s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
+    float n = v[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
+    ninth = n;
+    return s;
+}
+
+// ---- the blends of a training step: forward, loss and adjoint, a tile at a time ----
+// One block of T*T/2 threads takes tiles off a queue and, for each, runs the
+// forward blend, the loss of its pixels, and the blend's adjoint, so that each
+// pixel's final transmittance, last contributor and loss gradient stay in
+// registers between the two walks.
+//
+// Forward: warp w owns an 8x8 box of the tile and each lane two pixels of it,
+// (x, y) and (x, y + 4). Staging a batch of records, the block marks for each
+// record the boxes its footprint can reach (a conservative test: the box's least
+// power against the cutoff, with a margin); a warp then walks only the records
+// marked for its box, found 32 at a time by a ballot, in list order. A pixel
+// blends exactly the records it would blend walking the whole list: the
+// per-pixel test decides, the box test only skips records no pixel of the box can
+// pass. So the image does not depend on the tile size.
+//
+// Adjoint: the same boxes and masks, walked in reverse, in batches aligned with
+// the forward's (the forward's last batch, still staged, is the adjoint's first
+// when it holds the tile's last contributor): a warp takes the records marked for
+// its box from its pixels' last contributor down. What a lane sums over its two
+// pixels, and the warp over its 64, are moments of dL/dpower over the pixel
+// offsets in the factored frame (t = dx + fr dy, dy): sum dP t, sum dP dy,
+// sum dP t^2, sum dP t dy, sum dP dy^2; the record's centre and conic gradients
+// follow from them once a record, when the block flushes a batch. The loss has
+// no alpha term, so dL/d(alpha out) is 0 and the colour behind a record enters
+// only through S.dC, one value a pixel.
 template <uint32_t T, uint32_t NB>
 __global__ void __launch_bounds__(T * T / 2, 2)
-    blendBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
-                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
-                     const float4* __restrict__ recs,
-                     float4* __restrict__ colour, float* __restrict__ finalT, uint32_t* __restrict__ lastContrib,
-                     const float* __restrict__ target, float4* __restrict__ dL, float* __restrict__ loss,
-                     uint32_t* __restrict__ words) {
+    blendStepKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
+                    const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
+                    const float4* __restrict__ recs, float4* __restrict__ colour, const float* __restrict__ target,
+                    float* __restrict__ loss, float* __restrict__ grads, uint32_t* __restrict__ words) {
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
+    constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
+    constexpr uint32_t kPer = (NB + kThreads - 1) / kThreads;   // records a thread stages a batch
     __shared__ float2 sCentre[NB];
     __shared__ float4 sConic[NB];    // ca, fr, fs pre-scaled; alpha
     __shared__ float4 sColour[NB];   // r g b; the cutoff pre-scaled
     __shared__ uint32_t sMask[NB];
+    __shared__ uint32_t sRec[NB];
+    __shared__ float sAcc[NB * kWords];
     __shared__ uint32_t sTileBase[kMaxBatchViews];
-    __shared__ uint32_t sTile;
+    __shared__ uint32_t sTile, sMaxLast;
     for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
     const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
     const float kScale = -0.5f * 1.4426950408889634f;   // power -> base-2 exponent
+    const float kUnscale = 1.0f / kScale;                // for the gradients only
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
-    uint32_t evaluated = 0;   // (pixel, record) evaluations this thread made
+    uint32_t evaluated = 0;   // (pixel, record) evaluations of the forward this thread made
     float lossSum = 0.0f;     // this thread's pixels' share of the loss
     while (true) {
         __syncthreads();
-        if (threadIdx.x == 0) sTile = atomicAdd(&words[kBatchBlendTicket], 1u);
+        if (threadIdx.x == 0) {
+            sTile = atomicAdd(&words[kBatchBlendTicket], 1u);
+            sMaxLast = 0;
+        }
         __syncthreads();
         const uint32_t tile = sTile;
         if (tile >= B.totalTiles) break;
@@ -118,25 +168,32 @@ __global__ void __launch_bounds__(T * T / 2, 2)
         const uint2 range = ranges[tile];
         const float pxc = (float)px + 0.5f, pyc[2] = {(float)py[0] + 0.5f, (float)py[1] + 0.5f};
         const size_t recBase = (size_t)v * B.count;
+        // record s of this view into slot k: the factored conic's two weights and the
+        // cutoff pre-scaled to base-2 exponent units, and the boxes it can reach
+        auto stage = [&](uint32_t k, uint32_t s) {
+            sRec[k] = s;
+            const size_t at = (recBase + s) * 3;
+            const float4 sc = recs[at + 0];
+            const float4 c = recs[at + 1];
+            const float4 rgb = recs[at + 2];
+            sCentre[k] = make_float2(sc.x, sc.y);
+            sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
+            sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
+            sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
+        };
+
+        // ---- forward
         float r[2] = {0.0f, 0.0f}, g[2] = {0.0f, 0.0f}, bl[2] = {0.0f, 0.0f}, Tr[2] = {1.0f, 1.0f};
         uint32_t last[2] = {0, 0};
         bool done[2];
 #pragma unroll
         for (int p = 0; p < 2; ++p) done[p] = !(px < V.width && py[p] < V.height);
+        uint32_t staged = 0xFFFFFFFFu;   // the first pair of the batch in shared memory
         for (uint32_t first = range.x; first < range.y; first += NB) {
             if (__syncthreads_count(done[0] && done[1]) == kThreads) break;
             const uint32_t count = min(NB, range.y - first);
-            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
-                const size_t s = (recBase + gaussianOf(pairs, values, slotMask, first + k)) * 3;
-                const float4 sc = recs[s + 0];
-                const float4 c = recs[s + 1];
-                const float4 rgb = recs[s + 2];
-                sCentre[k] = make_float2(sc.x, sc.y);
-                // the factored conic's two weights pre-scaled to base-2 exponent units
-                sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
-                sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
-                sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
-            }
+            for (uint32_t k = threadIdx.x; k < count; k += kThreads) stage(k, gaussianOf(pairs, values, slotMask, first + k));
+            staged = first;
             __syncthreads();
             if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) continue;
             for (uint32_t base = 0; base < count; base += 32) {
@@ -173,161 +230,57 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                 if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
             }
         }
+
+        // ---- the pixels' colour, the loss (the view's mean L2 over its pixels and r g b) and its gradient
+        float sd[2], dC[2][3];
 #pragma unroll
         for (int p = 0; p < 2; ++p) {
-            if (!(px < V.width && py[p] < V.height)) continue;
-            const uint32_t at = V.pixelBase + py[p] * V.width + px;
-            const float coverage = 1.0f - Tr[p];
-            const float4 c = make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1], bl[p] + Tr[p] * B.bg[2],
-                                         coverage + Tr[p] * B.bg[3]);
-            colour[at] = c;
-            finalT[at] = Tr[p];
-            lastContrib[at] = last[p];
-            // the loss: the view's mean L2 over its pixels and r g b, and its gradient
-            const float er = c.x - target[(size_t)at * 3 + 0], eg = c.y - target[(size_t)at * 3 + 1],
-                        eb = c.z - target[(size_t)at * 3 + 2];
-            lossSum += (er * er + eg * eg + eb * eb) * V.lossScale;
-            const float k2 = 2.0f * V.lossScale;
-            dL[at] = make_float4(k2 * er, k2 * eg, k2 * eb, 0.0f);
+            dC[p][0] = dC[p][1] = dC[p][2] = 0.0f;
+            if (px < V.width && py[p] < V.height) {
+                const uint32_t at = V.pixelBase + py[p] * V.width + px;
+                const float coverage = 1.0f - Tr[p];
+                const float4 c = make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1],
+                                             bl[p] + Tr[p] * B.bg[2], coverage + Tr[p] * B.bg[3]);
+                colour[at] = c;
+                const float er = c.x - target[(size_t)at * 3 + 0], eg = c.y - target[(size_t)at * 3 + 1],
+                            eb = c.z - target[(size_t)at * 3 + 2];
+                lossSum += (er * er + eg * eg + eb * eb) * V.lossScale;
+                const float k2 = 2.0f * V.lossScale;
+                dC[p][0] = k2 * er;
+                dC[p][1] = k2 * eg;
+                dC[p][2] = k2 * eb;
+            }
+            sd[p] = (B.bg[0] * dC[p][0] + B.bg[1] * dC[p][1]) + B.bg[2] * dC[p][2];   // S.dC, S the colour behind
         }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lossSum += __shfl_xor_sync(0xFFFFFFFFu, lossSum, o);
-    if (lane == 0 && lossSum != 0.0f) atomicAdd(loss, lossSum);
-    uint64_t e = evaluated;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
-    if (lane == 0 && e)
-        atomicAdd(reinterpret_cast<unsigned long long*>(words + kBatchEvaluated), (unsigned long long)e);
-}
 
-// Nine values summed over a warp: the first eight by a transposed reduction
-// (each level sends half of the values still held and keeps the other half,
-// so three levels leave value (lane >> 2) spread over lanes differing in their
-// two low bits), the ninth by a butterfly. Lanes with lane % 4 == 0 hold value
-// lane >> 2; every lane holds the ninth.
-__device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
-    const uint32_t lane = threadIdx.x & 31u;
-#pragma unroll
-    for (int half = 4, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
-        const bool upper = (lane & (uint32_t)bit) != 0;
-#pragma unroll
-        for (int k = 0; k < half; ++k) {
-            const float send = upper ? v[k] : v[k + half];
-            const float keep = upper ? v[k + half] : v[k];
-            v[k] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, bit);
-        }
-    }
-    float s = v[0];
-    s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
-    s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
-    float n = v[8];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
-    ninth = n;
-    return s;
-}
-
-// ---- the blend's adjoint, over the same tile queue ------------------------------
-// The forward's warp boxes and masks, walked in reverse: a warp takes the records
-// marked for its box from its pixels' last contributor down. What a lane sums
-// over its two pixels, and the warp over its 64, are moments of dL/dpower over
-// the pixel offsets in the factored frame (t = dx + fr dy, dy): sum dP t,
-// sum dP dy, sum dP t^2, sum dP t dy, sum dP dy^2; the record's centre and conic
-// gradients follow from them once a record, when the block flushes. The batched
-// loss has no alpha term, so dL/d(alpha out) is 0 and the colour behind a
-// record enters only through S.dC, one value a pixel.
-template <uint32_t T, uint32_t NB>
-__global__ void __launch_bounds__(T * T / 2)
-    blendAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
-                            const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
-                            const float4* __restrict__ recs,
-                            const float* __restrict__ finalT, const uint32_t* __restrict__ lastContrib,
-                            const float4* __restrict__ dLdColour, float* __restrict__ grads,
-                            uint32_t* __restrict__ words) {
-    constexpr uint32_t kThreads = T * T / 2;
-    constexpr uint32_t kAcross = T / kBox;
-    constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
-    constexpr uint32_t kPer = (NB + kThreads - 1) / kThreads;   // records a thread stages a batch
-    __shared__ float2 sCentre[NB];
-    __shared__ float4 sConic[NB];
-    __shared__ float4 sColour[NB];
-    __shared__ uint32_t sRec[NB];
-    __shared__ uint32_t sMask[NB];
-    __shared__ float sAcc[NB * kWords];
-    __shared__ uint32_t sTileBase[kMaxBatchViews];
-    __shared__ uint32_t sTile, sMaxLast;
-    for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
-    const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
-    const float kScale = -0.5f * 1.4426950408889634f;
-    const float kUnscale = 1.0f / kScale;   // for the gradients only
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
-    while (true) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            sTile = atomicAdd(&words[kBatchBackTicket], 1u);
-            sMaxLast = 0;
-        }
-        __syncthreads();
-        const uint32_t tile = sTile;
-        if (tile >= B.totalTiles) break;
-        const uint32_t v = viewOf(sTileBase, B.views, tile);
-        const BatchView& V = views[v];
-        const uint32_t local = tile - V.tileBase;
-        const uint32_t tx = local % V.tilesX, ty = local / V.tilesX;
-        const float tileX0 = (float)(tx * T), tileY0 = (float)(ty * T);
-        const uint32_t px = tx * T + lx, py[2] = {ty * T + ly, ty * T + ly + 4};
-        const uint2 range = ranges[tile];
-        const float pxc = (float)px + 0.5f, pyc[2] = {(float)py[0] + 0.5f, (float)py[1] + 0.5f};
-        float Tr[2], sd[2], dC[2][3];
-        uint32_t last[2];
-#pragma unroll
-        for (int p = 0; p < 2; ++p) {
-            const bool inside = px < V.width && py[p] < V.height;
-            const uint32_t at = inside ? V.pixelBase + py[p] * V.width + px : 0u;
-            Tr[p] = inside ? finalT[at] : 1.0f;
-            last[p] = inside ? min(lastContrib[at], range.y - range.x) : 0u;
-            const float4 d = inside ? dLdColour[at] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            dC[p][0] = d.x; dC[p][1] = d.y; dC[p][2] = d.z;
-            sd[p] = (B.bg[0] * d.x + B.bg[1] * d.y) + B.bg[2] * d.z;   // S.dC, S the colour behind
-        }
+        // ---- adjoint
         const uint32_t warpLast = __reduce_max_sync(0xFFFFFFFFu, max(last[0], last[1]));
         if (lane == 0 && warpLast) atomicMax(&sMaxLast, warpLast);
         __syncthreads();
         const uint32_t end = range.x + sMaxLast;
-        const size_t recBase = (size_t)v * B.count;
-        uint32_t ahead[kPer];   // the batch's Gaussian indices, loaded a batch ahead
-        {
-            const uint32_t start = end - range.x > NB ? end - NB : range.x;
-            prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, start, end, ahead);
-        }
-        for (uint32_t batchEnd = end; batchEnd > range.x;) {
-            const uint32_t batchStart = batchEnd - range.x > NB ? batchEnd - NB : range.x;
+        if (end == range.x) continue;
+        uint32_t batchStart = range.x + ((end - 1u - range.x) / NB) * NB, batchEnd = end;
+        bool stagedAlready = batchStart == staged;   // the forward's last batch holds the last contributor
+        uint32_t ahead[kPer];   // the next batch's Gaussian indices, loaded a batch ahead
+        if (!stagedAlready) prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, batchStart, batchEnd, ahead);
+        while (true) {
             const uint32_t count = batchEnd - batchStart;
-            uint32_t gauss[kPer];
+            if (!stagedAlready) {
+                uint32_t gauss[kPer];
 #pragma unroll
-            for (uint32_t q = 0; q < kPer; ++q) gauss[q] = ahead[q];
-            if (batchStart > range.x) {
-                const uint32_t prevStart = batchStart - range.x > NB ? batchStart - NB : range.x;
-                prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, prevStart, batchStart, ahead);
-            }
+                for (uint32_t q = 0; q < kPer; ++q) gauss[q] = ahead[q];
+                if (batchStart > range.x)
+                    prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, batchStart - NB, batchStart, ahead);
 #pragma unroll
-            for (uint32_t q = 0; q < kPer; ++q) {
-                const uint32_t k = threadIdx.x + q * kThreads;
-                if (k >= count) break;
-                const uint32_t s = gauss[q];
-                sRec[k] = s;
-                const size_t at = (recBase + s) * 3;
-                const float4 sc = recs[at + 0];
-                const float4 c = recs[at + 1];
-                const float4 rgb = recs[at + 2];
-                sCentre[k] = make_float2(sc.x, sc.y);
-                // the forward's pre-scale, operation for operation (so the same records pass)
-                sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
-                sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
-                sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
+                for (uint32_t q = 0; q < kPer; ++q) {
+                    const uint32_t k = threadIdx.x + q * kThreads;
+                    if (k >= count) break;
+                    stage(k, gauss[q]);
+                }
+            } else if (batchStart > range.x) {
+                prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, batchStart - NB, batchStart, ahead);
             }
+            stagedAlready = false;
             for (uint32_t k = threadIdx.x; k < count * kWords; k += kThreads) sAcc[k] = 0.0f;
             __syncthreads();
             const uint32_t relStart = batchStart - range.x;
@@ -419,9 +372,19 @@ __global__ void __launch_bounds__(T * T / 2)
                     if (out[q] != 0.0f) atomicAdd(dst + q, out[q]);
             }
             __syncthreads();   // the next batch's loads overwrite what the flush reads
+            if (batchStart == range.x) break;
             batchEnd = batchStart;
+            batchStart -= NB;
         }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lossSum += __shfl_xor_sync(0xFFFFFFFFu, lossSum, o);
+    if (lane == 0 && lossSum != 0.0f) atomicAdd(loss, lossSum);
+    uint64_t e = evaluated;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
+    if (lane == 0 && e)
+        atomicAdd(reinterpret_cast<unsigned long long*>(words + kBatchEvaluated), (unsigned long long)e);
 }
 
 template <typename K>
@@ -432,20 +395,11 @@ int residentGrid(K kernel, int threads, int sms) {
 }
 
 template <uint32_t T, uint32_t NB>
-cudaError_t blendWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
-                      const float* target, float4* dL, float* loss) {
-    const int grid = residentGrid(blendBatchKernel<T, NB>, T * T / 2, L.sms);
-    blendBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs, colour,
-                                                                L.finalT, L.lastContrib, target, dL, loss, L.words);
-    return cudaGetLastError();
-}
-
-template <uint32_t T, uint32_t NB>
-cudaError_t adjointWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, const float4* dL,
-                        float* grads) {
-    const int grid = residentGrid(blendAdjointBatchKernel<T, NB>, T * T / 2, L.sms);
-    blendAdjointBatchKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs,
-                                                                       L.finalT, L.lastContrib, dL, grads, L.words);
+cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
+                     const float* target, float* loss, float* grads) {
+    const int grid = residentGrid(blendStepKernel<T, NB>, T * T / 2, L.sms);
+    blendStepKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs, colour,
+                                                               target, loss, grads, L.words);
     return cudaGetLastError();
 }
 
@@ -455,19 +409,10 @@ cudaError_t adjointWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t 
     CALL(8, 64) CALL(8, 128) CALL(8, 256) CALL(8, 512) CALL(16, 64) CALL(16, 128) CALL(16, 256) CALL(16, 512)     \
     CALL(32, 64) CALL(32, 128) CALL(32, 256) CALL(32, 512)
 
-cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
-                             const float* target, float4* dL, float* loss) {
+cudaError_t launchBatchBlendStep(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
+                                 const float* target, float* loss, float* grads) {
 #define ATH_CASE(T_, NB_) \
-    if (L.tile == T_ && L.blockBatch == NB_) return blendWith<T_, NB_>(B, L, stream, colour, target, dL, loss);
-    ATH_BLEND_CASES(ATH_CASE)
-#undef ATH_CASE
-    return cudaErrorInvalidValue;
-}
-
-cudaError_t launchBatchBlendAdjoint(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream,
-                                    const float4* dLdColour, float* grads) {
-#define ATH_CASE(T_, NB_) \
-    if (L.tile == T_ && L.blockBatch == NB_) return adjointWith<T_, NB_>(B, L, stream, dLdColour, grads);
+    if (L.tile == T_ && L.blockBatch == NB_) return stepWith<T_, NB_>(B, L, stream, colour, target, loss, grads);
     ATH_BLEND_CASES(ATH_CASE)
 #undef ATH_CASE
     return cudaErrorInvalidValue;

@@ -48,7 +48,7 @@ enum BatchWord : uint32_t {
     kBatchPairsLo = 3,
     kBatchPairsHi = 4,
     kBatchBlendTicket = 5,   // the persistent blend's tile queue
-    kBatchBackTicket = 6,    // the persistent backward's tile queue
+    kBatchBackTicket = 6,    // (unused)
     kBatchKept = 7,          // (view, Gaussian) records kept
     kBatchSortTickets = 8,   // one a sort pass (8)
     kBatchEvaluated = 16,    // 64-bit (16, 17): (pixel, record) evaluations of the forward blend
@@ -113,7 +113,7 @@ __device__ __forceinline__ uint32_t viewOf(const uint32_t* bases, uint32_t views
     return lo;
 }
 
-// What the persistent blends of batch_blend.cu need from a batch.
+// What the persistent blend of batch_blend.cu needs from a batch.
 struct BlendLaunch {
     const BatchView* views;
     const uint2* ranges;
@@ -121,20 +121,16 @@ struct BlendLaunch {
     const uint32_t* values;  // wide pairs: the Gaussian of each sorted pair; null when packed
     const float4* recs;
     uint32_t* words;
-    float* finalT;
-    uint32_t* lastContrib;
     int sms;
     uint32_t tile, blockBatch;
 };
 
-// The forward blend of every view's tiles (colour, final T, last contributor)
-// with the loss in its epilogue: each view's mean L2 against `target` (float3 a
+// A training step's blends over every view's tiles, in one kernel: the forward
+// blend into `colour`; the loss, each view's mean L2 against `target` (float3 a
 // pixel) over its pixels and r g b, summed over views into *loss (which the
-// caller zeroes), and dL/dcolour into `dL`.
-cudaError_t launchBatchBlend(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
-                             const float* target, float4* dL, float* loss);
-// Its adjoint: dL/d(record) for every (view, Gaussian) record, added into `grads`.
-cudaError_t launchBatchBlendAdjoint(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream,
-                                    const float4* dLdColour, float* grads);
+// caller zeroes); and the adjoint, dL/d(record) for every (view, Gaussian)
+// record, added into `grads` (which start at zero).
+cudaError_t launchBatchBlendStep(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
+                                 const float* target, float* loss, float* grads);
 
 }   // namespace ath

@@ -583,12 +583,12 @@ class BatchTrainer:
                     stream: torch.cuda.Stream | None = None) -> dict:
         """ath_batch_time_stages: one step, not captured, with events between its stages (ms)."""
         g = N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
-        ms = (C.c_float * 7)()
+        ms = (C.c_float * 5)()
         s = stream if stream is not None else torch.cuda.current_stream(colour.device)
         self._keep = (params, target, colour, loss, grads)
         check(N.lib().ath_batch_time_stages(self._h, C.byref(params._native()), _ptr(target), _ptr(colour),
                                             _ptr(loss), C.byref(g), ms, C.c_void_p(s.cuda_stream)))
-        names = ("project_emit", "sort", "ranges", "blend_and_loss", "clear_grads", "blend_adjoint", "project_adjoint")
+        names = ("project_emit", "sort", "ranges", "blends", "project_adjoint")
         return {n: float(v) for n, v in zip(names, ms)}
 
     def buffers(self) -> dict:

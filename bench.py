@@ -325,8 +325,8 @@ def run_ours(args) -> dict | None:
     total_tiles = sum(((W + T - 1) // T) * ((H + T - 1) // T) for _, W, H in views)
     passes = math.ceil((24 + max(1, math.ceil(math.log2(max(2, total_tiles))))) / 8)
     # the step's kernels: begin, projectEmit, histogram, the sort's passes, ranges,
-    # blend (with the loss), blend adjoint, projection adjoint (memsets are not counted)
-    launches = (2 + 1 + passes + 1 + 1 + 1 + 1) * args.steps
+    # the blends (forward, loss and adjoint), projection adjoint (memsets are not counted)
+    launches = (2 + 1 + passes + 1 + 1 + 1) * args.steps
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
                stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
                count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4,
@@ -432,17 +432,13 @@ def main():
         "project_emit": ("hbm", res["count"] * mixed_bytes + stats["kept"] * 48 + stats["pairs"] * 8),
         "sort": ("hbm", stats["pairs"] * (8 + 16 * res["passes"])),
         "ranges": ("hbm", stats["pairs"] * 8 + stats["pairs"] // 16 * 8),
-        "blend_and_loss": ("fp32", stats["evaluated"] * 20),
-        "clear_grads": ("hbm", V * res["count"] * 40),
-        "blend_adjoint": ("fp32", stats["evaluated"] * 60),
+        "blends": ("fp32", stats["evaluated"] * (20 + 60)),   # forward + adjoint an evaluation
         "project_adjoint": ("hbm", res["count"] * (mixed_bytes + 60 * 4) + stats["kept"] * 40),
     }
     bound, amount = work[dominant]
     secs = stages[dominant] * 1e-3
     kernel_names = {"project_emit": "projectEmitKernel", "sort": "onesweepKernel", "ranges": "rangesBatchKernel",
-                    "blend_and_loss": "blendBatchKernel", "clear_grads": "cudaMemsetAsync",
-                    "blend_adjoint": "blendAdjointBatchKernel",
-                    "project_adjoint": "projectAdjointBatchKernel"}
+                    "blends": "blendStepKernel", "project_adjoint": "projectAdjointBatchKernel"}
     if bound == "hbm":
         achieved = amount / secs / 1e9
         roofline = {"bound": "hbm", "achieved": achieved, "peak": P["hbm_gbs"], "unit": "GB/s",

@@ -338,11 +338,11 @@ ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* params, const fl
                           float* loss, ath_param_grads* grads, uint32_t repeats, ath_batch_stats* best, void* stream);
 
 /* One step as ath_batch_train_step runs it, not captured, with events between
- * its stages, waited for: ms[] = project+emit, sort, ranges, blend (with the
- * loss), clearing the record gradients, blend adjoint, projection adjoint. For
- * measurement. */
+ * its stages, waited for: ms[] = project+emit (with the record gradients'
+ * clearing), sort, ranges, blends (the forward blend, the loss and the blend
+ * adjoint, one kernel), projection adjoint. For measurement. */
 ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
-                                 float* loss, ath_param_grads* grads, float ms[7], void* stream);
+                                 float* loss, ath_param_grads* grads, float ms[5], void* stream);
 
 /* The last step's sorted pairs and tile ranges, for inspection: device
  * pointers the batch owns, valid until its next step. A packed pair is
