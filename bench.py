@@ -41,10 +41,9 @@ METRIC = "fwd+bwd ms/view, 1.5M Gaussians 1080p, batched+BF16 vs plain FP32, err
 # DRAM bytes a launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # batched kernels, from an ncu capture of this workload (profiles/).
 NCU_TRAFFIC: dict = {
-    # profiles/batched_kernels_1.5M_2x1080p_tile32.md: 158.9 MB on 2 views, scaled to 8
-    "blendAdjointBatchKernel": 4 * 158.95e6,
-    "blendBatchKernel": 4 * 212.91e6,
-    "projectEmitKernel": 4 * 459.14e6,
+    # profiles/batched_kernels_1.5M_2x1080p_tile32.md: DRAM bytes a launch on 2 views, scaled to 8
+    "blendStepKernel": 4 * 160.96e6,
+    "projectEmitKernel": 4 * 458.61e6,
 }
 
 
