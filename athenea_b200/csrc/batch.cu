@@ -614,10 +614,14 @@ struct ath_batch {
     uint32_t count = 0;
     uint64_t capacity = 0;
     bool resize = true;
-    // the captured step
+    // the captured steps: a few, keyed by the arrays a step reads and writes, so that a
+    // caller alternating input or output buffers (double-buffered targets) replays
+    // without capturing again
+    static constexpr int kGraphs = 4;
     cudaStream_t captureStream = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    uintptr_t graphKey[12] = {};
+    cudaGraphExec_t exec[kGraphs] = {};
+    uintptr_t graphKey[kGraphs][12] = {};
+    int nextGraph = 0;   // the slot the next capture replaces
 };
 
 namespace {
@@ -629,8 +633,11 @@ uint32_t bitsForValues(uint64_t values) {   // FrameParams.h:18-24
 }
 
 void dropGraph(ath_batch* b) {
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    b->exec = nullptr;
+    for (int k = 0; k < ath_batch::kGraphs; ++k) {
+        if (b->exec[k]) cudaGraphExecDestroy(b->exec[k]);
+        b->exec[k] = nullptr;
+    }
+    b->nextGraph = 0;
 }
 
 ath_status buildViews(ath_batch* b) {
@@ -990,8 +997,14 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
     const uintptr_t key[12] = {(uintptr_t)P.means, (uintptr_t)P.scales, (uintptr_t)P.quats, (uintptr_t)P.sh_low,
                                (uintptr_t)P.sh_high, (uintptr_t)P.sh_scale, (uintptr_t)target, (uintptr_t)colour,
                                (uintptr_t)loss, (uintptr_t)grads->means, (uintptr_t)grads->sh, (uintptr_t)P.count};
-    if (!b->exec || std::memcmp(key, b->graphKey, sizeof(key)) != 0) {
-        dropGraph(b);
+    int slot = -1;
+    for (int k = 0; k < ath_batch::kGraphs && slot < 0; ++k)
+        if (b->exec[k] && std::memcmp(key, b->graphKey[k], sizeof(key)) == 0) slot = k;
+    if (slot < 0) {
+        slot = b->nextGraph;
+        b->nextGraph = (b->nextGraph + 1) % ath_batch::kGraphs;
+        if (b->exec[slot]) cudaGraphExecDestroy(b->exec[slot]);
+        b->exec[slot] = nullptr;
         // Capture on the batch's own stream (the caller's may be the legacy one),
         // ordered after the caller's work so far.
         cudaEvent_t ready;
@@ -1009,15 +1022,15 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
             err = cudaStreamEndCapture(b->captureStream, &graph);
             if (enq != cudaSuccess) err = enq;
         }
-        if (err == cudaSuccess) err = cudaGraphInstantiate(&b->exec, graph, 0);
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&b->exec[slot], graph, 0);
         if (graph) cudaGraphDestroy(graph);
         if (err != cudaSuccess) {
-            b->exec = nullptr;
+            b->exec[slot] = nullptr;
             return failCuda(err, "capturing the batched step");
         }
-        std::memcpy(b->graphKey, key, sizeof(key));
+        std::memcpy(b->graphKey[slot], key, sizeof(key));
     }
-    err = cudaGraphLaunch(b->exec, stream);
+    err = cudaGraphLaunch(b->exec[slot], stream);
     if (err != cudaSuccess) return failCuda(err, "launching the batched step");
     return ATH_OK;
 }

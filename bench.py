@@ -256,23 +256,34 @@ def run_ours(args) -> dict | None:
     stats = bt.check()
 
     # e2e through the public API: each step's target images copied in from pinned
-    # host memory (into one of two staging buffers on a copy stream, overlapping
-    # the step before) and moved to the step's target on the compute stream; the
-    # loss read back to pinned host memory.
+    # host memory into one of two device buffers on a copy stream (overlapping the
+    # step before), the step reading that buffer directly (the library keeps one
+    # captured step for each); the loss read back to pinned host memory.
     copy = torch.cuda.Stream(dev)
     staging = [torch.empty_like(target), torch.empty_like(target)]
     h2d_done = [torch.cuda.Event(), torch.cuda.Event()]
-    moved = [torch.cuda.Event(), torch.cuda.Event()]
+    used = [torch.cuda.Event(), torch.cuda.Event()]
     loss_host = torch.empty(1, dtype=torch.float32, pin_memory=True)
 
     def upload(k):
-        copy.wait_event(moved[k % 2])
+        copy.wait_event(used[k % 2])
         with torch.cuda.stream(copy):
             staging[k % 2].copy_(host_target, non_blocking=True)
             h2d_done[k % 2].record(copy)
 
-    for e in moved:
+    def e2e_step(k):
+        stream.wait_event(h2d_done[k % 2])
+        bt.step(mixed, staging[k % 2], colour, loss, grads, stream=stream)
+        exchange.allreduce()
+        used[k % 2].record(stream)
+        loss_host.copy_(loss, non_blocking=True)
+
+    for e in used:
         e.record(stream)
+    # one untimed step on each buffer first: its graph is captured then
+    for k in range(2):
+        upload(k)
+        e2e_step(k)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -284,11 +295,7 @@ def run_ours(args) -> dict | None:
     for k in range(args.steps):
         if k + 1 < args.steps:
             upload(k + 1)
-        stream.wait_event(h2d_done[k % 2])
-        target.copy_(staging[k % 2], non_blocking=True)
-        moved[k % 2].record(stream)
-        batched_step()
-        loss_host.copy_(loss, non_blocking=True)
+        e2e_step(k)
     e2e_end.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e2e_start.elapsed_time(e2e_end) / args.steps

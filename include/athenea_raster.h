@@ -325,7 +325,10 @@ ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode);
  * (FP32, ath_param_grads' layout, sh 48 floats a Gaussian). colour: float4 a
  * pixel, target: float3 a pixel, both concatenated. The first call sizes the
  * pair buffers (one host read) and captures the step into a CUDA graph; later
- * calls with the same pointers replay it. */
+ * calls with the same pointers replay it. Up to four captured steps are kept,
+ * keyed by the arrays they read and write, so a caller that alternates two
+ * target (or colour) buffers, to upload one while the other is in use, replays
+ * both after their first call. */
 ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
                                 float* loss, ath_param_grads* grads, void* stream);
 /* Waits for `stream` and reports the last step; ATH_E_CAPACITY when its pairs

@@ -257,3 +257,32 @@ def test_dense_tiles_at_tile_32_are_sorted_and_ranged():
         got[mode] = (tiles, depths, splats)
     for k in range(3):
         np.testing.assert_array_equal(got[1][k], got[2][k])
+
+
+def test_alternating_target_buffers_replay_their_own_steps():
+    """Two target buffers used in turn (an upload into one while the other is in use):
+    each call replays the step captured for its buffer, and reads that buffer."""
+    _, M = _scene(30_000, 17)
+    views = _views()
+    gen = torch.Generator().manual_seed(9)
+    first = torch.cat([torch.rand((W * H, 3), generator=gen) for _, W, H in views]).cuda()
+    second = torch.cat([torch.rand((W * H, 3), generator=gen) for _, W, H in views]).cuda()
+    b = BatchTrainer()
+    b.set_views(views)
+    b.set_tuning(16, 256)
+    colour = torch.empty((b.pixels, 4), device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    grads = A.Params(torch.zeros_like(M.means), torch.zeros_like(M.scales), torch.zeros_like(M.quats),
+                     torch.zeros((M.count, 48), device="cuda"), 3)
+    seen = []
+    for target in (first, second, first, second):
+        b.step(M, target, colour, loss, grads)
+        torch.cuda.synchronize()
+        seen.append((loss.item(), colour.cpu().numpy().copy(), grads.means.cpu().numpy().copy()))
+    b.check()
+    assert seen[0][0] != seen[1][0]
+    for k in (0, 1):
+        assert abs(seen[k][0] - seen[k + 2][0]) <= 1e-6 * abs(seen[k][0])
+        np.testing.assert_array_equal(seen[k][1], seen[k + 2][1])
+        g, h = seen[k][2], seen[k + 2][2]
+        assert np.abs(g - h).max() <= 1e-5 * np.abs(g).max()
