@@ -282,7 +282,8 @@ def test_alternating_target_buffers_replay_their_own_steps():
     b.check()
     assert seen[0][0] != seen[1][0]
     for k in (0, 1):
-        assert abs(seen[k][0] - seen[k + 2][0]) <= 1e-6 * abs(seen[k][0])
+        # the loss is a sum by float atomics, in no fixed order
+        assert abs(seen[k][0] - seen[k + 2][0]) <= 1e-5 * abs(seen[k][0])
         np.testing.assert_array_equal(seen[k][1], seen[k + 2][1])
         g, h = seen[k][2], seen[k + 2][2]
         assert np.abs(g - h).max() <= 1e-5 * np.abs(g).max()
