@@ -59,7 +59,6 @@ __global__ void beginStepKernel(uint32_t* words) {
     words[kBatchPairsLo] = 0;
     words[kBatchPairsHi] = 0;
     words[kBatchBlendTicket] = 0;
-    words[kBatchBackTicket] = 0;
     words[kBatchKept] = 0;
     for (int p = 0; p < 8; ++p) words[kBatchSortTickets + p] = 0;
     words[kBatchEvaluated] = words[kBatchEvaluated + 1] = 0;

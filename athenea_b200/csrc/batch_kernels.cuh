@@ -48,7 +48,6 @@ enum BatchWord : uint32_t {
     kBatchPairsLo = 3,
     kBatchPairsHi = 4,
     kBatchBlendTicket = 5,   // the persistent blend's tile queue
-    kBatchBackTicket = 6,    // (unused)
     kBatchKept = 7,          // (view, Gaussian) records kept
     kBatchSortTickets = 8,   // one a sort pass (8)
     kBatchEvaluated = 16,    // 64-bit (16, 17): (pixel, record) evaluations of the forward blend
