@@ -1,10 +1,10 @@
 // The radix sort without allocation: ath_sort_pairs_static.
 //
 // Some callers cannot allocate device memory when they sort. A render
-// delegate or an OpenFX node runs inside a host application's frame loop and
-// is often held to a device-memory budget that it must not grow mid-frame; a
-// caller that records its work into a CUDA graph it captures itself cannot
-// have cudaMalloc called on the capturing stream. ath_sorter_sort allocates
+// delegate or an OpenFX node runs inside a host application's frame loop: the
+// host owns the device memory and holds the plugin to a budget it must not
+// grow mid-frame, and a real-time frame cannot afford the stall of an
+// allocation (cudaMalloc synchronises the device). ath_sorter_sort allocates
 // its look-back words on first use and whenever a larger sort needs more;
 // this entry point instead keeps the sort's working memory (digit histograms,
 // look-back words, tile tickets, a status word) in one fixed array that lives

@@ -414,8 +414,9 @@ ath_status ath_sorter_sort(ath_sorter* s, uint64_t* keys, uint32_t* values, uint
                            uint32_t* scratch_values, uint32_t count, uint32_t key_bits, void* stream);
 
 /* The same sort for callers that cannot allocate device memory while they
- * sort: a plugin held to its host application's memory budget mid-frame, or a
- * caller capturing its own work into a CUDA graph. It has no counterpart in
+ * sort: a plugin whose host application owns the device memory and holds it to
+ * a fixed budget mid-frame, or a real-time frame that cannot take the stall of
+ * an allocation. It has no counterpart in
  * the reference. The sort's own working memory (histograms, look-back words,
  * tickets) is a fixed 4 MiB array every GPU that loads the library holds until
  * exit; nothing is allocated. At most 1,048,576 pairs a call (larger counts

@@ -1,6 +1,6 @@
 """ath_sort_pairs_static: the radix sort for callers that cannot allocate device
-memory while they sort (a plugin held to its host's memory budget mid-frame, a
-caller capturing its own CUDA graph). Its working memory is a fixed array in
+memory while they sort (a plugin whose host application owns the device memory
+and holds it to a fixed budget mid-frame). Its working memory is a fixed array in
 the library, so the test checks that its results equal the allocating
 ath_sorter_sort's on two calls in a row (the second must not see the first's
 leftovers), that it rejects counts past its limit, and that a call takes no
