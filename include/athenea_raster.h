@@ -416,10 +416,9 @@ ath_status ath_sorter_sort(ath_sorter* s, uint64_t* keys, uint32_t* values, uint
 /* The same sort for callers that cannot allocate device memory while they
  * sort: a plugin whose host application owns the device memory and holds it to
  * a fixed budget mid-frame, or a real-time frame that cannot take the stall of
- * an allocation. It has no counterpart in
- * the reference. The sort's own working memory (histograms, look-back words,
- * tickets) is a fixed 4 MiB array every GPU that loads the library holds until
- * exit; nothing is allocated. At most 1,048,576 pairs a call (larger counts
+ * an allocation. It has no counterpart in the reference. The sort's own working
+ * memory (histograms, look-back words, tickets) is a fixed 4 MiB array every GPU
+ * that loads the library holds until exit; nothing is allocated. At most 1,048,576 pairs a call (larger counts
  * return ATH_E_INVALID_ARGUMENT). The first call on a device finds that array's
  * address and sets the kernel up: make it before any stream capture. Every call
  * shares the array, so calls that overlap on the GPU race; keys/values and the
