@@ -6,18 +6,20 @@
 //   projectEmit   one block = 256 Gaussians x one view (blocks of the same
 //                 Gaussians for every view run back to back, so the cloud is
 //                 read from DRAM once and from L2 after): the exact projection
-//                 geometry, the tiles touched (each division of the tile test
-//                 done once a rect row and once a tile), the scan over every
-//                 view's pairs by an epoch-tagged look-back, and the pairs,
-//                 written from a tile mask kept in registers.
+//                 geometry and the record, then the tiles touched, tested by a
+//                 warp over its 32 footprints' candidate tiles as one list, the
+//                 scan over every view's pairs by an epoch-tagged look-back, and
+//                 the pairs; it also clears the records' gradient words.
 //   sort          one onesweep sort of every view's pairs, packed into one
 //                 64-bit word (global tile | 24-bit depth key | Gaussian), on
 //                 the tile and depth bits only: stability keeps each tile's
 //                 ties in Gaussian order, the reference's (frame.slang:17-20).
-//   blend         a persistent kernel over every view's tiles (a tile queue),
-//                 tile size 8, 16 or 32 and a record batch of 64, 128, 256 or 512.
-//   loss          mean L2 a view against its target, summed over views.
-//   blendAdjoint  the same queue, reverse order, as backward.cu.
+//   ranges        each tile's [start, end) in the sorted pairs.
+//   blends        one persistent kernel over every view's tiles (a tile queue;
+//                 tile size 8, 16 or 32 and a record batch of 64, 128, 256 or
+//                 512): for each tile the forward blend, the loss of its pixels
+//                 (each view's mean L2 against its target, summed over views)
+//                 and the blend's adjoint (batch_blend.cu).
 //   projectAdjoint one thread a Gaussian over every view, its gradient kept in
 //                 registers and written once.
 //
