@@ -750,6 +750,7 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
 }
 
 // One step, enqueued (captured or not). `countOnly`: the projection alone, to size the pairs.
+// A null `target`: a render, the forward blend alone (no loss, no backward).
 cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* target, float4* colour, float* loss,
                         ath_param_grads& g, cudaStream_t stream, bool countOnly, cudaEvent_t* marks = nullptr) {
     auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], stream); };
@@ -790,12 +791,13 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
         err = cudaGetLastError();
     }
     mark(3);
-    if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
+    const bool train = target != nullptr;
+    if (err == cudaSuccess && train) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
     // the forward blend, the loss and the blend adjoint (the record gradients were cleared by the projection)
     if (err == cudaSuccess)
         err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr));
     mark(4);
-    if (err == cudaSuccess && P.count) {
+    if (err == cudaSuccess && train && P.count) {
         projectAdjointBatchKernel<<<(P.count + 127) / 128, 128, 0, stream>>>(
             B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
             reinterpret_cast<float4*>(g.means), reinterpret_cast<float4*>(g.scales), reinterpret_cast<float4*>(g.quats),
@@ -960,26 +962,27 @@ extern "C" ath_status ath_batch_pixels(ath_batch* b, uint32_t* pixels) {
     return ATH_OK;
 }
 
-extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target,
-                                           float* colour, float* loss, ath_param_grads* grads, void* streamPtr) {
-    if (!b || !params || !target || !colour || !loss || !grads || !grads->means || !grads->scales || !grads->quats ||
-        !grads->sh)
-        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: null argument");
-    if (b->views.empty()) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: no views (ath_batch_set_views)");
+namespace {
+
+// A training step (target, loss and gradients given) or a render (all three
+// null), checked, its buffers sized, captured once for its arrays and replayed.
+ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour, float* loss,
+                   ath_param_grads* grads, void* streamPtr, const char* what) {
+    if (b->views.empty()) return fail(ATH_E_INVALID_ARGUMENT, std::string(what) + ": no views (ath_batch_set_views)");
     const ath_mixed_params& P = *params;
     if (P.count && (!P.means || !P.scales || !P.quats || !P.sh_low || !P.sh_high || !P.sh_scale))
-        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: a cloud needs every array of the mixed layout");
-    if (P.sh_degree > 3) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: sh_degree must be 0..3");
+        return fail(ATH_E_INVALID_ARGUMENT, std::string(what) + ": a cloud needs every array of the mixed layout");
+    if (P.sh_degree > 3) return fail(ATH_E_INVALID_ARGUMENT, std::string(what) + ": sh_degree must be 0..3");
     if ((reinterpret_cast<uintptr_t>(P.sh_low) & 7u) || (reinterpret_cast<uintptr_t>(P.sh_high) & 3u) ||
         (reinterpret_cast<uintptr_t>(P.means) & 15u) || (reinterpret_cast<uintptr_t>(P.scales) & 15u) ||
         (reinterpret_cast<uintptr_t>(P.quats) & 15u))
-        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: a cloud array is not aligned to its element");
+        return fail(ATH_E_INVALID_ARGUMENT, std::string(what) + ": a cloud array is not aligned to its element");
     const uint32_t slotBits = bitsForValues(std::max<uint64_t>(P.count, 2));
     if (b->keyMode == 1 && 24 + slotBits + b->tileBits > 64)
-        return fail(ATH_E_UNSUPPORTED, "ath_batch_train_step: tiles, depth key and Gaussian index exceed 64 bits "
+        return fail(ATH_E_UNSUPPORTED, std::string(what) + ": tiles, depth key and Gaussian index exceed 64 bits "
                                        "(packed keys asked for; the wide form has no such limit)");
     if (24 + b->tileBits > 64)
-        return fail(ATH_E_UNSUPPORTED, "ath_batch_train_step: more than 2^40 tiles");
+        return fail(ATH_E_UNSUPPORTED, std::string(what) + ": more than 2^40 tiles");
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
     ath_status st = ATH_OK;
     if (P.count != b->count) {
@@ -997,7 +1000,8 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
     }
     const uintptr_t key[12] = {(uintptr_t)P.means, (uintptr_t)P.scales, (uintptr_t)P.quats, (uintptr_t)P.sh_low,
                                (uintptr_t)P.sh_high, (uintptr_t)P.sh_scale, (uintptr_t)target, (uintptr_t)colour,
-                               (uintptr_t)loss, (uintptr_t)grads->means, (uintptr_t)grads->sh, (uintptr_t)P.count};
+                               (uintptr_t)loss, (uintptr_t)(grads ? grads->means : nullptr),
+                               (uintptr_t)(grads ? grads->sh : nullptr), (uintptr_t)P.count};
     int slot = -1;
     for (int k = 0; k < ath_batch::kGraphs && slot < 0; ++k)
         if (b->exec[k] && std::memcmp(key, b->graphKey[k], sizeof(key)) == 0) slot = k;
@@ -1017,7 +1021,7 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
         cudaGraph_t graph = nullptr;
         if (err == cudaSuccess) err = cudaStreamBeginCapture(b->captureStream, cudaStreamCaptureModeThreadLocal);
         if (err == cudaSuccess) {
-            ath_param_grads g = *grads;
+            ath_param_grads g = grads ? *grads : ath_param_grads{};
             const cudaError_t enq =
                 enqueueStep(b, P, target, reinterpret_cast<float4*>(colour), loss, g, b->captureStream, false);
             err = cudaStreamEndCapture(b->captureStream, &graph);
@@ -1034,6 +1038,21 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
     err = cudaGraphLaunch(b->exec[slot], stream);
     if (err != cudaSuccess) return failCuda(err, "launching the batched step");
     return ATH_OK;
+}
+
+}   // namespace
+
+extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target,
+                                           float* colour, float* loss, ath_param_grads* grads, void* streamPtr) {
+    if (!b || !params || !target || !colour || !loss || !grads || !grads->means || !grads->scales || !grads->quats ||
+        !grads->sh)
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: null argument");
+    return runStep(b, params, target, colour, loss, grads, streamPtr, "ath_batch_train_step");
+}
+
+extern "C" ath_status ath_batch_render(ath_batch* b, const ath_mixed_params* params, float* colour, void* streamPtr) {
+    if (!b || !params || !colour) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_render: null argument");
+    return runStep(b, params, nullptr, colour, nullptr, nullptr, streamPtr, "ath_batch_render");
 }
 
 extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* streamPtr) {

@@ -124,7 +124,10 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
 // follow from them once a record, when the block flushes a batch. The loss has
 // no alpha term, so dL/d(alpha out) is 0 and the colour behind a record enters
 // only through S.dC, one value a pixel.
-template <uint32_t T, uint32_t NB>
+//
+// kTrain false: the forward blend alone (a batched render: colour only, no
+// target, loss or gradients).
+template <uint32_t T, uint32_t NB, bool kTrain>
 __global__ void __launch_bounds__(T * T / 2, 2)
     blendStepKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
@@ -229,6 +232,18 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                 }
                 if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
             }
+        }
+
+        if constexpr (!kTrain) {
+#pragma unroll
+            for (int p = 0; p < 2; ++p) {
+                if (!(px < V.width && py[p] < V.height)) continue;
+                const float coverage = 1.0f - Tr[p];
+                colour[V.pixelBase + py[p] * V.width + px] =
+                    make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1], bl[p] + Tr[p] * B.bg[2],
+                                coverage + Tr[p] * B.bg[3]);
+            }
+            continue;
         }
 
         // ---- the pixels' colour, the loss (the view's mean L2 over its pixels and r g b) and its gradient
@@ -379,7 +394,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lossSum += __shfl_xor_sync(0xFFFFFFFFu, lossSum, o);
-    if (lane == 0 && lossSum != 0.0f) atomicAdd(loss, lossSum);
+    if (kTrain && lane == 0 && lossSum != 0.0f) atomicAdd(loss, lossSum);
     uint64_t e = evaluated;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
@@ -397,9 +412,16 @@ int residentGrid(K kernel, int threads, int sms) {
 template <uint32_t T, uint32_t NB>
 cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
                      const float* target, float* loss, float* grads) {
-    const int grid = residentGrid(blendStepKernel<T, NB>, T * T / 2, L.sms);
-    blendStepKernel<T, NB><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs, colour,
-                                                               target, loss, grads, L.words);
+    if (target) {
+        const int grid = residentGrid(blendStepKernel<T, NB, true>, T * T / 2, L.sms);
+        blendStepKernel<T, NB, true><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs,
+                                                                         colour, target, loss, grads, L.words);
+    } else {
+        const int grid = residentGrid(blendStepKernel<T, NB, false>, T * T / 2, L.sms);
+        blendStepKernel<T, NB, false><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values,
+                                                                          L.recs, colour, nullptr, nullptr, nullptr,
+                                                                          L.words);
+    }
     return cudaGetLastError();
 }
 

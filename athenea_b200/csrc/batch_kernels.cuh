@@ -128,7 +128,8 @@ struct BlendLaunch {
 // blend into `colour`; the loss, each view's mean L2 against `target` (float3 a
 // pixel) over its pixels and r g b, summed over views into *loss (which the
 // caller zeroes); and the adjoint, dL/d(record) for every (view, Gaussian)
-// record, added into `grads` (which start at zero).
+// record, added into `grads` (which start at zero). A null `target`: the
+// forward blend alone (colour only).
 cudaError_t launchBatchBlendStep(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
                                  const float* target, float* loss, float* grads);
 

@@ -562,6 +562,12 @@ class BatchTrainer:
         check(N.lib().ath_batch_train_step(self._h, C.byref(params._native()), _ptr(target), _ptr(colour),
                                            _ptr(loss), C.byref(g), C.c_void_p(s.cuda_stream)))
 
+    def render(self, params: MixedParams, colour: torch.Tensor, stream: torch.cuda.Stream | None = None) -> None:
+        """ath_batch_render: every view's colour (float4 a pixel, views concatenated), no loss or backward."""
+        s = stream if stream is not None else torch.cuda.current_stream(colour.device)
+        self._keep_render = (params, colour)
+        check(N.lib().ath_batch_render(self._h, C.byref(params._native()), _ptr(colour), C.c_void_p(s.cuda_stream)))
+
     def check(self, stream: torch.cuda.Stream | None = None) -> dict:
         st = N.BatchStats()
         s = stream if stream is not None else torch.cuda.current_stream()

@@ -287,3 +287,31 @@ def test_alternating_target_buffers_replay_their_own_steps():
         np.testing.assert_array_equal(seen[k][1], seen[k + 2][1])
         g, h = seen[k][2], seen[k + 2][2]
         assert np.abs(g - h).max() <= 1e-5 * np.abs(g).max()
+
+
+def test_batched_render_draws_the_training_steps_colour():
+    """ath_batch_render: every view's forward alone gives, to the bit, the colour a
+    training step draws on the same cloud and views; the plain path's images agree
+    within the fast exponential's rounding; a render does not disturb the next step."""
+    Pq, M = _scene(40_000, 23)
+    views = _views()
+    gen = torch.Generator().manual_seed(10)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    images, _, _, _ = _plain(Pq, views, targets)
+    b, colour, loss, grads, _ = _batched(M, views, targets)
+    drawn = torch.full_like(colour, -1.0)
+    b.render(M, drawn)
+    torch.cuda.synchronize()
+    b.check()
+    np.testing.assert_array_equal(drawn.cpu().numpy(), colour.cpu().numpy())
+    got = drawn.cpu().numpy()
+    base = 0
+    for (proj, W, H), img in zip(views, images):
+        d = np.abs(got[base:base + W * H] - img.cpu().numpy()).max(axis=1)
+        assert np.mean(d <= 1e-4) >= 0.9999
+        base += W * H
+    # a training step after the render still trains (its own captured graph)
+    first_loss = loss.item()
+    b.step(M, torch.cat(targets).contiguous(), colour, loss, grads)
+    torch.cuda.synchronize()
+    assert abs(loss.item() - first_loss) <= 1e-5 * abs(first_loss)
