@@ -304,6 +304,23 @@ def run_ours(args) -> dict | None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     loss_batched = float(loss_host.item())
+
+    # the batched forward alone (ath_batch_render: every view's colour, no loss or backward)
+    for _ in range(2):
+        bt.render(mixed, colour, stream=stream)   # the first captures its graph
+    torch.cuda.synchronize()
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    for _ in range(args.steps):
+        bt.render(mixed, colour, stream=stream)
+    r1.record(stream)
+    torch.cuda.synchronize()
+    ms_render = r0.elapsed_time(r1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms_render], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_render = float(t.item())
+    bt.check()
     del bt, staging
 
     # ---- the plain FP32 path, one view at a time, same scene and views --------
@@ -334,6 +351,7 @@ def run_ours(args) -> dict | None:
     # the blends (forward, loss and adjoint), projection adjoint (memsets are not counted)
     launches = (2 + 1 + passes + 1 + 1 + 1) * args.steps
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
+               ms_render=ms_render,
                stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
                count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4,
                pixels=int(pixel_base[-1]), sizes=sorted({(W, H) for _, W, H in views}))
@@ -479,6 +497,8 @@ def main():
             "ms_per_view": res["ms_plain"] / V, "speedup": res["ms_plain"] / res["ms_batched"],
             "stages_ms": res["plain_stages"],
             "path": "ath_raster_render_params + ath_l2_loss + ath_raster_backward a view, same scene and views"},
+        "batched_render": {"ms_per_view": res["ms_render"] / V,
+                           "path": "ath_batch_render: every view's forward alone (colour), no loss or backward"},
         "stages_ms": stages, "pairs": stats["pairs"], "kept": stats["kept"], "evaluated": stats["evaluated"],
         "degenerate_fp64": stats["degenerate"], "loss": res["loss"],
         "roofline": roofline,
