@@ -605,6 +605,8 @@ struct ath_batch {
     uint32_t tile = 16, blockBatch = 256;
     float bg[4] = {0, 0, 0, 0};
     uint32_t shLimit = 3, antialias = 1;
+    uint32_t depthMode = 0;
+    float depthThreshold = 0.5f;
     std::vector<ath_projection> projections;
     std::vector<uint32_t> widths, heights, tileBases;
     uint32_t lastSorted = 0, lastSlotBits = 0;
@@ -621,7 +623,7 @@ struct ath_batch {
     static constexpr int kGraphs = 4;
     cudaStream_t captureStream = nullptr;
     cudaGraphExec_t exec[kGraphs] = {};
-    uintptr_t graphKey[kGraphs][12] = {};
+    uintptr_t graphKey[kGraphs][13] = {};
     int nextGraph = 0;   // the slot the next capture replaces
 };
 
@@ -707,6 +709,8 @@ BatchConst batchConst(const ath_batch* b, const ath_mixed_params& P) {
     B.totalTiles = b->totalTiles;
     B.totalPixels = b->totalPixels;
     B.shLimit = b->shLimit;
+    B.depthMode = b->depthMode;
+    B.depthThreshold = b->depthThreshold;
     B.antialias = b->antialias;
     B.linear = P.linear ? 1u : 0u;
     B.restPerColour = P.sh_degree >= 3 ? 15 : P.sh_degree == 2 ? 8 : P.sh_degree == 1 ? 3 : 0;
@@ -735,7 +739,7 @@ int residentBlocks(K kernel, int threads, int sms) {
 }
 
 cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t sorted, cudaStream_t stream,
-                            float4* colour, const float* target, float* loss, float* grads) {
+                            float4* colour, const float* target, float* loss, float* grads, float* depth) {
     BlendLaunch L{};
     L.views = static_cast<const BatchView*>(b->viewsDev.ptr);
     L.ranges = static_cast<const uint2*>(b->ranges.ptr);
@@ -746,13 +750,14 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
     L.sms = b->sms;
     L.tile = b->tile;
     L.blockBatch = b->blockBatch;
-    return launchBatchBlendStep(B, L, stream, colour, target, loss, grads);
+    return launchBatchBlendStep(B, L, stream, colour, target, loss, grads, depth);
 }
 
 // One step, enqueued (captured or not). `countOnly`: the projection alone, to size the pairs.
 // A null `target`: a render, the forward blend alone (no loss, no backward).
 cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* target, float4* colour, float* loss,
-                        ath_param_grads& g, cudaStream_t stream, bool countOnly, cudaEvent_t* marks = nullptr) {
+                        ath_param_grads& g, cudaStream_t stream, bool countOnly, cudaEvent_t* marks = nullptr,
+                        float* depth = nullptr) {
     auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], stream); };
     mark(0);
     BatchConst B = batchConst(b, P);
@@ -795,7 +800,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     if (err == cudaSuccess && train) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
     // the forward blend, the loss and the blend adjoint (the record gradients were cleared by the projection)
     if (err == cudaSuccess)
-        err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr));
+        err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr), depth);
     mark(4);
     if (err == cudaSuccess && train && P.count) {
         projectAdjointBatchKernel<<<(P.count + 127) / 128, 128, 0, stream>>>(
@@ -923,6 +928,8 @@ extern "C" ath_status ath_batch_set_views(ath_batch* b, const ath_view* views, u
         b->shLimit = settings->max_sh_degree;
         b->antialias = settings->antialias_override >= 0 ? (uint32_t)(settings->antialias_override != 0)
                                                          : (uint32_t)(settings->antialias != 0);
+        b->depthMode = settings->depth_mode;
+        b->depthThreshold = settings->depth_threshold;
     }
     buildViews(b);
     b->resize = true;
@@ -967,7 +974,7 @@ namespace {
 // A training step (target, loss and gradients given) or a render (all three
 // null), checked, its buffers sized, captured once for its arrays and replayed.
 ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour, float* loss,
-                   ath_param_grads* grads, void* streamPtr, const char* what) {
+                   ath_param_grads* grads, float* depth, void* streamPtr, const char* what) {
     if (b->views.empty()) return fail(ATH_E_INVALID_ARGUMENT, std::string(what) + ": no views (ath_batch_set_views)");
     const ath_mixed_params& P = *params;
     if (P.count && (!P.means || !P.scales || !P.quats || !P.sh_low || !P.sh_high || !P.sh_scale))
@@ -998,10 +1005,10 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
         if ((st = sizePairs(b, P, stream)) != ATH_OK) return st;
         dropGraph(b);
     }
-    const uintptr_t key[12] = {(uintptr_t)P.means, (uintptr_t)P.scales, (uintptr_t)P.quats, (uintptr_t)P.sh_low,
+    const uintptr_t key[13] = {(uintptr_t)P.means, (uintptr_t)P.scales, (uintptr_t)P.quats, (uintptr_t)P.sh_low,
                                (uintptr_t)P.sh_high, (uintptr_t)P.sh_scale, (uintptr_t)target, (uintptr_t)colour,
                                (uintptr_t)loss, (uintptr_t)(grads ? grads->means : nullptr),
-                               (uintptr_t)(grads ? grads->sh : nullptr), (uintptr_t)P.count};
+                               (uintptr_t)(grads ? grads->sh : nullptr), (uintptr_t)P.count, (uintptr_t)depth};
     int slot = -1;
     for (int k = 0; k < ath_batch::kGraphs && slot < 0; ++k)
         if (b->exec[k] && std::memcmp(key, b->graphKey[k], sizeof(key)) == 0) slot = k;
@@ -1023,7 +1030,8 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
         if (err == cudaSuccess) {
             ath_param_grads g = grads ? *grads : ath_param_grads{};
             const cudaError_t enq =
-                enqueueStep(b, P, target, reinterpret_cast<float4*>(colour), loss, g, b->captureStream, false);
+                enqueueStep(b, P, target, reinterpret_cast<float4*>(colour), loss, g, b->captureStream, false,
+                            nullptr, depth);
             err = cudaStreamEndCapture(b->captureStream, &graph);
             if (enq != cudaSuccess) err = enq;
         }
@@ -1047,12 +1055,13 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
     if (!b || !params || !target || !colour || !loss || !grads || !grads->means || !grads->scales || !grads->quats ||
         !grads->sh)
         return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: null argument");
-    return runStep(b, params, target, colour, loss, grads, streamPtr, "ath_batch_train_step");
+    return runStep(b, params, target, colour, loss, grads, nullptr, streamPtr, "ath_batch_train_step");
 }
 
-extern "C" ath_status ath_batch_render(ath_batch* b, const ath_mixed_params* params, float* colour, void* streamPtr) {
+extern "C" ath_status ath_batch_render(ath_batch* b, const ath_mixed_params* params, float* colour, float* depth,
+                                       void* streamPtr) {
     if (!b || !params || !colour) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_render: null argument");
-    return runStep(b, params, nullptr, colour, nullptr, nullptr, streamPtr, "ath_batch_render");
+    return runStep(b, params, nullptr, colour, nullptr, nullptr, depth, streamPtr, "ath_batch_render");
 }
 
 extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* streamPtr) {

@@ -125,14 +125,15 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
 // no alpha term, so dL/d(alpha out) is 0 and the colour behind a record enters
 // only through S.dC, one value a pixel.
 //
-// kTrain false: the forward blend alone (a batched render: colour only, no
-// target, loss or gradients).
+// kTrain false: the forward blend alone (a batched render: colour and, when
+// given, depth as the plain blend makes it; no target, loss or gradients).
 template <uint32_t T, uint32_t NB, bool kTrain>
 __global__ void __launch_bounds__(T * T / 2, 2)
     blendStepKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
                     const float4* __restrict__ recs, float4* __restrict__ colour, const float* __restrict__ target,
-                    float* __restrict__ loss, float* __restrict__ grads, uint32_t* __restrict__ words) {
+                    float* __restrict__ loss, float* __restrict__ grads, float* __restrict__ depth,
+                    uint32_t* __restrict__ words) {
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
     constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
@@ -183,10 +184,12 @@ __global__ void __launch_bounds__(T * T / 2, 2)
             sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
             sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
             sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
+            if constexpr (!kTrain) sAcc[k] = sc.z;   // a render's depth (its adjoint sums are unused)
         };
 
         // ---- forward
         float r[2] = {0.0f, 0.0f}, g[2] = {0.0f, 0.0f}, bl[2] = {0.0f, 0.0f}, Tr[2] = {1.0f, 1.0f};
+        float depthSum[2] = {0.0f, 0.0f}, depthAt[2] = {-1.0f, -1.0f};   // a render's depth
         uint32_t last[2] = {0, 0};
         bool done[2];
 #pragma unroll
@@ -225,8 +228,11 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                         r[p] = __fmaf_rn(w, c.x, r[p]);
                         g[p] = __fmaf_rn(w, c.y, g[p]);
                         bl[p] = __fmaf_rn(w, c.z, bl[p]);
+                        if constexpr (!kTrain) depthSum[p] = __fmaf_rn(w, sAcc[j], depthSum[p]);
                         Tr[p] = Tr[p] * (1.0f - alpha);
                         last[p] = first - range.x + j + 1;
+                        if constexpr (!kTrain)
+                            if (depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = sAcc[j];
                         if (Tr[p] < 1e-4f) done[p] = true;
                     }
                 }
@@ -239,9 +245,12 @@ __global__ void __launch_bounds__(T * T / 2, 2)
             for (int p = 0; p < 2; ++p) {
                 if (!(px < V.width && py[p] < V.height)) continue;
                 const float coverage = 1.0f - Tr[p];
-                colour[V.pixelBase + py[p] * V.width + px] =
-                    make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1], bl[p] + Tr[p] * B.bg[2],
-                                coverage + Tr[p] * B.bg[3]);
+                const uint32_t at = V.pixelBase + py[p] * V.width + px;
+                colour[at] = make_float4(r[p] + Tr[p] * B.bg[0], g[p] + Tr[p] * B.bg[1], bl[p] + Tr[p] * B.bg[2],
+                                         coverage + Tr[p] * B.bg[3]);
+                if (depth)
+                    depth[at] = B.depthMode == 0 ? (coverage > 1e-6f ? depthSum[p] / coverage : 0.0f)
+                                                 : fmaxf(depthAt[p], 0.0f);
             }
             continue;
         }
@@ -411,16 +420,17 @@ int residentGrid(K kernel, int threads, int sms) {
 
 template <uint32_t T, uint32_t NB>
 cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
-                     const float* target, float* loss, float* grads) {
+                     const float* target, float* loss, float* grads, float* depth) {
     if (target) {
         const int grid = residentGrid(blendStepKernel<T, NB, true>, T * T / 2, L.sms);
         blendStepKernel<T, NB, true><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs,
-                                                                         colour, target, loss, grads, L.words);
+                                                                         colour, target, loss, grads, nullptr,
+                                                                         L.words);
     } else {
         const int grid = residentGrid(blendStepKernel<T, NB, false>, T * T / 2, L.sms);
         blendStepKernel<T, NB, false><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values,
                                                                           L.recs, colour, nullptr, nullptr, nullptr,
-                                                                          L.words);
+                                                                          depth, L.words);
     }
     return cudaGetLastError();
 }
@@ -432,9 +442,9 @@ cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t str
     CALL(32, 64) CALL(32, 128) CALL(32, 256) CALL(32, 512)
 
 cudaError_t launchBatchBlendStep(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
-                                 const float* target, float* loss, float* grads) {
+                                 const float* target, float* loss, float* grads, float* depth) {
 #define ATH_CASE(T_, NB_) \
-    if (L.tile == T_ && L.blockBatch == NB_) return stepWith<T_, NB_>(B, L, stream, colour, target, loss, grads);
+    if (L.tile == T_ && L.blockBatch == NB_) return stepWith<T_, NB_>(B, L, stream, colour, target, loss, grads, depth);
     ATH_BLEND_CASES(ATH_CASE)
 #undef ATH_CASE
     return cudaErrorInvalidValue;

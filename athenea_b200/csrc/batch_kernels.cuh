@@ -35,6 +35,8 @@ struct BatchConst {
     uint32_t wide;           // 1: key (tile << 24 | depth) and a separate u32 Gaussian index a pair
     uint32_t totalTiles, totalPixels;
     uint32_t shLimit, antialias, linear, restPerColour;
+    uint32_t depthMode;      // a render's depth: 0 the alpha-weighted mean, 1 the first threshold crossing
+    float depthThreshold;
     float bg[4];
     uint64_t capacity;       // pairs the pair buffers hold
     InstanceConst inst;      // the cloud (params or mixed layout); m/eye per view
@@ -129,8 +131,8 @@ struct BlendLaunch {
 // pixel) over its pixels and r g b, summed over views into *loss (which the
 // caller zeroes); and the adjoint, dL/d(record) for every (view, Gaussian)
 // record, added into `grads` (which start at zero). A null `target`: the
-// forward blend alone (colour only).
+// forward blend alone, colour and (when `depth` is given) depth.
 cudaError_t launchBatchBlendStep(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
-                                 const float* target, float* loss, float* grads);
+                                 const float* target, float* loss, float* grads, float* depth = nullptr);
 
 }   // namespace ath

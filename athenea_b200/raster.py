@@ -562,11 +562,14 @@ class BatchTrainer:
         check(N.lib().ath_batch_train_step(self._h, C.byref(params._native()), _ptr(target), _ptr(colour),
                                            _ptr(loss), C.byref(g), C.c_void_p(s.cuda_stream)))
 
-    def render(self, params: MixedParams, colour: torch.Tensor, stream: torch.cuda.Stream | None = None) -> None:
-        """ath_batch_render: every view's colour (float4 a pixel, views concatenated), no loss or backward."""
+    def render(self, params: MixedParams, colour: torch.Tensor, depth: torch.Tensor | None = None,
+               stream: torch.cuda.Stream | None = None) -> None:
+        """ath_batch_render: every view's colour (float4 a pixel, views concatenated) and, when given, depth
+        (float a pixel), no loss or backward."""
         s = stream if stream is not None else torch.cuda.current_stream(colour.device)
-        self._keep_render = (params, colour)
-        check(N.lib().ath_batch_render(self._h, C.byref(params._native()), _ptr(colour), C.c_void_p(s.cuda_stream)))
+        self._keep_render = (params, colour, depth)
+        check(N.lib().ath_batch_render(self._h, C.byref(params._native()), _ptr(colour), _ptr(depth),
+                                       C.c_void_p(s.cuda_stream)))
 
     def check(self, stream: torch.cuda.Stream | None = None) -> dict:
         st = N.BatchStats()

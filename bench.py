@@ -498,7 +498,8 @@ def main():
             "stages_ms": res["plain_stages"],
             "path": "ath_raster_render_params + ath_l2_loss + ath_raster_backward a view, same scene and views"},
         "batched_render": {"ms_per_view": res["ms_render"] / V,
-                           "path": "ath_batch_render: every view's forward alone (colour), no loss or backward"},
+                           "path": "ath_batch_render: every view's forward alone (colour), no loss or backward, "
+                                   "same scene and views"},
         "stages_ms": stages, "pairs": stats["pairs"], "kept": stats["kept"], "evaluated": stats["evaluated"],
         "degenerate_fp64": stats["degenerate"], "loss": res["loss"],
         "roofline": roofline,

@@ -335,10 +335,12 @@ ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, co
  * reference's TileRasterizer::render draws one camera a call
  * (TileRasterizer.h:468-474): the same projection, sort and blend as a training
  * step, with no loss and no backward, into `colour` (float4 a pixel, views
- * concatenated; premultiplied linear, as ath_raster_render's colour target).
- * Depth and P are not written. Sized and captured like a step, in a captured
- * graph of its own. */
-ath_status ath_batch_render(ath_batch* b, const ath_mixed_params* params, float* colour, void* stream);
+ * concatenated; premultiplied linear, as ath_raster_render's colour target)
+ * and, when not null, `depth` (float a pixel, views concatenated; the view-z
+ * depth of ath_settings.depth_mode / depth_threshold as given to
+ * ath_batch_set_views, as ath_raster_render's depth target). P is not written.
+ * Sized and captured like a step, in a captured graph of its own. */
+ath_status ath_batch_render(ath_batch* b, const ath_mixed_params* params, float* colour, float* depth, void* stream);
 /* Waits for `stream` and reports the last step; ATH_E_CAPACITY when its pairs
  * outgrew the buffers (that step is not valid; the next one grows them). */
 ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* stream);

@@ -315,3 +315,36 @@ def test_batched_render_draws_the_training_steps_colour():
     b.step(M, torch.cat(targets).contiguous(), colour, loss, grads)
     torch.cuda.synchronize()
     assert abs(loss.item() - first_loss) <= 1e-5 * abs(first_loss)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batched_render_depth_is_the_plain_paths(mode):
+    """ath_batch_render's depth, in the mean and in the threshold mode, against the
+    plain path's depth target on the same cloud and views: equal but for the rare
+    blend decision the fast exponential takes the other way."""
+    Pq, M = _scene(40_000, 24)
+    views = _views()
+    settings = lambda W, H: A.RenderSettings(width=W, height=H, depth_mode=mode, depth_threshold=0.4)
+    raster = A.TileRasterizer.create()
+    plain = []
+    for proj, W, H in views:
+        t = A.RenderTargets.make(W, H)
+        raster.render_params(proj, Pq, settings(W, H), t)
+        plain.append((t.colour.clone(), t.depth.clone()))
+    b = BatchTrainer()
+    b.set_views(views, settings(1, 1))
+    b.set_tuning(16, 256)
+    colour = torch.empty((b.pixels, 4), device="cuda")
+    depth = torch.full((b.pixels,), -1.0, device="cuda")
+    b.render(M, colour, depth)
+    torch.cuda.synchronize()
+    b.check()
+    got = depth.cpu().numpy()
+    base = 0
+    for (_, W, H), (pc, pd) in zip(views, plain):
+        d, want = got[base:base + W * H], pd.cpu().numpy()
+        covered = pc.cpu().numpy()[:, 3] > 1e-2
+        rel = np.abs(d - want) / np.maximum(np.abs(want), 1e-6)
+        assert np.all(d[~covered] >= 0.0)
+        assert np.mean(rel[covered] <= 1e-4) >= 0.999, float(np.mean(rel[covered] <= 1e-4))
+        base += W * H
