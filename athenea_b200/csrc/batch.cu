@@ -305,10 +305,12 @@ __global__ void __launch_bounds__(kProjThreads, 6)   // six blocks an SM: the ke
     uint32_t area = 0;
     sHit[threadIdx.x] = 0u;
     if (i < B.count && gb < gaussBlocks) {
-        // the record's gradient words, which the blend adjoint sums into, start at zero
-        float2* zero = reinterpret_cast<float2*>(grads + ((size_t)v * B.count + i) * kGradWords);
+        // the record's gradient words, which the blend adjoint sums into, start at zero (a training step's)
+        if (grads) {
+            float2* zero = reinterpret_cast<float2*>(grads + ((size_t)v * B.count + i) * kGradWords);
 #pragma unroll
-        for (uint32_t k = 0; k < kGradWords / 2; ++k) zero[k] = make_float2(0.0f, 0.0f);
+            for (uint32_t k = 0; k < kGradWords / 2; ++k) zero[k] = make_float2(0.0f, 0.0f);
+        }
         InstanceConst I = B.inst;
 #pragma unroll
         for (int k = 0; k < 12; ++k) I.m[k] = sView.m[k];
@@ -771,7 +773,8 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
         projectEmitKernel<kLayoutMixed><<<gaussBlocks * V, kProjThreads, 0, stream>>>(
             B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<float4*>(b->recs.ptr),
             static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint32_t*>(b->values[0].ptr),
-            static_cast<uint64_t*>(b->projFlags.ptr), words, static_cast<float*>(b->grads.ptr), gaussBlocks);
+            static_cast<uint64_t*>(b->projFlags.ptr), words, target ? static_cast<float*>(b->grads.ptr) : nullptr,
+            gaussBlocks);
     if (err == cudaSuccess) err = cudaGetLastError();
     if (countOnly || err != cudaSuccess) return err;
     mark(1);
