@@ -56,18 +56,59 @@ def peaks() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi sampled every 200 ms over the timed region."""
+    """The SM clock, its maximum and the throttle reasons over the timed region: read
+    through NVML every 10 ms from a thread (the device found by its UUID, which
+    CUDA_VISIBLE_DEVICES does not renumber), or, without NVML, nvidia-smi every 200 ms."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device_index: int):
         self.device = device_index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []          # (sm MHz, max sm MHz, {reason names})
+        self.stop = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.device)
+        uuid = str(getattr(props, "uuid", "") or "")
+        if uuid:
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def __enter__(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            reasons_of = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            bits = [getattr(nv, "nvmlClocksEventReason" + n, getattr(nv, "nvmlClocksThrottleReason" + n, 0))
+                    for n in ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")]
+            self.stop = threading.Event()
+
+            def sample():
+                while not self.stop.is_set():
+                    try:
+                        r = reasons_of(h)
+                        self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                          nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                                          {self.NAMES[k] for k in range(4) if r & bits[k]}))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.01)
+
+            self.thread = threading.Thread(target=sample, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -79,6 +120,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -87,25 +131,26 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
-        rows = []
-        try:
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        finally:
+        if self.thread is None and self.path:
             try:
-                os.unlink(self.path)
-            except OSError:
-                pass
-        if not rows:
+                for line in open(self.path):
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                        self.rows.append((float(parts[1]), float(parts[2]) if parts[2].replace(".", "").isdigit()
+                                          else None, {self.NAMES[k] for k in range(4)
+                                                      if parts[5 + k].lower().startswith("active")}))
+            finally:
+                try:
+                    os.unlink(self.path)
+                except OSError:
+                    pass
+        if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        maxima = [m for _, m, _ in self.rows if m]
+        return {"sm_mhz": statistics.median(float(r[0]) for r in self.rows),
+                "sm_max_mhz": float(max(maxima)) if maxima else None,
+                "reasons": sorted(set().union(*(r[2] for r in self.rows))), "samples": len(self.rows),
+                "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
 def dist_env():
