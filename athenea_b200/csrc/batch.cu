@@ -995,7 +995,9 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
         return fail(ATH_E_UNSUPPORTED, std::string(what) + ": more than 2^40 tiles");
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
     ath_status st = ATH_OK;
-    if (P.count != b->count) {
+    // the buffers a view, a tile or a Gaussian holds: grown whenever the cloud, the
+    // views or the tile size changed (set_views and set_tuning mark a resize)
+    if (P.count != b->count || b->resize) {
         if ((st = reserveBatch(b, P.count)) != ATH_OK) return st;
         b->resize = true;
         dropGraph(b);
@@ -1149,7 +1151,14 @@ extern "C" ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* param
         for (uint32_t nb : batches) {
             ath_status st = ath_batch_set_tuning(b, t, nb);
             if (st == ATH_OK) st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);
-            if (st != ATH_OK) continue;   // e.g. too many tile bits for this tile size
+            // a setting that does not fit (too many tile bits for packed keys, or its pairs
+            // past the memory) is skipped; any other failure ends the tuning
+            if (st == ATH_E_UNSUPPORTED || st == ATH_E_OUT_OF_MEMORY) continue;
+            if (st != ATH_OK) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return st;
+            }
             cudaEventRecord(e0, stream);
             for (uint32_t r = 0; r < std::max(repeats, 1u); ++r)
                 st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);

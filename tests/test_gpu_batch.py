@@ -146,6 +146,23 @@ def test_tile_size_and_block_batch_change_no_image_bit():
                 np.testing.assert_array_equal(img, ref, err_msg=f"tile {tile}, batch {nb}")
 
 
+def test_one_trainer_through_tile_and_view_changes_draws_as_fresh_ones():
+    """ath_batch_set_tuning to a smaller tile (four times the tiles) and
+    ath_batch_set_views with more views, after steps on the same trainer: its
+    buffers grow with them, and each step draws what a new trainer draws."""
+    Pq, M = _scene(30_000, 12)
+    gen = torch.Generator().manual_seed(6)
+    every = _views(6)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in every]
+    b = BatchTrainer()
+    for n, tile, nb in ((2, 32, 512), (2, 8, 256), (6, 16, 128), (3, 32, 64)):
+        views, tg = every[:n], targets[:n]
+        _, colour, _, _, stats = _batched(M, views, tg, tile, nb, trainer=b)
+        _, fresh, _, _, fresh_stats = _batched(M, views, tg, tile, nb)
+        np.testing.assert_array_equal(colour.cpu().numpy(), fresh.cpu().numpy(), err_msg=f"{n} views, tile {tile}")
+        assert stats["pairs"] == fresh_stats["pairs"]
+
+
 def test_replayed_step_draws_the_same_image_and_tune_picks_a_setting():
     Pq, M = _scene(30_000, 9)
     views = _views()
