@@ -836,7 +836,10 @@ ath_status reserveBatch(ath_batch* b, uint32_t count) {
 // made before capture), and the pair buffers grown to 1.15 times it.
 ath_status sizePairs(ath_batch* b, const ath_mixed_params& P, cudaStream_t stream) {
     ath_param_grads none{};
-    cudaError_t err = enqueueStep(b, P, nullptr, nullptr, nullptr, none, stream, true);
+    // the projection's look-back words start "not ready": a buffer just allocated may
+    // hold another batch's words, whose epoch tags the look-back would take as ready
+    cudaError_t err = cudaMemsetAsync(b->projFlags.ptr, 0, b->projFlags.bytes, stream);
+    if (err == cudaSuccess) err = enqueueStep(b, P, nullptr, nullptr, nullptr, none, stream, true);
     uint32_t w[kBatchWords];
     if (err == cudaSuccess) err = cudaMemcpyAsync(w, b->words.ptr, sizeof(w), cudaMemcpyDeviceToHost, stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
@@ -1057,8 +1060,9 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
 
 extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target,
                                            float* colour, float* loss, ath_param_grads* grads, void* streamPtr) {
-    if (!b || !params || !target || !colour || !loss || !grads || !grads->means || !grads->scales || !grads->quats ||
-        !grads->sh)
+    // an empty cloud has no gradient rows: its gradient arrays may be null
+    if (!b || !params || !target || !colour || !loss || !grads ||
+        (params->count && (!grads->means || !grads->scales || !grads->quats || !grads->sh)))
         return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: null argument");
     return runStep(b, params, target, colour, loss, grads, nullptr, streamPtr, "ath_batch_train_step");
 }

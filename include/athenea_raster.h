@@ -328,7 +328,10 @@ ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode);
  * calls with the same pointers replay it. Up to four captured steps are kept,
  * keyed by the arrays they read and write, so a caller that alternates two
  * target (or colour) buffers, to upload one while the other is in use, replays
- * both after their first call. */
+ * both after their first call. ath_batch_set_views, ath_batch_set_tuning and
+ * ath_batch_set_key_mode may be called between steps, and the cloud may change
+ * size: the next step grows the buffers and captures again. An empty cloud
+ * (count 0) draws the background, and its gradient arrays may be null. */
 ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
                                 float* loss, ath_param_grads* grads, void* stream);
 /* Every view's forward alone, for rendering many cameras at once, where the
