@@ -90,14 +90,16 @@ struct ParamGrad {
     }
 };
 
-// The projection's adjoint past the colour, for one Gaussian and one view:
-// dL/d(record) `gw` -> dL/d(position, opacity logit, log scales, quaternion).
-// `G` is projectGeometry's result for (F, I, g); `dp` holds what the colour's
-// adjoint gave the position and ends, with the geometry's share, in `acc`.
-template <uint32_t L>
-__device__ __forceinline__ void geometryAdjoint(const FrameConst& F, const InstanceConst& I, uint32_t i, const Gauss& g,
-                                                const Geometry& G, const float gw[kGradWords], float dp[3],
-                                                ParamGrad& acc) {
+// The projection's adjoint past the colour, for one Gaussian and one view, up
+// to the covariance's factor M = R diag(s): dL/d(record) `gw` -> dL/d(position,
+// opacity logit) into `acc`, and dL/dM into `dM`. `G` is projectGeometry's
+// result for (F, I, g); `dp` holds what the colour's adjoint gave the position
+// and ends, with the geometry's share, in `acc`. dL/dM is linear in the views,
+// so a caller that sums it over views takes it to the scales and the
+// quaternion once (shapeAdjoint).
+__device__ __forceinline__ void geometryAdjointToM(const FrameConst& F, const InstanceConst& I, const Gauss& g,
+                                                   const Geometry& G, const float gw[kGradWords], float dp[3],
+                                                   ParamGrad& acc, float dM[3][3]) {
     const float* m = I.m;
     // ---- opacity and the payback: alpha = paidOpacity(sigmoid(logit), paid) ----
     const float o = g.opacity;
@@ -165,33 +167,14 @@ __device__ __forceinline__ void geometryAdjoint(const FrameConst& F, const Insta
         dax[j] = 2.0f * da * ax[j] + db * ay[j];
         day[j] = db * ax[j] + 2.0f * dc * ay[j];
     }
-    float dt3[3], du3[3], dScale[3] = {0.0f, 0.0f, 0.0f}, dR[3][3];
+    float dt3[3], du3[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
         dt3[r] = G.M[r][0] * dax[0] + G.M[r][1] * dax[1] + G.M[r][2] * dax[2];
         du3[r] = G.M[r][0] * day[0] + G.M[r][1] * day[1] + G.M[r][2] * day[2];
 #pragma unroll
-        for (int col = 0; col < 3; ++col) {
-            const float dM = G.t3[r] * dax[col] + G.u3[r] * day[col];
-            dScale[col] += dM * G.R[r][col];
-            dR[r][col] = dM * g.scale[col];
-        }
+        for (int col = 0; col < 3; ++col) dM[r][col] = G.t3[r] * dax[col] + G.u3[r] * day[col];
     }
-    // ---- the rotation: R(q), q = raw / |raw| --------------------------------
-    const float x = g.q[0], y = g.q[1], z = g.q[2], w = g.q[3];
-    float dq[4];   // x y z w
-    dq[0] = 2.0f * (y * dR[0][1] + z * dR[0][2] + y * dR[1][0] - 2.0f * x * dR[1][1] - w * dR[1][2] + z * dR[2][0] +
-                    w * dR[2][1] - 2.0f * x * dR[2][2]);
-    dq[1] = 2.0f * (-2.0f * y * dR[0][0] + x * dR[0][1] + w * dR[0][2] + x * dR[1][0] + z * dR[1][2] - w * dR[2][0] +
-                    z * dR[2][1] - 2.0f * y * dR[2][2]);
-    dq[2] = 2.0f * (-2.0f * z * dR[0][0] - w * dR[0][1] + x * dR[0][2] + w * dR[1][0] - 2.0f * z * dR[1][1] +
-                    y * dR[1][2] + x * dR[2][0] + y * dR[2][1]);
-    dq[3] = 2.0f * (-z * dR[0][1] + y * dR[0][2] + z * dR[1][0] - x * dR[1][2] - y * dR[2][0] + x * dR[2][1]);
-    const float4 qraw = __ldg(reinterpret_cast<const float4*>(I.quats) + i);
-    const float qlen = sqrtf(((qraw.x * qraw.x + qraw.y * qraw.y) + qraw.z * qraw.z) + qraw.w * qraw.w);
-    const float qd = dq[0] * x + dq[1] * y + dq[2] * z + dq[3] * w;
-    const float4 dQuat = make_float4((dq[3] - w * qd) / qlen, (dq[0] - x * qd) / qlen, (dq[1] - y * qd) / qlen,
-                                     (dq[2] - z * qd) / qlen);   // w x y z
 
     // ---- the Jacobian and the centre: t = W p + tw -------------------------
     const float djx0 = dt3[0] * m[0] + dt3[1] * m[1] + dt3[2] * m[2];
@@ -226,9 +209,50 @@ __device__ __forceinline__ void geometryAdjoint(const FrameConst& F, const Insta
 
     acc.dp[0] += dp[0]; acc.dp[1] += dp[1]; acc.dp[2] += dp[2];
     acc.dLogit += dLogit;
+}
+
+// dL/dM (M = R diag(s), R the rotation projectGeometry builds from g.q) ->
+// dL/d(log scales, raw quaternion), added into `acc`.
+__device__ __forceinline__ void shapeAdjoint(const InstanceConst& I, uint32_t i, const Gauss& g, const float R[3][3],
+                                             const float dM[3][3], ParamGrad& acc) {
+    float dScale[3] = {0.0f, 0.0f, 0.0f}, dR[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int col = 0; col < 3; ++col) {
+            dScale[col] += dM[r][col] * R[r][col];
+            dR[r][col] = dM[r][col] * g.scale[col];
+        }
+    // ---- the rotation: R(q), q = raw / |raw| --------------------------------
+    const float x = g.q[0], y = g.q[1], z = g.q[2], w = g.q[3];
+    float dq[4];   // x y z w
+    dq[0] = 2.0f * (y * dR[0][1] + z * dR[0][2] + y * dR[1][0] - 2.0f * x * dR[1][1] - w * dR[1][2] + z * dR[2][0] +
+                    w * dR[2][1] - 2.0f * x * dR[2][2]);
+    dq[1] = 2.0f * (-2.0f * y * dR[0][0] + x * dR[0][1] + w * dR[0][2] + x * dR[1][0] + z * dR[1][2] - w * dR[2][0] +
+                    z * dR[2][1] - 2.0f * y * dR[2][2]);
+    dq[2] = 2.0f * (-2.0f * z * dR[0][0] - w * dR[0][1] + x * dR[0][2] + w * dR[1][0] - 2.0f * z * dR[1][1] +
+                    y * dR[1][2] + x * dR[2][0] + y * dR[2][1]);
+    dq[3] = 2.0f * (-z * dR[0][1] + y * dR[0][2] + z * dR[1][0] - x * dR[1][2] - y * dR[2][0] + x * dR[2][1]);
+    const float4 qraw = __ldg(reinterpret_cast<const float4*>(I.quats) + i);
+    const float qlen = sqrtf(((qraw.x * qraw.x + qraw.y * qraw.y) + qraw.z * qraw.z) + qraw.w * qraw.w);
+    const float qd = dq[0] * x + dq[1] * y + dq[2] * z + dq[3] * w;
+    const float4 dQuat = make_float4((dq[3] - w * qd) / qlen, (dq[0] - x * qd) / qlen, (dq[1] - y * qd) / qlen,
+                                     (dq[2] - z * qd) / qlen);   // w x y z
+
 #pragma unroll
     for (int k = 0; k < 3; ++k) acc.dLogScale[k] += dScale[k] * g.scale[k];
     acc.dQuat[0] += dQuat.x; acc.dQuat[1] += dQuat.y; acc.dQuat[2] += dQuat.z; acc.dQuat[3] += dQuat.w;
+}
+
+// The projection's adjoint past the colour, for one Gaussian and one view:
+// dL/d(record) `gw` -> dL/d(position, opacity logit, log scales, quaternion).
+template <uint32_t L>
+__device__ __forceinline__ void geometryAdjoint(const FrameConst& F, const InstanceConst& I, uint32_t i, const Gauss& g,
+                                                const Geometry& G, const float gw[kGradWords], float dp[3],
+                                                ParamGrad& acc) {
+    float dM[3][3];
+    geometryAdjointToM(F, I, g, G, gw, dp, acc, dM);
+    shapeAdjoint(I, i, g, G.R, dM, acc);
 }
 
 // The projection's adjoint for one Gaussian and one view: dL/d(record) `gw`

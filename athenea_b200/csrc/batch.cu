@@ -495,8 +495,10 @@ __global__ void __launch_bounds__(256)
 // ---- the projection's adjoint over every view: one thread a Gaussian ---------
 // Two passes over the views, so that what is live across them stays small: the
 // colour's adjoint (the SH gradient, 48 values, and the position's share through
-// the view direction), then the geometry's (position, opacity, scales,
-// rotation). The cloud's loads and the SH (packed in registers) are read once.
+// the view direction), then the geometry's (position and opacity a view; the
+// covariance factor's gradient dL/dM summed over the views and taken to the
+// scales and the rotation once). The cloud's loads and the SH (packed in
+// registers) are read once.
 __global__ void __launch_bounds__(128)
     projectAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float* __restrict__ grads,
                               float4* __restrict__ gMeans, float4* __restrict__ gScales, float4* __restrict__ gQuats,
@@ -536,6 +538,8 @@ __global__ void __launch_bounds__(128)
     acc.dLogit = 0.0f;
     acc.dLogScale[0] = acc.dLogScale[1] = acc.dLogScale[2] = 0.0f;
     acc.dQuat[0] = acc.dQuat[1] = acc.dQuat[2] = acc.dQuat[3] = 0.0f;
+    float dMsum[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    bool shaped = false;
     float next[kGradWords];
 #pragma unroll
     for (int k = 0; k < (int)kGradWords; ++k) next[k] = grads[(size_t)i * kGradWords + k];
@@ -563,7 +567,19 @@ __global__ void __launch_bounds__(128)
         I.eye[0] = V.eye[0]; I.eye[1] = V.eye[1]; I.eye[2] = V.eye[2];
         const Geometry G = projectGeometry<true>(F, I, g, g.opacity);
         float dpv[3] = {0.0f, 0.0f, 0.0f};
-        geometryAdjoint<kLayoutMixed>(F, I, i, g, G, gw, dpv, acc);
+        float dM[3][3];
+        geometryAdjointToM(F, I, g, G, gw, dpv, acc, dM);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int col = 0; col < 3; ++col) dMsum[r][col] += dM[r][col];
+        shaped = true;
+    }
+    // dL/dM summed over the views, to the scales and the quaternion once
+    if (shaped) {
+        float R[3][3];
+        rotationOf(g, R);
+        shapeAdjoint(I, i, g, R, dMsum, acc);
     }
     gMeans[i] = make_float4(acc.dp[0] + dp[0], acc.dp[1] + dp[1], acc.dp[2] + dp[2], acc.dLogit);
     gScales[i] = make_float4(acc.dLogScale[0], acc.dLogScale[1], acc.dLogScale[2], 0.0f);

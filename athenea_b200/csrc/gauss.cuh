@@ -211,6 +211,14 @@ __device__ __forceinline__ WideCovariance wideCovariance(const float t3[3], cons
     return W;
 }
 
+// The rotation of the splat's normalised quaternion g.q (x y z w), row-major.
+__device__ __forceinline__ void rotationOf(const Gauss& g, float R[3][3]) {
+    const float x = g.q[0], y = g.q[1], z = g.q[2], w = g.q[3];
+    R[0][0] = 1.0f - 2.0f * (y * y + z * z); R[0][1] = 2.0f * (x * y - w * z); R[0][2] = 2.0f * (x * z + w * y);
+    R[1][0] = 2.0f * (x * y + w * z); R[1][1] = 1.0f - 2.0f * (x * x + z * z); R[1][2] = 2.0f * (y * z - w * x);
+    R[2][0] = 2.0f * (x * z - w * y); R[2][1] = 2.0f * (y * z + w * x); R[2][2] = 1.0f - 2.0f * (x * x + y * y);
+}
+
 // splat_project.slang:519-757 for one splat (no lens, no shutter, no catcher or
 // sheet; a surfel is drawn as the thin Gaussian it projects to).
 // kWide: the mixed-precision path, which takes near-degenerate footprints
@@ -229,10 +237,7 @@ __device__ __forceinline__ Geometry projectGeometry(const FrameConst& F, const I
         G.cull = kCullDepth;
         return G;
     }
-    const float x = g.q[0], y = g.q[1], z = g.q[2], w = g.q[3];
-    G.R[0][0] = 1.0f - 2.0f * (y * y + z * z); G.R[0][1] = 2.0f * (x * y - w * z); G.R[0][2] = 2.0f * (x * z + w * y);
-    G.R[1][0] = 2.0f * (x * y + w * z); G.R[1][1] = 1.0f - 2.0f * (x * x + z * z); G.R[1][2] = 2.0f * (y * z - w * x);
-    G.R[2][0] = 2.0f * (x * z - w * y); G.R[2][1] = 2.0f * (y * z + w * x); G.R[2][2] = 1.0f - 2.0f * (x * x + y * y);
+    rotationOf(g, G.R);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
