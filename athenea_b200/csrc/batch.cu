@@ -67,14 +67,23 @@ __global__ void beginStepKernel(uint32_t* words) {
     words[kBatchDegenerate] = 0;
 }
 
+// Block b's word of an epoch-tagged look-back: its aggregate (its inclusive
+// sum for block 0), stored ahead of lookbackEpoch so that the block can do
+// other work before it waits.
+__device__ __forceinline__ void publishEpoch(uint64_t* flags, uint32_t b, uint32_t aggregate, uint32_t epoch) {
+    if ((threadIdx.x & 31u) == 0) storeRelaxed(flags + b, tagged(epoch, b == 0 ? 2 : 1, aggregate));
+}
+
 // The decoupled look-back of lookbackExclusive with epoch-tagged 32-bit values.
-__device__ uint32_t lookbackEpoch(uint64_t* flags, uint32_t b, uint32_t aggregate, uint32_t epoch, uint32_t* status) {
+// `published`: block b's word was stored already (publishEpoch).
+__device__ uint32_t lookbackEpoch(uint64_t* flags, uint32_t b, uint32_t aggregate, uint32_t epoch, uint32_t* status,
+                                  bool published = false) {
     const uint32_t lane = threadIdx.x & 31u;
     if (b == 0) {
-        if (lane == 0) storeRelaxed(flags, tagged(epoch, 2, aggregate));
+        if (lane == 0 && !published) storeRelaxed(flags, tagged(epoch, 2, aggregate));
         return 0;
     }
-    if (lane == 0) storeRelaxed(flags + b, tagged(epoch, 1, aggregate));
+    if (lane == 0 && !published) storeRelaxed(flags + b, tagged(epoch, 1, aggregate));
     uint64_t exclusive = 0;
     int64_t window = (int64_t)b - 1;
     uint32_t spins = 0;
@@ -262,8 +271,9 @@ __device__ __forceinline__ uint32_t ownerOf(uint32_t incl, uint32_t q) {
 // warp's 32 footprints (each footprint's screen rect, row-major) are one list,
 // lane l taking entry 32 c + l, so a warp's work is the sum of its rects, not 32
 // times the largest. A first walk counts the pairs (its ballots kept in shared
-// memory), the block's total is scanned across blocks by the epoch look-back, and
-// a second walk writes the pairs in list order: a footprint's pairs in its rect's
+// memory), the block's total is published for the epoch look-back, the records'
+// SH colours are computed while the blocks before finish theirs, the block's
+// place among the pairs is read back, and a second walk writes the pairs in list order: a footprint's pairs in its rect's
 // row-major order, footprints in thread order (splat_emit.slang:37-49).
 constexpr uint32_t kBallotCache = 16;   // chunks of 32 candidates whose ballots a warp keeps
 
@@ -343,15 +353,11 @@ __global__ void __launch_bounds__(kProjThreads, 6)   // six blocks an SM: the ke
                 sFb[threadIdx.x] = make_float4(G.cc, G.cutoff, G.fr, G.fs);
                 sRect[threadIdx.x] = make_uint4(rx0, ry0, cols, (__float_as_uint(G.tz) >> 7) | (G.wide ? 1u << 31 : 0u));
                 sInvCols[threadIdx.x] = 1.0f / (float)cols;
-                // the record (read only through the pairs, so written for any rect on screen)
-                const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
-                float colour[3];
-                colourFast(loadMixedSh(I, i), g, degree, I.linear, g.px - I.eye[0], g.py - I.eye[1], g.pz - I.eye[2],
-                           colour);
+                // the record (read only through the pairs, so written for any rect on screen);
+                // its colour once the block's pair count is published
                 const size_t r = ((size_t)v * B.count + i) * 3;
                 recs[r + 0] = make_float4(G.cx, G.cy, G.tz, G.cutoff);
                 recs[r + 1] = make_float4(G.ca, G.fr, G.fs, G.alpha);
-                recs[r + 2] = make_float4(colour[0], colour[1], colour[2], 0.0f);
             }
         }
     }
@@ -396,8 +402,25 @@ __global__ void __launch_bounds__(kProjThreads, 6)   // six blocks an SM: the ke
         warpBase += w < warp ? sWarp[w] : 0u;
         blockTotal += sWarp[w];
     }
+    if (warp == 0) publishEpoch(flags, t, blockTotal, epoch);
+    // the record's colour (SH seen from the view's eye), which needs no place among the
+    // pairs: computed while the blocks before this one finish their counts
+    if (area > 0) {
+        const InstanceConst& I = B.inst;
+        const float4 m = __ldg(reinterpret_cast<const float4*>(I.means) + i);
+        Gauss g;
+        const __nv_bfloat16* bl = reinterpret_cast<const __nv_bfloat16*>(I.shLow) + (size_t)i * 12;
+        g.base[0] = 0.5f + kSH0 * __bfloat162float(bl[0]);
+        g.base[1] = 0.5f + kSH0 * __bfloat162float(bl[1]);
+        g.base[2] = 0.5f + kSH0 * __bfloat162float(bl[2]);
+        const uint32_t degree = min(degreeOf(I.restPerColour), F.shLimit);
+        float colour[3];
+        colourFast(loadMixedSh(I, i), g, degree, I.linear, m.x - sView.eye[0], m.y - sView.eye[1],
+                   m.z - sView.eye[2], colour);
+        recs[((size_t)v * B.count + i) * 3 + 2] = make_float4(colour[0], colour[1], colour[2], 0.0f);
+    }
     if (warp == 0) {
-        const uint32_t prefix = lookbackEpoch(flags, t, blockTotal, epoch, &words[kBatchStatus]);
+        const uint32_t prefix = lookbackEpoch(flags, t, blockTotal, epoch, &words[kBatchStatus], true);
         if (lane == 0) {
             sPrefix = prefix;
             if (kept) atomicAdd(&words[kBatchKept], kept);
