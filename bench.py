@@ -42,8 +42,8 @@ METRIC = "fwd+bwd ms/view, 1.5M Gaussians 1080p, batched+BF16 vs plain FP32, err
 # batched kernels, from an ncu capture of this workload (profiles/).
 NCU_TRAFFIC: dict = {
     # profiles/batched_kernels_1.5M_2x1080p_tile32.md: DRAM bytes a launch on 2 views, scaled to 8
-    "blendStepKernel": 4 * 160.72e6,
-    "projectEmitKernel": 4 * 531.33e6,
+    "blendStepKernel": 4 * 161.94e6,
+    "projectEmitKernel": 4 * 489.20e6,
 }
 
 
