@@ -39,9 +39,10 @@ METRIC = "fwd+bwd ms/view, 1.5M Gaussians 1080p, batched+BF16 vs plain FP32, err
 
 
 # DRAM bytes a launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# batched kernels, from an ncu capture of this workload (profiles/).
+# batched kernels, from an ncu capture of this workload at 2 views (tile 32,
+# 512 records a batch), scaled by 4 to its 8 views: records and pairs grow
+# with the views.
 NCU_TRAFFIC: dict = {
-    # profiles/batched_kernels_1.5M_2x1080p_tile32.md: DRAM bytes a launch on 2 views, scaled to 8
     "blendStepKernel": 4 * 161.94e6,
     "projectEmitKernel": 4 * 489.20e6,
 }
@@ -495,7 +496,7 @@ def main():
     stats, stages = res["stats"], res["stages"]
     dominant = max(stages, key=stages.get)
     fp32_peak = 148 * 128 * 2 * P.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-    # algorithmic work a launch, per stage (per-unit figures stated in DESIGN.md)
+    # algorithmic work a launch, per stage: bytes a unit times the units, or FLOPs a evaluation
     mixed_bytes = 16 + 16 + 16 + 24 + 36 + 4          # a Gaussian in the mixed layout
     work = {
         "project_emit": ("hbm", res["count"] * mixed_bytes + stats["kept"] * 48 + stats["pairs"] * 8),
