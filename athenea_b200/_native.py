@@ -113,7 +113,8 @@ class BatchStats(C.Structure):
 class BatchBuffers(C.Structure):
     _fields_ = [("pairs", C.c_uint64), ("key_shift", C.c_uint32), ("slot_bits", C.c_uint32),
                 ("total_tiles", C.c_uint32), ("views", C.c_uint32), ("sorted_pairs", C.c_void_p),
-                ("ranges", C.c_void_p), ("sorted_values", C.c_void_p), ("tile_bases", C.POINTER(C.c_uint32))]
+                ("ranges", C.c_void_p), ("sorted_values", C.c_void_p), ("tile_bases", C.POINTER(C.c_uint32)),
+                ("depth_bits", C.c_uint32), ("exp_base", C.c_uint32)]
 
 
 class Encoding(C.Structure):

@@ -65,6 +65,8 @@ __global__ void beginStepKernel(uint32_t* words) {
     for (int p = 0; p < 8; ++p) words[kBatchSortTickets + p] = 0;
     words[kBatchEvaluated] = words[kBatchEvaluated + 1] = 0;
     words[kBatchDegenerate] = 0;
+    words[kBatchExpMin] = 0xFFu;
+    words[kBatchExpMax] = 0u;
 }
 
 // Block b's word of an epoch-tagged look-back: its aggregate (its inclusive
@@ -313,6 +315,7 @@ __global__ void __launch_bounds__(kProjThreads, 6)   // six blocks an SM: the ke
     const uint32_t i = gb * kProjThreads + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t area = 0;
+    uint32_t expByte = 0;   // the record's depth exponent byte, when its rect is on screen
     sHit[threadIdx.x] = 0u;
     if (i < B.count && gb < gaussBlocks) {
         // the record's gradient words, which the blend adjoint sums into, start at zero (a training step's)
@@ -351,7 +354,22 @@ __global__ void __launch_bounds__(kProjThreads, 6)   // six blocks an SM: the ke
                 area = cols * (ry1 - ry0 + 1);
                 sFa[threadIdx.x] = make_float4(G.cx, G.cy, G.ca, G.cb);
                 sFb[threadIdx.x] = make_float4(G.cc, G.cutoff, G.fr, G.fs);
-                sRect[threadIdx.x] = make_uint4(rx0, ry0, cols, (__float_as_uint(G.tz) >> 7) | (G.wide ? 1u << 31 : 0u));
+                // the depth field: the 24-bit depth key (exponent byte, 16 mantissa bits; z > 0),
+                // or with the exponent renumbered from the step's planned base, which keeps the
+                // order while every exponent lies in the plan's range
+                const uint32_t depthKey = __float_as_uint(G.tz) >> 7;
+                expByte = depthKey >> 16;
+                uint32_t field = depthKey;
+                if (B.depthBits < 24) {
+                    const uint32_t span = 1u << (B.depthBits - 16);
+                    uint32_t r = expByte - B.expBase;
+                    if (expByte < B.expBase || r >= span) {
+                        atomicOr(&words[kBatchStatus], kStatusDepthRange);
+                        r = expByte < B.expBase ? 0u : span - 1u;
+                    }
+                    field = (r << 16) | (depthKey & 0xFFFFu);
+                }
+                sRect[threadIdx.x] = make_uint4(rx0, ry0, cols, field | (G.wide ? 1u << 31 : 0u));
                 sInvCols[threadIdx.x] = 1.0f / (float)cols;
                 // the record (read only through the pairs, so written for any rect on screen);
                 // its colour once the block's pair count is published
@@ -359,6 +377,16 @@ __global__ void __launch_bounds__(kProjThreads, 6)   // six blocks an SM: the ke
                 recs[r + 0] = make_float4(G.cx, G.cy, G.tz, G.cutoff);
                 recs[r + 1] = make_float4(G.ca, G.fr, G.fs, G.alpha);
             }
+        }
+    }
+    {
+        // the step's range of depth exponents, for planning the next sizing's keys (an atomic
+        // only where this warp widens what the words already hold)
+        const uint32_t lo = __reduce_min_sync(0xFFFFFFFFu, area ? expByte : 0xFFu);
+        const uint32_t hi = __reduce_max_sync(0xFFFFFFFFu, area ? expByte : 0u);
+        if (lane == 0 && lo <= hi) {
+            if (lo < *reinterpret_cast<volatile uint32_t*>(&words[kBatchExpMin])) atomicMin(&words[kBatchExpMin], lo);
+            if (hi > *reinterpret_cast<volatile uint32_t*>(&words[kBatchExpMax])) atomicMax(&words[kBatchExpMax], hi);
         }
     }
     // the warp's candidate list: lane k's rect at [incl - area, incl)
@@ -653,8 +681,11 @@ struct ath_batch {
     uint32_t lastSorted = 0, lastSlotBits = 0;
     // scratch
     DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges;
-    uint32_t keyMode = 0;      // 0 packed when it fits in 64 bits, else wide; 1 packed; 2 wide
+    uint32_t keyMode = 0;      // 0 automatic; 1 packed; 2 wide; 3 packed, depth exponent renumbered
     bool lastWide = false;
+    // the pairs' form, planned by each sizing from its depths' exponents
+    bool planned = false, planWide = false;
+    uint32_t depthBits = 24, expBase = 0, lastDepthBits = 24, lastExpBase = 0;
     uint32_t count = 0;
     uint64_t capacity = 0;
     bool resize = true;
@@ -744,9 +775,11 @@ BatchConst batchConst(const ath_batch* b, const ath_mixed_params& P) {
     B.views = (uint32_t)b->views.size();
     B.count = P.count;
     B.tile = b->tile;
-    B.wide = wideKeys(b, P.count) ? 1u : 0u;
+    B.wide = (b->planned ? b->planWide : wideKeys(b, P.count)) ? 1u : 0u;
     B.slotBits = B.wide ? 0u : bitsForValues(std::max<uint64_t>(P.count, 2));
-    B.keyShift = 24 + B.slotBits;
+    B.depthBits = b->planned && !B.wide ? b->depthBits : 24u;
+    B.expBase = B.depthBits < 24 ? b->expBase : 0u;
+    B.keyShift = B.depthBits + B.slotBits;
     B.totalTiles = b->totalTiles;
     B.totalPixels = b->totalPixels;
     B.shLimit = b->shLimit;
@@ -819,7 +852,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     mark(1);
     uint64_t* keys[2] = {static_cast<uint64_t*>(b->pairs[0].ptr), static_cast<uint64_t*>(b->pairs[1].ptr)};
     uint32_t* vals[2] = {static_cast<uint32_t*>(b->values[0].ptr), static_cast<uint32_t*>(b->values[1].ptr)};
-    const uint32_t bits = 24 + b->tileBits;
+    const uint32_t bits = B.depthBits + b->tileBits;
     err = launchSortDevice(keys, B.wide ? vals : nullptr, (uint32_t)b->capacity, words + kBatchPairsLo,
                            words + kBatchEpoch, B.slotBits, bits, static_cast<uint32_t*>(b->sortHist.ptr),
                            static_cast<uint64_t*>(b->sortFlags.ptr), words + kBatchSortTickets, words + kBatchStatus,
@@ -829,6 +862,8 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     b->lastSorted = sorted;
     b->lastSlotBits = B.slotBits;
     b->lastWide = B.wide != 0;
+    b->lastDepthBits = B.depthBits;
+    b->lastExpBase = B.expBase;
     if (err == cudaSuccess) err = cudaMemsetAsync(b->ranges.ptr, 0, (size_t)b->totalTiles * 8, stream);
     if (err == cudaSuccess) {
         const uint32_t grid = std::max<uint32_t>(
@@ -887,7 +922,40 @@ ath_status sizePairs(ath_batch* b, const ath_mixed_params& P, cudaStream_t strea
     const uint64_t pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
     const uint64_t want = pairs + pairs / 7 + 65536;
     if (want > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 pairs in one batched step");
-    const bool wide = wideKeys(b, b->count);
+    // The pairs' form: packed with the 24-bit depth key while tile, depth and Gaussian
+    // bits fit in 64; else packed with the depth's exponent byte renumbered from a base
+    // two below the least exponent seen here, in the fewest bits that hold two above
+    // the greatest (a step whose depths leave that range reports it, and the next
+    // step plans again); else wide.
+    const uint32_t slot = bitsForValues(std::max<uint64_t>(b->count, 2));
+    const uint32_t eLo = w[kBatchExpMin], eHi = w[kBatchExpMax];
+    uint32_t depthBits = 24, expBase = 0;
+    auto renumbered = [&]() {
+        const uint32_t lo = eLo <= eHi && eLo > 2 ? eLo - 2 : 0;
+        const uint32_t hi = eLo <= eHi ? std::min(255u, eHi + 2) : 0;
+        const uint32_t e = bitsForValues(hi - lo + 1);
+        if (16 + e + slot + b->tileBits > 64) return false;
+        depthBits = 16 + e;
+        expBase = lo;
+        return true;
+    };
+    bool wide;
+    if (b->keyMode == 2) {
+        wide = true;
+    } else if (b->keyMode == 1) {
+        wide = false;
+    } else if (b->keyMode == 3) {
+        if (!renumbered())
+            return fail(ATH_E_UNSUPPORTED, "tiles, the renumbered depth and the Gaussian index exceed 64 bits "
+                                           "(packed keys asked for; the wide form has no such limit)");
+        wide = false;
+    } else {
+        wide = 24 + slot + b->tileBits > 64 && !renumbered();
+    }
+    b->planned = true;
+    b->planWide = wide;
+    b->depthBits = wide ? 24u : depthBits;
+    b->expBase = wide ? 0u : expBase;
     if (want > b->capacity || !b->pairs[0].ptr || (wide && !b->values[0].ptr)) {
         const uint64_t room = std::max<uint64_t>(want, b->capacity);
         for (int k = 0; k < 2; ++k) {
@@ -897,7 +965,7 @@ ath_status sizePairs(ath_batch* b, const ath_mixed_params& P, cudaStream_t strea
         }
         b->capacity = room;
     }
-    const uint32_t bits = 24 + b->tileBits;
+    const uint32_t bits = b->depthBits + b->tileBits;
     err = b->sortFlags.reserve(sortFlagWords((uint32_t)b->capacity, bits) * 8);
     if (err != cudaSuccess) return failCuda(err, "reserving the sort's look-back words");
     // the look-back words carry epochs: start them all at "not ready"
@@ -984,7 +1052,7 @@ extern "C" ath_status ath_batch_set_views(ath_batch* b, const ath_view* views, u
 
 extern "C" ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode) {
     if (!b) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_key_mode: null batch");
-    if (mode > 2) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_key_mode: mode must be 0, 1 or 2");
+    if (mode > 3) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_key_mode: mode must be 0, 1, 2 or 3");
     if (mode != b->keyMode) {
         b->keyMode = mode;
         b->resize = true;   // the next step sizes (and, for wide pairs, allocates) again
@@ -1033,6 +1101,9 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
     if (b->keyMode == 1 && 24 + slotBits + b->tileBits > 64)
         return fail(ATH_E_UNSUPPORTED, std::string(what) + ": tiles, depth key and Gaussian index exceed 64 bits "
                                        "(packed keys asked for; the wide form has no such limit)");
+    if (b->keyMode == 3 && 17 + slotBits + b->tileBits > 64)
+        return fail(ATH_E_UNSUPPORTED, std::string(what) + ": tiles, a renumbered depth and Gaussian index exceed "
+                                       "64 bits (packed keys asked for; the wide form has no such limit)");
     if (24 + b->tileBits > 64)
         return fail(ATH_E_UNSUPPORTED, std::string(what) + ": more than 2^40 tiles");
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
@@ -1134,6 +1205,11 @@ extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* 
             b->resize = true;   // the next step sizes the pairs again
             return fail(ATH_E_CAPACITY, "a step had more pairs than its buffers; the next step grows them");
         }
+        if (bits & kStatusDepthRange) {
+            b->resize = true;   // the next step plans the pairs' depth field again
+            return fail(ATH_E_CAPACITY, "a step's depths left the exponent range its pair keys were planned for "
+                                        "(that step's order is not valid); the next step plans them again");
+        }
         if (bits & kStatusLookbackTimeout) return fail(ATH_E_TIMEOUT, "a look-back wait of a batched step gave up");
         return fail(ATH_E_INTERNAL, "a batched step met an index outside its buffers");
     }
@@ -1168,7 +1244,9 @@ extern "C" ath_status ath_batch_buffers_of(ath_batch* b, ath_batch_buffers* out,
     if (err == cudaSuccess) err = cudaStreamSynchronize(static_cast<cudaStream_t>(streamPtr));
     if (err != cudaSuccess) return failCuda(err, "ath_batch_buffers_of");
     out->pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
-    out->key_shift = 24 + b->lastSlotBits;
+    out->key_shift = b->lastDepthBits + b->lastSlotBits;
+    out->depth_bits = b->lastDepthBits;
+    out->exp_base = b->lastExpBase;
     out->slot_bits = b->lastSlotBits;
     out->sorted_values = b->lastWide ? static_cast<const uint32_t*>(b->values[b->lastSorted].ptr) : nullptr;
     out->total_tiles = b->totalTiles;

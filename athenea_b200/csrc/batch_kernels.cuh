@@ -31,8 +31,10 @@ struct BatchConst {
     uint32_t count;          // Gaussians
     uint32_t tile;           // 8, 16 or 32
     uint32_t slotBits;       // bits of a Gaussian index in a packed pair (0 when wide)
-    uint32_t keyShift;       // where the global tile starts in a pair's key: 24 + slotBits, or 24 when wide
+    uint32_t keyShift;       // where the global tile starts in a pair's key: depthBits + slotBits
     uint32_t wide;           // 1: key (tile << 24 | depth) and a separate u32 Gaussian index a pair
+    uint32_t depthBits;      // a pair's depth field: 24 (the depth key), or 16 + e bits for a key whose
+    uint32_t expBase;        // exponent byte is renumbered from expBase (e bits; packed pairs only)
     uint32_t totalTiles, totalPixels;
     uint32_t shLimit, antialias, linear, restPerColour;
     uint32_t depthMode;      // a render's depth: 0 the alpha-weighted mean, 1 the first threshold crossing
@@ -54,6 +56,8 @@ enum BatchWord : uint32_t {
     kBatchSortTickets = 8,   // one a sort pass (8)
     kBatchEvaluated = 16,    // 64-bit (16, 17): (pixel, record) evaluations of the forward blend
     kBatchDegenerate = 18,   // records whose conic took the FP64 path
+    kBatchExpMin = 22,       // least and greatest exponent byte of the depths of the records on
+    kBatchExpMax = 23,       // screen (for planning a renumbered depth key)
     kBatchWords = 32,
 };
 

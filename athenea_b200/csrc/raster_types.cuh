@@ -64,6 +64,7 @@ enum StatusBit : uint32_t {
     kStatusLookbackTimeout = 1u,   // a look-back gave up waiting (bounded spin)
     kStatusPairOverflow = 2u,      // more pairs than the pair buffers hold
     kStatusIndexRange = 4u,        // a data-dependent index fell outside its buffer (skipped)
+    kStatusDepthRange = 8u,        // a depth's exponent outside the range a step's pair keys were planned for
 };
 
 // The backward's gradient with respect to one record: ten floats a slot.

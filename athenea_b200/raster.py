@@ -551,7 +551,7 @@ class BatchTrainer:
         check(N.lib().ath_batch_set_tuning(self._h, tile, block_batch))
 
     def set_key_mode(self, mode: int) -> None:
-        """ath_batch_set_key_mode: 0 packed while it fits in 64 bits, 1 packed, 2 wide."""
+        """ath_batch_set_key_mode: 0 automatic, 1 packed, 2 wide, 3 packed with the depth exponent renumbered."""
         check(N.lib().ath_batch_set_key_mode(self._h, mode))
 
     def step(self, params: MixedParams, target: torch.Tensor, colour: torch.Tensor, loss: torch.Tensor,
@@ -605,4 +605,5 @@ class BatchTrainer:
         check(N.lib().ath_batch_buffers_of(self._h, C.byref(b), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
         return dict(pairs=b.pairs, key_shift=b.key_shift, slot_bits=b.slot_bits, total_tiles=b.total_tiles,
                     sorted_pairs=b.sorted_pairs, ranges=b.ranges, sorted_values=b.sorted_values,
-                    tile_bases=[b.tile_bases[k] for k in range(b.views)])
+                    tile_bases=[b.tile_bases[k] for k in range(b.views)], depth_bits=b.depth_bits,
+                    exp_base=b.exp_base)

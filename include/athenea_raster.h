@@ -311,11 +311,18 @@ ath_status ath_batch_set_tuning(ath_batch* b, uint32_t tile, uint32_t block_batc
 ath_status ath_batch_pixels(ath_batch* b, uint32_t* pixels);
 /* How a step's (tile, Gaussian) pairs are keyed. 0 (default): one 64-bit word
  * (global tile | 24-bit depth key | Gaussian index), sorted keys-only, while
- * those bits fit in 64, else 1 the wide form; 1: always the packed word (a step
- * whose bits do not fit fails with ATH_E_UNSUPPORTED); 2: the wide form, a
- * 64-bit (global tile << 24 | depth key) key and a 32-bit Gaussian index,
- * sorted as key and value (50M Gaussians in 8 views of 3840x2160 need it). The
- * pairs' order, and so the image, is the same either way. */
+ * those bits fit in 64; else the packed word with the depth key's exponent byte
+ * renumbered (below) while that fits; else the wide form. 1: always the packed
+ * word with the 24-bit depth key (a step whose bits do not fit fails with
+ * ATH_E_UNSUPPORTED). 2: the wide form, a 64-bit (global tile << 24 | depth key)
+ * key and a 32-bit Gaussian index, sorted as key and value. 3: always the packed
+ * word with the renumbered depth. Renumbered: the depth field is 16 mantissa bits
+ * under the exponent byte less a base, in as few bits as the exponents a sizing
+ * saw (with two to spare on each side) need; the order is the depth key's. A
+ * step whose depths fall outside that range is reported by ath_batch_check as
+ * ATH_E_CAPACITY (that step's order is not valid) and the next step plans again.
+ * 50M Gaussians in 8 views of 3840x2160 take the renumbered form. The pairs'
+ * order, and so the image, is the same in every form. */
 ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode);
 /* One training step over every view, with nothing read back to the host:
  * project and emit every view's pairs (one launch), sort them all (one packed
@@ -362,10 +369,11 @@ ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params* params, c
 
 /* The last step's sorted pairs and tile ranges, for inspection: device
  * pointers the batch owns, valid until its next step. A packed pair is
- * (global tile << key_shift) | (24-bit depth key << slot_bits) | Gaussian; a
- * wide pair's key is (global tile << 24) | depth key (slot_bits 0, key_shift 24)
- * with its Gaussian in sorted_values. View v's tiles start at tile_bases[v]
- * (host array of `views` entries). */
+ * (global tile << key_shift) | (depth field << slot_bits) | Gaussian; a wide
+ * pair's key is (global tile << 24) | depth key (slot_bits 0, key_shift 24) with
+ * its Gaussian in sorted_values. The depth field is the 24-bit depth key when
+ * depth_bits is 24, else ((exponent byte - exp_base) << 16) | its 16 low bits.
+ * View v's tiles start at tile_bases[v] (host array of `views` entries). */
 typedef struct {
     uint64_t pairs;
     uint32_t key_shift, slot_bits, total_tiles, views;
@@ -373,6 +381,7 @@ typedef struct {
     const uint32_t* ranges;      /* 2 a global tile: [start, end) */
     const uint32_t* sorted_values; /* wide pairs: the Gaussian of each sorted pair; NULL when packed */
     const uint32_t* tile_bases;  /* host */
+    uint32_t depth_bits, exp_base;
 } ath_batch_buffers;
 
 ath_status ath_batch_buffers_of(ath_batch* b, ath_batch_buffers* out, void* stream);

@@ -73,6 +73,14 @@ def _batched(M, views, targets, tile=16, block_batch=256, trainer=None):
     return b, colour, loss, grads, stats
 
 
+def _depth_keys(field, buf):
+    """The 24-bit depth keys of packed pairs' depth fields: as they are, or with the
+    renumbered exponent (depth_bits < 24) put back from exp_base."""
+    if buf["depth_bits"] >= 24:
+        return field
+    return (((field >> np.uint64(16)) + np.uint64(buf["exp_base"])) << np.uint64(16)) | (field & np.uint64(0xFFFF))
+
+
 def _same_pairs(b, frames):
     """The batched step's sorted pairs and tile ranges against the plain path's, view by view, to the bit."""
     from tests import gpu_helpers as G
@@ -83,7 +91,7 @@ def _same_pairs(b, frames):
     tiles = (keys >> np.uint64(buf["key_shift"])).astype(np.int64)
     if buf["sorted_values"] is None:
         splats = (keys & np.uint64((1 << buf["slot_bits"]) - 1)).astype(np.uint32)
-        depths = (keys >> np.uint64(buf["slot_bits"])) & np.uint64(0xFFFFFF)
+        depths = _depth_keys((keys >> np.uint64(buf["slot_bits"])) & np.uint64((1 << buf["depth_bits"]) - 1), buf)
     else:
         splats = G.fetch(buf["sorted_values"], (buf["pairs"],), np.uint32)
         depths = keys & np.uint64(0xFFFFFF)
@@ -214,6 +222,58 @@ def test_wide_pairs_sort_and_draw_as_the_packed_ones():
         assert np.abs(a - c).max() <= 1e-5 * (np.abs(c).max() + 1e-30) + 1e-12, name
 
 
+def test_renumbered_depth_pairs_sort_and_draw_as_the_plain_path():
+    """Key mode 3: the packed pairs' depth field holds the depth key's exponent
+    byte renumbered from the sizing's planned base. The sorted pairs and ranges
+    are the plain path's to the bit, and the image is the 24-bit packed form's."""
+    Pq, M = _scene(40_000, 13)
+    views = _views()
+    gen = torch.Generator().manual_seed(7)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    _, frames, _, _ = _plain(Pq, views, targets)
+    b = BatchTrainer()
+    b.set_key_mode(3)
+    b, colour, _, _, stats = _batched(M, views, targets, trainer=b)
+    buf = b.buffers()
+    assert buf["depth_bits"] < 24 and buf["sorted_values"] is None
+    assert buf["key_shift"] == buf["depth_bits"] + buf["slot_bits"]
+    assert stats["pairs"] == sum(f["pairs"] for f in frames)
+    _same_pairs(b, frames)
+    b1 = BatchTrainer()
+    b1.set_key_mode(1)
+    _, colour1, _, _, _ = _batched(M, views, targets, trainer=b1)
+    np.testing.assert_array_equal(colour.cpu().numpy(), colour1.cpu().numpy())
+
+
+def test_depths_leaving_the_planned_range_are_reported_and_planned_again():
+    """A renumbered depth field covers the exponents its sizing saw, two to spare
+    on each side. A step whose cloud has moved eight times nearer the eye falls
+    outside: ath_batch_check reports Capacity, and the next step plans again and
+    draws what a new trainer draws."""
+    _, M = _scene(20_000, 14)
+    views = _views(1)
+    gen = torch.Generator().manual_seed(8)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    b = BatchTrainer()
+    b.set_key_mode(3)
+    b, colour, loss, grads, _ = _batched(M, views, targets, trainer=b)
+    planned = b.buffers()["exp_base"]
+    eye = torch.tensor(scenes.circle_eye(0, 8, 3.0, 0.3), dtype=torch.float32, device="cuda")
+    with torch.no_grad():
+        M.means[:, :3] = eye + (M.means[:, :3] - eye) * 0.125   # in place: the same arrays
+    target = torch.cat(targets).contiguous()
+    b.step(M, target, colour, loss, grads)
+    with pytest.raises(A.AtheneaError) as e:
+        b.check()
+    assert e.value.name == "Capacity"
+    b.step(M, target, colour, loss, grads)
+    b.check()
+    assert b.buffers()["exp_base"] < planned
+    _, fresh, _, _, _ = _batched(M, views, targets)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(colour.cpu().numpy(), fresh.cpu().numpy())
+
+
 def _sorted_pairs(b):
     """(tile, depth, Gaussian) of the batched step's sorted pairs, and its ranges."""
     from tests import gpu_helpers as G
@@ -223,19 +283,19 @@ def _sorted_pairs(b):
     tiles = (keys >> np.uint64(buf["key_shift"])).astype(np.int64)
     if buf["sorted_values"] is None:
         splats = (keys & np.uint64((1 << buf["slot_bits"]) - 1)).astype(np.int64)
-        depths = ((keys >> np.uint64(buf["slot_bits"])) & np.uint64(0xFFFFFF)).astype(np.int64)
+        depths = _depth_keys((keys >> np.uint64(buf["slot_bits"])) & np.uint64((1 << buf["depth_bits"]) - 1),
+                             buf).astype(np.int64)
     else:
         splats = G.fetch(buf["sorted_values"], (n,), np.uint32).astype(np.int64)
         depths = (keys & np.uint64(0xFFFFFF)).astype(np.int64)
     return tiles, depths, splats, G.fetch(buf["ranges"], (buf["total_tiles"], 2), np.uint32).astype(np.int64)
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 def test_dense_tiles_sort_as_the_plain_path(mode):
-    """A cloud squeezed to a few tiles: buckets of every size the bucket sort has
-    (a warp's, a block's, and past a block's, sorted in chunks through global
-    memory), in packed and wide pairs, against the plain path's pairs to the bit
-    (at its tile size, 16)."""
+    """A cloud squeezed to a few tiles (tiles of a few pairs up to tens of
+    thousands), in packed, wide and renumbered-depth pairs, against the plain
+    path's pairs to the bit (at its tile size, 16)."""
     Pq, M = _scene(40_000, 21, squeeze=0.04)
     views = _views()
     gen = torch.Generator().manual_seed(8)
