@@ -379,8 +379,8 @@ __global__ void __launch_bounds__(kProjThreads, 6)   // six blocks an SM: the ke
             }
         }
     }
-    {
-        // the step's range of depth exponents, for planning the next sizing's keys (an atomic
+    if (B.sizing) {
+        // the depths' range of exponents, for planning the pairs' depth field (an atomic
         // only where this warp widens what the words already hold)
         const uint32_t lo = __reduce_min_sync(0xFFFFFFFFu, area ? expByte : 0xFFu);
         const uint32_t hi = __reduce_max_sync(0xFFFFFFFFu, area ? expByte : 0u);
@@ -835,7 +835,10 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], stream); };
     mark(0);
     BatchConst B = batchConst(b, P);
-    if (countOnly) B.capacity = 0;
+    if (countOnly) {
+        B.capacity = 0;
+        B.sizing = 1;
+    }
     uint32_t* words = static_cast<uint32_t*>(b->words.ptr);
     const uint32_t V = B.views;
     const uint32_t gaussBlocks = (P.count + kProjThreads - 1) / kProjThreads;

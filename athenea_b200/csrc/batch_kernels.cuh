@@ -35,6 +35,7 @@ struct BatchConst {
     uint32_t wide;           // 1: key (tile << 24 | depth) and a separate u32 Gaussian index a pair
     uint32_t depthBits;      // a pair's depth field: 24 (the depth key), or 16 + e bits for a key whose
     uint32_t expBase;        // exponent byte is renumbered from expBase (e bits; packed pairs only)
+    uint32_t sizing;         // 1: the sizing pass (counts only; it also records the depths' exponent range)
     uint32_t totalTiles, totalPixels;
     uint32_t shLimit, antialias, linear, restPerColour;
     uint32_t depthMode;      // a render's depth: 0 the alpha-weighted mean, 1 the first threshold crossing
