@@ -280,7 +280,7 @@ __device__ __forceinline__ uint32_t ownerOf(uint32_t incl, uint32_t q) {
 constexpr uint32_t kBallotCache = 16;   // chunks of 32 candidates whose ballots a warp keeps
 
 template <uint32_t L>
-__global__ void __launch_bounds__(kProjThreads, 6)   // six blocks an SM: the kernel is latency-bound
+__global__ void __launch_bounds__(kProjThreads, 5)   // five blocks an SM: the kernel is latency-bound
     projectEmitKernel(const BatchConst B, const BatchView* __restrict__ views, float4* __restrict__ recs,
                       uint64_t* __restrict__ pairs, uint32_t* __restrict__ values, uint64_t* __restrict__ flags,
                       uint32_t* __restrict__ words, float* __restrict__ grads, uint32_t gaussBlocks) {
