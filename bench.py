@@ -300,6 +300,10 @@ def run_ours(args) -> dict | None:
     stats = bt.check()   # raises if a timed step overflowed its buffers or a wait gave up
     stages = bt.time_stages(mixed, target, colour, loss, grads, stream=stream)
     stats = bt.check()
+    buf = bt.buffers()   # the pairs' form the sizing chose
+    pair_form = ("wide: 64-bit (tile, depth) key and 32-bit Gaussian" if buf["sorted_values"] is not None else
+                 "packed 64-bit word, 24-bit depth key" if buf["depth_bits"] >= 24 else
+                 f"packed 64-bit word, depth exponent renumbered ({buf['depth_bits']}-bit depth field)")
 
     # e2e through the public API: each step's target images copied in from pinned
     # host memory into one of two device buffers on a copy stream (overlapping the
@@ -392,14 +396,14 @@ def run_ours(args) -> dict | None:
 
     T = tuned["tile"]
     total_tiles = sum(((W + T - 1) // T) * ((H + T - 1) // T) for _, W, H in views)
-    passes = math.ceil((24 + max(1, math.ceil(math.log2(max(2, total_tiles))))) / 8)
+    passes = math.ceil((buf["depth_bits"] + max(1, math.ceil(math.log2(max(2, total_tiles))))) / 8)
     # the step's kernels: begin, projectEmit, histogram, the sort's passes, ranges,
     # the blends (forward, loss and adjoint), projection adjoint (memsets are not counted)
     launches = (2 + 1 + passes + 1 + 1 + 1) * args.steps
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
                ms_render=ms_render,
                stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
-               count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4,
+               count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4, pair_form=pair_form,
                pixels=int(pixel_base[-1]), sizes=sorted({(W, H) for _, W, H in views}))
     if world > 1:
         dist.barrier()
@@ -531,7 +535,7 @@ def main():
         "config": {"workload": WORKLOAD["name"], "gaussians": WORKLOAD["count"],
                    "sizes": [f"{w}x{h}" for w, h in res["sizes"]], "pixels_per_gpu": res["pixels"],
                    "views_per_gpu": V, "sh_degree": 3, "tile": res["tuned"]["tile"],
-                   "block_batch": res["tuned"]["block_batch"],
+                   "block_batch": res["tuned"]["block_batch"], "pair_form": res["pair_form"],
                    "path": "batched mixed-precision step: every view in one launch a stage, replayed from a CUDA "
                            "graph; forward, mean-L2 loss, backward to FP32 gradients",
                    "loss": "mean L2 a view against a target uniform in [0,1]^3, summed over views",
