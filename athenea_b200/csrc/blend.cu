@@ -81,8 +81,8 @@ struct CryptoList {
     }
 };
 
-// kContribution: the contributionMode hooks of splat_blend.slang:364-398 (modes
-// 1 and 4). kUnder: the composite over an opaque layer under the splats
+// kContribution: the contributionMode hooks of splat_blend.slang:364-407 (modes
+// 1 to 4). kUnder: the composite over an opaque layer under the splats
 // (:249-251,329-333,516-523,555-575): a pixel's walk stops at the first record
 // at or behind the layer's depth, and the layer takes the rest of the pixel.
 // The plain frame builds without either.
@@ -152,6 +152,30 @@ __global__ void __launch_bounds__(kBlendThreads)
                 const uint32_t slot = sSlot[j];
                 if (contrib.mode == 1u) {
                     atomicAdd(&contrib.words[slot], (uint32_t)(weight * 4096.0f + 0.5f));
+                } else if (contrib.mode == 2u) {
+                    // splat_blend.slang:366-380: the pixel with the splat taken away shows what is
+                    // behind it, recovered from the whole frame; the squared change, capped at one,
+                    // in 2^-24 into a 64-bit sum of two words (low, then its carries)
+                    const uint32_t at = py * F.width + px;
+                    const float4 whole = reinterpret_cast<const float4*>(contrib.finalColour)[at];
+                    const float4 c = sColour[j];
+                    const float after = fmaxf(T * (1.0f - alpha), 1.0e-4f);
+                    const float cx = weight * (c.x - (whole.x - (r + weight * c.x)) / after);
+                    const float cy = weight * (c.y - (whole.y - (g + weight * c.y)) / after);
+                    const float cz = weight * (c.z - (whole.z - (bl + weight * c.z)) / after);
+                    const float d2 = (cx * cx + cy * cy) + cz * cz;
+                    const uint32_t add = (uint32_t)(fminf(d2, 1.0f) * 16777216.0f + 0.5f);
+                    const uint32_t before = atomicAdd(&contrib.words[slot * 2], add);
+                    if (before + add < before) atomicAdd(&contrib.words[slot * 2 + 1], 1u);
+                } else if (contrib.mode == 3u) {
+                    // splat_blend.slang:399-407: the weight, and the weight times the mask, in 1/1024
+                    const uint32_t seen = (uint32_t)(weight * 1024.0f + 0.5f);
+                    if (seen != 0u) {
+                        atomicAdd(&contrib.words[slot * 2 + 1], seen);
+                        const float m = fminf(fmaxf(contrib.liftMask[py * F.width + px], 0.0f), 1.0f);
+                        const uint32_t within = (uint32_t)((weight * m) * 1024.0f + 0.5f);
+                        if (within != 0u) atomicAdd(&contrib.words[slot * 2], within);
+                    }
                 } else {
                     const uint32_t at = py * F.width + px;
                     const float4 dl = reinterpret_cast<const float4*>(contrib.finalColour)[at];

@@ -372,10 +372,14 @@ ath_status checkFrame(const ath_settings& s, const ath_targets& targets) {
     if (targets.width != s.width || targets.height != s.height)
         return fail(ATH_E_INVALID_ARGUMENT, "the targets are not the frame's size");
     if (!targets.colour || !targets.depth) return fail(ATH_E_INVALID_ARGUMENT, "the targets need colour and depth");
-    if (s.contribution_mode != 0 && s.contribution_mode != 1 && s.contribution_mode != 4)
-        return fail(ATH_E_UNSUPPORTED, "contribution modes 2 and 3 are not built; 1 and 4 are");
+    if (s.contribution_mode > 4)
+        return fail(ATH_E_UNSUPPORTED, "contribution modes are 0 to 4 (TileRasterizer.h:357-366)");
     if (s.contribution_mode != 0 && !s.contribution)
         return fail(ATH_E_INVALID_ARGUMENT, "a contribution mode needs its contribution buffer");
+    if (s.contribution_mode == 2 && !s.final_colour)
+        return fail(ATH_E_INVALID_ARGUMENT, "contribution mode 2 needs final_colour (the frame drawn whole)");
+    if (s.contribution_mode == 3 && !s.lift_mask)
+        return fail(ATH_E_INVALID_ARGUMENT, "contribution mode 3 needs lift_mask (a float a pixel)");
     if (s.contribution_mode == 4 && !s.final_colour)
         return fail(ATH_E_INVALID_ARGUMENT, "contribution mode 4 needs final_colour (dL/dpixel)");
     if ((s.crypto != nullptr) != (s.crypto_ids != nullptr))
@@ -472,7 +476,7 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
                           targets->depth, reinterpret_cast<float4*>(targets->position),
                           training ? static_cast<float*>(r->finalT.ptr) : nullptr,
                           training ? static_cast<uint32_t*>(r->lastContrib.ptr) : nullptr, words + kWordSticky, stream,
-                          Contribution{s.contribution_mode, s.contribution, s.final_colour},
+                          Contribution{s.contribution_mode, s.contribution, s.final_colour, s.lift_mask},
                           under ? Under{under->colour, under->depth} : Under{},
                           Matte{s.crypto_ids, s.crypto, under ? s.under_crypto : nullptr});
     mark(5);

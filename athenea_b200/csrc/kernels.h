@@ -47,9 +47,10 @@ cudaError_t launchSortDevice(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, c
 // blend.cu
 // The reference's contributionMode hooks of the blend (modes 1 and 4).
 struct Contribution {
-    uint32_t mode = 0;                   // 0 none, 1 weights, 4 colour gradients
+    uint32_t mode = 0;                   // 0 none, 1 weights, 2 squared change, 3 lifted mask, 4 colour gradients
     uint32_t* words = nullptr;
-    const float* finalColour = nullptr;  // mode 4: dL/dpixel, float4 a pixel
+    const float* finalColour = nullptr;  // float4 a pixel: mode 2 the whole frame, mode 4 dL/dpixel
+    const float* liftMask = nullptr;     // mode 3: a float a pixel
 };
 
 // An opaque layer under the splats (TileRasterizer::render's `under`): its

@@ -210,12 +210,13 @@ class RenderSettings:
     time_stages: bool = False
     count_splats: bool = False
     counters_tag: int = 0
-    contribution_mode: int = 0    # 1 weights, 4 colour gradients (TileRasterizer.h:351-367)
-    contribution: torch.Tensor | None = None    # int32: a word a slot (mode 1) or four (mode 4)
-    final_colour: torch.Tensor | None = None    # float4 a pixel: dL/dpixel for mode 4
+    contribution_mode: int = 0    # 1 weights, 2 squared change, 3 lifted mask, 4 colour gradients (TileRasterizer.h:351-371)
+    contribution: torch.Tensor | None = None    # int32: a word a slot (mode 1), two (modes 2, 3) or four (mode 4)
+    final_colour: torch.Tensor | None = None    # float4 a pixel: the whole frame (mode 2) or dL/dpixel (mode 4)
     crypto_ids: torch.Tensor | None = None      # int32 a slot: the Cryptomatte id (0 names nothing)
     crypto: torch.Tensor | None = None          # (3, height * width, 4) float32: the matte's layers
     under_crypto: torch.Tensor | None = None    # int32 a pixel: the under layer's id
+    lift_mask: torch.Tensor | None = None       # float a pixel, 0 to 1: mode 3's mask
 
     def _native(self) -> N.Settings:
         s = N.Settings()
@@ -237,6 +238,7 @@ class RenderSettings:
         s.crypto_ids = _ptr(self.crypto_ids) if self.crypto_ids is not None else None
         s.crypto = _ptr(self.crypto) if self.crypto is not None else None
         s.under_crypto = _ptr(self.under_crypto) if self.under_crypto is not None else None
+        s.lift_mask = _ptr(self.lift_mask) if self.lift_mask is not None else None
         return s
 
 

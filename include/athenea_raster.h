@@ -123,12 +123,17 @@ typedef struct {
     /* What each splat gave the frame, added into `contribution` (device memory,
      * never cleared here, so frames from many cameras sum into it), in the
      * reference's contributionMode (TileRasterizer.h:351-367,
-     * splat_blend.slang:364-398): 0 nothing; 1 a uint a slot, the transmittance
-     * times alpha it blended with summed over its pixels, in 1/4096; 4 four
-     * words a slot, three signed (the weight times `final_colour`, here a
-     * loss's derivative at each pixel, float4 a pixel, summed in 1/256 with
-     * hash-dithered rounding) and the weight in 1/256. Slots are the instances'
-     * splats one after another. Modes 2 and 3 are ATH_E_UNSUPPORTED. */
+     * splat_blend.slang:364-407): 0 nothing; 1 a uint a slot, the transmittance
+     * times alpha it blended with summed over its pixels, in 1/4096; 2 two
+     * uint a slot (low, then high word of one 64-bit sum), the squared colour
+     * change taking the splat away would leave in each pixel, capped at one, in
+     * 2^-24, against `final_colour`, the frame drawn whole from the same camera
+     * (float4 a pixel, as the colour target holds it); 3 two uint a slot, the
+     * weight times `lift_mask` (one float a pixel, 0 to 1) and the weight, in
+     * 1/1024; 4 four words a slot, three signed (the weight times
+     * `final_colour`, here a loss's derivative at each pixel, float4 a pixel,
+     * summed in 1/256 with hash-dithered rounding) and the weight in 1/256.
+     * Slots are the instances' splats one after another. */
     uint32_t contribution_mode;
     uint32_t* contribution;
     const float* final_colour;
@@ -141,6 +146,7 @@ typedef struct {
     const uint32_t* crypto_ids;
     float* crypto;
     const uint32_t* under_crypto;
+    const float* lift_mask;     /* contribution mode 3's mask: one float a pixel, 0 to 1 */
 } ath_settings;
 
 /* RenderTargets (TileRasterizer.h:421-450) plus the P layer

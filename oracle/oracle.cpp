@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -572,7 +573,9 @@ struct Walk {
 };
 
 // underZ > 0: an opaque layer under the splats at that depth ends the walk at
-// the first record at or behind it (splat_blend.slang:249-251,329-333).
+// the first record at or behind it (splat_blend.slang:249-251,329-333). `visit`
+// sees each blended splat before the walk adds it: (slot, weight), or (slot,
+// weight, the walk so far, alpha, the record) where it takes those.
 template <typename Visit>
 Walk walkPixel(const orc_frame& f, uint32_t start, uint32_t end, const uint32_t* pairSplats, const float* records,
                float pxc, float pyc, Visit visit, float underZ = 0.0f) {
@@ -589,7 +592,10 @@ Walk walkPixel(const orc_frame& f, uint32_t start, uint32_t end, const uint32_t*
         const float alpha = std::min(0.99f, falloffAlpha(std::fabs(rec[7]), expf_((-0.5f) * power)));
         if (alpha < 1.0f / 255.0f) continue;
         const float weight = wk.t * alpha;
-        visit(s, weight);
+        if constexpr (std::is_invocable_v<Visit, uint32_t, float, const Walk&, float, const float*>)
+            visit(s, weight, static_cast<const Walk&>(wk), alpha, rec);
+        else
+            visit(s, weight);
         for (int k = 0; k < 3; ++k) wk.rgb[k] = wk.rgb[k] + weight * rec[8 + k];
         wk.depthSum = wk.depthSum + weight * rec[2];
         wk.t = wk.t * (1.0f - alpha);
@@ -1099,6 +1105,62 @@ void orc_contribution_weight(const orc_frame* f, const uint32_t* ranges, const u
                           (float)py + 0.5f, [&](uint32_t s, float weight) {
                               // splat_blend.slang:364-365
                               contribution[s] += (uint32_t)(weight * 4096.0f + 0.5f);
+                          });
+            }
+        }
+    }
+}
+
+void orc_contribution_change(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                             const float* records, const float* wholeFrame, uint32_t* contribution) {
+    // splat_blend.slang:366-380, summed in 64 bits a slot and written as (low, high) words
+    const uint32_t tiles = f->tilesX * f->tilesY;
+    uint32_t slots = 0;
+    for (uint32_t t = 0; t < tiles; ++t)
+        for (uint32_t j = ranges[t * 2]; j < ranges[t * 2 + 1]; ++j) slots = std::max(slots, pairSplats[j] + 1);
+    std::vector<uint64_t> sums(slots, 0);
+    for (uint32_t t = 0; t < tiles; ++t) {
+        const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
+        for (uint32_t ly = 0; ly < kTile; ++ly) {
+            for (uint32_t lx = 0; lx < kTile; ++lx) {
+                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+                if (px >= f->width || py >= f->height) continue;
+                const float* whole = wholeFrame + (size_t)(py * f->width + px) * 4;
+                walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
+                          (float)py + 0.5f, [&](uint32_t s, float weight, const Walk& wk, float alpha, const float* rec) {
+                              const float after = std::fmax(wk.t * (1.0f - alpha), 1.0e-4f);
+                              float ch[3];
+                              for (int k = 0; k < 3; ++k)
+                                  ch[k] = weight * (rec[8 + k] - (whole[k] - (wk.rgb[k] + weight * rec[8 + k])) / after);
+                              const float d2 = (ch[0] * ch[0] + ch[1] * ch[1]) + ch[2] * ch[2];
+                              sums[s] += (uint32_t)(std::fmin(d2, 1.0f) * 16777216.0f + 0.5f);
+                          });
+            }
+        }
+    }
+    for (uint32_t s = 0; s < slots; ++s) {
+        contribution[s * 2] += (uint32_t)sums[s];
+        contribution[s * 2 + 1] += (uint32_t)(sums[s] >> 32);
+    }
+}
+
+void orc_contribution_lift(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                           const float* records, const float* liftMask, uint32_t* contribution) {
+    // splat_blend.slang:399-407
+    const uint32_t tiles = f->tilesX * f->tilesY;
+    for (uint32_t t = 0; t < tiles; ++t) {
+        const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
+        for (uint32_t ly = 0; ly < kTile; ++ly) {
+            for (uint32_t lx = 0; lx < kTile; ++lx) {
+                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+                if (px >= f->width || py >= f->height) continue;
+                const float m = std::fmin(std::fmax(liftMask[py * f->width + px], 0.0f), 1.0f);
+                walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
+                          (float)py + 0.5f, [&](uint32_t s, float weight) {
+                              const uint32_t seen = (uint32_t)(weight * 1024.0f + 0.5f);
+                              if (seen == 0u) return;
+                              contribution[s * 2 + 1] += seen;
+                              contribution[s * 2] += (uint32_t)((weight * m) * 1024.0f + 0.5f);
                           });
             }
         }

@@ -164,6 +164,18 @@ void orc_colour_gradient_exact(const orc_frame* f, const uint32_t* ranges, const
 void orc_contribution_weight(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
                              const float* records, uint32_t* contribution);
 
+/* contributionMode 2 (splat_blend.slang:366-380): per slot the squared colour
+ * change taking it away would leave in each pixel, capped at one, in 2^-24,
+ * against `wholeFrame` (float4 a pixel), added as a 64-bit sum into two words
+ * (low, high). */
+void orc_contribution_change(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                             const float* records, const float* wholeFrame, uint32_t* contribution);
+
+/* contributionMode 3 (splat_blend.slang:399-407): per slot two words, the
+ * weight times liftMask (clamped to [0, 1]) and the weight, in 1/1024. */
+void orc_contribution_lift(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
+                           const float* records, const float* liftMask, uint32_t* contribution);
+
 /* P: usd/aov_position.slang:34-52; viewToWorld rows (3x4, float). */
 void orc_position(uint32_t width, uint32_t height, uint32_t orthographic, float focalX, float focalY,
                   float centreX, float centreY, const float viewToWorld[12], const float* depth,

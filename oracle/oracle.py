@@ -108,6 +108,8 @@ def lib():
         L.orc_blend.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P, _P, _P, C.c_int]
         L.orc_colour_gradient.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
         L.orc_contribution_weight.argtypes = [C.POINTER(Frame), _P, _P, _P, _P]
+        L.orc_contribution_change.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
+        L.orc_contribution_lift.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
         L.orc_position.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float,
                                    _P, _P, _P]
         L.orc_frame64_from.argtypes = [C.POINTER(Projection), _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -350,6 +352,28 @@ def contribution_weight(f: Frame, binned: dict, proj: dict) -> np.ndarray:
     out = np.zeros(slots, np.uint32)
     ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
     lib().orc_contribution_weight(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]), _ptr(out))
+    return out
+
+
+def contribution_change(f: Frame, binned: dict, proj: dict, whole: np.ndarray) -> np.ndarray:
+    """contributionMode 2: (slots, 2) uint32 words, the low and high word of each slot's 64-bit sum."""
+    slots = proj["touched"].shape[0]
+    out = np.zeros((slots, 2), np.uint32)
+    w = np.ascontiguousarray(whole, np.float32)
+    ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
+    lib().orc_contribution_change(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]), _ptr(w),
+                                  _ptr(out))
+    return out
+
+
+def contribution_lift(f: Frame, binned: dict, proj: dict, mask: np.ndarray) -> np.ndarray:
+    """contributionMode 3: (slots, 2) uint32 words, the weight times the mask and the weight, in 1/1024."""
+    slots = proj["touched"].shape[0]
+    out = np.zeros((slots, 2), np.uint32)
+    m = np.ascontiguousarray(mask, np.float32)
+    ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
+    lib().orc_contribution_lift(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]), _ptr(m),
+                                _ptr(out))
     return out
 
 

@@ -1,6 +1,8 @@
-"""The blend's contribution hooks (TileRasterizer.h:351-367, splat_blend.slang:
-364-398) on a B200, against the CPU restatement: mode 1 (each splat's summed
-weight in 1/4096) and mode 4 (each splat's colour gradient in 1/256 with the
+"""The blend's contribution hooks (TileRasterizer.h:351-371, splat_blend.slang:
+364-407) on a B200, against the CPU restatement: mode 1 (each splat's summed
+weight in 1/4096), mode 2 (the squared colour change taking it away would
+leave, in 2^-24, a 64-bit sum a slot), mode 3 (a mask lifted to the splats, in
+1/1024) and mode 4 (each splat's colour gradient in 1/256 with the
 hash-dithered rounding, and its weight) are integer sums of the same FP32
 weights, so they must match word for word; frames add into the buffer."""
 import numpy as np
@@ -57,17 +59,56 @@ def test_mode_4_colour_gradients_are_the_references(oracle):
     assert np.abs(ref[:, :3]).sum() > 0
 
 
-def test_modes_2_and_3_are_refused(oracle):
-    W, H = 64, 48
-    proj, splats, _ = _frame(oracle, W, H)
+def test_mode_2_squared_changes_are_the_references(oracle):
+    """Mode 2: each splat's squared colour change against the frame drawn whole,
+    a 64-bit sum in two words a slot (low, high); two frames add in."""
+    W, H = 250, 190
+    proj, splats, want = _frame(oracle, W, H)
+    raster = A.TileRasterizer.create()
+    t = A.RenderTargets.make(W, H)
+    raster.render(proj, [A.SplatInstance(splats)], A.RenderSettings(width=W, height=H), t)
+    whole = t.colour.clone()
+    words = torch.zeros((splats.count, 2), dtype=torch.int32, device="cuda")
+    s = A.RenderSettings(width=W, height=H, contribution_mode=2, contribution=words, final_colour=whole)
+    raster.render(proj, [A.SplatInstance(splats)], s, t)
+    raster.render(proj, [A.SplatInstance(splats)], s, t)
+    torch.cuda.synchronize()
+    ref = oracle.contribution_change(want["frame"], want["binned"], want["proj"], whole.cpu().numpy())
+    w = words.cpu().numpy().view(np.uint32).astype(np.uint64)
+    r = ref.astype(np.uint64)
+    np.testing.assert_array_equal(w[:, 0] + (w[:, 1] << np.uint64(32)), 2 * (r[:, 0] + (r[:, 1] << np.uint64(32))))
+    assert r[:, 0].sum() > 0
+
+
+def test_mode_3_lifted_mask_is_the_references(oracle):
+    """Mode 3: each splat's weight times the mask (clamped to [0, 1]) and its
+    weight, in 1/1024, two words a slot."""
+    W, H = 250, 190
+    proj, splats, want = _frame(oracle, W, H)
+    mask = torch.rand((W * H,), generator=torch.Generator().manual_seed(11)) * 1.4 - 0.2
     words = torch.zeros((splats.count, 2), dtype=torch.int32, device="cuda")
     raster = A.TileRasterizer.create()
     t = A.RenderTargets.make(W, H)
-    for mode in (2, 3):
+    s = A.RenderSettings(width=W, height=H, contribution_mode=3, contribution=words, lift_mask=mask.cuda())
+    raster.render(proj, [A.SplatInstance(splats)], s, t)
+    torch.cuda.synchronize()
+    ref = oracle.contribution_lift(want["frame"], want["binned"], want["proj"], mask.numpy())
+    np.testing.assert_array_equal(words.cpu().numpy().view(np.uint32), ref)
+    assert ref[:, 1].sum() > ref[:, 0].sum() > 0
+
+
+def test_contribution_modes_need_their_inputs(oracle):
+    """Modes 0 to 4 only; mode 2 needs the whole frame and mode 3 its mask."""
+    W, H = 64, 48
+    proj, splats, _ = _frame(oracle, W, H)
+    words = torch.zeros((splats.count, 4), dtype=torch.int32, device="cuda")
+    raster = A.TileRasterizer.create()
+    t = A.RenderTargets.make(W, H)
+    for mode, code in ((5, 4), (2, 3), (3, 3)):
         with pytest.raises(A.AtheneaError) as e:
             raster.render(proj, [A.SplatInstance(splats)],
                           A.RenderSettings(width=W, height=H, contribution_mode=mode, contribution=words), t)
-        assert e.value.code == 4
+        assert e.value.code == code, mode
 
 
 def test_composite_over_an_under_layer_is_the_references(oracle):

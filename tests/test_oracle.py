@@ -247,3 +247,25 @@ def test_raster_matches_the_fp64_ground_truth(oracle, section):
     d = np.abs(ours - ref).max(axis=1)
     assert np.percentile(d, 99) <= 2
     assert d.max() <= 16
+
+
+# ---- contributionMode 2 and 3 (splat_blend.slang:366-380, :399-407) ----------
+def test_lifted_mask_and_squared_change_contributions(oracle):
+    """Mode 3 with a mask of one lifts each splat's weight itself, and with a mask
+    of zero nothing. Mode 2 against the frame's own colour: one splat over an
+    empty background changes each pixel by its weight times its colour, so its
+    sum is the squared weights times |colour|^2, in 2^-24."""
+    b = CloudBuilder().add(0.0, 0.0, -5.0, 0.8, 0.3, 0.3, 0.3, (1, 0, 0, 0), (0.8, 0.4, 0.2))
+    pos, shape, sh, _, shw = _decode(oracle, b)
+    out, _ = _render(oracle, oracle.default_camera(), [(pos, shape, sh, None, shw)], 160, 120)
+    f, binned, proj = out["frame"], out["binned"], out["proj"]
+    ones = oracle.contribution_lift(f, binned, proj, np.ones(160 * 120, np.float32))
+    assert ones[0, 1] > 0 and ones[0, 0] == ones[0, 1]
+    zeros = oracle.contribution_lift(f, binned, proj, np.full(160 * 120, -0.5, np.float32))   # clamped to 0
+    assert zeros[0, 0] == 0 and zeros[0, 1] == ones[0, 1]
+    words = oracle.contribution_change(f, binned, proj, out["colour"])
+    got = int(words[0, 0]) + (int(words[0, 1]) << 32)
+    colour = proj["records"][0, 8:11].astype(np.float64)
+    alpha = out["colour"][:, 3].astype(np.float64)   # one splat: the coverage is its weight
+    want = np.sum(np.minimum(alpha ** 2 * np.dot(colour, colour), 1.0) * 16777216.0)
+    assert got > 0 and abs(got - want) <= 1e-4 * want + alpha.size
