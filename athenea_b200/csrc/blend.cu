@@ -116,6 +116,7 @@ __global__ void __launch_bounds__(kBlendThreads)
 
     float r = 0.0f, g = 0.0f, bl = 0.0f;
     float T = 1.0f, depthSum = 0.0f, depthAt = -1.0f;
+    float matteKnown = 0.0f, matteInside = 0.0f, matteUntold = 0.0f;   // the lifted matte's sums
     uint32_t last = 0;
     bool done = !inside;
     for (uint32_t first = range.x; first < range.y; first += kBlendThreads) {
@@ -188,7 +189,21 @@ __global__ void __launch_bounds__(kBlendThreads)
                     atomicAdd(&contrib.words[slot * 4 + 3], (uint32_t)(weight * kColourGradScale + 0.5f));
                 }
             }
-            if (kMatte) list.add(matte.ids[sSlot[j]], weight);
+            if (kMatte && matte.out) list.add(matte.ids[sSlot[j]], weight);
+            if (kMatte && matte.lifted) {
+                // splat_blend.slang:423-435: the share a lift told the splat, or, for one no
+                // lifting camera saw, its weight kept aside
+                const uint32_t told = sSlot[j] * 2u;
+                const uint32_t seen = matte.liftSums[told + 1u];
+                if (seen != 0u) {
+                    float share = (float)matte.liftSums[told] / (float)seen;
+                    if (matte.hard) share = share > matte.threshold ? 1.0f : 0.0f;
+                    matteKnown = matteKnown + weight;
+                    matteInside = matteInside + weight * share;
+                } else {
+                    matteUntold = matteUntold + weight;
+                }
+            }
             const float4 c = sColour[j];
             r = r + weight * c.x;
             g = g + weight * c.y;
@@ -210,7 +225,12 @@ __global__ void __launch_bounds__(kBlendThreads)
         if (depthAt < 0.0f) depthAt = underZ;
     }
     const float total = kUnder && underHit ? 1.0f : coverage;
-    if (kMatte) {
+    if (kMatte && matte.lifted) {
+        // splat_blend.slang:536-539: the untold weight at the share of the known
+        const float share = matteKnown > 0.0f ? matteInside / matteKnown : 0.0f;
+        matte.lifted[at] = fminf(fmaxf(matteInside + matteUntold * share, 0.0f), 1.0f);
+    }
+    if (kMatte && matte.out) {
         // what closed the walk takes the rest of the pixel (splat_blend.slang:525-534)
         list.add(kUnder && underHit && matte.underIds ? matte.underIds[at] : 0u, kUnder && underHit ? T : 0.0f);
         list.write(reinterpret_cast<float4*>(matte.out), at, F.width * F.height);
@@ -248,7 +268,7 @@ cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, con
     blendKernel<C_, U_, M_><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, \
                                                                 depth, position, finalT, lastContrib, status,     \
                                                                 contrib, under, matte)
-    const bool c = contrib.mode != 0u, u = under.depth != nullptr, m = matte.out != nullptr;
+    const bool c = contrib.mode != 0u, u = under.depth != nullptr, m = matte.out != nullptr || matte.lifted != nullptr;
     if (m) {
         if (c && u) ATH_BLEND(true, true, true);
         else if (c) ATH_BLEND(true, false, true);

@@ -200,6 +200,7 @@ extern "C" ath_status ath_settings_default(ath_settings* out) {
     out->surfels = 1;
     out->max_sh_degree = 3;
     out->depth_threshold = 0.5f;
+    out->matte_threshold = 0.5f;
     return ATH_OK;
 }
 
@@ -384,6 +385,8 @@ ath_status checkFrame(const ath_settings& s, const ath_targets& targets) {
         return fail(ATH_E_INVALID_ARGUMENT, "contribution mode 4 needs final_colour (dL/dpixel)");
     if ((s.crypto != nullptr) != (s.crypto_ids != nullptr))
         return fail(ATH_E_INVALID_ARGUMENT, "a Cryptomatte needs both its ids and its layers");
+    if ((s.matte_lift != nullptr) != (s.matte != nullptr))
+        return fail(ATH_E_INVALID_ARGUMENT, "a lifted matte needs both the lift's sums and the matte target");
     return ATH_OK;
 }
 
@@ -478,7 +481,8 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
                           training ? static_cast<uint32_t*>(r->lastContrib.ptr) : nullptr, words + kWordSticky, stream,
                           Contribution{s.contribution_mode, s.contribution, s.final_colour, s.lift_mask},
                           under ? Under{under->colour, under->depth} : Under{},
-                          Matte{s.crypto_ids, s.crypto, under ? s.under_crypto : nullptr});
+                          Matte{s.crypto_ids, s.crypto, under ? s.under_crypto : nullptr, s.matte_lift, s.matte,
+                                s.matte_hard != 0 ? 1u : 0u, s.matte_threshold});
     mark(5);
     if (err != cudaSuccess) return failCuda(err, "drawing the frame");
     r->lastSlots = slots;

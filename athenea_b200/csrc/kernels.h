@@ -62,9 +62,13 @@ struct Under {
 
 // Cryptomatte: a uint id a slot in, 3 float4 layers a pixel out.
 struct Matte {
-    const uint32_t* ids = nullptr;
+    const uint32_t* ids = nullptr;        // Cryptomatte: the id a slot, the layers out, the under layer's ids
     float* out = nullptr;
     const uint32_t* underIds = nullptr;
+    const uint32_t* liftSums = nullptr;   // the matte a lift told the splats: two words a slot (inside, seen)
+    float* lifted = nullptr;              // and the matte a pixel it sums to
+    uint32_t hard = 0;
+    float threshold = 0.5f;
 };
 
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,

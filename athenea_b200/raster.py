@@ -217,6 +217,10 @@ class RenderSettings:
     crypto: torch.Tensor | None = None          # (3, height * width, 4) float32: the matte's layers
     under_crypto: torch.Tensor | None = None    # int32 a pixel: the under layer's id
     lift_mask: torch.Tensor | None = None       # float a pixel, 0 to 1: mode 3's mask
+    matte_lift: torch.Tensor | None = None      # int32, two a slot: what mode 3 lifted (weight x mask, weight)
+    matte: torch.Tensor | None = None           # float a pixel: the matte those sums give
+    matte_hard: bool = False
+    matte_threshold: float = 0.5
 
     def _native(self) -> N.Settings:
         s = N.Settings()
@@ -239,6 +243,10 @@ class RenderSettings:
         s.crypto = _ptr(self.crypto) if self.crypto is not None else None
         s.under_crypto = _ptr(self.under_crypto) if self.under_crypto is not None else None
         s.lift_mask = _ptr(self.lift_mask) if self.lift_mask is not None else None
+        s.matte_lift = _ptr(self.matte_lift) if self.matte_lift is not None else None
+        s.matte = _ptr(self.matte) if self.matte is not None else None
+        s.matte_hard = 1 if self.matte_hard else 0
+        s.matte_threshold = self.matte_threshold
         return s
 
 

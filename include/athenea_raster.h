@@ -147,6 +147,17 @@ typedef struct {
     float* crypto;
     const uint32_t* under_crypto;
     const float* lift_mask;     /* contribution mode 3's mask: one float a pixel, 0 to 1 */
+    /* The matte summed by the blend (TileRasterizer.h:319-326, splat_blend.slang:
+     * 423-435,536-539): with matte_lift (two uint a slot, as contribution mode 3
+     * wrote them: the weight times a mask and the weight) and matte (one float a
+     * pixel), each blended splat that a lift saw adds its weight times its share
+     * (inside / seen; 1 above matte_threshold and 0 below when matte_hard), one
+     * it did not is counted at the pixel's known share, and the pixel's matte is
+     * that sum clamped to [0, 1]. matte_threshold defaults to 0.5. */
+    const uint32_t* matte_lift;
+    float* matte;
+    int32_t matte_hard;
+    float matte_threshold;
 } ath_settings;
 
 /* RenderTargets (TileRasterizer.h:421-450) plus the P layer

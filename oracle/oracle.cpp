@@ -1167,6 +1167,36 @@ void orc_contribution_lift(const orc_frame* f, const uint32_t* ranges, const uin
     }
 }
 
+void orc_matte_lift(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
+                    const uint32_t* liftSums, uint32_t hard, float threshold, float* matte) {
+    // splat_blend.slang:423-435,536-539
+    const uint32_t tiles = f->tilesX * f->tilesY;
+    for (uint32_t t = 0; t < tiles; ++t) {
+        const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
+        for (uint32_t ly = 0; ly < kTile; ++ly) {
+            for (uint32_t lx = 0; lx < kTile; ++lx) {
+                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+                if (px >= f->width || py >= f->height) continue;
+                float known = 0.0f, inside = 0.0f, untold = 0.0f;
+                walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
+                          (float)py + 0.5f, [&](uint32_t s, float weight) {
+                              const uint32_t seen = liftSums[s * 2 + 1];
+                              if (seen != 0u) {
+                                  float share = (float)liftSums[s * 2] / (float)seen;
+                                  if (hard) share = share > threshold ? 1.0f : 0.0f;
+                                  known = known + weight;
+                                  inside = inside + weight * share;
+                              } else {
+                                  untold = untold + weight;
+                              }
+                          });
+                const float share = known > 0.0f ? inside / known : 0.0f;
+                matte[py * f->width + px] = std::fmin(std::fmax(inside + untold * share, 0.0f), 1.0f);
+            }
+        }
+    }
+}
+
 void orc_position(uint32_t width, uint32_t height, uint32_t orthographic, float focalX, float focalY, float centreX,
                   float centreY, const float r[12], const float* depth, float* position) {
     // usd/aov_position.slang:34-52

@@ -176,6 +176,11 @@ void orc_contribution_change(const orc_frame* f, const uint32_t* ranges, const u
 void orc_contribution_lift(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats,
                            const float* records, const float* liftMask, uint32_t* contribution);
 
+/* The matte summed by the blend (splat_blend.slang:423-435,536-539) from a
+ * lift's two words a slot (weight x mask, weight): one float a pixel. */
+void orc_matte_lift(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
+                    const uint32_t* liftSums, uint32_t hard, float threshold, float* matte);
+
 /* P: usd/aov_position.slang:34-52; viewToWorld rows (3x4, float). */
 void orc_position(uint32_t width, uint32_t height, uint32_t orthographic, float focalX, float focalY,
                   float centreX, float centreY, const float viewToWorld[12], const float* depth,

@@ -110,6 +110,7 @@ def lib():
         L.orc_contribution_weight.argtypes = [C.POINTER(Frame), _P, _P, _P, _P]
         L.orc_contribution_change.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
         L.orc_contribution_lift.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
+        L.orc_matte_lift.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, C.c_uint32, C.c_float, _P]
         L.orc_position.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float,
                                    _P, _P, _P]
         L.orc_frame64_from.argtypes = [C.POINTER(Projection), _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -374,6 +375,17 @@ def contribution_lift(f: Frame, binned: dict, proj: dict, mask: np.ndarray) -> n
     ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
     lib().orc_contribution_lift(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]), _ptr(m),
                                 _ptr(out))
+    return out
+
+
+def matte_lift(f: Frame, binned: dict, proj: dict, lift: np.ndarray, hard: bool = False,
+               threshold: float = 0.5) -> np.ndarray:
+    """The matte a lift's sums (two uint32 a slot) give each pixel of this frame."""
+    out = np.zeros(f.width * f.height, np.float32)
+    sums = np.ascontiguousarray(lift, np.uint32)
+    ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
+    lib().orc_matte_lift(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]), _ptr(sums),
+                         1 if hard else 0, threshold, _ptr(out))
     return out
 
 

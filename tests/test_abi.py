@@ -60,6 +60,7 @@ def test_settings_defaults_are_the_references(native):
     assert native.lib().ath_settings_default(C.byref(s)) == 0
     assert (s.width, s.height, s.antialias, s.antialias_override, s.surfels, s.max_sh_degree) == (1920, 1080, 1, -1, 1, 3)
     assert s.depth_threshold == pytest.approx(0.5) and list(s.background) == [0, 0, 0, 0]
+    assert s.matte_threshold == pytest.approx(0.5) and not s.matte_lift and not s.matte and s.matte_hard == 0
 
 
 def test_argument_errors_come_back_as_status_codes(native):

@@ -97,6 +97,33 @@ def test_mode_3_lifted_mask_is_the_references(oracle):
     assert ref[:, 1].sum() > ref[:, 0].sum() > 0
 
 
+@pytest.mark.parametrize("hard", [False, True])
+def test_lifted_matte_is_the_references(oracle, hard):
+    """A mask lifted to the splats (contribution mode 3), then the matte the
+    blend sums from those words (TileRasterizer.h:319-326): every pixel equals
+    the restatement's, soft and hard (threshold 0.4)."""
+    W, H = 250, 190
+    proj, splats, want = _frame(oracle, W, H)
+    mask = torch.zeros((H, W))
+    mask[:, :W // 2] = 1.0   # the left half is inside
+    words = torch.zeros((splats.count, 2), dtype=torch.int32, device="cuda")
+    raster = A.TileRasterizer.create()
+    t = A.RenderTargets.make(W, H)
+    raster.render(proj, [A.SplatInstance(splats)],
+                  A.RenderSettings(width=W, height=H, contribution_mode=3, contribution=words,
+                                   lift_mask=mask.reshape(-1).cuda()), t)
+    matte = torch.full((W * H,), -1.0, device="cuda")
+    raster.render(proj, [A.SplatInstance(splats)],
+                  A.RenderSettings(width=W, height=H, matte_lift=words, matte=matte, matte_hard=hard,
+                                   matte_threshold=0.4), t)
+    torch.cuda.synchronize()
+    ref = oracle.matte_lift(want["frame"], want["binned"], want["proj"], words.cpu().numpy().view(np.uint32),
+                            hard, 0.4)
+    np.testing.assert_array_equal(matte.cpu().numpy(), ref)
+    m = ref.reshape(H, W)
+    assert m[:, :W // 4].mean() > m[:, 3 * W // 4:].mean()
+
+
 def test_contribution_modes_need_their_inputs(oracle):
     """Modes 0 to 4 only; mode 2 needs the whole frame and mode 3 its mask."""
     W, H = 64, 48
