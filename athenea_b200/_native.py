@@ -59,7 +59,8 @@ class Settings(C.Structure):
                 ("counters_tag", C.c_uint64), ("contribution_mode", C.c_uint32), ("contribution", C.c_void_p),
                 ("final_colour", C.c_void_p), ("crypto_ids", C.c_void_p), ("crypto", C.c_void_p),
                 ("under_crypto", C.c_void_p), ("lift_mask", C.c_void_p), ("matte_lift", C.c_void_p),
-                ("matte", C.c_void_p), ("matte_hard", C.c_int32), ("matte_threshold", C.c_float)]
+                ("matte", C.c_void_p), ("matte_hard", C.c_int32), ("matte_threshold", C.c_float),
+                ("trace", C.c_void_p)]
 
 
 class Targets(C.Structure):

@@ -8,6 +8,7 @@
 // counted with a block-wide ballot (__syncthreads_count). Per pixel the walk
 // is sequential in the tile's (depth key, slot) order, so the result is the
 // CPU restatement's to the bit (built with --fmad=false; see splat_math.cuh).
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -26,6 +27,84 @@ constexpr uint32_t kCryptoSlots = 6;         // splat_blend.slang:82
 // list gives its lightest slot up to a heavier id. Written ranked by weight,
 // descending (a stable insertion sort), as 3 float4 (id bits, weight, id bits,
 // weight).
+// The trace's list (splat_trace.slang:33-128): the kTraceSlots heaviest splats
+// of a pixel's walk by weight, the lightest rank kept so that a splat too light
+// for the list costs one comparison, and everything the walk blended.
+constexpr uint32_t kTraceSlots = 4;
+constexpr uint32_t kTraceWords = kTraceSlots * 2 + kTraceSlots / 2 + 1;
+constexpr uint32_t kTraceNone = 0xFFFFFFFFu, kTraceEmpty = 0xFFFFFFFEu;
+
+__device__ __forceinline__ uint32_t halfBits(float v) { return (uint32_t)__half_as_ushort(__float2half_rn(v)); }
+
+struct TraceList {
+    uint32_t slots[kTraceSlots];
+    float weights[kTraceSlots];
+    float total, floor;
+    uint32_t lightest;
+
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (uint32_t k = 0; k < kTraceSlots; ++k) {
+            slots[k] = kTraceNone;
+            weights[k] = 0.0f;
+        }
+        total = floor = 0.0f;
+        lightest = 0;
+    }
+    // a splat heavier than the lightest rank takes its place
+    __device__ __forceinline__ void enter(uint32_t slot, float weight) {
+#pragma unroll
+        for (uint32_t k = 0; k < kTraceSlots; ++k)
+            if (k == lightest) {
+                slots[k] = slot;
+                weights[k] = weight;
+            }
+        lightest = 0;
+        float w = weights[0];
+#pragma unroll
+        for (uint32_t k = 1; k < kTraceSlots; ++k)
+            if (weights[k] < w) {
+                lightest = k;
+                w = weights[k];
+            }
+        floor = w;
+    }
+    // planes of `pixels` words: the slots heaviest first, their view depths (as
+    // the floats' bits), the weights as halves two a word, and (rest, under) as
+    // halves; a pixel nothing reached writes kTraceEmpty in its first word alone
+    __device__ void write(uint32_t* trace, uint32_t at, uint32_t pixels, float under,
+                          const float4* __restrict__ recs) const {
+        if (!(total > 0.0f) && !(under > 0.0f)) {
+            trace[at] = kTraceEmpty;
+            return;
+        }
+        uint32_t order[kTraceSlots];
+#pragma unroll
+        for (uint32_t k = 0; k < kTraceSlots; ++k) order[k] = k;
+        for (uint32_t i = 1; i < kTraceSlots; ++i) {
+            const uint32_t pick = order[i];
+            uint32_t j = i;
+            while (j > 0 && weights[order[j - 1]] < weights[pick]) {
+                order[j] = order[j - 1];
+                --j;
+            }
+            order[j] = pick;
+        }
+        float held = 0.0f;
+        for (uint32_t k = 0; k < kTraceSlots; ++k) {
+            const uint32_t from = order[k];
+            const bool some = weights[from] > 0.0f;
+            trace[k * pixels + at] = some ? slots[from] : kTraceNone;
+            trace[(kTraceSlots + k) * pixels + at] = some ? __float_as_uint(recs[(size_t)slots[from] * 3].z) : 0u;
+            held = held + weights[from];
+        }
+        for (uint32_t pair = 0; pair < kTraceSlots / 2; ++pair)
+            trace[(kTraceSlots * 2 + pair) * pixels + at] =
+                halfBits(weights[order[pair * 2]]) | (halfBits(weights[order[pair * 2 + 1]]) << 16);
+        trace[(kTraceWords - 1) * pixels + at] = halfBits(fmaxf(total - held, 0.0f)) | (halfBits(fmaxf(under, 0.0f)) << 16);
+    }
+};
+
 struct CryptoList {
     uint32_t ids[kCryptoSlots];
     float weights[kCryptoSlots];
@@ -99,6 +178,8 @@ __global__ void __launch_bounds__(kBlendThreads)
     __shared__ uint32_t sSlot[kContribution || kMatte ? kBlendThreads : 1];
     CryptoList list;
     if (kMatte) list.clear();
+    TraceList trace;
+    if (kMatte && matte.trace) trace.clear();
 
     const uint32_t tile = blockIdx.x;
     const uint32_t tx = tile % F.tilesX, ty = tile / F.tilesX;
@@ -190,6 +271,11 @@ __global__ void __launch_bounds__(kBlendThreads)
                 }
             }
             if (kMatte && matte.out) list.add(matte.ids[sSlot[j]], weight);
+            if (kMatte && matte.trace) {
+                // splat_blend.slang:445-451
+                trace.total = trace.total + weight;
+                if (weight > trace.floor) trace.enter(sSlot[j], weight);
+            }
             if (kMatte && matte.lifted) {
                 // splat_blend.slang:423-435: the share a lift told the splat, or, for one no
                 // lifting camera saw, its weight kept aside
@@ -225,6 +311,8 @@ __global__ void __launch_bounds__(kBlendThreads)
         if (depthAt < 0.0f) depthAt = underZ;
     }
     const float total = kUnder && underHit ? 1.0f : coverage;
+    if (kMatte && matte.trace)   // splat_blend.slang:545-551: what closed the walk from behind is `under`
+        trace.write(matte.trace, at, F.width * F.height, kUnder && underHit ? T : 0.0f, recs);
     if (kMatte && matte.lifted) {
         // splat_blend.slang:536-539: the untold weight at the share of the known
         const float share = matteKnown > 0.0f ? matteInside / matteKnown : 0.0f;
@@ -268,7 +356,8 @@ cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, con
     blendKernel<C_, U_, M_><<<tiles, kBlendThreads, 0, stream>>>(F, pairs, slots, ranges, pairValues, recs, colour, \
                                                                 depth, position, finalT, lastContrib, status,     \
                                                                 contrib, under, matte)
-    const bool c = contrib.mode != 0u, u = under.depth != nullptr, m = matte.out != nullptr || matte.lifted != nullptr;
+    const bool c = contrib.mode != 0u, u = under.depth != nullptr,
+               m = matte.out != nullptr || matte.lifted != nullptr || matte.trace != nullptr;
     if (m) {
         if (c && u) ATH_BLEND(true, true, true);
         else if (c) ATH_BLEND(true, false, true);

@@ -482,7 +482,7 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
                           Contribution{s.contribution_mode, s.contribution, s.final_colour, s.lift_mask},
                           under ? Under{under->colour, under->depth} : Under{},
                           Matte{s.crypto_ids, s.crypto, under ? s.under_crypto : nullptr, s.matte_lift, s.matte,
-                                s.matte_hard != 0 ? 1u : 0u, s.matte_threshold});
+                                s.matte_hard != 0 ? 1u : 0u, s.matte_threshold, s.trace});
     mark(5);
     if (err != cudaSuccess) return failCuda(err, "drawing the frame");
     r->lastSlots = slots;

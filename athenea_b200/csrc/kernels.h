@@ -69,6 +69,7 @@ struct Matte {
     float* lifted = nullptr;              // and the matte a pixel it sums to
     uint32_t hard = 0;
     float threshold = 0.5f;
+    uint32_t* trace = nullptr;            // the splats a pixel is made of (splat_trace.slang), kTraceWords planes
 };
 
 cudaError_t launchBlend(const FrameConst& F, uint32_t pairs, uint32_t slots, const uint2* ranges,

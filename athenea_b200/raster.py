@@ -221,6 +221,7 @@ class RenderSettings:
     matte: torch.Tensor | None = None           # float a pixel: the matte those sums give
     matte_hard: bool = False
     matte_threshold: float = 0.5
+    trace: torch.Tensor | None = None           # int32 (11, height * width): the splats each pixel is made of
 
     def _native(self) -> N.Settings:
         s = N.Settings()
@@ -247,6 +248,7 @@ class RenderSettings:
         s.matte = _ptr(self.matte) if self.matte is not None else None
         s.matte_hard = 1 if self.matte_hard else 0
         s.matte_threshold = self.matte_threshold
+        s.trace = _ptr(self.trace) if self.trace is not None else None
         return s
 
 

@@ -158,6 +158,14 @@ typedef struct {
     float* matte;
     int32_t matte_hard;
     float matte_threshold;
+    /* The trace (TileRasterizer.h:282-288, splat/splat_trace.slang): the four
+     * splats that weighed most in each pixel, 11 planes of width*height uint:
+     * their slots heaviest first (0xFFFFFFFF where a rank is empty), their view
+     * depths as float bits, their weights as halves two a word, and the weight
+     * the list had no room for with what closed the walk from behind (the under
+     * layer) as halves; a pixel nothing reached has 0xFFFFFFFE in its first word
+     * and nothing else written. NULL: no trace. */
+    uint32_t* trace;
 } ath_settings;
 
 /* RenderTargets (TileRasterizer.h:421-450) plus the P layer

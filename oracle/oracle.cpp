@@ -1197,6 +1197,64 @@ void orc_matte_lift(const orc_frame* f, const uint32_t* ranges, const uint32_t* 
     }
 }
 
+void orc_trace(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
+               uint32_t* trace) {
+    // splat_blend.slang:445-451,545-551 with splat_trace.slang:33-128 (no layer under the splats)
+    constexpr uint32_t K = 4, kWords = K * 2 + K / 2 + 1;
+    const uint32_t pixels = f->width * f->height, tiles = f->tilesX * f->tilesY;
+    for (uint32_t t = 0; t < tiles; ++t) {
+        const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
+        for (uint32_t ly = 0; ly < kTile; ++ly) {
+            for (uint32_t lx = 0; lx < kTile; ++lx) {
+                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+                if (px >= f->width || py >= f->height) continue;
+                uint32_t slots[K] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
+                float weights[K] = {0, 0, 0, 0}, total = 0.0f, floor = 0.0f;
+                uint32_t lightest = 0;
+                walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
+                          (float)py + 0.5f, [&](uint32_t s, float weight) {
+                              total = total + weight;
+                              if (!(weight > floor)) return;
+                              slots[lightest] = s;
+                              weights[lightest] = weight;
+                              lightest = 0;
+                              for (uint32_t k = 1; k < K; ++k)
+                                  if (weights[k] < weights[lightest]) lightest = k;
+                              floor = weights[lightest];
+                          });
+                const uint32_t at = py * f->width + px;
+                if (!(total > 0.0f)) {
+                    trace[at] = 0xFFFFFFFEu;
+                    continue;
+                }
+                uint32_t order[K] = {0, 1, 2, 3};
+                for (uint32_t i = 1; i < K; ++i) {
+                    const uint32_t pick = order[i];
+                    uint32_t j = i;
+                    while (j > 0 && weights[order[j - 1]] < weights[pick]) {
+                        order[j] = order[j - 1];
+                        --j;
+                    }
+                    order[j] = pick;
+                }
+                float held = 0.0f;
+                for (uint32_t k = 0; k < K; ++k) {
+                    const uint32_t from = order[k];
+                    const bool some = weights[from] > 0.0f;
+                    trace[k * pixels + at] = some ? slots[from] : 0xFFFFFFFFu;
+                    uint32_t bits = 0;
+                    if (some) std::memcpy(&bits, &records[(size_t)slots[from] * 12 + 2], 4);
+                    trace[(K + k) * pixels + at] = bits;
+                    held = held + weights[from];
+                }
+                for (uint32_t pair = 0; pair < K / 2; ++pair)
+                    trace[(K * 2 + pair) * pixels + at] = packHalves(weights[order[pair * 2]], weights[order[pair * 2 + 1]]);
+                trace[(kWords - 1) * pixels + at] = packHalves(std::fmax(total - held, 0.0f), 0.0f);
+            }
+        }
+    }
+}
+
 void orc_position(uint32_t width, uint32_t height, uint32_t orthographic, float focalX, float focalY, float centreX,
                   float centreY, const float r[12], const float* depth, float* position) {
     // usd/aov_position.slang:34-52

@@ -181,6 +181,11 @@ void orc_contribution_lift(const orc_frame* f, const uint32_t* ranges, const uin
 void orc_matte_lift(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
                     const uint32_t* liftSums, uint32_t hard, float threshold, float* matte);
 
+/* The trace (splat_trace.slang): 11 planes of width*height words, as the
+ * product writes them, for a frame with no layer under the splats. */
+void orc_trace(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
+               uint32_t* trace);
+
 /* P: usd/aov_position.slang:34-52; viewToWorld rows (3x4, float). */
 void orc_position(uint32_t width, uint32_t height, uint32_t orthographic, float focalX, float focalY,
                   float centreX, float centreY, const float viewToWorld[12], const float* depth,

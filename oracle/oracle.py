@@ -111,6 +111,7 @@ def lib():
         L.orc_contribution_change.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
         L.orc_contribution_lift.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
         L.orc_matte_lift.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, C.c_uint32, C.c_float, _P]
+        L.orc_trace.argtypes = [C.POINTER(Frame), _P, _P, _P, _P]
         L.orc_position.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float,
                                    _P, _P, _P]
         L.orc_frame64_from.argtypes = [C.POINTER(Projection), _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -386,6 +387,14 @@ def matte_lift(f: Frame, binned: dict, proj: dict, lift: np.ndarray, hard: bool 
     ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
     lib().orc_matte_lift(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]), _ptr(sums),
                          1 if hard else 0, threshold, _ptr(out))
+    return out
+
+
+def trace(f: Frame, binned: dict, proj: dict) -> np.ndarray:
+    """The trace's 11 planes (uint32, (11, width * height)); words the product leaves unwritten are 0 here."""
+    out = np.zeros((11, f.width * f.height), np.uint32)
+    ps = binned["pair_splats"] if binned["pairs"] else np.zeros(1, np.uint32)
+    lib().orc_trace(C.byref(f), _ptr(binned["ranges"]), _ptr(ps), _ptr(proj["records"]), _ptr(out))
     return out
 
 

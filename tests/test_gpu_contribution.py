@@ -124,6 +124,32 @@ def test_lifted_matte_is_the_references(oracle, hard):
     assert m[:, :W // 4].mean() > m[:, 3 * W // 4:].mean()
 
 
+def test_trace_is_the_references(oracle):
+    """The trace (TileRasterizer.h:282-288, splat_trace.slang): each pixel's four
+    heaviest splats, their depths and weights, and the weight the list had no
+    room for, word for word the restatement's; the weights and the rest sum to
+    the pixel's coverage (within the halves' rounding)."""
+    W, H = 250, 190
+    proj, splats, want = _frame(oracle, W, H)
+    tr = torch.zeros((11, W * H), dtype=torch.int32, device="cuda")
+    raster = A.TileRasterizer.create()
+    t = A.RenderTargets.make(W, H)
+    raster.render(proj, [A.SplatInstance(splats)], A.RenderSettings(width=W, height=H, trace=tr), t)
+    torch.cuda.synchronize()
+    got = tr.cpu().numpy().view(np.uint32)
+    ref = oracle.trace(want["frame"], want["binned"], want["proj"])
+    empty = ref[0] == 0xFFFFFFFE
+    np.testing.assert_array_equal(got[0], ref[0])
+    np.testing.assert_array_equal(got[:, ~empty], ref[:, ~empty])
+    halves = got[8:11, ~empty].astype(np.uint32)
+    parts = np.concatenate([(halves & 0xFFFF).astype(np.uint16).view(np.float16)[None],
+                            (halves >> 16).astype(np.uint16).view(np.float16)[None]]).astype(np.float64)
+    held_and_rest = parts[0, 0] + parts[1, 0] + parts[0, 1] + parts[1, 1] + parts[0, 2]
+    coverage = t.colour.cpu().numpy()[~empty, 3].astype(np.float64)
+    assert np.abs(held_and_rest - coverage).max() <= 4e-3
+    assert (~empty).sum() > 1000
+
+
 def test_contribution_modes_need_their_inputs(oracle):
     """Modes 0 to 4 only; mode 2 needs the whole frame and mode 3 its mask."""
     W, H = 64, 48
