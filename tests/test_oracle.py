@@ -269,3 +269,24 @@ def test_lifted_mask_and_squared_change_contributions(oracle):
     alpha = out["colour"][:, 3].astype(np.float64)   # one splat: the coverage is its weight
     want = np.sum(np.minimum(alpha ** 2 * np.dot(colour, colour), 1.0) * 16777216.0)
     assert got > 0 and abs(got - want) <= 1e-4 * want + alpha.size
+
+
+# ---- the trace (splat_trace.slang) ------------------------------------------------
+def test_trace_ranks_by_weight_and_sums_to_the_coverage(oracle):
+    """Each pixel's ranks come heaviest first, empty ranks last, and the ranked
+    weights plus the rest the list had no room for are the pixel's coverage
+    (within the halves' rounding); a pixel nothing reached is marked empty."""
+    packed = _decode(oracle, random_cloud(400, 3))
+    out, _ = _render(oracle, oracle.default_camera(), [packed], 96, 64)
+    tr = oracle.trace(out["frame"], out["binned"], out["proj"])
+    empty = tr[0] == 0xFFFFFFFE
+    coverage = out["colour"][:, 3].astype(np.float64)
+    assert np.all(coverage[empty] == 0) and (~empty).sum() > 100
+    words = tr[8:11, ~empty]
+    lo = (words & 0xFFFF).astype(np.uint16).view(np.float16).astype(np.float64)
+    hi = (words >> 16).astype(np.uint16).view(np.float16).astype(np.float64)
+    w = np.stack([lo[0], hi[0], lo[1], hi[1]])
+    assert np.all(np.diff(w, axis=0) <= 0)                      # heaviest first
+    slots = tr[0:4, ~empty]
+    assert np.all((slots == 0xFFFFFFFF) == (w == 0))            # an empty rank weighs nothing
+    assert np.abs(w.sum(axis=0) + lo[2] - coverage[~empty]).max() <= 4e-3
