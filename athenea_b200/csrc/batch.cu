@@ -497,6 +497,32 @@ __global__ void __launch_bounds__(kProjThreads, 5)   // five blocks an SM: the k
     }
 }
 
+// The tiles in the order the blends take them: heaviest first (by the bit
+// length of their pair count), so that the last tiles of the queue are light.
+__global__ void __launch_bounds__(1024)
+    tileOrderKernel(const uint2* __restrict__ ranges, uint32_t totalTiles, uint32_t* __restrict__ order) {
+    __shared__ uint32_t sCount[33], sStart[33];
+    if (threadIdx.x < 33) sCount[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < totalTiles; t += blockDim.x) {
+        const uint2 r = ranges[t];
+        atomicAdd(&sCount[32 - __clz(r.y - r.x)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t s = 0;
+        for (int k = 32; k >= 0; --k) {
+            sStart[k] = s;
+            s += sCount[k];
+        }
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < totalTiles; t += blockDim.x) {
+        const uint2 r = ranges[t];
+        order[atomicAdd(&sStart[32 - __clz(r.y - r.x)], 1u)] = t;
+    }
+}
+
 // Each tile's range in the sorted pairs: a thread takes a run of eight keys (four
 // 16-byte loads) and the key before it, and writes a range's start and the
 // previous range's end where the tile changes.
@@ -680,7 +706,7 @@ struct ath_batch {
     std::vector<uint32_t> widths, heights, tileBases;
     uint32_t lastSorted = 0, lastSlotBits = 0;
     // scratch
-    DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges;
+    DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges, tileOrder;
     uint32_t keyMode = 0;      // 0 automatic; 1 packed; 2 wide; 3 packed, depth exponent renumbered
     bool lastWide = false;
     // the pairs' form, planned by each sizing from its depths' exponents
@@ -821,6 +847,7 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
     L.values = B.wide ? static_cast<const uint32_t*>(b->values[sorted].ptr) : nullptr;
     L.recs = static_cast<const float4*>(b->recs.ptr);
     L.words = static_cast<uint32_t*>(b->words.ptr);
+    L.order = static_cast<const uint32_t*>(b->tileOrder.ptr);
     L.sms = b->sms;
     L.tile = b->tile;
     L.blockBatch = b->blockBatch;
@@ -875,6 +902,11 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
                                                     static_cast<uint2*>(b->ranges.ptr), words + kBatchStatus);
         err = cudaGetLastError();
     }
+    if (err == cudaSuccess && b->totalTiles) {
+        tileOrderKernel<<<1, 1024, 0, stream>>>(static_cast<const uint2*>(b->ranges.ptr), b->totalTiles,
+                                               static_cast<uint32_t*>(b->tileOrder.ptr));
+        err = cudaGetLastError();
+    }
     mark(3);
     const bool train = target != nullptr;
     if (err == cudaSuccess && train) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
@@ -902,6 +934,7 @@ ath_status reserveBatch(ath_batch* b, uint32_t count) {
     if (err == cudaSuccess) err = b->grads.reserve((size_t)V * count * kGradWords * sizeof(float));
     if (err == cudaSuccess) err = b->projFlags.reserve((size_t)std::max(1u, gaussBlocks * V) * 8);
     if (err == cudaSuccess) err = b->ranges.reserve((size_t)std::max(1u, b->totalTiles) * 8);
+    if (err == cudaSuccess) err = b->tileOrder.reserve((size_t)std::max(1u, b->totalTiles) * 4);
     if (err == cudaSuccess) err = b->sortHist.reserve(8 * 256 * sizeof(uint32_t));
     if (err == cudaSuccess) err = b->viewsDev.reserve(std::max<size_t>(1, b->views.size()) * sizeof(BatchView));
     if (err != cudaSuccess) return failCuda(err, "reserving the batch's scratch");

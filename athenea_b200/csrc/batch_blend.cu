@@ -100,7 +100,9 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
 }
 
 // ---- the blends of a training step: forward, loss and adjoint, a tile at a time ----
-// One block of T*T/2 threads takes tiles off a queue and, for each, runs the
+// One block of T*T/2 threads takes tiles off a queue (heaviest first: `order`,
+// by the bit length of their pair counts, so the queue ends on light tiles)
+// and, for each, runs the
 // forward blend, the loss of its pixels, and the blend's adjoint, so that each
 // pixel's final transmittance, last contributor and loss gradient stay in
 // registers between the two walks.
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
                     const float4* __restrict__ recs, float4* __restrict__ colour, const float* __restrict__ target,
                     float* __restrict__ loss, float* __restrict__ grads, float* __restrict__ depth,
-                    uint32_t* __restrict__ words) {
+                    uint32_t* __restrict__ words, const uint32_t* __restrict__ order) {
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
     constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
@@ -157,7 +159,8 @@ __global__ void __launch_bounds__(T * T / 2, 2)
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) {
-            sTile = atomicAdd(&words[kBatchBlendTicket], 1u);
+            const uint32_t ticket = atomicAdd(&words[kBatchBlendTicket], 1u);
+            sTile = ticket < B.totalTiles ? order[ticket] : ticket;
             sMaxLast = 0;
         }
         __syncthreads();
@@ -425,12 +428,12 @@ cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t str
         const int grid = residentGrid(blendStepKernel<T, NB, true>, T * T / 2, L.sms);
         blendStepKernel<T, NB, true><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs,
                                                                          colour, target, loss, grads, nullptr,
-                                                                         L.words);
+                                                                         L.words, L.order);
     } else {
         const int grid = residentGrid(blendStepKernel<T, NB, false>, T * T / 2, L.sms);
         blendStepKernel<T, NB, false><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values,
                                                                           L.recs, colour, nullptr, nullptr, nullptr,
-                                                                          depth, L.words);
+                                                                          depth, L.words, L.order);
     }
     return cudaGetLastError();
 }

@@ -127,6 +127,7 @@ struct BlendLaunch {
     const uint32_t* values;  // wide pairs: the Gaussian of each sorted pair; null when packed
     const float4* recs;
     uint32_t* words;
+    const uint32_t* order;   // the tiles, heaviest first
     int sms;
     uint32_t tile, blockBatch;
 };

@@ -398,8 +398,9 @@ def run_ours(args) -> dict | None:
     total_tiles = sum(((W + T - 1) // T) * ((H + T - 1) // T) for _, W, H in views)
     passes = math.ceil((buf["depth_bits"] + max(1, math.ceil(math.log2(max(2, total_tiles))))) / 8)
     # the step's kernels: begin, projectEmit, histogram, the sort's passes, ranges,
-    # the blends (forward, loss and adjoint), projection adjoint (memsets are not counted)
-    launches = (2 + 1 + passes + 1 + 1 + 1) * args.steps
+    # the tile order, the blends (forward, loss and adjoint), projection adjoint
+    # (memsets are not counted)
+    launches = (2 + 1 + passes + 1 + 1 + 1 + 1) * args.steps
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
                ms_render=ms_render,
                stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
