@@ -75,9 +75,14 @@ class FrameStats(C.Structure):
                 ("total_ms", C.c_double)]
 
 
+class CloudCounts(C.Structure):
+    _fields_ = [("visible", C.c_uint32), ("pairs", C.c_uint32)]
+
+
 class SplatCounters(C.Structure):
     _fields_ = [("tag", C.c_uint64), ("slots", C.c_uint32), ("visible", C.c_uint32), ("pairs", C.c_uint32),
-                ("max_tiles", C.c_uint32), ("culled", C.c_uint32 * 7)]
+                ("max_tiles", C.c_uint32), ("culled", C.c_uint32 * 7), ("cloud_count", C.c_uint32),
+                ("clouds", CloudCounts * 64)]
 
 
 class FrameBuffers(C.Structure):
@@ -138,6 +143,7 @@ SIGNATURES = {
     "ath_raster_render": (C.c_int32, [_P, C.POINTER(Projection), _P, C.c_uint32, C.POINTER(Settings),
                                       C.POINTER(Targets), C.POINTER(FrameStats), _P]),
     "ath_raster_latest_counters": (C.c_int32, [_P, C.POINTER(SplatCounters)]),
+    "ath_raster_check": (C.c_int32, [_P, C.POINTER(FrameStats)]),
     "ath_raster_render_over": (C.c_int32, [_P, C.POINTER(Projection), _P, C.c_uint32, C.POINTER(Settings),
                                            C.POINTER(Targets), C.POINTER(Targets), C.POINTER(FrameStats), _P]),
     "ath_raster_render_params": (C.c_int32, [_P, C.POINTER(Projection), C.POINTER(Params), C.POINTER(Settings),
@@ -168,7 +174,9 @@ SIGNATURES = {
     "ath_sorter_create": (C.c_int32, [C.POINTER(C.c_void_p)]),
     "ath_sorter_destroy": (None, [_P]),
     "ath_sorter_sort": (C.c_int32, [_P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, _P]),
+    "ath_sorter_check": (C.c_int32, [_P]),
     "ath_sort_pairs_static": (C.c_int32, [_P, _P, _P, _P, C.c_uint32, C.c_uint32, _P]),
+    "ath_sort_pairs_static_status": (C.c_int32, [_P]),
     "ath_decode_records": (C.c_int32, [_P, C.c_uint32, C.POINTER(Encoding), _P, _P, _P, C.POINTER(C.c_uint32), _P]),
     "ath_last_error_message": (C.c_char_p, []),
     "ath_version": (C.c_char_p, []),

@@ -29,12 +29,30 @@ struct ath_raster {
     DeviceBuffer recs, rects, keys, offsets, projectFlags, instances;
     DeviceBuffer pairKeys[2], pairVals[2], sortHist, sortFlags, ranges;
     DeviceBuffer words;          // kFrameWords
-    PinnedBuffer wordsHost;      // kFrameWords, the mid-frame read
+    PinnedBuffer wordsHost;      // kFrameWords: a frame that waits (its handle's first, or timed) reads them here
     PinnedBuffer instanceStage;  // InstanceConst staging for the H2D copy
+    // The last frame's words, copied at its end behind `frameDone` (ath_raster_check,
+    // and the next frame's capacity, read them once that event has passed).
+    PinnedBuffer statusHost;
+    cudaEvent_t frameDone = nullptr;
+    bool frameRecorded = false;
+    uint32_t frameSlots = 0;
+    // Counted frames' words: a ring of kCountDepth copies behind events, as the
+    // reference's AsyncReadback (TileRasterizer.cpp:1297-1381; depth 3), so that
+    // ath_raster_latest_counters returns the newest finished one without waiting.
+    static constexpr int kCountDepth = 3;
+    PinnedBuffer countHost[kCountDepth];
+    cudaEvent_t countDone[kCountDepth] = {};
+    struct CountMeta {
+        uint64_t seq = 0, tag = 0;
+        uint32_t slots = 0, clouds = 0;
+    } countMeta[kCountDepth];
+    uint64_t countSeq = 0;
     bool haveCounters = false;
+    uint64_t countersSeq = 0;   // the sequence number of `counters`
     ath_splat_counters counters{};
     cudaEvent_t marks[8] = {};
-    uint32_t lastSlots = 0, lastPairs = 0, lastTiles = 0, lastSorted = 0;   // what frame_buffers describes
+    uint32_t lastSlots = 0, lastTiles = 0, lastSorted = 0;   // what frame_buffers describes
     FrameConst lastFrame{};
     // the differentiable frame's state (ath_raster_render_params -> ath_raster_backward)
     DeviceBuffer finalT, lastContrib, grads;
@@ -45,8 +63,10 @@ struct ath_raster {
 
 struct ath_sorter {
     int device = 0;
-    DeviceBuffer hist, flags, words;   // words: 8 pass tickets, then the sticky status
+    DeviceBuffer hist, flags, words;   // words: 8 pass tickets, then the status, kept until ath_sorter_check
     PinnedBuffer wordsHost;
+    cudaEvent_t done = nullptr;        // after the last sort
+    bool recorded = false;
 };
 
 namespace {
@@ -286,9 +306,15 @@ extern "C" ath_status ath_raster_create(ath_raster** out) {
     cudaError_t err = cudaGetDevice(&r->device);
     if (err == cudaSuccess) err = cudaDeviceGetAttribute(&r->sms, cudaDevAttrMultiProcessorCount, r->device);
     if (err == cudaSuccess) err = sortPrepare();
-    if (err == cudaSuccess) err = r->words.reserve((kFrameWords + 1) * sizeof(uint32_t));
-    if (err == cudaSuccess) err = r->wordsHost.reserve((kFrameWords + 1) * sizeof(uint32_t));
-    if (err == cudaSuccess) err = cudaMemset(r->words.ptr, 0, (kFrameWords + 1) * sizeof(uint32_t));
+    if (err == cudaSuccess) err = r->words.reserve(kFrameWords * sizeof(uint32_t));
+    if (err == cudaSuccess) err = r->wordsHost.reserve(kFrameWords * sizeof(uint32_t));
+    if (err == cudaSuccess) err = r->statusHost.reserve(kFrameWords * sizeof(uint32_t));
+    for (int k = 0; k < ath_raster::kCountDepth && err == cudaSuccess; ++k) {
+        err = r->countHost[k].reserve(kFrameWords * sizeof(uint32_t));
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&r->countDone[k], cudaEventDisableTiming);
+    }
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&r->frameDone, cudaEventDisableTiming);
+    if (err == cudaSuccess) err = cudaMemset(r->words.ptr, 0, kFrameWords * sizeof(uint32_t));
     for (int k = 0; k < 8 && err == cudaSuccess; ++k) err = cudaEventCreate(&r->marks[k]);
     if (err != cudaSuccess) {
         ath_status s = failCuda(err, "ath_raster_create");
@@ -304,6 +330,9 @@ extern "C" void ath_raster_destroy(ath_raster* r) {
     DeviceGuard guard(r->device);
     for (cudaEvent_t& e : r->marks)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : r->countDone)
+        if (e) cudaEventDestroy(e);
+    if (r->frameDone) cudaEventDestroy(r->frameDone);
     delete r;
 }
 
@@ -318,13 +347,55 @@ extern "C" ath_status ath_raster_release_scratch(ath_raster* r) {
                             &r->sortFlags, &r->ranges, &r->finalT, &r->lastContrib, &r->grads})
         b->release();
     r->trainingValid = false;
+    r->frameRecorded = false;
     r->instanceStage.release();
     return ATH_OK;
 }
 
+namespace {
+
+// A counted frame's words as SplatCounters (TileRasterizer.cpp:1356-1381).
+ath_splat_counters countersOf(const uint32_t* w, const ath_raster::CountMeta& m) {
+    ath_splat_counters c{};
+    c.tag = m.tag;
+    c.slots = m.slots;
+    c.visible = w[kWordVisible];
+    c.pairs = w[kWordPairsLo];
+    c.max_tiles = w[kWordMaxTiles];
+    for (int k = 0; k < 7; ++k) c.culled[k] = w[kWordCulled + k];
+    c.cloud_count = std::min(m.clouds, kMaxClouds);
+    for (uint32_t k = 0; k < c.cloud_count; ++k) {
+        c.clouds[k].visible = w[kWordClouds + 2 * k];
+        c.clouds[k].pairs = w[kWordClouds + 2 * k + 1];
+    }
+    return c;
+}
+
+// The newest counted frame the device has finished, into r->counters; never waits.
+void pollCounters(ath_raster* r) {
+    int newest = -1;
+    for (int k = 0; k < ath_raster::kCountDepth; ++k) {
+        const ath_raster::CountMeta& m = r->countMeta[k];
+        if (m.seq == 0 || m.seq <= r->countersSeq) continue;
+        if (cudaEventQuery(r->countDone[k]) != cudaSuccess) continue;
+        if (newest < 0 || m.seq > r->countMeta[newest].seq) newest = k;
+    }
+    cudaGetLastError();   // a not-ready query leaves cudaErrorNotReady as the last error
+    if (newest < 0) return;
+    r->counters = countersOf(static_cast<const uint32_t*>(r->countHost[newest].ptr), r->countMeta[newest]);
+    r->countersSeq = r->countMeta[newest].seq;
+    r->haveCounters = true;
+}
+
+}   // namespace
+
+// latestCounters (TileRasterizer.h:478; TileRasterizer.cpp:1356-1381): the newest
+// counted frame the device has finished, read from pinned memory its copy
+// landed in; never waits. A frame drawn without count_splats leaves it as it was.
 extern "C" ath_status ath_raster_latest_counters(ath_raster* r, ath_splat_counters* out) {
     if (!r || !out) return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_latest_counters: null argument");
-    if (!r->haveCounters) return fail(ATH_E_NOT_FOUND, "no frame has counted its splats yet");
+    pollCounters(r);
+    if (!r->haveCounters) return fail(ATH_E_NOT_FOUND, "no counted frame has finished yet");
     *out = r->counters;
     return ATH_OK;
 }
@@ -390,10 +461,44 @@ ath_status checkFrame(const ath_settings& s, const ath_targets& targets) {
     return ATH_OK;
 }
 
-// One frame: project (scan fused), the one mid-frame read, emit, sort, ranges,
-// blend. `staged` is the instance table in host memory (pinned staging).
-// `training` also keeps, per pixel, the final transmittance and the last
-// record blended, for the backward.
+// The status bits of a frame's words as a status: the frame is not valid when any is set.
+ath_status frameStatusOf(const uint32_t* w) {
+    const uint32_t bits = w[kWordStatus] | w[kWordSticky];
+    if (bits & kStatusLookbackTimeout)
+        return fail(ATH_E_TIMEOUT, "a look-back wait gave up (bounded spin); the frame is not valid");
+    if (bits & kStatusPairOverflow)
+        return fail(ATH_E_CAPACITY, "the frame's pairs outgrew the pair buffers; the frame is not valid "
+                                    "(the next frame grows them)");
+    if (bits & kStatusIndexRange)
+        return fail(ATH_E_INTERNAL, "the frame met an index outside its buffers (skipped, not written)");
+    return ATH_OK;
+}
+
+uint64_t pairsOf(const uint32_t* w) { return (uint64_t)w[kWordPairsLo] | ((uint64_t)w[kWordPairsHi] << 32); }
+
+// What the last frame asked of the pairs, once the device has finished it (never
+// waits): the capacity the next frame needs.
+uint64_t lastFrameNeed(ath_raster* r) {
+    if (!r->frameRecorded) return 0;
+    if (cudaEventQuery(r->frameDone) != cudaSuccess) {
+        cudaGetLastError();   // not ready
+        return 0;
+    }
+    return pairsOf(static_cast<const uint32_t*>(r->statusHost.ptr));
+}
+
+// One frame: project (scan fused), emit, sort, ranges, blend, with nothing read
+// back in between. The pairs are sized from a capacity: a handle's first frame
+// (and its first after release_scratch) reads the pair total back once and sizes
+// them exactly, as the reference does every frame (TileRasterizer.cpp:1093-1102);
+// later frames use the capacity the earlier ones needed. A frame whose pairs
+// outgrow it raises an overflow status (ath_raster_check reports ATH_E_CAPACITY)
+// and the next frame grows the pairs. The sort, the ranges and the blends take
+// the pair count from the device. At its end the frame's words are copied to
+// pinned memory behind an event (its status, for ath_raster_check), and, when it
+// counts, to the counters' ring. `staged` is the instance table in host memory
+// (pinned staging). `training` also keeps, per pixel, the final transmittance
+// and the last record blended, for the backward.
 ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, uint32_t instanceCount,
                      uint32_t slots, uint32_t layout, const ath_settings& s, ath_targets* targets,
                      ath_frame_stats* stats, cudaStream_t stream, bool training, const ath_targets* under = nullptr) {
@@ -413,9 +518,16 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
         if (err == cudaSuccess) err = r->lastContrib.reserve(pixels * 4);
         if (err != cudaSuccess) return failCuda(err, "reserving the backward's per-pixel state");
     }
+    // The pairs an earlier frame needed, if the device has finished it: grow to them.
+    if (const uint64_t need = lastFrameNeed(r); need > r->pairCapacity) {
+        if (need > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 (tile, splat) pairs in one frame");
+        if ((st = reservePairs(r, (uint32_t)std::min<uint64_t>(need + need / 7 + 4096, 0xFFFFFFFFull), bits)) != ATH_OK)
+            return st;
+    }
     uint32_t* words = static_cast<uint32_t*>(r->words.ptr);
     uint32_t* wordsHost = static_cast<uint32_t*>(r->wordsHost.ptr);
     const bool timed = s.time_stages != 0;
+    const bool sizing = r->pairCapacity == 0 || !r->pairKeys[0].bytes;   // no capacity yet: read the total once
     auto mark = [&](int k) { if (timed) cudaEventRecord(r->marks[k], stream); };
 
     // --- project, with the tiles-touched scan fused in --------------------
@@ -432,49 +544,47 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
                             static_cast<uint32_t*>(r->keys.ptr), static_cast<uint32_t*>(r->offsets.ptr),
                             static_cast<uint64_t*>(r->projectFlags.ptr), words, stream);
     mark(1);
-    // The one mid-frame read, as the reference's (TileRasterizer.cpp:1093-1102).
-    if (err == cudaSuccess)
-        err = cudaMemcpyAsync(wordsHost, words, (kFrameWords + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
-    if (err != cudaSuccess) return failCuda(err, "projecting the splats");
-    mark(2);
-    if (wordsHost[kWordSticky] & (kStatusLookbackTimeout | kStatusIndexRange)) {
-        // Raised after the read of a frame that did not wait for its end: that
-        // frame is not valid, and this call reports it.
-        const uint32_t b = wordsHost[kWordSticky];
-        cudaMemsetAsync(words + kWordSticky, 0, sizeof(uint32_t), stream);
-        if (b & kStatusLookbackTimeout)
-            return fail(ATH_E_TIMEOUT, "a look-back wait of the previous frame's sort gave up (bounded spin)");
-        return fail(ATH_E_INTERNAL, "the previous frame met an index outside its buffers (skipped, not written)");
+    bool haveTotals = false;
+    if (sizing && err == cudaSuccess) {
+        // The handle's sizing read: the frame's pair total, to size the pairs exactly.
+        err = cudaMemcpyAsync(wordsHost, words, kFrameWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+        if (err != cudaSuccess) return failCuda(err, "projecting the splats");
+        if (wordsHost[kWordStatus] & kStatusLookbackTimeout)
+            return fail(ATH_E_TIMEOUT, "a look-back wait gave up (bounded spin); the frame is not valid");
+        const uint64_t pairs64 = pairsOf(wordsHost);
+        if (pairs64 > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 (tile, splat) pairs in one frame");
+        // room for the next frames to vary without outgrowing it (a seventh over)
+        const uint64_t plan = std::min<uint64_t>(std::max<uint64_t>(pairs64, 1) + pairs64 / 7, 0xFFFFFFFFull);
+        if ((st = reservePairs(r, (uint32_t)plan, bits)) != ATH_OK) return st;
+        haveTotals = true;
     }
-    if (wordsHost[kWordStatus] & kStatusLookbackTimeout)
-        return fail(ATH_E_TIMEOUT, "a look-back wait gave up (bounded spin); the frame is not valid");
-    const uint64_t pairs64 = (uint64_t)wordsHost[kWordPairsLo] | ((uint64_t)wordsHost[kWordPairsHi] << 32);
-    if (pairs64 > 0xFFFFFFFFull) return fail(ATH_E_UNSUPPORTED, "more than 2^32 (tile, splat) pairs in one frame");
-    const uint32_t pairs = (uint32_t)pairs64;
-    const uint32_t visible = wordsHost[kWordVisible];
-    st = reservePairs(r, std::max(pairs, 1u), bits);
-    if (st != ATH_OK) return st;
+    if (err != cudaSuccess) return failCuda(err, "projecting the splats");
+    if ((st = reservePairs(r, r->pairCapacity, bits)) != ATH_OK) return st;   // the sort's scratch for this frame's bits
+    mark(2);
 
-    // --- emit, sort, ranges --------------------------------------------------
+    // --- emit, sort, ranges (the pair count on the device) ------------------
+    const uint32_t capacity = r->pairCapacity;
+    uint32_t* kept = words + kWordPairsKept;
     uint64_t* keysBuf[2] = {static_cast<uint64_t*>(r->pairKeys[0].ptr), static_cast<uint64_t*>(r->pairKeys[1].ptr)};
     uint32_t* valsBuf[2] = {static_cast<uint32_t*>(r->pairVals[0].ptr), static_cast<uint32_t*>(r->pairVals[1].ptr)};
     err = launchEmit(F, slots, static_cast<const float4*>(r->recs.ptr), static_cast<const uint2*>(r->rects.ptr),
                      static_cast<const uint32_t*>(r->keys.ptr), static_cast<const uint32_t*>(r->offsets.ptr), words,
-                     r->pairCapacity, keysBuf[0], valsBuf[0], stream);
+                     capacity, keysBuf[0], valsBuf[0], stream);
     mark(3);
     if (err == cudaSuccess)
-        err = launchSort(keysBuf, valsBuf, pairs, bits, static_cast<uint32_t*>(r->sortHist.ptr),
-                         static_cast<uint64_t*>(r->sortFlags.ptr), words + kWordSortTickets, words + kWordSticky,
-                         stream);
-    const uint32_t sorted = sortResultIndex(pairs, bits);
+        err = launchSortDevice(keysBuf, valsBuf, capacity, kept, nullptr, 0, bits, static_cast<uint32_t*>(r->sortHist.ptr),
+                               static_cast<uint64_t*>(r->sortFlags.ptr), words + kWordSortTickets, words + kWordSticky,
+                               stream);
+    const uint32_t sorted = sortPasses(bits) & 1u;
     if (err == cudaSuccess) err = cudaMemsetAsync(r->ranges.ptr, 0, (size_t)tiles * 8, stream);
     if (err == cudaSuccess)
-        err = launchRanges(pairs, tiles, keysBuf[sorted], static_cast<uint2*>(r->ranges.ptr), words + kWordSticky, stream);
+        err = launchRanges(capacity, kept, tiles, keysBuf[sorted], static_cast<uint2*>(r->ranges.ptr),
+                           words + kWordSticky, stream);
     mark(4);
     // --- blend ---------------------------------------------------------------
     if (err == cudaSuccess)
-        err = launchBlend(F, pairs, slots, static_cast<const uint2*>(r->ranges.ptr), valsBuf[sorted],
+        err = launchBlend(F, capacity, slots, static_cast<const uint2*>(r->ranges.ptr), valsBuf[sorted],
                           static_cast<const float4*>(r->recs.ptr), reinterpret_cast<float4*>(targets->colour),
                           targets->depth, reinterpret_cast<float4*>(targets->position),
                           training ? static_cast<float*>(r->finalT.ptr) : nullptr,
@@ -484,52 +594,49 @@ ath_status drawFrame(ath_raster* r, const FrameConst& F, InstanceConst* staged, 
                           Matte{s.crypto_ids, s.crypto, under ? s.under_crypto : nullptr, s.matte_lift, s.matte,
                                 s.matte_hard != 0 ? 1u : 0u, s.matte_threshold, s.trace});
     mark(5);
+    // --- the frame's words: its counters into the ring; its status behind an event
+    // (last, so that a wait for the frame covers both)
+    if (err == cudaSuccess && s.count_splats) {
+        const int k = (int)(r->countSeq % ath_raster::kCountDepth);
+        r->countMeta[k] = ath_raster::CountMeta{};   // not readable until its new copy has landed
+        err = cudaMemcpyAsync(r->countHost[k].ptr, words, kFrameWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+        if (err == cudaSuccess) err = cudaEventRecord(r->countDone[k], stream);
+        if (err == cudaSuccess) r->countMeta[k] = ath_raster::CountMeta{++r->countSeq, s.counters_tag, slots, instanceCount};
+    }
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(r->statusHost.ptr, words, kFrameWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    if (err == cudaSuccess) err = cudaEventRecord(r->frameDone, stream);
     if (err != cudaSuccess) return failCuda(err, "drawing the frame");
+    r->frameRecorded = true;
+    r->frameSlots = slots;
     r->lastSlots = slots;
-    r->lastPairs = pairs;
     r->lastTiles = tiles;
     r->lastSorted = sorted;
     r->lastFrame = F;
 
     ath_frame_stats out{};
     out.splats = slots;
-    out.visible = visible;
-    out.pairs = pairs;
-    if (s.count_splats || timed) {
-        // Waited for, as a frame that asks for its counts or its stage times is.
-        err = cudaMemcpyAsync(wordsHost, words, (kFrameWords + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
-        if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
-        if (err != cudaSuccess) return failCuda(err, "reading the frame's counters");
-        if (wordsHost[kWordSticky] & (kStatusLookbackTimeout | kStatusIndexRange)) {
-            const uint32_t b = wordsHost[kWordSticky];
-            cudaMemsetAsync(words + kWordSticky, 0, sizeof(uint32_t), stream);
-            if (b & kStatusLookbackTimeout)
-                return fail(ATH_E_TIMEOUT, "a look-back wait in the sort gave up (bounded spin); the frame is not valid");
-            return fail(ATH_E_INTERNAL, "the frame met an index outside its buffers (skipped, not written)");
-        }
-        if (s.count_splats) {
-            ath_splat_counters& c = r->counters;
-            c = ath_splat_counters{};
-            c.tag = s.counters_tag;
-            c.slots = slots;
-            c.visible = visible;
-            c.pairs = pairs;
-            c.max_tiles = wordsHost[kWordMaxTiles];
-            for (int k = 0; k < 7; ++k) c.culled[k] = wordsHost[kWordCulled + k];
-            r->haveCounters = true;
-        }
-        if (timed) {
-            auto ms = [&](int a, int b) {
-                float v = 0.0f;
-                cudaEventElapsedTime(&v, r->marks[a], r->marks[b]);
-                return (double)v;
-            };
-            out.project_ms = ms(0, 1);
-            out.counts_ms = ms(1, 2);
-            out.emit_ms = ms(2, 3);
-            out.tile_sort_ms = ms(3, 4);
-            out.blend_ms = ms(4, 5);
-        }
+    if (haveTotals) {
+        out.visible = wordsHost[kWordVisible];
+        out.pairs = (uint32_t)pairsOf(wordsHost);
+    }
+    if (timed) {
+        // A frame that asks for its stage times waits for its end, and so reports its own status.
+        if ((err = cudaEventSynchronize(r->frameDone)) != cudaSuccess) return failCuda(err, "timing the frame");
+        const uint32_t* w = static_cast<const uint32_t*>(r->statusHost.ptr);
+        if ((st = frameStatusOf(w)) != ATH_OK) return st;
+        out.visible = w[kWordVisible];
+        out.pairs = (uint32_t)pairsOf(w);
+        auto ms = [&](int a, int b) {
+            float v = 0.0f;
+            cudaEventElapsedTime(&v, r->marks[a], r->marks[b]);
+            return (double)v;
+        };
+        out.project_ms = ms(0, 1);
+        out.counts_ms = ms(1, 2);
+        out.emit_ms = ms(2, 3);
+        out.tile_sort_ms = ms(3, 4);
+        out.blend_ms = ms(4, 5);
     }
     out.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - frameStart).count();
     if (stats) *stats = out;
@@ -671,7 +778,7 @@ extern "C" ath_status ath_raster_backward(ath_raster* r, const float* dlDcolour,
     if (err == cudaSuccess) err = cudaMemsetAsync(r->grads.ptr, 0, (size_t)slots * kGradWords * sizeof(float), stream);
     uint32_t* words = static_cast<uint32_t*>(r->words.ptr);
     if (err == cudaSuccess)
-        err = launchBlendBackward(F, r->lastPairs, slots, static_cast<const uint2*>(r->ranges.ptr),
+        err = launchBlendBackward(F, r->pairCapacity, slots, static_cast<const uint2*>(r->ranges.ptr),
                                   static_cast<const uint32_t*>(r->pairVals[r->lastSorted].ptr),
                                   static_cast<const float4*>(r->recs.ptr), static_cast<const float*>(r->finalT.ptr),
                                   static_cast<const uint32_t*>(r->lastContrib.ptr),
@@ -681,8 +788,30 @@ extern "C" ath_status ath_raster_backward(ath_raster* r, const float* dlDcolour,
         err = launchProjectBackward(F, I, static_cast<const uint32_t*>(r->keys.ptr), static_cast<const float*>(r->grads.ptr),
                                     reinterpret_cast<float4*>(grads->means), reinterpret_cast<float4*>(grads->scales),
                                     reinterpret_cast<float4*>(grads->quats), grads->sh, stream);
+    // the frame's words again, with what the backward raised, for ath_raster_check
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(r->statusHost.ptr, words, kFrameWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    if (err == cudaSuccess) err = cudaEventRecord(r->frameDone, stream);
     if (err != cudaSuccess) return failCuda(err, "the backward");
     return ATH_OK;
+}
+
+// The last frame (and the backward after it, if any): waits for its end and
+// reports its status and totals.
+extern "C" ath_status ath_raster_check(ath_raster* r, ath_frame_stats* out) {
+    if (!r) return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_check: null handle");
+    if (!r->frameRecorded) return fail(ATH_E_NOT_FOUND, "no frame has been drawn on this handle");
+    DeviceGuard guard(r->device);
+    if (const cudaError_t err = cudaEventSynchronize(r->frameDone); err != cudaSuccess)
+        return failCuda(err, "waiting for the frame");
+    const uint32_t* w = static_cast<const uint32_t*>(r->statusHost.ptr);
+    if (out) {
+        *out = ath_frame_stats{};
+        out->splats = r->frameSlots;
+        out->visible = w[kWordVisible];
+        out->pairs = (uint32_t)std::min<uint64_t>(pairsOf(w), 0xFFFFFFFFull);
+    }
+    return frameStatusOf(w);
 }
 
 extern "C" ath_status ath_l2_loss(const float* colour, const float* target, uint32_t pixels, float* dlDcolour,
@@ -697,9 +826,13 @@ extern "C" ath_status ath_l2_loss(const float* colour, const float* target, uint
 
 extern "C" ath_status ath_raster_frame_buffers(ath_raster* r, ath_frame_buffers* out) {
     if (!r || !out) return fail(ATH_E_INVALID_ARGUMENT, "ath_raster_frame_buffers: null argument");
-    if (!r->recs.ptr) return fail(ATH_E_NOT_FOUND, "no frame has been drawn since the scratch was made");
+    if (!r->recs.ptr || !r->frameRecorded) return fail(ATH_E_NOT_FOUND, "no frame has been drawn since the scratch was made");
+    DeviceGuard guard(r->device);
+    // inspection: waits for the frame, whose pair count only the device knew
+    if (const cudaError_t err = cudaEventSynchronize(r->frameDone); err != cudaSuccess)
+        return failCuda(err, "waiting for the frame");
     out->slots = r->lastSlots;
-    out->pairs = r->lastPairs;
+    out->pairs = static_cast<const uint32_t*>(r->statusHost.ptr)[kWordPairsKept];
     out->tiles = r->lastTiles;
     out->records = static_cast<const float*>(r->recs.ptr);
     out->rects = static_cast<const uint32_t*>(r->rects.ptr);
@@ -724,8 +857,10 @@ extern "C" ath_status ath_sorter_create(ath_sorter** out) {
     if (err == cudaSuccess) err = s->words.reserve(16 * sizeof(uint32_t));
     if (err == cudaSuccess) err = s->wordsHost.reserve(16 * sizeof(uint32_t));
     if (err == cudaSuccess) err = cudaMemset(s->words.ptr, 0, 16 * sizeof(uint32_t));
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming);
     if (err != cudaSuccess) {
         const ath_status st = failCuda(err, "ath_sorter_create");
+        if (s->done) cudaEventDestroy(s->done);
         delete s;
         return st;
     }
@@ -736,6 +871,7 @@ extern "C" ath_status ath_sorter_create(ath_sorter** out) {
 extern "C" void ath_sorter_destroy(ath_sorter* s) {
     if (!s) return;
     DeviceGuard guard(s->device);
+    if (s->done) cudaEventDestroy(s->done);
     delete s;
 }
 
@@ -749,17 +885,7 @@ extern "C" ath_status ath_sorter_sort(ath_sorter* s, uint64_t* keys, uint32_t* v
     DeviceGuard guard(s->device);
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
     uint32_t* words = static_cast<uint32_t*>(s->words.ptr);
-    // A look-back that gave up in an earlier sort is reported here.
-    cudaError_t err = cudaMemcpyAsync(s->wordsHost.ptr, words, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
-    if (err != cudaSuccess) return failCuda(err, "ath_sorter_sort");
-    if (const uint32_t bits = static_cast<uint32_t*>(s->wordsHost.ptr)[8]; bits != 0) {
-        cudaMemsetAsync(words + 8, 0, sizeof(uint32_t), stream);
-        if (bits & kStatusLookbackTimeout)
-            return fail(ATH_E_TIMEOUT, "a look-back wait of an earlier sort gave up (bounded spin)");
-        return fail(ATH_E_INTERNAL, "an earlier sort met an index outside its buffers (skipped)");
-    }
-    err = s->flags.reserve(sortFlagWords(count, keyBits) * 8);
+    cudaError_t err = s->flags.reserve(sortFlagWords(count, keyBits) * 8);
     if (err != cudaSuccess) return failCuda(err, "reserving the sort's look-back words");
     uint64_t* k[2] = {keys, scratchKeys};
     uint32_t* v[2] = {values, scratchValues};
@@ -771,7 +897,27 @@ extern "C" ath_status ath_sorter_sort(ath_sorter* s, uint64_t* keys, uint32_t* v
         if (err == cudaSuccess)
             err = cudaMemcpyAsync(values, scratchValues, (size_t)count * 4, cudaMemcpyDeviceToDevice, stream);
     }
+    if (err == cudaSuccess) err = cudaEventRecord(s->done, stream);
     if (err != cudaSuccess) return failCuda(err, "sorting");
+    s->recorded = true;
+    return ATH_OK;
+}
+
+// Waits for the sorter's last sort and reports what its sorts since the last
+// check raised (then clears it).
+extern "C" ath_status ath_sorter_check(ath_sorter* s) {
+    if (!s) return fail(ATH_E_INVALID_ARGUMENT, "ath_sorter_check: null handle");
+    if (!s->recorded) return ATH_OK;
+    DeviceGuard guard(s->device);
+    uint32_t* words = static_cast<uint32_t*>(s->words.ptr);
+    uint32_t* host = static_cast<uint32_t*>(s->wordsHost.ptr);
+    cudaError_t err = cudaEventSynchronize(s->done);
+    if (err == cudaSuccess) err = cudaMemcpy(host, words + 8, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    const uint32_t bits = host[0];
+    if (err == cudaSuccess && bits) err = cudaMemset(words + 8, 0, sizeof(uint32_t));
+    if (err != cudaSuccess) return failCuda(err, "ath_sorter_check");
+    if (bits & kStatusLookbackTimeout) return fail(ATH_E_TIMEOUT, "a look-back wait of a sort gave up (bounded spin)");
+    if (bits) return fail(ATH_E_INTERNAL, "a sort met an index outside its buffers (skipped)");
     return ATH_OK;
 }
 

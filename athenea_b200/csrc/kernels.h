@@ -22,11 +22,14 @@ uint32_t projectBlocks(uint32_t slots);
 cudaError_t launchProject(const FrameConst& F, const InstanceConst* inst, uint32_t nInst, uint32_t slots,
                           uint32_t layout, bool countCulls, float4* recs, uint2* rects, uint32_t* keys,
                           uint32_t* offsets, uint64_t* flags, uint32_t* words, cudaStream_t stream);
+// Writes the pairs the buffers hold, min(pairs, capacity), into words[kWordPairsKept],
+// and raises kStatusPairOverflow in words[kWordSticky] past the capacity.
 cudaError_t launchEmit(const FrameConst& F, uint32_t slots, const float4* recs, const uint2* rects,
-                       const uint32_t* keys, const uint32_t* offsets, const uint32_t* words, uint64_t capacity,
+                       const uint32_t* keys, const uint32_t* offsets, uint32_t* words, uint64_t capacity,
                        uint64_t* pairKeys, uint32_t* pairValues, cudaStream_t stream);
-cudaError_t launchRanges(uint32_t pairs, uint32_t tiles, const uint64_t* pairKeys, uint2* ranges, uint32_t* status,
-                         cudaStream_t stream);
+// Ranges over at most `pairs` sorted keys; `pairsDevice`, when given, holds the count.
+cudaError_t launchRanges(uint32_t pairs, const uint32_t* pairsDevice, uint32_t tiles, const uint64_t* pairKeys,
+                         uint2* ranges, uint32_t* status, cudaStream_t stream);
 
 // sort.cu
 uint32_t sortPasses(uint32_t bits);

@@ -7,6 +7,8 @@
 // (splat/splat_ranges.slang:11-25).
 //
 // Built with --fmad=false: see splat_math.cuh.
+#include <algorithm>
+
 #include <cuda_runtime.h>
 
 #include "gauss.cuh"
@@ -151,8 +153,10 @@ __global__ void __launch_bounds__(kProjectThreads)
     __shared__ uint32_t sWarp[kProjectThreads / 32];
     __shared__ uint64_t sPrefix;
     __shared__ uint32_t sCulled[8];
+    __shared__ uint32_t sCloud[2 * kMaxClouds];   // count_splats: (visible, pairs) a cloud, this block's share
     if (threadIdx.x == 0) sTicket = atomicAdd(&words[kWordTicket], 1u);
     if (threadIdx.x < 8) sCulled[threadIdx.x] = 0;
+    if (countCulls && threadIdx.x < 2 * kMaxClouds) sCloud[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t b = sTicket;
     const uint32_t slot = b * kProjectThreads + threadIdx.x;
@@ -166,6 +170,11 @@ __global__ void __launch_bounds__(kProjectThreads)
         touched = p.touched;
         kept = p.key < kCulledKey;
         if (countCulls && !kept) atomicAdd(&sCulled[p.key & 7u], 1u);
+        // splatCountersCloud's rows (TileRasterizer.cpp:1335-1346): the first 64 clouds one by one
+        if (countCulls && kept && k < kMaxClouds) {
+            atomicAdd(&sCloud[2 * k], 1u);
+            atomicAdd(&sCloud[2 * k + 1], touched);
+        }
     }
     // block-wide exclusive scan of `touched`
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -204,6 +213,8 @@ __global__ void __launch_bounds__(kProjectThreads)
     }
     __syncthreads();
     if (countCulls && threadIdx.x < 7 && sCulled[threadIdx.x]) atomicAdd(&words[kWordCulled + threadIdx.x], sCulled[threadIdx.x]);
+    if (countCulls && threadIdx.x < 2 * kMaxClouds && sCloud[threadIdx.x])
+        atomicAdd(&words[kWordClouds + threadIdx.x], sCloud[threadIdx.x]);
     if (slot < slots) offsets[slot] = (uint32_t)(sPrefix + (incl - touched) + warpBase);
 }
 
@@ -216,13 +227,18 @@ __global__ void __launch_bounds__(kProjectThreads)
 __global__ void __launch_bounds__(256)
     emitKernel(uint32_t width, uint32_t height, uint32_t tilesX, uint32_t slots, const float4* __restrict__ recs,
                const uint2* __restrict__ rects, const uint32_t* __restrict__ keys,
-               const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ words, uint64_t capacity,
+               const uint32_t* __restrict__ offsets, uint32_t* __restrict__ words, uint64_t capacity,
                uint64_t* __restrict__ pairKeys, uint32_t* __restrict__ pairValues) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t total = (uint64_t)words[kWordPairsLo] | ((uint64_t)words[kWordPairsHi] << 32);
+    if (slot == 0) {
+        // what the sort, the ranges and the blends take: the pairs the buffers hold
+        words[kWordPairsKept] = (uint32_t)min(total, capacity);
+        if (total > capacity) atomicOr(&words[kWordSticky], kStatusPairOverflow);
+    }
     if (slot >= slots) return;
     const uint32_t key = keys[slot];
     if (key >= kCulledKey) return;
-    const uint64_t total = (uint64_t)words[kWordPairsLo] | ((uint64_t)words[kWordPairsHi] << 32);
     const uint32_t first = offsets[slot];
     const uint32_t expected = (slot + 1 < slots ? offsets[slot + 1] : (uint32_t)total) - first;
     const float4 s = recs[(size_t)slot * 3 + 0];
@@ -245,10 +261,12 @@ __global__ void __launch_bounds__(256)
 
 // splat_ranges.slang:11-25 over the sorted keys; ranges were cleared first
 // (splat_tiles_clear.slang).
+// `pairsDevice`, when given, holds the pair count (at most `pairs`, the grid's bound).
 __global__ void __launch_bounds__(256)
-    rangesKernel(uint32_t pairs, uint32_t tiles, const uint64_t* __restrict__ pairKeys, uint2* __restrict__ ranges,
-                 uint32_t* __restrict__ status) {
+    rangesKernel(uint32_t pairs, const uint32_t* __restrict__ pairsDevice, uint32_t tiles,
+                 const uint64_t* __restrict__ pairKeys, uint2* __restrict__ ranges, uint32_t* __restrict__ status) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pairsDevice) pairs = min(pairs, *pairsDevice);
     if (i >= pairs) return;
     const uint32_t t = (uint32_t)(pairKeys[i] >> 24);
     if (t >= tiles) {
@@ -282,18 +300,17 @@ cudaError_t launchProject(const FrameConst& F, const InstanceConst* inst, uint32
 uint32_t projectBlocks(uint32_t slots) { return (slots + kProjectThreads - 1) / kProjectThreads; }
 
 cudaError_t launchEmit(const FrameConst& F, uint32_t slots, const float4* recs, const uint2* rects,
-                       const uint32_t* keys, const uint32_t* offsets, const uint32_t* words, uint64_t capacity,
+                       const uint32_t* keys, const uint32_t* offsets, uint32_t* words, uint64_t capacity,
                        uint64_t* pairKeys, uint32_t* pairValues, cudaStream_t stream) {
-    if (slots == 0) return cudaSuccess;
-    emitKernel<<<(slots + 255) / 256, 256, 0, stream>>>(F.width, F.height, F.tilesX, slots, recs, rects, keys,
+    emitKernel<<<std::max(1u, (slots + 255) / 256), 256, 0, stream>>>(F.width, F.height, F.tilesX, slots, recs, rects, keys,
                                                         offsets, words, capacity, pairKeys, pairValues);
     return cudaGetLastError();
 }
 
-cudaError_t launchRanges(uint32_t pairs, uint32_t tiles, const uint64_t* pairKeys, uint2* ranges, uint32_t* status,
-                         cudaStream_t stream) {
+cudaError_t launchRanges(uint32_t pairs, const uint32_t* pairsDevice, uint32_t tiles, const uint64_t* pairKeys,
+                         uint2* ranges, uint32_t* status, cudaStream_t stream) {
     if (pairs == 0) return cudaSuccess;
-    rangesKernel<<<(pairs + 255) / 256, 256, 0, stream>>>(pairs, tiles, pairKeys, ranges, status);
+    rangesKernel<<<(pairs + 255) / 256, 256, 0, stream>>>(pairs, pairsDevice, tiles, pairKeys, ranges, status);
     return cudaGetLastError();
 }
 

@@ -46,18 +46,24 @@ struct InstanceConst {
     EditConst edit;
 };
 
-// Words of the small device block every frame reads back once.
+// Words of the small device block a frame keeps its counts and status in. All
+// of them are cleared at a frame's start; at its end they are copied to pinned
+// host memory behind an event (the frame's status, and its counters when it
+// counts), so nothing waits for them.
+constexpr uint32_t kMaxClouds = 64;   // SplatCounters::kMaxClouds (TileRasterizer.h:376)
 enum FrameWord : uint32_t {
     kWordTicket = 0,        // the projection's block ticket
     kWordVisible = 1,       // splats kept
-    kWordStatus = 2,        // kStatus* bits
+    kWordStatus = 2,        // kStatus* bits of the projection's scan
     kWordPairsLo = 3,       // pairs (the sum of tiles touched), 64-bit
     kWordPairsHi = 4,
     kWordMaxTiles = 5,
     kWordCulled = 6,        // 7 words: culled by reason (count_splats)
+    kWordPairsKept = 13,    // the pairs the buffers hold: min(pairs, capacity), what the sort sorts
     kWordSortTickets = 16,  // one a sort pass (up to 8)
-    kFrameWords = 32,       // reset at the start of every frame
-    kWordSticky = 32,       // status the sort raises; kept until a frame reads and clears it
+    kWordClouds = 24,       // 2 words a cloud (visible, pairs) for the first kMaxClouds instances (count_splats)
+    kWordSticky = kWordClouds + 2 * kMaxClouds,   // status the emit, sort, ranges, blends and backward raise
+    kFrameWords = kWordSticky + 1,                // cleared at the start of every frame
 };
 
 enum StatusBit : uint32_t {

@@ -13,8 +13,11 @@
 // The limit follows from that array's size: at most kStaticMaxCount pairs a
 // call, 4 MiB of device memory a GPU for the library's lifetime. Every call
 // shares the array and it keeps the last call's contents, so each call clears
-// what must start at zero; calls that overlap on the GPU (on different
-// streams, or from different threads without ordering) race on it.
+// what must start at zero (histograms, look-back words, tickets); calls that
+// overlap on the GPU (on different streams, or from different threads without
+// ordering) race on it. A call neither reads anything back nor waits: what the
+// calls raise collects in the array's status word until the caller asks for it
+// with ath_sort_pairs_static_status, which waits for the stream.
 #include <mutex>
 
 #include <cuda_runtime.h>
@@ -91,17 +94,9 @@ extern "C" ath_status ath_sort_pairs_static(uint64_t* keys, uint32_t* values, ui
     uint32_t* hist = reinterpret_cast<uint32_t*>(scratch + kFlagWords);
     uint32_t* counters = reinterpret_cast<uint32_t*>(scratch + kFlagWords + kHistWords);
     uint32_t* status = counters + 8;
-    // A look-back that gave up in an earlier call is reported here, and cleared.
-    uint32_t earlier = 0;
-    err = cudaMemcpyAsync(&earlier, status, sizeof(earlier), cudaMemcpyDeviceToHost, stream);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
-    if (err != cudaSuccess) return failCuda(err, "ath_sort_pairs_static");
-    if (earlier != 0) {
-        cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
-        if (earlier & kStatusLookbackTimeout)
-            return fail(ATH_E_TIMEOUT, "ath_sort_pairs_static: a look-back wait of an earlier call gave up");
-        return fail(ATH_E_INTERNAL, "ath_sort_pairs_static: an earlier call met an index outside its buffers");
-    }
+    // The status word is not read here: the call enqueues its work and returns.
+    // What a call raises (a look-back that gave up, an index outside the buffers)
+    // stays in the word until ath_sort_pairs_static_status reads and clears it.
     // launchSort clears the histograms, the look-back words and the tickets it uses.
     uint64_t* k[2] = {keys, scratchKeys};
     uint32_t* v[2] = {values, scratchValues};
@@ -112,5 +107,29 @@ extern "C" ath_status ath_sort_pairs_static(uint64_t* keys, uint32_t* values, ui
             err = cudaMemcpyAsync(values, scratchValues, (size_t)count * 4, cudaMemcpyDeviceToDevice, stream);
     }
     if (err != cudaSuccess) return failCuda(err, "ath_sort_pairs_static");
+    return ATH_OK;
+}
+
+// The sorts' status, when the caller chooses to look: waits for `stream` (the
+// stream the sorts were enqueued on), reads what the calls since the last look
+// raised from the static array, and clears it. Allocates nothing: the word is
+// read into a host variable by a plain copy.
+extern "C" ath_status ath_sort_pairs_static_status(void* streamPtr) {
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) return failCuda(err, "ath_sort_pairs_static_status");
+    uint64_t* scratch = nullptr;
+    const ath_status st = scratchOf(device, &scratch);
+    if (st != ATH_OK) return st;
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    uint32_t* status = reinterpret_cast<uint32_t*>(scratch + kFlagWords + kHistWords) + 8;
+    uint32_t bits = 0;
+    err = cudaStreamSynchronize(stream);
+    if (err == cudaSuccess) err = cudaMemcpy(&bits, status, sizeof(bits), cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess && bits != 0) err = cudaMemset(status, 0, sizeof(uint32_t));
+    if (err != cudaSuccess) return failCuda(err, "ath_sort_pairs_static_status");
+    if (bits & kStatusLookbackTimeout)
+        return fail(ATH_E_TIMEOUT, "ath_sort_pairs_static: a look-back wait of a sort gave up (bounded spin)");
+    if (bits != 0) return fail(ATH_E_INTERNAL, "ath_sort_pairs_static: a sort met an index outside its buffers");
     return ATH_OK;
 }

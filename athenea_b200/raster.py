@@ -309,14 +309,22 @@ class FrameStats:
 
 
 @dataclass
+class CloudCounts:
+    """SplatCounters::Cloud (TileRasterizer.h:396-399)."""
+    visible: int
+    pairs: int
+
+
+@dataclass
 class SplatCounters:
-    """TileRasterizer.h:333-401."""
+    """TileRasterizer.h:373-401."""
     tag: int
     slots: int
     visible: int
     pairs: int
     max_tiles: int
     culled: list
+    clouds: list
 
 
 class TileRasterizer:
@@ -342,10 +350,15 @@ class TileRasterizer:
             self._h = None
 
     def render(self, camera, instances, settings: RenderSettings, targets: RenderTargets,
-               stream: torch.cuda.Stream | None = None, under: "RenderTargets | None" = None) -> FrameStats:
+               stream: torch.cuda.Stream | None = None, under: "RenderTargets | None" = None,
+               do_check: bool = True) -> FrameStats:
         """render(const Camera&/const Projection&, ..., const RenderTargets* under) -> FrameStats
         (TileRasterizer.cpp:287-1295); `under`, when given, is an opaque layer the splats are
-        composited over (ath_raster_render_over)."""
+        composited over (ath_raster_render_over). The native frame neither reads back nor
+        waits; with `do_check` (the default, as the reference's render returns its totals and
+        errors) this waits for the frame through ath_raster_check, raising its status (an
+        overflow of the pairs is ATH_E_CAPACITY) and filling visible and pairs. do_check=False
+        returns at once, the totals 0 unless the frame read them."""
         proj = camera.projection_for(settings.width, settings.height) if isinstance(camera, Camera) else camera
         arr, n = _instances(instances)
         t = N.Targets(targets.width, targets.height, _ptr(targets.colour), _ptr(targets.depth),
@@ -360,16 +373,32 @@ class TileRasterizer:
             u = N.Targets(under.width, under.height, _ptr(under.colour), _ptr(under.depth), None)
             check(N.lib().ath_raster_render_over(self._h, C.byref(proj), arr, n, C.byref(settings._native()),
                                                  C.byref(t), C.byref(u), C.byref(stats), C.c_void_p(s.cuda_stream)))
+        if do_check:
+            self._check_into(stats)
         return FrameStats(*[getattr(stats, f) for f, _ in N.FrameStats._fields_])
 
+    def _check_into(self, stats) -> None:
+        totals = N.FrameStats()
+        check(N.lib().ath_raster_check(self._h, C.byref(totals)))
+        stats.visible, stats.pairs = totals.visible, totals.pairs
+
+    def check(self) -> FrameStats:
+        """ath_raster_check: waits for the last frame (and its backward) and returns its totals;
+        raises its status (ATH_E_CAPACITY when its pairs outgrew the buffers)."""
+        totals = N.FrameStats()
+        check(N.lib().ath_raster_check(self._h, C.byref(totals)))
+        return FrameStats(*[getattr(totals, f) for f, _ in N.FrameStats._fields_])
+
     def latest_counters(self) -> SplatCounters | None:
-        """latestCounters (TileRasterizer.h:478): None until a counted frame finished."""
+        """latestCounters (TileRasterizer.h:478): the newest counted frame the device has
+        finished, never waiting; None until one has."""
         c = N.SplatCounters()
         status = N.lib().ath_raster_latest_counters(self._h, C.byref(c))
         if status == 2:
             return None
         check(status)
-        return SplatCounters(c.tag, c.slots, c.visible, c.pairs, c.max_tiles, list(c.culled))
+        return SplatCounters(c.tag, c.slots, c.visible, c.pairs, c.max_tiles, list(c.culled),
+                             [CloudCounts(c.clouds[k].visible, c.clouds[k].pairs) for k in range(c.cloud_count)])
 
     def release_scratch(self) -> None:
         """releaseScratch (TileRasterizer.h:482)."""
@@ -437,9 +466,9 @@ class Params:
 
 
 def _render_params(self, camera, params: Params, settings: RenderSettings, targets: RenderTargets,
-                   stream: torch.cuda.Stream | None = None) -> FrameStats:
+                   stream: torch.cuda.Stream | None = None, do_check: bool = True) -> FrameStats:
     """A differentiable frame (ath_raster_render_params): render() for one cloud of training
-    parameters, keeping what backward() needs."""
+    parameters, keeping what backward() needs. do_check as for render()."""
     proj = camera.projection_for(settings.width, settings.height) if isinstance(camera, Camera) else camera
     t = N.Targets(targets.width, targets.height, _ptr(targets.colour), _ptr(targets.depth), _ptr(targets.position))
     stats = N.FrameStats()
@@ -448,6 +477,8 @@ def _render_params(self, camera, params: Params, settings: RenderSettings, targe
     check(N.lib().ath_raster_render_params(self._h, C.byref(proj), C.byref(params._native()),
                                            C.byref(settings._native()), C.byref(t), C.byref(stats),
                                            C.c_void_p(s.cuda_stream)))
+    if do_check:
+        self._check_into(stats)
     return FrameStats(*[getattr(stats, f) for f, _ in N.FrameStats._fields_])
 
 

@@ -214,7 +214,7 @@ class PlainTrainer:
         for v, (proj, W, H) in enumerate(self.views):
             frames, dl = self.frames[(W, H)], self.dl[(W, H)]
             stats = self.raster.render_params(proj, self.P, self.A.RenderSettings(width=W, height=H), frames,
-                                              stream=stream)
+                                              stream=stream, do_check=False)
             self.A.l2_loss(frames.colour, targets[v], dl, self.loss, stream=stream)
             self.raster.backward(dl, self.grads, stream=stream)
         return stats

@@ -33,7 +33,8 @@ extern "C" {
 
 /* core/Error.h:14-26 (ErrorCode), in its order, after ATH_OK; plus ATH_E_TIMEOUT
  * for a bounded device wait that gave up (the sort's look-back) and
- * ATH_E_CAPACITY for a frame whose pairs outgrew a caller-fixed capacity. */
+ * ATH_E_CAPACITY for a frame or step whose pairs outgrew the pair buffers'
+ * capacity (it is not valid; the next one grows them). */
 typedef enum {
     ATH_OK = 0,
     ATH_E_UNKNOWN = 1,
@@ -118,7 +119,7 @@ typedef struct {
     uint32_t depth_mode;        /* 0 alpha-weighted mean, 1 first threshold crossing */
     float depth_threshold;      /* default 0.5 */
     int32_t time_stages;        /* wait after each stage and fill the *_ms stats */
-    int32_t count_splats;       /* count culls by reason (ath_raster_latest_counters) */
+    int32_t count_splats;       /* count culls by reason and clouds (ath_raster_latest_counters); does not wait */
     uint64_t counters_tag;
     /* What each splat gave the frame, added into `contribution` (device memory,
      * never cleared here, so frames from many cameras sum into it), in the
@@ -184,11 +185,21 @@ typedef struct {
     double project_ms, counts_ms, depth_sort_ms, emit_ms, tile_sort_ms, blend_ms, total_ms;
 } ath_frame_stats;
 
-/* SplatCounters (TileRasterizer.h:333-401); culled[] in splat/frame.slang:42-49's numbering. */
+/* SplatCounters::Cloud (TileRasterizer.h:396-399): one instance's share. */
+typedef struct {
+    uint32_t visible, pairs;
+} ath_cloud_counts;
+
+/* SplatCounters (TileRasterizer.h:373-401); culled[] in splat/frame.slang:42-49's
+ * numbering. clouds[] holds the first cloud_count instances of the counted frame,
+ * in the order it was given them (at most 64, SplatCounters::kMaxClouds); later
+ * instances are only in the totals. */
 typedef struct {
     uint64_t tag;
     uint32_t slots, visible, pairs, max_tiles;
     uint32_t culled[7];
+    uint32_t cloud_count;
+    ath_cloud_counts clouds[64];
 } ath_splat_counters;
 
 /* ---- camera helpers ----------------------------------------------------- */
@@ -214,9 +225,20 @@ ath_status ath_raster_release_scratch(ath_raster* r);
 /* TileRasterizer::render(const Projection&, span<const SplatInstance>,
  * const RenderSettings&, RenderTargets&) (TileRasterizer.h:468-474;
  * TileRasterizer.cpp:296-1295). Enqueued on `stream` (a cudaStream_t; NULL:
- * the legacy default stream). Like the reference it reads the frame's visible
- * and pair totals back once mid-frame to size the pairs exactly; `stats` is
- * filled from those. Targets must be width x height of `settings`. */
+ * the legacy default stream) with nothing read back and no wait, where the
+ * reference waits once mid-frame for its visible and pair totals
+ * (TileRasterizer.cpp:1093-1102): the pairs are sized from a capacity the
+ * handle keeps, and the sort, ranges and blend take the pair count from the
+ * device. The one exception is a handle's first frame (and its first after
+ * ath_raster_release_scratch), which reads the pair total back once to size
+ * that capacity. A frame whose pairs outgrow the capacity is not valid:
+ * ath_raster_check reports it as ATH_E_CAPACITY, and the next frame grows the
+ * capacity (to what the last finished frame needed). `stats`: splats always;
+ * visible and pairs when the frame read them back (the sizing frame, or
+ * time_stages, whose frame waits for its end and returns its own status),
+ * else 0 -- ath_raster_check gives them. count_splats does not wait: the
+ * counters come back through ath_raster_latest_counters. Targets must be
+ * width x height of `settings`. */
 ath_status ath_raster_render(ath_raster* r, const ath_projection* projection, const ath_instance* instances,
                              uint32_t instance_count, const ath_settings* settings, ath_targets* targets,
                              ath_frame_stats* stats, void* stream);
@@ -411,9 +433,22 @@ typedef struct {
 
 ath_status ath_batch_buffers_of(ath_batch* b, ath_batch_buffers* out, void* stream);
 
-/* TileRasterizer::latestCounters (TileRasterizer.h:478). ATH_E_NOT_FOUND
- * until a frame drawn with count_splats has finished. */
+/* TileRasterizer::latestCounters (TileRasterizer.h:478; TileRasterizer.cpp:
+ * 1356-1381): the newest frame drawn with count_splats that the device has
+ * finished, read from pinned memory its counts were copied to behind an event
+ * (a ring of three, as the reference's AsyncReadback). Never waits: right after
+ * a frame it may still give an older one. A frame drawn without count_splats
+ * leaves it as it was. ATH_E_NOT_FOUND until a counted frame has finished. */
 ath_status ath_raster_latest_counters(ath_raster* r, ath_splat_counters* out);
+
+/* The last frame's status, and its totals (splats, visible, pairs) into `out`
+ * (may be NULL): waits for that frame (and for the ath_raster_backward after
+ * it, when there is one) to finish. ATH_E_CAPACITY: its pairs outgrew the
+ * handle's capacity (the frame is not valid; the next frame grows it).
+ * ATH_E_TIMEOUT: a bounded look-back wait gave up. ATH_E_INTERNAL: an index
+ * fell outside its buffer (skipped). ATH_E_NOT_FOUND: no frame yet. The
+ * reference reports these from render itself, which waits mid-frame. */
+ath_status ath_raster_check(ath_raster* r, ath_frame_stats* out);
 
 /* The last frame's intermediate buffers, for inspection (what the reference's
  * tests read through its Buffer handles). Device pointers owned by the
@@ -456,22 +491,34 @@ void ath_sorter_destroy(ath_sorter* s);
  * eight bits a pass. keys/values hold the input and receive the result; the
  * scratch pair (as SortBuffers' scratchKeys/scratchValues) holds count
  * entries each. An odd number of passes ends with a copy back. Enqueued on
- * `stream`, not waited for. */
+ * `stream`, not waited for, and nothing is read back: what the sorts raise is
+ * kept for ath_sorter_check. */
 ath_status ath_sorter_sort(ath_sorter* s, uint64_t* keys, uint32_t* values, uint64_t* scratch_keys,
                            uint32_t* scratch_values, uint32_t count, uint32_t key_bits, void* stream);
+/* Waits for the sorter's last sort and reports what its sorts raised since the
+ * last check: ATH_E_TIMEOUT for a look-back wait that gave up (bounded spin),
+ * ATH_E_INTERNAL for an index outside the buffers. Then clears it. */
+ath_status ath_sorter_check(ath_sorter* s);
 
 /* The same sort for callers that cannot allocate device memory while they
  * sort: a plugin whose host application owns the device memory and holds it to
  * a fixed budget mid-frame, or a real-time frame that cannot take the stall of
  * an allocation. It has no counterpart in the reference. The sort's own working
- * memory (histograms, look-back words, tickets) is a fixed 4 MiB array every GPU
- * that loads the library holds until exit; nothing is allocated. At most 1,048,576 pairs a call (larger counts
- * return ATH_E_INVALID_ARGUMENT). The first call on a device finds that array's
- * address and sets the kernel up: make it before any stream capture. Every call
- * shares the array, so calls that overlap on the GPU race; keys/values and the
- * scratch pair are as for ath_sorter_sort. */
+ * memory (histograms, look-back words, tickets, a status word) is a fixed 4 MiB
+ * array every GPU that loads the library holds until exit; nothing is
+ * allocated. At most 1,048,576 pairs a call (larger counts return
+ * ATH_E_INVALID_ARGUMENT). The first call on a device (or the first status
+ * query) finds that array's address and sets the kernel up: make it before any
+ * stream capture. A call enqueues its work and returns: it reads nothing back
+ * and does not wait. Every call shares the array, so calls that overlap on the
+ * GPU race; keys/values and the scratch pair are as for ath_sorter_sort. */
 ath_status ath_sort_pairs_static(uint64_t* keys, uint32_t* values, uint64_t* scratch_keys, uint32_t* scratch_values,
                                  uint32_t count, uint32_t key_bits, void* stream);
+/* What the calls of ath_sort_pairs_static on this device raised since the last
+ * query, when the caller chooses to look: waits for `stream`, then reports
+ * ATH_E_TIMEOUT (a look-back wait gave up) or ATH_E_INTERNAL (an index outside
+ * the buffers) and clears it. Allocates nothing. No counterpart in the reference. */
+ath_status ath_sort_pairs_static_status(void* stream);
 
 /* ---- decode: scene::CloudLoader::upload's kernels ------------------------ */
 

@@ -51,7 +51,14 @@ def digest(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()
 
 
-REFERENCE_SPLATS = "/root/reference/tests/data/splats"
+def reference_splats(root: str | None = None) -> str:
+    """The reference checkout's tests/data/splats: `root` (or ATHENEA_REFERENCE, the
+    checkout's top directory) joined with that path; "" when neither is given."""
+    root = root if root is not None else os.environ.get("ATHENEA_REFERENCE", "")
+    return os.path.join(root, "tests", "data", "splats") if root else ""
+
+
+REFERENCE_SPLATS = reference_splats()
 
 
 def read_ply_numpy(path):
@@ -72,12 +79,12 @@ def read_ply_numpy(path):
     return records, names, hashlib.sha256(raw).hexdigest()
 
 
-def ply_fixtures():
+def ply_fixtures(splats_dir: str):
     """tiny.ply (64 splats, degree 0) and sh3.ply (64 splats, degree 3) of the
     reference's tests/data/splats, as their records and property names."""
     out = {}
     for name in ("tiny", "sh3"):
-        records, names, sha = read_ply_numpy(os.path.join(REFERENCE_SPLATS, name + ".ply"))
+        records, names, sha = read_ply_numpy(os.path.join(splats_dir, name + ".ply"))
         out[name + "_records"] = records
         out[name + "_names"] = np.array(names)
         out[name + "_sha256"] = sha
@@ -86,6 +93,8 @@ def ply_fixtures():
 
 
 def main():
+    """python tests/golden/make_golden.py [reference checkout]: the checkout (or
+    ATHENEA_REFERENCE) is read only for its two splat fixture files."""
     from oracle import oracle as O
     O.build()
     records, packed, proj = scene()
@@ -98,8 +107,9 @@ def main():
         ranges=b["ranges"], colour_sha256=digest(out["colour"]), depth_sha256=digest(out["depth"]),
         colour_sample=out["colour"][::STRIDE], depth_sample=out["depth"][::STRIDE])
     print("wrote raster_random3000_250x190.npz:", b["pairs"], "pairs,", int(out["proj"]["visible"].sum()), "visible")
-    if os.path.isdir(REFERENCE_SPLATS):
-        ply_fixtures()
+    splats = reference_splats(sys.argv[1] if len(sys.argv) > 1 else None)
+    if splats and os.path.isdir(splats):
+        ply_fixtures(splats)
 
 
 if __name__ == "__main__":

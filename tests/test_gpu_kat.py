@@ -81,6 +81,7 @@ def test_counters_say_how_many_were_kept_and_why(native):   # :1831-1917
     cam.lens.focal = cam.lens.haperture
     assert raster.latest_counters() is None
     for tag in (41, 42):
+        # the frame is waited for (ath_raster_check), so its counts are the newest finished
         stats, _, _ = _draw(raster, cam, [a, b], 320, 240, count_splats=True, counters_tag=tag)
         c = raster.latest_counters()
         assert c is not None and c.tag == tag
@@ -89,8 +90,64 @@ def test_counters_say_how_many_were_kept_and_why(native):   # :1831-1917
         assert c.culled[2] == 4 and c.culled[4] == 3 and c.culled[5] == 5
         assert c.culled[1] == 0 and c.culled[0] == 0
         assert sum(c.culled) + c.visible == c.slots
+        # per cloud (:1900-1903)
+        assert len(c.clouds) == 2
+        assert c.clouds[0].visible == 10 and c.clouds[1].visible == 6
+        assert c.clouds[0].pairs + c.clouds[1].pairs == c.pairs
     _draw(raster, cam, [a, b], 320, 240, count_splats=False)
     assert raster.latest_counters().tag == 42
+
+
+def test_counters_come_back_without_waiting(native):
+    """latestCounters never waits (TileRasterizer.h:373-374): frames drawn without a check
+    return at once, and the counters name the newest counted frame the device finished."""
+    raster = A.TileRasterizer.create()
+    cloud = _upload(random_cloud(3000, 7))
+    cam = A.Camera.looking_at((1.5, 1.0, 6.0), (0, 0, 0))
+    s = A.RenderSettings(width=250, height=190, count_splats=True)
+    t = A.RenderTargets.make(250, 190)
+    seen = []
+    for tag in range(1, 8):
+        s.counters_tag = tag
+        stats = raster.render(cam, [A.SplatInstance(cloud)], s, t, do_check=False)
+        assert stats.splats == 3000
+        c = raster.latest_counters()
+        if c is not None:
+            seen.append(c.tag)
+    assert seen == sorted(seen)   # never an older frame after a newer one
+    torch.cuda.synchronize()
+    c = raster.latest_counters()
+    assert c.tag == 7 and c.slots == 3000 and len(c.clouds) == 1 and c.clouds[0].visible == c.visible
+    assert raster.check().pairs == c.pairs
+
+
+def test_a_frame_past_its_capacity_is_reported_then_grown(oracle, native):
+    """A frame is drawn with no read back: its pairs are sized from what earlier frames
+    needed. A frame that outgrows that is reported (ATH_E_CAPACITY) and the next is drawn
+    whole, equal to the restatement."""
+    from tests import gpu_helpers as G
+    raster = A.TileRasterizer.create()
+    cam = A.Camera.looking_at((1.5, 1.0, 6.0), (0, 0, 0))
+    W, H = 250, 190
+    small = _upload(random_cloud(300, 7))
+    big_rec = random_cloud(3000, 7)
+    big = _upload(big_rec)
+    _draw(raster, cam, [small], W, H)   # the handle's first frame sizes the pairs for the small cloud
+    s = A.RenderSettings(width=W, height=H)
+    t = A.RenderTargets.make(W, H)
+    raster.render(cam, [A.SplatInstance(big)], s, t, do_check=False)
+    with pytest.raises(AtheneaError) as e:
+        raster.check()
+    assert e.value.name == "Capacity"
+    stats = raster.render(cam, [A.SplatInstance(big)], s, t)   # grown from the frame before
+    got = G.frame_buffers(raster)
+    pos, shape, sh, _, shw = oracle.decode(big_rec.records().reshape(-1), ENC_BUILDER, 3)
+    want = oracle.render([(pos, shape, sh, 3, shw, np.eye(4), 0)], G.oracle_projection(oracle, cam.projection_for(W, H)),
+                         W, H)
+    assert stats.pairs == got["pairs"] == want["binned"]["pairs"]
+    np.testing.assert_array_equal(got["pair_splats"], want["binned"]["pair_splats"])
+    np.testing.assert_array_equal(got["ranges"].reshape(-1), want["binned"]["ranges"])
+    assert np.abs(t.colour.cpu().numpy() - want["colour"]).max() <= 1e-5
 
 
 def test_a_frame_of_no_splats_draws_the_background(raster):   # :1919-1954, the splat half

@@ -5,7 +5,8 @@ the library, so the test checks that its results equal the allocating
 ath_sorter_sort's on two calls in a row (the second must not see the first's
 leftovers), that it rejects counts past its limit, and that a call takes no
 device memory. Collected last, so that a run stopping at its first failure has
-run everything else first; it passes alone in a fresh process too.
+run everything else first; it passes alone in a fresh process too. A call reads
+nothing back: its status is asked for separately (ath_sort_pairs_static_status).
 """
 import ctypes as C
 
@@ -37,12 +38,15 @@ def _sort(N, fn, keys, vals, key_bits, handle=None):
     return k.cpu().numpy().view(np.uint64), v.cpu().numpy().view(np.uint32)
 
 
-@pytest.mark.parametrize("count,key_bits", [(65537, 40), (LIMIT, 37)])
+# (LIMIT, 64) fills the whole static array: 256 tiles x 8 passes of look-back words;
+# 48 bits is an even pass count (6) at the limit, whose result needs no copy back.
+@pytest.mark.parametrize("count,key_bits", [(65537, 40), (LIMIT, 37), (LIMIT, 64), (LIMIT, 48)])
 def test_static_sort_equals_the_allocating_sort_twice_in_a_row(native, count, key_bits):
     N = native
     lib = N.lib()
     h = C.c_void_p()
     N.check(lib.ath_sorter_create(C.byref(h)))
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     try:
         for call, seed in enumerate((1, 2)):
             keys, vals = _keys(count, key_bits, seed + count)
@@ -50,6 +54,9 @@ def test_static_sort_equals_the_allocating_sort_twice_in_a_row(native, count, ke
             got = _sort(N, lib.ath_sort_pairs_static, keys, vals, key_bits)
             np.testing.assert_array_equal(got[0], want[0], err_msg=f"keys, call {call}")
             np.testing.assert_array_equal(got[1], want[1], err_msg=f"values, call {call}")
+        # neither call raised anything: the status, asked for once both are done
+        N.check(lib.ath_sort_pairs_static_status(stream))
+        N.check(lib.ath_sorter_check(h))
     finally:
         lib.ath_sorter_destroy(h)
 
