@@ -17,6 +17,10 @@
 namespace {
 
 constexpr uint32_t kTile = 16;                    // splat/frame.slang:34
+
+// The frame's tile size: the reference's 16 (frame.slang:34), or another the
+// batched path bins at (8 or 32), set by orc_frame_set_tile.
+inline uint32_t tileOf(const orc_frame& f) { return f.tile ? f.tile : kTile; }
 constexpr uint32_t kCulledKey = 0xFF000000u;      // frame.slang:42-49
 constexpr uint32_t kCullEdit = 1, kCullDepth = 2, kCullDegenerate = 3, kCullFaint = 4, kCullOffscreen = 5,
                    kCullNoTile = 6;
@@ -297,10 +301,10 @@ float minPowerOverBox(float a, float b, float c, float lox, float loy, float hix
 // frame.slang:374-379
 inline bool tileTouched(const orc_frame& f, float cx, float cy, float ca, float cb, float cc, float cutoff,
                         uint32_t tx, uint32_t ty) {
-    const float fx = (float)(tx * kTile) + 0.5f;
-    const float fy = (float)(ty * kTile) + 0.5f;
-    const float lx = (float)(std::min((tx + 1) * kTile, f.width) - 1) + 0.5f;
-    const float ly = (float)(std::min((ty + 1) * kTile, f.height) - 1) + 0.5f;
+    const float fx = (float)(tx * tileOf(f)) + 0.5f;
+    const float fy = (float)(ty * tileOf(f)) + 0.5f;
+    const float lx = (float)(std::min((tx + 1) * tileOf(f), f.width) - 1) + 0.5f;
+    const float ly = (float)(std::min((ty + 1) * tileOf(f), f.height) - 1) + 0.5f;
     return minPowerOverBox(ca, cb, cc, fx - cx, fy - cy, lx - cx, ly - cy) <= cutoff;
 }
 
@@ -506,10 +510,10 @@ void projectCore(const orc_frame& f, const G32& g, RestFn rest3, uint32_t slot, 
     if (x2 < 0.0f || y2 < 0.0f || x1 >= (float)f.width || y1 >= (float)f.height) {
         rx0 = 1; ry0 = 1; rx1 = 0; ry1 = 0;
     } else {
-        rx0 = (uint32_t)std::max(x1, 0.0f) / kTile;
-        ry0 = (uint32_t)std::max(y1, 0.0f) / kTile;
-        rx1 = (uint32_t)std::min(x2, (float)f.width - 1.0f) / kTile;
-        ry1 = (uint32_t)std::min(y2, (float)f.height - 1.0f) / kTile;
+        rx0 = (uint32_t)std::max(x1, 0.0f) / tileOf(f);
+        ry0 = (uint32_t)std::max(y1, 0.0f) / tileOf(f);
+        rx1 = (uint32_t)std::min(x2, (float)f.width - 1.0f) / tileOf(f);
+        ry1 = (uint32_t)std::min(y2, (float)f.height - 1.0f) / tileOf(f);
     }
     if (rx0 > rx1 || ry0 > ry1) {
         cullSlot(slot, kCullOffscreen, records, rects, touchedOut, depthKeys, visible);
@@ -789,6 +793,7 @@ void orc_frame_for(const orc_projection* p, const double objectToWorld[16], uint
     std::memset(f, 0, sizeof(*f));
     f->width = width;
     f->height = height;
+    f->tile = kTile;
     f->tilesX = (width + kTile - 1) / kTile;
     f->tilesY = (height + kTile - 1) / kTile;
     f->focalX = (float)p->focalX;
@@ -853,9 +858,9 @@ void orc_colour_gradient_exact(const orc_frame* f, const uint32_t* ranges, const
     const uint32_t tiles = f->tilesX * f->tilesY;
     for (uint32_t t = 0; t < tiles; ++t) {
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 const uint32_t at = py * f->width + px;
                 walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
@@ -868,9 +873,23 @@ void orc_colour_gradient_exact(const orc_frame* f, const uint32_t* ranges, const
     }
 }
 
-uint64_t orc_bin(const orc_frame* f, uint32_t slots, const float* records, const uint32_t* rects,
-                 const uint32_t* touched, const uint32_t* depthKeys, const uint32_t* visible, uint32_t* pairTiles,
-                 uint32_t* pairSplats, uint32_t* ranges, uint32_t* visibleCount) {
+void orc_frame_set_tile(orc_frame* f, uint32_t tile) {
+    f->tile = tile;
+    f->tilesX = (f->width + tile - 1) / tile;
+    f->tilesY = (f->height + tile - 1) / tile;
+}
+
+namespace {
+
+// The two-sort binning of orc_bin; with tileStride > 1, only the pairs of tiles
+// t with t % tileStride == tileOffset are written (in the same relative order:
+// the emit's test is per pair, and dropping whole tiles leaves each kept tile's
+// run as the stable tile sort makes it).
+uint64_t binSampled(const orc_frame* f, uint32_t slots, const float* records, const uint32_t* rects,
+                    const uint32_t* touched, const uint32_t* depthKeys, const uint32_t* visible, uint32_t* pairTiles,
+                    uint32_t* pairSplats, uint32_t* ranges, uint32_t* visibleCount, uint32_t tileStride,
+                    uint32_t tileOffset) {
+    const bool sampled = tileStride > 1;
     // splat_compact.slang:16-26 -- visible slots in slot order
     std::vector<uint32_t> order;
     order.reserve(slots);
@@ -887,6 +906,7 @@ uint64_t orc_bin(const orc_frame* f, uint32_t slots, const float* records, const
         offsets[k] = pairs;
         pairs += touched[order[k]];
     }
+    uint64_t kept = 0;   // sampled: pairs written so far, in emit order
     for (size_t k = 0; k < order.size(); ++k) {
         const uint32_t s = order[k];
         const uint32_t expected = touched[s];
@@ -897,13 +917,18 @@ uint64_t orc_bin(const orc_frame* f, uint32_t slots, const float* records, const
         for (uint32_t ty = rect[1]; ty <= rect[3] && written < expected; ++ty) {
             for (uint32_t tx = rect[0]; tx <= rect[2] && written < expected; ++tx) {
                 if (!tileTouched(*f, rec[0], rec[1], rec[4], rec[5], rec[6], rec[3], tx, ty)) continue;
-                const uint64_t at = offsets[k] + written;
-                pairTiles[at] = ty * f->tilesX + tx;
-                pairSplats[at] = s;
+                const uint32_t t = ty * f->tilesX + tx;
                 written += 1;
+                if (sampled && t % tileStride != tileOffset) continue;
+                const uint64_t at = sampled ? kept++ : offsets[k] + written - 1;
+                if (!pairTiles) continue;   // counting only
+                pairTiles[at] = t;
+                pairSplats[at] = s;
             }
         }
     }
+    if (sampled) pairs = kept;
+    if (!pairTiles) return pairs;
     // RadixSort::sort(tileSort_, P, bitsFor(tiles)): stable on the tile
     std::vector<uint64_t> idx(pairs);
     std::iota(idx.begin(), idx.end(), 0);
@@ -926,6 +951,23 @@ uint64_t orc_bin(const orc_frame* f, uint32_t slots, const float* records, const
     return pairs;
 }
 
+}   // namespace
+
+uint64_t orc_bin(const orc_frame* f, uint32_t slots, const float* records, const uint32_t* rects,
+                 const uint32_t* touched, const uint32_t* depthKeys, const uint32_t* visible, uint32_t* pairTiles,
+                 uint32_t* pairSplats, uint32_t* ranges, uint32_t* visibleCount) {
+    return binSampled(f, slots, records, rects, touched, depthKeys, visible, pairTiles, pairSplats, ranges,
+                      visibleCount, 1, 0);
+}
+
+uint64_t orc_bin_sampled(const orc_frame* f, uint32_t slots, const float* records, const uint32_t* rects,
+                         const uint32_t* touched, const uint32_t* depthKeys, const uint32_t* visible,
+                         uint32_t* pairTiles, uint32_t* pairSplats, uint32_t* ranges, uint32_t tileStride,
+                         uint32_t tileOffset) {
+    return binSampled(f, slots, records, rects, touched, depthKeys, visible, pairTiles, pairSplats, ranges, nullptr,
+                      std::max(tileStride, 1u), tileOffset);
+}
+
 uint64_t orc_blend(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairSplats, const float* records,
                    float* colour, float* depth, float* finalT, uint32_t* lastContrib, int threads) {
     const uint32_t tiles = f->tilesX * f->tilesY;
@@ -935,9 +977,9 @@ uint64_t orc_blend(const orc_frame* f, const uint32_t* ranges, const uint32_t* p
         const uint32_t t = (uint32_t)ti;
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
         const uint32_t start = ranges[t * 2], end = ranges[t * 2 + 1];
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 const Walk wk = walkPixel(*f, start, end, pairSplats, records, (float)px + 0.5f, (float)py + 0.5f,
                                           [](uint32_t, float) {});
@@ -969,9 +1011,9 @@ void orc_blend_over(const orc_frame* f, const uint32_t* ranges, const uint32_t* 
         const uint32_t t = (uint32_t)ti;
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
         const uint32_t start = ranges[t * 2], end = ranges[t * 2 + 1];
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 const uint32_t at = py * f->width + px;
                 const float underZ = underDepth[at];
@@ -1010,9 +1052,9 @@ void orc_blend_matte(const orc_frame* f, const uint32_t* ranges, const uint32_t*
     for (int64_t ti = 0; ti < (int64_t)tiles; ++ti) {
         const uint32_t t = (uint32_t)ti;
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 const uint32_t at = py * f->width + px;
                 uint32_t ids[kSlots] = {0, 0, 0, 0, 0, 0};
@@ -1071,9 +1113,9 @@ void orc_colour_gradient(const orc_frame* f, const uint32_t* ranges, const uint3
     const float kScale = 256.0f;   // frame.slang:36
     for (uint32_t t = 0; t < tiles; ++t) {
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 const uint32_t at = py * f->width + px;
                 walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
@@ -1097,9 +1139,9 @@ void orc_contribution_weight(const orc_frame* f, const uint32_t* ranges, const u
     const uint32_t tiles = f->tilesX * f->tilesY;
     for (uint32_t t = 0; t < tiles; ++t) {
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
                           (float)py + 0.5f, [&](uint32_t s, float weight) {
@@ -1121,9 +1163,9 @@ void orc_contribution_change(const orc_frame* f, const uint32_t* ranges, const u
     std::vector<uint64_t> sums(slots, 0);
     for (uint32_t t = 0; t < tiles; ++t) {
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 const float* whole = wholeFrame + (size_t)(py * f->width + px) * 4;
                 walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
@@ -1150,9 +1192,9 @@ void orc_contribution_lift(const orc_frame* f, const uint32_t* ranges, const uin
     const uint32_t tiles = f->tilesX * f->tilesY;
     for (uint32_t t = 0; t < tiles; ++t) {
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 const float m = std::fmin(std::fmax(liftMask[py * f->width + px], 0.0f), 1.0f);
                 walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
@@ -1173,9 +1215,9 @@ void orc_matte_lift(const orc_frame* f, const uint32_t* ranges, const uint32_t* 
     const uint32_t tiles = f->tilesX * f->tilesY;
     for (uint32_t t = 0; t < tiles; ++t) {
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 float known = 0.0f, inside = 0.0f, untold = 0.0f;
                 walkPixel(*f, ranges[t * 2], ranges[t * 2 + 1], pairSplats, records, (float)px + 0.5f,
@@ -1204,9 +1246,9 @@ void orc_trace(const orc_frame* f, const uint32_t* ranges, const uint32_t* pairS
     const uint32_t pixels = f->width * f->height, tiles = f->tilesX * f->tilesY;
     for (uint32_t t = 0; t < tiles; ++t) {
         const uint32_t tx = t % f->tilesX, ty = t / f->tilesX;
-        for (uint32_t ly = 0; ly < kTile; ++ly) {
-            for (uint32_t lx = 0; lx < kTile; ++lx) {
-                const uint32_t px = tx * kTile + lx, py = ty * kTile + ly;
+        for (uint32_t ly = 0; ly < tileOf(*f); ++ly) {
+            for (uint32_t lx = 0; lx < tileOf(*f); ++lx) {
+                const uint32_t px = tx * tileOf(*f) + lx, py = ty * tileOf(*f) + ly;
                 if (px >= f->width || py >= f->height) continue;
                 uint32_t slots[K] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
                 float weights[K] = {0, 0, 0, 0}, total = 0.0f, floor = 0.0f;

@@ -54,6 +54,7 @@ typedef struct {
     float depthThreshold;
     float bg[4];
     orc_edit edit;
+    uint32_t tile;    /* tile size: 16 (frame.slang:34) unless orc_frame_set_tile changed it */
 } orc_frame;
 
 /* 3DGS record layout (io::SplatEncoding) for the decode. Field indices into a
@@ -126,6 +127,20 @@ void orc_project_params(const orc_frame* f, uint32_t count, uint32_t base, const
 uint64_t orc_bin(const orc_frame* f, uint32_t slots, const float* records, const uint32_t* rects,
                  const uint32_t* touched, const uint32_t* depthKeys, const uint32_t* visible,
                  uint32_t* pairTiles, uint32_t* pairSplats, uint32_t* ranges, uint32_t* visibleCount);
+
+/* The frame at another tile size (the batched path bins at 8, 16 or 32): the
+ * tile rects, the tile test (frame.slang:374-402), the tile count and the
+ * blends' tiles all follow it. */
+void orc_frame_set_tile(orc_frame* f, uint32_t tile);
+
+/* orc_bin writing only the pairs of tiles t with t % tileStride == tileOffset
+ * (each such tile's pairs in the order orc_bin gives them): a sampled check of
+ * a frame too large to bin whole. Returns the pairs written; ranges cover every tile.
+ * With pairTiles NULL it only counts them (nothing else is written). */
+uint64_t orc_bin_sampled(const orc_frame* f, uint32_t slots, const float* records, const uint32_t* rects,
+                         const uint32_t* touched, const uint32_t* depthKeys, const uint32_t* visible,
+                         uint32_t* pairTiles, uint32_t* pairSplats, uint32_t* ranges, uint32_t tileStride,
+                         uint32_t tileOffset);
 
 /* ---- (d) blend: splat/splat_blend.slang:236-578 (blendPixel<false,false,false>) ----
  * colour float4 and depth per pixel, bottom row first. finalT / lastContrib

@@ -36,7 +36,7 @@ class Frame(C.Structure):
                 ("paidAt", C.c_float), ("surfels", C.c_uint32), ("m", C.c_float * 12), ("eye", C.c_float * 3),
                 ("restPerColour", C.c_uint32), ("shWords", C.c_uint32), ("shLimit", C.c_uint32),
                 ("linearCloud", C.c_uint32), ("depthMode", C.c_uint32), ("depthThreshold", C.c_float),
-                ("bg", C.c_float * 4), ("edit", Edit)]
+                ("bg", C.c_float * 4), ("edit", Edit), ("tile", C.c_uint32)]
 
 
 class Encoding(C.Structure):
@@ -104,6 +104,10 @@ def lib():
                                            C.c_uint32, C.c_double, _P, C.POINTER(C.c_double), C.c_int]
         L.orc_bin.restype = C.c_uint64
         L.orc_bin.argtypes = [C.POINTER(Frame), C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.orc_bin_sampled.restype = C.c_uint64
+        L.orc_bin_sampled.argtypes = [C.POINTER(Frame), C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, C.c_uint32,
+                                      C.c_uint32]
+        L.orc_frame_set_tile.argtypes = [C.POINTER(Frame), C.c_uint32]
         L.orc_blend.restype = C.c_uint64
         L.orc_blend.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P, _P, _P, C.c_int]
         L.orc_colour_gradient.argtypes = [C.POINTER(Frame), _P, _P, _P, _P, _P]
@@ -299,6 +303,27 @@ def bin_(f: Frame, proj: dict):
     assert n == pairs
     return dict(pair_tiles=pair_tiles[:pairs], pair_splats=pair_splats[:pairs], ranges=ranges, pairs=pairs,
                 visible=visible.value)
+
+
+def set_tile(f: Frame, tile: int) -> Frame:
+    """The frame at tile size `tile` (orc_frame_set_tile): rects, the tile test and tiles follow it."""
+    lib().orc_frame_set_tile(C.byref(f), tile)
+    return f
+
+
+def bin_sampled(f: Frame, proj: dict, tile_stride: int, tile_offset: int = 0):
+    """bin_ keeping only the pairs of tiles t with t % tile_stride == tile_offset."""
+    slots = proj["touched"].shape[0]
+    tiles = f.tilesX * f.tilesY
+    args = (C.byref(f), slots, _ptr(proj["records"]), _ptr(proj["rects"]), _ptr(proj["touched"]), _ptr(proj["keys"]),
+            _ptr(proj["visible"]))
+    pairs = lib().orc_bin_sampled(*args, None, None, None, tile_stride, tile_offset)
+    pair_tiles = np.zeros(max(pairs, 1), np.uint32)
+    pair_splats = np.zeros(max(pairs, 1), np.uint32)
+    ranges = np.zeros(2 * tiles, np.uint32)
+    n = lib().orc_bin_sampled(*args, _ptr(pair_tiles), _ptr(pair_splats), _ptr(ranges), tile_stride, tile_offset)
+    assert n == pairs
+    return dict(pair_tiles=pair_tiles[:pairs], pair_splats=pair_splats[:pairs], ranges=ranges, pairs=pairs)
 
 
 def blend(f: Frame, binned: dict, proj: dict, threads=0):

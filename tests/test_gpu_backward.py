@@ -65,6 +65,12 @@ def _fd(O, proj, p, W, H, target, which, eps):
     return fd, loss
 
 
+# cos, median and 95th percentile of the relative error against FP64 central differences
+# (Richardson-combined), for every parameter group; the C2 workload reaches cos 1.0 and
+# p95 of a few 1e-5, so these leave a decade
+COS_MIN, MEDIAN_MAX, P95_MAX = 0.9999, 1e-4, 1e-3
+
+
 def _check_groups(ours, fd, label):
     report = {}
     for name, sl in GROUPS.items():
@@ -73,11 +79,11 @@ def _check_groups(ours, fd, label):
         err = np.abs(a - b) / (np.abs(b) + 0.05 * scale)
         cos = float(np.dot(a, b) / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
         report[name] = (cos, float(np.median(err)), float(np.percentile(err, 95)))
-    print(label, {k: tuple(round(v, 5) for v in r) for k, r in report.items()})
+    print(label, {k: (round(r[0], 7), float(f"{r[1]:.3g}"), float(f"{r[2]:.3g}")) for k, r in report.items()})
     for name, (cos, med, p95) in report.items():
-        assert cos > 0.995, (label, name, report[name])
-        assert med < 0.02, (label, name, report[name])
-        assert p95 < 0.15, (label, name, report[name])
+        assert cos > COS_MIN, (label, name, report[name])
+        assert med < MEDIAN_MAX, (label, name, report[name])
+        assert p95 < P95_MAX, (label, name, report[name])
     return report
 
 

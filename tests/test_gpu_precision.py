@@ -13,9 +13,20 @@ which moves its power at the cutoff by up to about 1e-4 relative); the stop at
 T = 1e-4 within a relative 1e-3 (T is a product of as many FP32 factors as
 the walk blends). The blend order is not an arithmetic result but the method's
 choice: both orders follow the FP32 depth key, as the reference computes it. PSNR (peak 1)
-is over all sampled pixels, near decisions included. What the quantisation
-itself does to the image (FP64 of the FP32 coefficients against FP64 of the
-stored ones) is printed beside it.
+is over all sampled pixels, near decisions included.
+
+Two more numbers are reported and bounded for every view, over ALL sampled
+pixels:
+- against the same FP64 walk, near decisions included: a decision that flips
+  moves one splat of alpha about 1/255 in or out of the pixel (at the cutoff
+  alpha = opacity * exp(-cutoff/2) is 1/255 by the cutoff's definition, and
+  1/255 is the faint threshold), so the bound is 2/255 plus the arithmetic's;
+- against FP64 of the FP32 coefficients (the parameters before the BF16/FP8
+  storage): what a user comparing with an FP32 model sees. The storage alone
+  exceeds 1e-4: BF16 keeps 8 significant bits, so a DC coefficient near 0.5 is
+  off by up to 2^-9 and its colour (times SH0 = 0.282) by up to 2.8e-4, and
+  e4m3 keeps 4 significant bits of bands 2-3. This error is bounded in PSNR and
+  max-abs here, not at 1e-4.
 """
 import math
 
@@ -30,6 +41,9 @@ pytestmark = pytest.mark.gpu
 
 TOLERANCE = 1e-4   # max-abs against FP64, pixels clear of a decision
 MARGIN = 1e-4      # the relative window of a decision
+FLIP_BOUND = 2.0 / 255.0 + TOLERANCE   # max-abs against FP64 over every pixel: one flipped faint splat
+STORAGE_PSNR = 40.0                    # against FP64 of the FP32 coefficients (the storage's own error)
+STORAGE_MAX_ABS = 0.1
 
 # name: (Gaussians, clustered, seed, view sizes, tile stride of the FP64 sample)
 CASES = {
@@ -95,9 +109,24 @@ def _errors(img, ref):
     diff = np.abs(img.astype(np.float64) - ref["colour"])
     mse = float(np.mean(diff[sampled] ** 2))
     worst = np.where(clear)[0][np.argmax(diff[clear].max(axis=1))]
-    return dict(max_abs=float(diff[clear].max()), psnr=10 * math.log10(1.0 / max(mse, 1e-30)),
+    return dict(max_abs=float(diff[clear].max()), max_abs_all=float(diff[sampled].max()),
+                psnr=10 * math.log10(1.0 / max(mse, 1e-30)),
                 sampled=int(sampled.sum()), near=float(1.0 - clear.sum() / max(sampled.sum(), 1)),
                 worst_pixel=int(worst), worst_fp64_T=float(1.0 - ref["colour"][worst, 3]))
+
+
+def _report_and_check(label, img, ref, full):
+    """`ref`: FP64 of the stored coefficients; `full`: FP64 of the FP32 coefficients."""
+    e = _errors(img, ref)
+    t = _errors(img, full)
+    print(f"{label}: against FP64 of the stored SH: max-abs {e['max_abs']:.3g} (clear of a decision), "
+          f"{e['max_abs_all']:.3g} (every pixel), PSNR {e['psnr']:.1f} dB over {e['sampled']} pixels "
+          f"({100 * e['near']:.3f}% near a decision); against FP64 of the FP32 SH: max-abs {t['max_abs_all']:.3g} "
+          f"(every pixel), PSNR {t['psnr']:.1f} dB")
+    assert e["max_abs"] <= TOLERANCE, (label, e)
+    assert e["max_abs_all"] <= FLIP_BOUND, (label, e)
+    assert t["psnr"] >= STORAGE_PSNR and t["max_abs_all"] <= STORAGE_MAX_ABS, (label, t)
+    return e, t
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -111,13 +140,8 @@ def test_mixed_precision_image_error_against_fp64(oracle, name):
     images, stats = _batched_images(M, views)
     for v, ((proj, W, H), img) in enumerate(zip(views, images)):
         ref = _f64(oracle, proj, W, H, p, stored_sh, stride, v % stride)
-        e = _errors(img, ref)
         full = _f64(oracle, proj, W, H, p, p["sh"], stride, v % stride)
-        q = _errors(ref["colour"], full)
-        print(f"{name} view {v} {W}x{H}: max-abs {e['max_abs']:.3g} (pixels clear of a decision), "
-              f"PSNR {e['psnr']:.1f} dB over {e['sampled']} sampled pixels ({100 * e['near']:.3f}% near a decision); "
-              f"quantisation alone: PSNR {q['psnr']:.1f} dB, max-abs {q['max_abs']:.3g}")
-        assert e["max_abs"] <= TOLERANCE, (name, v, e)
+        e, _ = _report_and_check(f"{name} view {v} {W}x{H}", img, ref, full)
         assert e["near"] < 0.03, (name, v, e)
     assert stats["degenerate"] == 0   # these scenes hold no near-degenerate footprint
 
@@ -155,13 +179,12 @@ def test_near_degenerate_footprints_take_fp64_and_stay_within_tolerance(oracle):
     images, stats = _batched_images(M, views)
     assert stats["degenerate"] >= needles, stats
     ref = _f64(oracle, views[0][0], W, H, p, stored_sh, 1, 0)
-    e = _errors(images[0], ref)
+    full = _f64(oracle, views[0][0], W, H, p, p["sh"], 1, 0)
+    e, _ = _report_and_check(f"needles ({stats['degenerate']} FP64 footprints)", images[0], ref, full)
     Pq = A.Params(P.means, P.scales, P.quats, M.dequantized_sh().contiguous(), 3)
     plain = _errors(_plain_image(Pq, views[0][0], W, H), ref)
-    print(f"needles: {stats['degenerate']} FP64 footprints; mixed path max-abs {e['max_abs']:.3g}, "
-          f"PSNR {e['psnr']:.1f} dB; plain FP32 path on the same footprints: max-abs {plain['max_abs']:.3g}, "
+    print(f"needles: plain FP32 path on the same footprints: max-abs {plain['max_abs']:.3g}, "
           f"PSNR {plain['psnr']:.1f} dB")
-    assert e["max_abs"] <= TOLERANCE, e
     assert e["near"] < 0.05, e
 
 
@@ -180,8 +203,7 @@ def test_50m_gaussians_at_4k_against_fp64(oracle):
     images, stats = _batched_images(M, views)
     assert stats["degenerate"] == 0
     ref = _f64(oracle, views[0][0], W, H, p, stored_sh, stride, 0)
-    e = _errors(images[0], ref)
-    print(f"50M at 3840x2160: {stats['pairs']} pairs; max-abs {e['max_abs']:.3g} (pixels clear of a decision), "
-          f"PSNR {e['psnr']:.1f} dB over {e['sampled']} sampled pixels ({100 * e['near']:.3f}% near a decision)")
-    assert e["max_abs"] <= TOLERANCE, e
+    del stored_sh
+    full = _f64(oracle, views[0][0], W, H, p, p["sh"], stride, 0)
+    e, _ = _report_and_check(f"50M at 3840x2160 ({stats['pairs']} pairs)", images[0], ref, full)
     assert e["near"] < 0.05, e

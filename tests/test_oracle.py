@@ -221,6 +221,39 @@ def test_depth_sort_then_stable_tile_sort_equals_one_64bit_sort(oracle):
     assert [t for t, _ in sorted_pairs] == out["binned"]["pair_tiles"].tolist()
 
 
+def test_sampled_binning_keeps_each_sampled_tile_whole(oracle):
+    """orc_bin_sampled: the pairs of every tile t % 7 == 3, each tile's run as orc_bin has it."""
+    packed = _decode(oracle, random_cloud(3000, 7))
+    out, _ = _render(oracle, oracle.looking_at((1.5, 1.0, 6.0), (0, 0, 0)), [packed], 250, 190)
+    f, p, full = out["frame"], out["proj"], out["binned"]
+    part = oracle.bin_sampled(f, p, 7, 3)
+    keep = full["pair_tiles"] % 7 == 3
+    np.testing.assert_array_equal(part["pair_tiles"], full["pair_tiles"][keep])
+    np.testing.assert_array_equal(part["pair_splats"], full["pair_splats"][keep])
+    r = full["ranges"].reshape(-1, 2)
+    rp = part["ranges"].reshape(-1, 2)
+    tiles = np.arange(r.shape[0])
+    np.testing.assert_array_equal(np.diff(rp, axis=1)[tiles % 7 == 3], np.diff(r, axis=1)[tiles % 7 == 3])
+
+
+@pytest.mark.parametrize("tile", [8, 32])
+def test_other_tile_sizes_bin_each_pixel_to_the_same_records(oracle, tile):
+    """At tile 8 or 32 a pixel's records (its tile's pairs whose footprint holds the
+    pixel centre) are the tile-16 frame's, in the same order, and the image is the same."""
+    packed = _decode(oracle, random_cloud(3000, 7))
+    cam = oracle.looking_at((1.5, 1.0, 6.0), (0, 0, 0))
+    W, H = 250, 190
+    base, _ = _render(oracle, cam, [packed], W, H)
+    proj = oracle.projection_for(cam, W, H)
+    f = oracle.set_tile(oracle.frame_for(proj, np.eye(4), W, H, rest_per_colour=3, sh_words=5), tile)
+    assert f.tilesX == (W + tile - 1) // tile
+    pr = oracle.project(f, *packed[:3])
+    binned = oracle.bin_(f, pr)
+    img = oracle.blend(f, binned, pr)
+    np.testing.assert_array_equal(pr["keys"][pr["visible"] != 0], base["proj"]["keys"][pr["visible"] != 0])
+    np.testing.assert_array_equal(img["colour"], base["colour"])
+
+
 # ---- :77-128: the raster against the ground truth, 250x190, randomCloud(3000, 7) --
 @pytest.mark.parametrize("section", ["perspective", "frustum", "orthographic", "no-aa-window-roll"])
 def test_raster_matches_the_fp64_ground_truth(oracle, section):
