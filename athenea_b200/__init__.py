@@ -8,12 +8,13 @@ backward) and the batched mixed-precision step (MixedParams, BatchTrainer).
 """
 from ._native import AtheneaError  # noqa: F401
 from .parallel import GradientBuffer, shard_views  # noqa: F401
-from .raster import (BatchTrainer, Camera, CloudLoader, FrameStats, GpuSplats, Lens, MixedParams,  # noqa: F401
-                     Params, RenderSettings, RenderTargets, SplatCounters, SplatEdit, SplatInstance, TileRasterizer,
-                     check_bounded_wait, encoding_3dgs, l2_loss, memory_held, pinhole_for_vertical_fov,
-                     read_splat_ply, set_memory_budget)
+from .raster import (BatchTrainer, Camera, CloudCounts, CloudLoader, FrameStats, GpuSplats, Lens,  # noqa: F401
+                     MixedParams, Params, RenderSettings, RenderTargets, SplatCounters, SplatEdit, SplatInstance,
+                     TileRasterizer, check_bounded_wait, encoding_3dgs, l2_loss, measure_peaks, memory_held,
+                     pinhole_for_vertical_fov, read_splat_ply, set_memory_budget)
 
-__all__ = ["AtheneaError", "BatchTrainer", "GradientBuffer", "shard_views", "Camera", "CloudLoader", "FrameStats", "GpuSplats", "Lens", "MixedParams",
-           "Params", "RenderSettings", "RenderTargets", "SplatCounters", "SplatEdit", "SplatInstance",
-           "TileRasterizer", "check_bounded_wait", "encoding_3dgs", "l2_loss", "memory_held",
-           "pinhole_for_vertical_fov", "read_splat_ply", "set_memory_budget"]
+__all__ = ["AtheneaError", "BatchTrainer", "GradientBuffer", "shard_views", "Camera", "CloudCounts", "CloudLoader",
+           "FrameStats", "GpuSplats", "Lens", "MixedParams", "Params", "RenderSettings", "RenderTargets",
+           "SplatCounters", "SplatEdit", "SplatInstance", "TileRasterizer", "check_bounded_wait", "encoding_3dgs",
+           "l2_loss", "measure_peaks", "memory_held", "pinhole_for_vertical_fov", "read_splat_ply",
+           "set_memory_budget"]

@@ -114,7 +114,8 @@ class View(C.Structure):
 class BatchStats(C.Structure):
     _fields_ = [("pairs", C.c_uint64), ("capacity", C.c_uint64), ("kept", C.c_uint32), ("tile", C.c_uint32),
                 ("block_batch", C.c_uint32), ("ms_per_step", C.c_float), ("degenerate", C.c_uint32),
-                ("evaluated", C.c_uint64)]
+                ("evaluated", C.c_uint64), ("blended", C.c_uint64), ("adjoint_visited", C.c_uint64),
+                ("adjoint_live", C.c_uint64)]
 
 
 class BatchBuffers(C.Structure):
@@ -164,6 +165,7 @@ SIGNATURES = {
     "ath_set_memory_budget": (C.c_int32, [C.c_uint64]),
     "ath_memory_held": (C.c_int32, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ath_check_bounded_wait": (C.c_int32, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), _P]),
+    "ath_measure_peaks": (C.c_int32, [C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double), _P]),
     "ath_ply_read_header": (C.c_int32, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(Encoding)]),
     "ath_ply_read": (C.c_int32, [C.c_char_p, _P, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(Encoding)]),
     "ath_batch_time_stages": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads),

@@ -64,6 +64,9 @@ __global__ void beginStepKernel(uint32_t* words) {
     words[kBatchKept] = 0;
     for (int p = 0; p < 8; ++p) words[kBatchSortTickets + p] = 0;
     words[kBatchEvaluated] = words[kBatchEvaluated + 1] = 0;
+    words[kBatchBlended] = words[kBatchBlended + 1] = 0;
+    words[kBatchAdjVisited] = words[kBatchAdjVisited + 1] = 0;
+    words[kBatchAdjLive] = words[kBatchAdjLive + 1] = 0;
     words[kBatchDegenerate] = 0;
     words[kBatchExpMin] = 0xFFu;
     words[kBatchExpMax] = 0u;
@@ -1229,7 +1232,11 @@ extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* 
     if (err != cudaSuccess) return failCuda(err, "ath_batch_check");
     out->pairs = (uint64_t)w[kBatchPairsLo] | ((uint64_t)w[kBatchPairsHi] << 32);
     out->kept = w[kBatchKept];
-    out->evaluated = (uint64_t)w[kBatchEvaluated] | ((uint64_t)w[kBatchEvaluated + 1] << 32);
+    auto word64 = [&](uint32_t k) { return (uint64_t)w[k] | ((uint64_t)w[k + 1] << 32); };
+    out->evaluated = word64(kBatchEvaluated);
+    out->blended = word64(kBatchBlended);
+    out->adjoint_visited = word64(kBatchAdjVisited);
+    out->adjoint_live = word64(kBatchAdjLive);
     out->degenerate = w[kBatchDegenerate];
     out->tile = b->tile;
     out->block_batch = b->blockBatch;

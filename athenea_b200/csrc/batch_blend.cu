@@ -155,6 +155,8 @@ __global__ void __launch_bounds__(T * T / 2, 2)
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
     uint32_t evaluated = 0;   // (pixel, record) evaluations of the forward this thread made
+    uint32_t blended = 0;     // of them, those that blended
+    uint32_t adjVisited = 0, adjLive = 0;   // the adjoint's evaluations, and those that blended
     float lossSum = 0.0f;     // this thread's pixels' share of the loss
     while (true) {
         __syncthreads();
@@ -226,6 +228,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                         if (e < limit) continue;
                         const float alpha = fminf(0.99f, k.w * fastExp2(e));
                         if (alpha < kFaint) continue;
+                        ++blended;
                         const float w = Tr[p] * alpha;
                         const float4 c = sColour[j];
                         r[p] = __fmaf_rn(w, c.x, r[p]);
@@ -334,6 +337,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
 #pragma unroll
                         for (int p = 0; p < 2; ++p) {
                             if (rel >= last[p]) continue;
+                            ++adjVisited;
                             const float dy = pyc[p] - ce.y;
                             const float t = __fmaf_rn(k.y, dy, dx);
                             const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
@@ -343,6 +347,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                             const float alpha = fminf(0.99f, raw);
                             if (alpha < kFaint) continue;
                             live = true;
+                            ++adjLive;
                             const float inv = fastRcp(1.0f - alpha);
                             const float Tb = Tr[p] * inv;
                             const float w = Tb * alpha;
@@ -407,11 +412,16 @@ __global__ void __launch_bounds__(T * T / 2, 2)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lossSum += __shfl_xor_sync(0xFFFFFFFFu, lossSum, o);
     if (kTrain && lane == 0 && lossSum != 0.0f) atomicAdd(loss, lossSum);
-    uint64_t e = evaluated;
+    // the work counts: a warp's sums, one atomic each
+    const uint32_t counts[4] = {evaluated, blended, adjVisited, adjLive};
+    const uint32_t at[4] = {kBatchEvaluated, kBatchBlended, kBatchAdjVisited, kBatchAdjLive};
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
-    if (lane == 0 && e)
-        atomicAdd(reinterpret_cast<unsigned long long*>(words + kBatchEvaluated), (unsigned long long)e);
+    for (int c = 0; c < 4; ++c) {
+        uint64_t e = counts[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
+        if (lane == 0 && e) atomicAdd(reinterpret_cast<unsigned long long*>(words + at[c]), (unsigned long long)e);
+    }
 }
 
 template <typename K>

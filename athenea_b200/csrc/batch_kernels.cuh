@@ -59,6 +59,9 @@ enum BatchWord : uint32_t {
     kBatchDegenerate = 18,   // records whose conic took the FP64 path
     kBatchExpMin = 22,       // least and greatest exponent byte of the depths of the records on
     kBatchExpMax = 23,       // screen (for planning a renumbered depth key)
+    kBatchBlended = 24,      // 64-bit (24, 25): forward evaluations that blended (passed the cutoff and 1/255)
+    kBatchAdjVisited = 26,   // 64-bit (26, 27): adjoint evaluations (a pixel, a record before its last contributor)
+    kBatchAdjLive = 28,      // 64-bit (28, 29): adjoint evaluations that blended, whose gradient terms were summed
     kBatchWords = 32,
 };
 

@@ -405,6 +405,15 @@ class TileRasterizer:
         check(N.lib().ath_raster_release_scratch(self._h))
 
 
+def measure_peaks(repeats: int = 5, stream: torch.cuda.Stream | None = None) -> dict:
+    """ath_measure_peaks: the current device's FP32 FMA rate (TFLOP/s) and hardware base-2
+    exponential rate (G results/s), measured."""
+    fma, ex2 = C.c_double(), C.c_double()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    check(N.lib().ath_measure_peaks(repeats, C.byref(fma), C.byref(ex2), C.c_void_p(s.cuda_stream)))
+    return {"fp32_tflops": fma.value, "ex2_gops": ex2.value}
+
+
 def set_memory_budget(nbytes: int) -> None:
     """A cap on this library's device memory, in bytes (0: none), as the reference's
     ATHENEA_GPU_BUDGET (modules/gpu/src/Device.cpp:434-449): a frame whose scratch would
@@ -619,7 +628,8 @@ class BatchTrainer:
         s = stream if stream is not None else torch.cuda.current_stream()
         check(N.lib().ath_batch_check(self._h, C.byref(st), C.c_void_p(s.cuda_stream)))
         return dict(pairs=st.pairs, capacity=st.capacity, kept=st.kept, tile=st.tile, block_batch=st.block_batch,
-                    degenerate=st.degenerate, evaluated=st.evaluated)
+                    degenerate=st.degenerate, evaluated=st.evaluated, blended=st.blended,
+                    adjoint_visited=st.adjoint_visited, adjoint_live=st.adjoint_live)
 
     def tune(self, params: MixedParams, target, colour, loss, grads: "Params", repeats: int = 3,
              stream: torch.cuda.Stream | None = None) -> dict:

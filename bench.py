@@ -401,7 +401,9 @@ def run_ours(args) -> dict | None:
     # the tile order, the blends (forward, loss and adjoint), projection adjoint
     # (memsets are not counted)
     launches = (2 + 1 + passes + 1 + 1 + 1 + 1) * args.steps
+    arith = A.measure_peaks(5, stream=stream)   # the blends' denominators: FP32 FMA and ex2 rates, measured here
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
+               arith=arith,
                ms_render=ms_render,
                stats=stats, tuned=tuned, clocks=clocks.summary(), launches=launches, passes=passes,
                count=params.count, loss=loss_batched, h2d=host_target.numel() * 4, d2h=4, pair_form=pair_form,
@@ -500,14 +502,21 @@ def main():
     headline = args.workload == 1 and WORKLOAD["count"] == 1_500_000 and V == 8
     stats, stages = res["stats"], res["stages"]
     dominant = max(stages, key=stages.get)
-    fp32_peak = 148 * 128 * 2 * P.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-    # algorithmic work a launch, per stage: bytes a unit times the units, or FLOPs a evaluation
+    fp32_peak = res["arith"]["fp32_tflops"]
+    # algorithmic work a launch, per stage: bytes a unit times the units, or FLOPs counted on the
+    # device. The blends' FLOPs: a forward evaluation 8 (offsets, the quadratic form, the cutoff
+    # test) and 12 more when it blends (weight, three colour FMAs, transmittance, stop test); an
+    # adjoint evaluation 8, and 37 more when it blends (alpha, the behind-colour recursion, the
+    # transmittance recovery, the nine gradient sums)
+    fwd_flops = 8 * stats["evaluated"] + 12 * stats["blended"]
+    adj_flops = 8 * stats["adjoint_visited"] + 37 * stats["adjoint_live"]
+    ex2_ops = stats["blended"] + 2 * stats["adjoint_live"]   # an exp a blend, an exp and a reciprocal an adjoint
     mixed_bytes = 16 + 16 + 16 + 24 + 36 + 4          # a Gaussian in the mixed layout
     work = {
         "project_emit": ("hbm", res["count"] * mixed_bytes + stats["kept"] * 48 + stats["pairs"] * 8),
         "sort": ("hbm", stats["pairs"] * (8 + 16 * res["passes"])),
         "ranges": ("hbm", stats["pairs"] * 8 + stats["pairs"] // 16 * 8),
-        "blends": ("fp32", stats["evaluated"] * (20 + 60)),   # forward + adjoint an evaluation
+        "blends": ("fp32", fwd_flops + adj_flops),
         "project_adjoint": ("hbm", res["count"] * (mixed_bytes + 60 * 4) + stats["kept"] * 40),
     }
     bound, amount = work[dominant]
@@ -522,8 +531,10 @@ def main():
         achieved = amount / secs / 1e12
         roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                     "frac": achieved / fp32_peak,
-                    "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2) at the measured max SM clock; "
-                                   "no FP32 peak is measured"}
+                    "peak_source": "of measured: ath_measure_peaks' FP32 FMA rate on this GPU in this run",
+                    "flops": {"forward": fwd_flops, "adjoint": adj_flops},
+                    "ex2": {"achieved_gops": ex2_ops / secs / 1e9, "peak_gops": res["arith"]["ex2_gops"],
+                            "frac": ex2_ops / secs / 1e9 / res["arith"]["ex2_gops"]}}
     roofline["kernel"] = kernel_names[dominant]
     roofline["traffic"] = NCU_TRAFFIC.get(kernel_names[dominant]) if headline else None
     roofline["stage_share"] = stages[dominant] / sum(stages.values())
@@ -552,6 +563,8 @@ def main():
                            "path": "ath_batch_render: every view's forward alone (colour), no loss or backward, "
                                    "same scene and views"},
         "stages_ms": stages, "pairs": stats["pairs"], "kept": stats["kept"], "evaluated": stats["evaluated"],
+        "blended": stats["blended"], "adjoint_visited": stats["adjoint_visited"],
+        "adjoint_live": stats["adjoint_live"], "arith_peaks": res["arith"],
         "degenerate_fp64": stats["degenerate"], "loss": res["loss"],
         "roofline": roofline,
         "e2e": {"value": res["e2e_ms"] / V, "unit": "ms/view", "h2d_bytes_per_step": res["h2d"],

@@ -343,6 +343,9 @@ typedef struct {
     float ms_per_step;     /* ath_batch_tune: the chosen setting's time */
     uint32_t degenerate;   /* records whose 2D conic was inverted in FP64 (det < 1e-6 trace^2) */
     uint64_t evaluated;    /* (pixel, record) evaluations of the forward blend */
+    uint64_t blended;      /* of them, those that blended (inside the cutoff, alpha at least 1/255) */
+    uint64_t adjoint_visited;  /* (pixel, record) evaluations of the blend adjoint (before the pixel's last contributor) */
+    uint64_t adjoint_live;     /* of them, those that blended and whose gradient terms were summed */
 } ath_batch_stats;
 
 ath_status ath_batch_create(ath_batch** out);
@@ -569,6 +572,13 @@ ath_status ath_memory_held(uint64_t* bytes, uint64_t* budget);
  * at most `limit` spins, and reports how many it took: ATH_E_TIMEOUT when the
  * flag was never set. For failure-detection tests; no counterpart in the reference. */
 ath_status ath_check_bounded_wait(uint32_t preset, uint32_t limit, uint32_t* spins, void* stream);
+
+/* The current device's FP32 FMA rate (TFLOP/s, two a fused multiply-add) and
+ * hardware base-2 exponential rate (G results/s), each the best of `repeats`
+ * timed launches of a kernel that keeps every SM's pipe busy: the denominators
+ * of the blends' arithmetic roofline. Waits for `stream`. No counterpart in the
+ * reference. */
+ath_status ath_measure_peaks(uint32_t repeats, double* fma_tflops, double* ex2_gops, void* stream);
 
 /* The message of the last failure on this thread ("" when none). */
 const char* ath_last_error_message(void);
