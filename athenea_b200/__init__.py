@@ -7,13 +7,13 @@ not have: differentiable frames (Params, TileRasterizer.render_params /
 backward) and the batched mixed-precision step (MixedParams, BatchTrainer).
 """
 from ._native import AtheneaError  # noqa: F401
-from .parallel import GradientBuffer, shard_views  # noqa: F401
+from .parallel import BucketedGradients, GradientBuffer, gradient_bucket, shard_views  # noqa: F401
 from .raster import (BatchTrainer, Camera, CloudCounts, CloudLoader, FrameStats, GpuSplats, Lens,  # noqa: F401
                      MixedParams, Params, RenderSettings, RenderTargets, SplatCounters, SplatEdit, SplatInstance,
                      TileRasterizer, check_bounded_wait, encoding_3dgs, l2_loss, measure_peaks, memory_held,
                      pinhole_for_vertical_fov, read_splat_ply, set_memory_budget)
 
-__all__ = ["AtheneaError", "BatchTrainer", "GradientBuffer", "shard_views", "Camera", "CloudCounts", "CloudLoader",
+__all__ = ["AtheneaError", "BatchTrainer", "BucketedGradients", "GradientBuffer", "gradient_bucket", "shard_views", "Camera", "CloudCounts", "CloudLoader",
            "FrameStats", "GpuSplats", "Lens", "MixedParams", "Params", "RenderSettings", "RenderTargets",
            "SplatCounters", "SplatEdit", "SplatInstance", "TileRasterizer", "check_bounded_wait", "encoding_3dgs",
            "l2_loss", "measure_peaks", "memory_held", "pinhole_for_vertical_fov", "read_splat_ply",

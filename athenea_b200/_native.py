@@ -162,6 +162,9 @@ SIGNATURES = {
     "ath_batch_check": (C.c_int32, [_P, C.POINTER(BatchStats), _P]),
     "ath_batch_buffers_of": (C.c_int32, [_P, C.POINTER(BatchBuffers), _P]),
     "ath_batch_set_key_mode": (C.c_int32, [_P, C.c_uint32]),
+    "ath_batch_set_buckets": (C.c_int32, [_P, C.c_uint32, C.c_uint32, _P, _P]),
+    "ath_gradient_bucket": (C.c_int32, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_uint32)]),
     "ath_set_memory_budget": (C.c_int32, [C.c_uint64]),
     "ath_memory_held": (C.c_int32, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ath_check_bounded_wait": (C.c_int32, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), _P]),

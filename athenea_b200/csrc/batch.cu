@@ -579,12 +579,15 @@ __global__ void __launch_bounds__(256)
 // covariance factor's gradient dL/dM summed over the views and taken to the
 // scales and the rotation once). The cloud's loads and the SH (packed in
 // registers) are read once.
+// Gaussians [first, end) a launch (a gradient bucket, or the whole cloud), whose
+// gradients go to g*[i - first].
 __global__ void __launch_bounds__(128)
     projectAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float* __restrict__ grads,
                               float4* __restrict__ gMeans, float4* __restrict__ gScales, float4* __restrict__ gQuats,
-                              float* __restrict__ gSh, uint32_t shStride) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.count) return;
+                              float* __restrict__ gSh, uint32_t shStride, uint32_t first, uint32_t end) {
+    const uint32_t i = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= min(end, B.count)) return;
+    const uint32_t o = i - first;   // the row in this launch's gradient arrays
     InstanceConst I = B.inst;
     const Gauss g = loadGauss<kLayoutMixed>(I, i);
     const uint32_t degree = min(degreeOf(I.restPerColour), B.shLimit);
@@ -608,7 +611,7 @@ __global__ void __launch_bounds__(128)
             if (gc[0] == 0.0f && gc[1] == 0.0f && gc[2] == 0.0f) continue;
             colourAdjointFast(sh, g, degree, I.linear, views[v].eye, gc, dSh, dp);
         }
-        float* row = gSh + (size_t)i * shStride;
+        float* row = gSh + (size_t)o * shStride;
 #pragma unroll
         for (uint32_t k = 0; k < 48; ++k)
             if (k < shStride) row[k] = dSh[k];
@@ -661,9 +664,9 @@ __global__ void __launch_bounds__(128)
         rotationOf(g, R);
         shapeAdjoint(I, i, g, R, dMsum, acc);
     }
-    gMeans[i] = make_float4(acc.dp[0] + dp[0], acc.dp[1] + dp[1], acc.dp[2] + dp[2], acc.dLogit);
-    gScales[i] = make_float4(acc.dLogScale[0], acc.dLogScale[1], acc.dLogScale[2], 0.0f);
-    gQuats[i] = make_float4(acc.dQuat[0], acc.dQuat[1], acc.dQuat[2], acc.dQuat[3]);
+    gMeans[o] = make_float4(acc.dp[0] + dp[0], acc.dp[1] + dp[1], acc.dp[2] + dp[2], acc.dLogit);
+    gScales[o] = make_float4(acc.dLogScale[0], acc.dLogScale[1], acc.dLogScale[2], 0.0f);
+    gQuats[o] = make_float4(acc.dQuat[0], acc.dQuat[1], acc.dQuat[2], acc.dQuat[3]);
 }
 
 // ---- FP32 SH -> the mixed layout ------------------------------------------------
@@ -726,6 +729,11 @@ struct ath_batch {
     cudaGraphExec_t exec[kGraphs] = {};
     uintptr_t graphKey[kGraphs][13] = {};
     int nextGraph = 0;   // the slot the next capture replaces
+    // the gradient buckets (ath_batch_set_buckets): each bucket's arrays, and the event
+    // the step records after its projection adjoint; empty: the whole cloud into `grads`
+    std::vector<ath_param_grads> bucketGrads;
+    std::vector<cudaEvent_t> bucketEvents;
+    uint32_t bucketCount = 0;   // the Gaussians the buckets were set for
 };
 
 namespace {
@@ -918,11 +926,22 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
         err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr), depth);
     mark(4);
     if (err == cudaSuccess && train && P.count) {
-        projectAdjointBatchKernel<<<(P.count + 127) / 128, 128, 0, stream>>>(
-            B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
-            reinterpret_cast<float4*>(g.means), reinterpret_cast<float4*>(g.scales), reinterpret_cast<float4*>(g.quats),
-            g.sh, 48);
-        err = cudaGetLastError();
+        // the whole cloud into `g`, or bucket by bucket into each bucket's arrays, each
+        // bucket's event recorded after it (a caller's exchange starts on it)
+        const uint32_t buckets = b->bucketGrads.empty() ? 1u : (uint32_t)b->bucketGrads.size();
+        for (uint32_t k = 0; k < buckets && err == cudaSuccess; ++k) {
+            uint32_t first = 0, n = P.count;
+            if (!b->bucketGrads.empty()) ath_gradient_bucket(P.count, buckets, k, &first, &n);
+            const ath_param_grads& gk = b->bucketGrads.empty() ? g : b->bucketGrads[k];
+            if (n)
+                projectAdjointBatchKernel<<<(n + 127) / 128, 128, 0, stream>>>(
+                    B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
+                    reinterpret_cast<float4*>(gk.means), reinterpret_cast<float4*>(gk.scales),
+                    reinterpret_cast<float4*>(gk.quats), gk.sh, 48, first, first + n);
+            err = cudaGetLastError();
+            if (err == cudaSuccess && !b->bucketEvents.empty() && b->bucketEvents[k])
+                err = cudaEventRecord(b->bucketEvents[k], stream);
+        }
     }
     mark(5);
     return err;
@@ -1209,11 +1228,55 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
 
 extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target,
                                            float* colour, float* loss, ath_param_grads* grads, void* streamPtr) {
-    // an empty cloud has no gradient rows: its gradient arrays may be null
-    if (!b || !params || !target || !colour || !loss || !grads ||
-        (params->count && (!grads->means || !grads->scales || !grads->quats || !grads->sh)))
+    if (!b || !params || !target || !colour || !loss)
         return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: null argument");
-    return runStep(b, params, target, colour, loss, grads, nullptr, streamPtr, "ath_batch_train_step");
+    // with gradient buckets the buckets' arrays receive the gradients; an empty cloud
+    // has no gradient rows, so its gradient arrays may be null
+    if (b->bucketGrads.empty() &&
+        (!grads || (params->count && (!grads->means || !grads->scales || !grads->quats || !grads->sh))))
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: null gradient arrays");
+    if (!b->bucketGrads.empty() && params->count != b->bucketCount)
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: the gradient buckets were set for " +
+                                                std::to_string(b->bucketCount) + " Gaussians, the cloud has " +
+                                                std::to_string(params->count));
+    return runStep(b, params, target, colour, loss, b->bucketGrads.empty() ? grads : nullptr, nullptr, streamPtr,
+                   "ath_batch_train_step");
+}
+
+// Bucket k of `buckets` over `count` Gaussians: consecutive ranges in whole blocks
+// of the projection adjoint (128 Gaussians), their sizes differing by at most one block.
+extern "C" ath_status ath_gradient_bucket(uint32_t count, uint32_t buckets, uint32_t k, uint32_t* first,
+                                          uint32_t* n) {
+    if (!first || !n || buckets == 0 || k >= buckets)
+        return fail(ATH_E_INVALID_ARGUMENT, "ath_gradient_bucket: bucket outside 0 .. buckets - 1");
+    const uint64_t units = ((uint64_t)count + 127) / 128;
+    const uint64_t base = units / buckets, extra = units % buckets;
+    const uint64_t start = 128 * (k * base + std::min<uint64_t>(k, extra));
+    const uint64_t end = std::min<uint64_t>(count, start + 128 * (base + (k < extra ? 1 : 0)));
+    *first = (uint32_t)std::min<uint64_t>(start, count);
+    *n = (uint32_t)(end > start ? end - start : 0);
+    return ATH_OK;
+}
+
+extern "C" ath_status ath_batch_set_buckets(ath_batch* b, uint32_t count, uint32_t buckets,
+                                            const ath_param_grads* grads, void* const* events) {
+    if (!b) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_buckets: null handle");
+    if (buckets && !grads) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_buckets: null bucket arrays");
+    if (buckets > 1024) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_buckets: at most 1024 buckets");
+    for (uint32_t k = 0; k < buckets; ++k) {
+        uint32_t first = 0, n = 0;
+        ath_gradient_bucket(count, buckets, k, &first, &n);
+        if (n && (!grads[k].means || !grads[k].scales || !grads[k].quats || !grads[k].sh))
+            return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_set_buckets: bucket " + std::to_string(k) +
+                                                    " needs its four gradient arrays");
+    }
+    b->bucketGrads.assign(grads, grads + buckets);
+    b->bucketEvents.clear();
+    if (buckets && events)
+        for (uint32_t k = 0; k < buckets; ++k) b->bucketEvents.push_back(static_cast<cudaEvent_t>(events[k]));
+    b->bucketCount = count;
+    dropGraph(b);   // the arrays and events are part of the captured step
+    return ATH_OK;
 }
 
 extern "C" ath_status ath_batch_render(ath_batch* b, const ath_mixed_params* params, float* colour, float* depth,

@@ -602,13 +602,33 @@ class BatchTrainer:
     def set_tuning(self, tile: int, block_batch: int) -> None:
         check(N.lib().ath_batch_set_tuning(self._h, tile, block_batch))
 
+    def set_buckets(self, buckets, events=None) -> None:
+        """ath_batch_set_buckets: the step's gradients bucket by bucket into `buckets` (a
+        parallel.BucketedGradients), recording events[k] (torch.cuda.Event) after bucket k;
+        None: back to one gradient set a step."""
+        if buckets is None:
+            check(N.lib().ath_batch_set_buckets(self._h, 0, 0, None, None))
+            self._buckets = None
+            return
+        arr = buckets.native()
+        ev = None
+        if events is not None:
+            for e in events:
+                if e.cuda_event == 0:          # torch makes the event on its first record
+                    e.record()
+            ev = (C.c_void_p * len(events))(*[e.cuda_event for e in events])
+        self._buckets = (buckets, arr, events, ev)
+        check(N.lib().ath_batch_set_buckets(self._h, buckets.count, len(buckets.params), arr, ev))
+
     def set_key_mode(self, mode: int) -> None:
         """ath_batch_set_key_mode: 0 automatic, 1 packed, 2 wide, 3 packed with the depth exponent renumbered."""
         check(N.lib().ath_batch_set_key_mode(self._h, mode))
 
     def step(self, params: MixedParams, target: torch.Tensor, colour: torch.Tensor, loss: torch.Tensor,
-             grads: "Params", stream: torch.cuda.Stream | None = None) -> None:
-        g = N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
+             grads: "Params | None", stream: torch.cuda.Stream | None = None) -> None:
+        """ath_batch_train_step; `grads` None when gradient buckets are set."""
+        g = N.ParamGrads(None, None, None, None) if grads is None else \
+            N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
         s = stream if stream is not None else torch.cuda.current_stream(colour.device)
         self._keep = (params, target, colour, loss, grads)
         check(N.lib().ath_batch_train_step(self._h, C.byref(params._native()), _ptr(target), _ptr(colour),

@@ -391,6 +391,25 @@ ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode);
  * (count 0) draws the background, and its gradient arrays may be null. */
 ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
                                 float* loss, ath_param_grads* grads, void* stream);
+/* Gradient buckets, for a step whose gradients are summed over GPUs while it
+ * still runs (no counterpart in the reference, which is single-device): with
+ * `buckets` > 0, the step's projection adjoint runs bucket by bucket over
+ * consecutive ranges of the `count` Gaussians (ath_gradient_bucket gives bucket
+ * k's first Gaussian and size), writes bucket k's gradients into grads[k]'s four
+ * arrays (rows of that bucket's Gaussians only, ath_param_grads' layout), and,
+ * when `events` is given, records the cudaEvent_t events[k] on the step's stream
+ * right after bucket k: a caller's stream that waits on it can start bucket k's
+ * all-reduce while the later buckets are computed. ath_batch_train_step's
+ * `grads` is then unused (may be NULL), and the cloud must have `count`
+ * Gaussians. 0 buckets: the whole cloud into `grads` again. The next step
+ * captures again. */
+ath_status ath_batch_set_buckets(ath_batch* b, uint32_t count, uint32_t buckets, const ath_param_grads* grads,
+                                 void* const* events);
+/* Bucket k of `buckets` over `count` Gaussians: its first Gaussian and its size.
+ * Consecutive ranges in whole blocks of 128 Gaussians, their sizes differing by
+ * at most one block, covering every Gaussian once. */
+ath_status ath_gradient_bucket(uint32_t count, uint32_t buckets, uint32_t k, uint32_t* first, uint32_t* n);
+
 /* Every view's forward alone, for rendering many cameras at once, where the
  * reference's TileRasterizer::render draws one camera a call
  * (TileRasterizer.h:468-474): the same projection, sort and blend as a training

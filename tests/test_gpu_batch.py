@@ -425,3 +425,40 @@ def test_batched_render_depth_is_the_plain_paths(mode):
         assert np.all(d[~covered] >= 0.0)
         assert np.mean(rel[covered] <= 1e-4) >= 0.999, float(np.mean(rel[covered] <= 1e-4))
         base += W * H
+
+
+def test_gradient_buckets_give_the_same_gradients_and_signal_each_bucket():
+    """ath_batch_set_buckets: the projection adjoint bucket by bucket, an event after each. A
+    side stream that waits on bucket k's event and copies that bucket out (where a multi-GPU
+    step posts its all-reduce) sees it final; the gradients equal the one-set step's bit for bit."""
+    Pq, M = _scene(40_000, 21)
+    views = _views()
+    gen = torch.Generator().manual_seed(8)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    b, _, loss_one, grads_one, _ = _batched(M, views, targets)
+    buckets = A.BucketedGradients(M.count, 4, 48, 3, device="cuda")
+    events = [torch.cuda.Event() for _ in range(4)]
+    b.set_buckets(buckets, events)
+    colour = torch.empty((b.pixels, 4), device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    target = torch.cat(targets).contiguous()
+    side = torch.cuda.Stream()
+    copies = [torch.empty_like(s) for s in buckets.slices]
+    for _ in range(2):   # the first step captures its graph, the second replays it
+        buckets.flat.fill_(float("nan"))
+        b.step(M, target, colour, loss, None)
+        for k, e in enumerate(events):
+            side.wait_event(e)
+            with torch.cuda.stream(side):
+                copies[k].copy_(buckets.slices[k])
+        torch.cuda.current_stream().wait_stream(side)
+        b.check()
+        torch.cuda.synchronize()
+        for k in range(4):
+            np.testing.assert_array_equal(copies[k].cpu().numpy(), buckets.slices[k].cpu().numpy())
+        got = buckets.gather()
+        for name in ("means", "scales", "quats", "sh"):
+            np.testing.assert_array_equal(getattr(got, name).cpu().numpy(), getattr(grads_one, name).cpu().numpy(),
+                                          err_msg=name)
+        assert loss.item() == loss_one.item()
+    b.set_buckets(None)

@@ -46,6 +46,30 @@ def _scene():
     return scenes.params(COUNT, True, 77, 3)
 
 
+def _rank_buckets(rank, world, port, out_path, buckets):
+    """As _rank, with the gradients in buckets, each summed over ranks by its own all-reduce,
+    the buckets' all-reduces in flight together (as a step posts them while it runs)."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        import athenea_b200 as A
+        from oracle import oracle as O
+        p = _scene()
+        buf = A.BucketedGradients(COUNT, buckets, 48, 3, device="cpu")
+        for v in A.shard_views(VIEWS, rank, world):
+            g = torch.from_numpy(_view_gradient(O, p, v).astype(np.float32))
+            for (first, n), P in zip(buf.ranges, buf.params):
+                P.sh[:, :3] += g[first:first + n]
+        works = [buf.allreduce_bucket(k, async_op=True) for k in range(buckets)]
+        for w in works:
+            w.wait()
+        if rank == 0:
+            np.save(out_path, buf.gather().sh.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
 def _rank(rank, world, port, out_path):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world,
@@ -88,3 +112,33 @@ def test_gradients_summed_over_two_ranks_equal_one_process(oracle, tmp_path):
         want.params.sh[:, :3] += torch.from_numpy(_view_gradient(oracle, p, v).astype(np.float32))
     assert np.abs(want.flat.numpy()).max() > 0
     np.testing.assert_allclose(got, want.flat.numpy(), rtol=1e-6, atol=1e-9)
+
+
+def test_gradient_buckets_cover_every_gaussian_once():
+    import athenea_b200 as A
+    for count in (0, 1, 127, 128, 129, 3000, 1_500_000, 50_000_000):
+        for buckets in (1, 2, 3, 4, 7, 16):
+            ranges = [A.gradient_bucket(count, buckets, k) for k in range(buckets)]
+            at = 0
+            for first, n in ranges:
+                assert first == at and (n % 128 == 0 or first + n == count)
+                at += n
+            assert at == count
+            blocks = [(n + 127) // 128 for _, n in ranges]   # whole blocks of the projection adjoint
+            assert max(blocks) - min(blocks) <= 1
+    with pytest.raises(A.AtheneaError):
+        A.gradient_bucket(10, 2, 2)
+
+
+def test_bucketed_gradients_summed_over_two_ranks_equal_one_process(oracle, tmp_path):
+    out_path = str(tmp_path / "sh.npy")
+    buckets = 3
+    mp.start_processes(_rank_buckets, args=(2, _free_port(), out_path, buckets), nprocs=2, join=True,
+                       start_method="spawn")
+    got = np.load(out_path)
+    p = _scene()
+    want = np.zeros((COUNT, 48), np.float32)
+    for v in range(VIEWS):
+        want[:, :3] += _view_gradient(oracle, p, v).astype(np.float32)
+    assert np.abs(want).max() > 0
+    np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-9)
