@@ -15,6 +15,7 @@ OK = 0
 STATUS_NAMES = {0: "OK", 1: "Unknown", 2: "NotFound", 3: "InvalidArgument", 4: "Unsupported", 5: "IoFailure",
                 6: "DeviceFailure", 7: "ShaderFailure", 8: "PluginFailure", 9: "OutOfMemory", 10: "Cancelled",
                 11: "InternalError", 12: "Timeout", 13: "Capacity"}
+STATUS_CODES = {name: code for code, name in STATUS_NAMES.items()}
 
 
 class AtheneaError(RuntimeError):

@@ -363,24 +363,40 @@ class TileRasterizer:
         arr, n = _instances(instances)
         t = N.Targets(targets.width, targets.height, _ptr(targets.colour), _ptr(targets.depth),
                       _ptr(targets.position))
-        stats = N.FrameStats()
         dev = targets.colour.device if targets.colour is not None else torch.device("cuda")
         s = stream if stream is not None else torch.cuda.current_stream(dev)
-        if under is None:
-            check(N.lib().ath_raster_render(self._h, C.byref(proj), arr, n, C.byref(settings._native()), C.byref(t),
-                                            C.byref(stats), C.c_void_p(s.cuda_stream)))
-        else:
-            u = N.Targets(under.width, under.height, _ptr(under.colour), _ptr(under.depth), None)
-            check(N.lib().ath_raster_render_over(self._h, C.byref(proj), arr, n, C.byref(settings._native()),
-                                                 C.byref(t), C.byref(u), C.byref(stats), C.c_void_p(s.cuda_stream)))
-        if do_check:
-            self._check_into(stats)
+        native = settings._native()
+        u = None if under is None else N.Targets(under.width, under.height, _ptr(under.colour), _ptr(under.depth),
+                                                 None)
+
+        def draw():
+            stats = N.FrameStats()
+            if u is None:
+                check(N.lib().ath_raster_render(self._h, C.byref(proj), arr, n, C.byref(native), C.byref(t),
+                                                C.byref(stats), C.c_void_p(s.cuda_stream)))
+            else:
+                check(N.lib().ath_raster_render_over(self._h, C.byref(proj), arr, n, C.byref(native), C.byref(t),
+                                                     C.byref(u), C.byref(stats), C.c_void_p(s.cuda_stream)))
+            return stats
+
+        stats = self._drawn(draw, do_check)
         return FrameStats(*[getattr(stats, f) for f, _ in N.FrameStats._fields_])
 
-    def _check_into(self, stats) -> None:
+    def _drawn(self, draw, do_check: bool):
+        """Draws, and with do_check waits for the frame: a frame whose pairs outgrew the
+        handle's capacity (ATH_E_CAPACITY) is drawn once more, the capacity grown from it, so
+        that the frame returned is whole, as the reference's render always returns one."""
+        stats = draw()
+        if not do_check:
+            return stats
         totals = N.FrameStats()
-        check(N.lib().ath_raster_check(self._h, C.byref(totals)))
+        status = N.lib().ath_raster_check(self._h, C.byref(totals))
+        if status == N.STATUS_CODES["Capacity"]:
+            stats = draw()
+            status = N.lib().ath_raster_check(self._h, C.byref(totals))
+        check(status)
         stats.visible, stats.pairs = totals.visible, totals.pairs
+        return stats
 
     def check(self) -> FrameStats:
         """ath_raster_check: waits for the last frame (and its backward) and returns its totals;
@@ -480,14 +496,17 @@ def _render_params(self, camera, params: Params, settings: RenderSettings, targe
     parameters, keeping what backward() needs. do_check as for render()."""
     proj = camera.projection_for(settings.width, settings.height) if isinstance(camera, Camera) else camera
     t = N.Targets(targets.width, targets.height, _ptr(targets.colour), _ptr(targets.depth), _ptr(targets.position))
-    stats = N.FrameStats()
     s = stream if stream is not None else torch.cuda.current_stream(targets.colour.device)
     self._params_keep = params   # the backward reads them again
-    check(N.lib().ath_raster_render_params(self._h, C.byref(proj), C.byref(params._native()),
-                                           C.byref(settings._native()), C.byref(t), C.byref(stats),
-                                           C.c_void_p(s.cuda_stream)))
-    if do_check:
-        self._check_into(stats)
+    native_params, native = params._native(), settings._native()
+
+    def draw():
+        st = N.FrameStats()
+        check(N.lib().ath_raster_render_params(self._h, C.byref(proj), C.byref(native_params), C.byref(native),
+                                               C.byref(t), C.byref(st), C.c_void_p(s.cuda_stream)))
+        return st
+
+    stats = self._drawn(draw, do_check)
     return FrameStats(*[getattr(stats, f) for f, _ in N.FrameStats._fields_])
 
 

@@ -205,7 +205,10 @@ class PlainTrainer:
         self.loss = torch.zeros(1, dtype=torch.float32, device=dev)
         self.grads = params.zeros_like()
 
-    def step(self, stream, targets=None):
+    def step(self, stream, targets=None, check=False):
+        """One step over every view; `check` waits for each frame (and redraws one whose pairs
+        outgrew the handle's capacity), which a warm-up step does so that the capacity covers
+        every view before the timed steps, which do not wait."""
         targets = targets if targets is not None else self.targets
         self.loss.zero_()
         for g in (self.grads.means, self.grads.scales, self.grads.quats, self.grads.sh):
@@ -214,7 +217,7 @@ class PlainTrainer:
         for v, (proj, W, H) in enumerate(self.views):
             frames, dl = self.frames[(W, H)], self.dl[(W, H)]
             stats = self.raster.render_params(proj, self.P, self.A.RenderSettings(width=W, height=H), frames,
-                                              stream=stream, do_check=False)
+                                              stream=stream, do_check=check)
             self.A.l2_loss(frames.colour, targets[v], dl, self.loss, stream=stream)
             self.raster.backward(dl, self.grads, stream=stream)
         return stats
@@ -378,8 +381,8 @@ def run_ours(args) -> dict | None:
     if not args.no_plain:
         dev_targets = [target[int(pixel_base[v]):int(pixel_base[v + 1])] for v in range(len(views))]
         plain = PlainTrainer(params, views, dev_targets, dev)
-        for _ in range(args.warmup):
-            plain.step(stream)
+        for w in range(args.warmup):
+            plain.step(stream, check=w == 0)
         ms_plain = _timed(lambda: plain.step(stream), args.steps, stream, world, dev)
         proj0, W0, H0 = views[0]
         timed = A.RenderSettings(width=W0, height=H0, time_stages=True)
