@@ -116,7 +116,8 @@ class BatchStats(C.Structure):
     _fields_ = [("pairs", C.c_uint64), ("capacity", C.c_uint64), ("kept", C.c_uint32), ("tile", C.c_uint32),
                 ("block_batch", C.c_uint32), ("ms_per_step", C.c_float), ("degenerate", C.c_uint32),
                 ("evaluated", C.c_uint64), ("blended", C.c_uint64), ("adjoint_visited", C.c_uint64),
-                ("adjoint_live", C.c_uint64)]
+                ("adjoint_live", C.c_uint64), ("warp_visits_forward", C.c_uint64),
+                ("warp_visits_adjoint", C.c_uint64), ("warp_visits_adjoint_summed", C.c_uint64)]
 
 
 class BatchBuffers(C.Structure):

@@ -67,6 +67,7 @@ __global__ void beginStepKernel(uint32_t* words) {
     words[kBatchBlended] = words[kBatchBlended + 1] = 0;
     words[kBatchAdjVisited] = words[kBatchAdjVisited + 1] = 0;
     words[kBatchAdjLive] = words[kBatchAdjLive + 1] = 0;
+    for (uint32_t k = kBatchFwdVisits; k < kBatchAdjSummed + 2; ++k) words[k] = 0;
     words[kBatchDegenerate] = 0;
     words[kBatchExpMin] = 0xFFu;
     words[kBatchExpMax] = 0u;
@@ -1300,6 +1301,9 @@ extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* 
     out->blended = word64(kBatchBlended);
     out->adjoint_visited = word64(kBatchAdjVisited);
     out->adjoint_live = word64(kBatchAdjLive);
+    out->warp_visits_forward = word64(kBatchFwdVisits);
+    out->warp_visits_adjoint = word64(kBatchAdjVisits);
+    out->warp_visits_adjoint_summed = word64(kBatchAdjSummed);
     out->degenerate = w[kBatchDegenerate];
     out->tile = b->tile;
     out->block_batch = b->blockBatch;

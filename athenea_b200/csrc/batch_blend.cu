@@ -157,6 +157,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
     uint32_t evaluated = 0;   // (pixel, record) evaluations of the forward this thread made
     uint32_t blended = 0;     // of them, those that blended
     uint32_t adjVisited = 0, adjLive = 0;   // the adjoint's evaluations, and those that blended
+    uint32_t fwdVisits = 0, adjVisits = 0, adjSummed = 0;   // a warp's record visits (counted by lane 0)
     float lossSum = 0.0f;     // this thread's pixels' share of the loss
     while (true) {
         __syncthreads();
@@ -213,6 +214,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                 while (todo) {
                     const uint32_t j = base + (uint32_t)__ffs(todo) - 1u;
                     todo &= todo - 1u;
+                    ++fwdVisits;
                     const float2 ce = sCentre[j];
                     const float4 k = sConic[j];
                     const float limit = sColour[j].w;
@@ -324,6 +326,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                     while (todo) {
                         const uint32_t hb = 31u - (uint32_t)__clz(todo);
                         todo &= ~(1u << hb);
+                        ++adjVisits;
                         const uint32_t j = (uint32_t)base + hb;
                         const uint32_t rel = relStart + j;
                         const float2 ce = sCentre[j];
@@ -371,6 +374,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                         }
                         const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, live);
                         if (!lanes) continue;
+                        ++adjSummed;
                         float* acc = sAcc + j * kWords;
                         // the warp's sums, however few lanes are live (shared-memory atomics from
                         // each live lane were slower: they serialise on the record's nine words)
@@ -413,10 +417,13 @@ __global__ void __launch_bounds__(T * T / 2, 2)
     for (int o = 16; o > 0; o >>= 1) lossSum += __shfl_xor_sync(0xFFFFFFFFu, lossSum, o);
     if (kTrain && lane == 0 && lossSum != 0.0f) atomicAdd(loss, lossSum);
     // the work counts: a warp's sums, one atomic each
-    const uint32_t counts[4] = {evaluated, blended, adjVisited, adjLive};
-    const uint32_t at[4] = {kBatchEvaluated, kBatchBlended, kBatchAdjVisited, kBatchAdjLive};
+    const uint32_t visits = lane == 0;   // a warp's visits, once
+    const uint32_t counts[7] = {evaluated, blended, adjVisited, adjLive, fwdVisits * visits, adjVisits * visits,
+                                adjSummed * visits};
+    const uint32_t at[7] = {kBatchEvaluated, kBatchBlended, kBatchAdjVisited, kBatchAdjLive, kBatchFwdVisits,
+                            kBatchAdjVisits, kBatchAdjSummed};
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < 7; ++c) {
         uint64_t e = counts[c];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);

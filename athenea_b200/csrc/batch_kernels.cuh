@@ -62,7 +62,10 @@ enum BatchWord : uint32_t {
     kBatchBlended = 24,      // 64-bit (24, 25): forward evaluations that blended (passed the cutoff and 1/255)
     kBatchAdjVisited = 26,   // 64-bit (26, 27): adjoint evaluations (a pixel, a record before its last contributor)
     kBatchAdjLive = 28,      // 64-bit (28, 29): adjoint evaluations that blended, whose gradient terms were summed
-    kBatchWords = 32,
+    kBatchFwdVisits = 32,    // 64-bit (32, 33): (warp, record) visits of the forward walk
+    kBatchAdjVisits = 34,    // 64-bit (34, 35): (warp, record) visits of the adjoint walk
+    kBatchAdjSummed = 36,    // 64-bit (36, 37): adjoint visits with a live lane, whose sums the warp reduced
+    kBatchWords = 48,
 };
 
 // An epoch-tagged look-back word: [epoch:30][status:2][value:32]. A word with

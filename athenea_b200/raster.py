@@ -668,7 +668,9 @@ class BatchTrainer:
         check(N.lib().ath_batch_check(self._h, C.byref(st), C.c_void_p(s.cuda_stream)))
         return dict(pairs=st.pairs, capacity=st.capacity, kept=st.kept, tile=st.tile, block_batch=st.block_batch,
                     degenerate=st.degenerate, evaluated=st.evaluated, blended=st.blended,
-                    adjoint_visited=st.adjoint_visited, adjoint_live=st.adjoint_live)
+                    adjoint_visited=st.adjoint_visited, adjoint_live=st.adjoint_live,
+                    warp_visits_forward=st.warp_visits_forward, warp_visits_adjoint=st.warp_visits_adjoint,
+                    warp_visits_adjoint_summed=st.warp_visits_adjoint_summed)
 
     def tune(self, params: MixedParams, target, colour, loss, grads: "Params", repeats: int = 3,
              stream: torch.cuda.Stream | None = None) -> dict:

@@ -567,7 +567,9 @@ def main():
                                    "same scene and views"},
         "stages_ms": stages, "pairs": stats["pairs"], "kept": stats["kept"], "evaluated": stats["evaluated"],
         "blended": stats["blended"], "adjoint_visited": stats["adjoint_visited"],
-        "adjoint_live": stats["adjoint_live"], "arith_peaks": res["arith"],
+        "adjoint_live": stats["adjoint_live"], "warp_visits": {
+            "forward": stats["warp_visits_forward"], "adjoint": stats["warp_visits_adjoint"],
+            "adjoint_summed": stats["warp_visits_adjoint_summed"]}, "arith_peaks": res["arith"],
         "degenerate_fp64": stats["degenerate"], "loss": res["loss"],
         "roofline": roofline,
         "e2e": {"value": res["e2e_ms"] / V, "unit": "ms/view", "h2d_bytes_per_step": res["h2d"],

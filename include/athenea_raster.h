@@ -346,6 +346,9 @@ typedef struct {
     uint64_t blended;      /* of them, those that blended (inside the cutoff, alpha at least 1/255) */
     uint64_t adjoint_visited;  /* (pixel, record) evaluations of the blend adjoint (before the pixel's last contributor) */
     uint64_t adjoint_live;     /* of them, those that blended and whose gradient terms were summed */
+    uint64_t warp_visits_forward;   /* (warp, record) visits of the forward walk (a warp: 64 pixels) */
+    uint64_t warp_visits_adjoint;   /* (warp, record) visits of the adjoint walk */
+    uint64_t warp_visits_adjoint_summed;  /* of them, those with a live pixel, whose sums the warp reduced */
 } ath_batch_stats;
 
 ath_status ath_batch_create(ath_batch** out);
