@@ -63,11 +63,6 @@ __global__ void beginStepKernel(uint32_t* words) {
     words[kBatchBlendTicket] = 0;
     words[kBatchKept] = 0;
     for (int p = 0; p < 8; ++p) words[kBatchSortTickets + p] = 0;
-    words[kBatchEvaluated] = words[kBatchEvaluated + 1] = 0;
-    words[kBatchBlended] = words[kBatchBlended + 1] = 0;
-    words[kBatchAdjVisited] = words[kBatchAdjVisited + 1] = 0;
-    words[kBatchAdjLive] = words[kBatchAdjLive + 1] = 0;
-    for (uint32_t k = kBatchFwdVisits; k < kBatchAdjSummed + 2; ++k) words[k] = 0;
     words[kBatchDegenerate] = 0;
     words[kBatchExpMin] = 0xFFu;
     words[kBatchExpMax] = 0u;
@@ -650,6 +645,7 @@ __global__ void __launch_bounds__(128)
         for (int k = 0; k < 12; ++k) I.m[k] = V.m[k];
         I.eye[0] = V.eye[0]; I.eye[1] = V.eye[1]; I.eye[2] = V.eye[2];
         const Geometry G = projectGeometry<true>(F, I, g, g.opacity);
+        batchMomentsToRecordGrad(G.ca, G.fr, G.fs, gw);   // the blend's moments, to the record's terms
         float dpv[3] = {0.0f, 0.0f, 0.0f};
         float dM[3][3];
         geometryAdjointToM(F, I, g, G, gw, dpv, acc, dM);
@@ -851,7 +847,8 @@ int residentBlocks(K kernel, int threads, int sms) {
 }
 
 cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t sorted, cudaStream_t stream,
-                            float4* colour, const float* target, float* loss, float* grads, float* depth) {
+                            float4* colour, const float* target, float* loss, float* grads, float* depth,
+                            bool count) {
     BlendLaunch L{};
     L.views = static_cast<const BatchView*>(b->viewsDev.ptr);
     L.ranges = static_cast<const uint2*>(b->ranges.ptr);
@@ -863,6 +860,7 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
     L.sms = b->sms;
     L.tile = b->tile;
     L.blockBatch = b->blockBatch;
+    L.count = count;
     return launchBatchBlendStep(B, L, stream, colour, target, loss, grads, depth);
 }
 
@@ -924,7 +922,8 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     if (err == cudaSuccess && train) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
     // the forward blend, the loss and the blend adjoint (the record gradients were cleared by the projection)
     if (err == cudaSuccess)
-        err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr), depth);
+        err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr), depth,
+                              marks != nullptr);
     mark(4);
     if (err == cudaSuccess && train && P.count) {
         // the whole cloud into `g`, or bucket by bucket into each bucket's arrays, each
@@ -1339,7 +1338,14 @@ extern "C" ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params
     cudaEvent_t marks[6];
     for (auto& e : marks) cudaEventCreate(&e);
     ath_param_grads g = *grads;
-    cudaError_t err = enqueueStep(b, *params, target, reinterpret_cast<float4*>(colour), loss, g, stream, false, marks);
+    // the blends' work counts start at zero for the counted step (the captured steps leave them)
+    uint32_t* words = static_cast<uint32_t*>(b->words.ptr);
+    cudaError_t err = cudaMemsetAsync(words + kBatchEvaluated, 0, 2 * sizeof(uint32_t), stream);
+    if (err == cudaSuccess)
+        err = cudaMemsetAsync(words + kBatchBlended, 0, (kBatchAdjSummed + 2 - kBatchBlended) * sizeof(uint32_t),
+                              stream);
+    if (err == cudaSuccess)
+        err = enqueueStep(b, *params, target, reinterpret_cast<float4*>(colour), loss, g, stream, false, marks);
     if (err == cudaSuccess) err = cudaEventSynchronize(marks[5]);
     for (int k = 0; k < 5 && err == cudaSuccess; ++k) cudaEventElapsedTime(&ms[k], marks[k], marks[k + 1]);
     for (auto& e : marks) cudaEventDestroy(e);

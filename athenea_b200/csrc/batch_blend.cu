@@ -77,8 +77,7 @@ __device__ __forceinline__ void prefetchIndices(const uint64_t* pairs, const uin
 // so three levels leave value (lane >> 2) spread over lanes differing in their
 // two low bits), the ninth by a butterfly. Lanes with lane % 4 == 0 hold value
 // lane >> 2; every lane holds the ninth.
-__device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
-    const uint32_t lane = threadIdx.x & 31u;
+__device__ __forceinline__ float warpSum9(float v[9], float& ninth, uint32_t lane) {
 #pragma unroll
     for (int half = 4, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
         const bool upper = (lane & (uint32_t)bit) != 0;
@@ -122,14 +121,18 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth) {
 // its box from its pixels' last contributor down. What a lane sums over its two
 // pixels, and the warp over its 64, are moments of dL/dpower over the pixel
 // offsets in the factored frame (t = dx + fr dy, dy): sum dP t, sum dP dy,
-// sum dP t^2, sum dP t dy, sum dP dy^2; the record's centre and conic gradients
-// follow from them once a record, when the block flushes a batch. The loss has
+// sum dP t^2, sum dP t dy, sum dP dy^2. Each visit's warp sums are added into the
+// record's gradient words in global memory as they are (moments, dL/dalpha,
+// dL/dcolour); the projection's adjoint turns the moments into the centre and
+// conic gradients (batchMomentsToRecordGrad), once a record. The loss has
 // no alpha term, so dL/d(alpha out) is 0 and the colour behind a record enters
 // only through S.dC, one value a pixel.
 //
 // kTrain false: the forward blend alone (a batched render: colour and, when
 // given, depth as the plain blend makes it; no target, loss or gradients).
-template <uint32_t T, uint32_t NB, bool kTrain>
+// kCount: also count the walks' work (evaluations and warp visits) into the
+// batch's words; a step timed stage by stage counts, the captured steps do not.
+template <uint32_t T, uint32_t NB, bool kTrain, bool kCount>
 __global__ void __launch_bounds__(T * T / 2, 2)
     blendStepKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
@@ -145,13 +148,12 @@ __global__ void __launch_bounds__(T * T / 2, 2)
     __shared__ float4 sColour[NB];   // r g b; the cutoff pre-scaled
     __shared__ uint32_t sMask[NB];
     __shared__ uint32_t sRec[NB];
-    __shared__ float sAcc[NB * kWords];
+    __shared__ float sDepth[kTrain ? 1 : NB];   // a render's record depths
     __shared__ uint32_t sTileBase[kMaxBatchViews];
     __shared__ uint32_t sTile, sMaxLast;
     for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
     const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
     const float kScale = -0.5f * 1.4426950408889634f;   // power -> base-2 exponent
-    const float kUnscale = 1.0f / kScale;                // for the gradients only
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lx = (warp % kAcross) * kBox + (lane & 7u), ly = (warp / kAcross) * kBox + (lane >> 3);
     uint32_t evaluated = 0;   // (pixel, record) evaluations of the forward this thread made
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
             sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
             sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
             sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
-            if constexpr (!kTrain) sAcc[k] = sc.z;   // a render's depth (its adjoint sums are unused)
+            if constexpr (!kTrain) sDepth[k] = sc.z;
         };
 
         // ---- forward
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                 while (todo) {
                     const uint32_t j = base + (uint32_t)__ffs(todo) - 1u;
                     todo &= todo - 1u;
-                    ++fwdVisits;
+                    if constexpr (kCount) ++fwdVisits;
                     const float2 ce = sCentre[j];
                     const float4 k = sConic[j];
                     const float limit = sColour[j].w;
@@ -222,7 +224,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
 #pragma unroll
                     for (int p = 0; p < 2; ++p) {
                         if (done[p]) continue;
-                        ++evaluated;
+                        if constexpr (kCount) ++evaluated;
                         const float dy = pyc[p] - ce.y;
                         // e = -log2(e)/2 * power; power > cutoff  <=>  e < -log2(e)/2 * cutoff
                         const float t = __fmaf_rn(k.y, dy, dx);
@@ -230,17 +232,17 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                         if (e < limit) continue;
                         const float alpha = fminf(0.99f, k.w * fastExp2(e));
                         if (alpha < kFaint) continue;
-                        ++blended;
+                        if constexpr (kCount) ++blended;
                         const float w = Tr[p] * alpha;
                         const float4 c = sColour[j];
                         r[p] = __fmaf_rn(w, c.x, r[p]);
                         g[p] = __fmaf_rn(w, c.y, g[p]);
                         bl[p] = __fmaf_rn(w, c.z, bl[p]);
-                        if constexpr (!kTrain) depthSum[p] = __fmaf_rn(w, sAcc[j], depthSum[p]);
+                        if constexpr (!kTrain) depthSum[p] = __fmaf_rn(w, sDepth[j], depthSum[p]);
                         Tr[p] = Tr[p] * (1.0f - alpha);
                         last[p] = first - range.x + j + 1;
                         if constexpr (!kTrain)
-                            if (depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = sAcc[j];
+                            if (depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = sDepth[j];
                         if (Tr[p] < 1e-4f) done[p] = true;
                     }
                 }
@@ -313,7 +315,6 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                 prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, batchStart - NB, batchStart, ahead);
             }
             stagedAlready = false;
-            for (uint32_t k = threadIdx.x; k < count * kWords; k += kThreads) sAcc[k] = 0.0f;
             __syncthreads();
             const uint32_t relStart = batchStart - range.x;
             if (relStart < warpLast) {
@@ -326,7 +327,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                     while (todo) {
                         const uint32_t hb = 31u - (uint32_t)__clz(todo);
                         todo &= ~(1u << hb);
-                        ++adjVisits;
+                        if constexpr (kCount) ++adjVisits;
                         const uint32_t j = (uint32_t)base + hb;
                         const uint32_t rel = relStart + j;
                         const float2 ce = sCentre[j];
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
 #pragma unroll
                         for (int p = 0; p < 2; ++p) {
                             if (rel >= last[p]) continue;
-                            ++adjVisited;
+                            if constexpr (kCount) ++adjVisited;
                             const float dy = pyc[p] - ce.y;
                             const float t = __fmaf_rn(k.y, dy, dx);
                             const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                             const float alpha = fminf(0.99f, raw);
                             if (alpha < kFaint) continue;
                             live = true;
-                            ++adjLive;
+                            if constexpr (kCount) ++adjLive;
                             const float inv = fastRcp(1.0f - alpha);
                             const float Tb = Tr[p] * inv;
                             const float w = Tb * alpha;
@@ -374,40 +375,22 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                         }
                         const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, live);
                         if (!lanes) continue;
-                        ++adjSummed;
-                        float* acc = sAcc + j * kWords;
-                        // the warp's sums, however few lanes are live (shared-memory atomics from
-                        // each live lane were slower: they serialise on the record's nine words)
+                        if constexpr (kCount) ++adjSummed;
+                        // the warp's sums, however few lanes are live, added by nine lanes at once
+                        // into the record's words in global memory (reductions, not read back):
+                        // the five moments, dL/dalpha and dL/dcolour, which the projection's
+                        // adjoint turns into centre and conic gradients (linear in the moments,
+                        // so sums from every box, tile and batch add up)
                         float ninth;
-                        const float s = warpSum9(gv, ninth);
-                        if ((lane & 3u) == 0u && s != 0.0f) atomicAdd(acc + (lane >> 2), s);
-                        if (lane == 0 && ninth != 0.0f) atomicAdd(acc + 8, ninth);
+                        const float sum = warpSum9(gv, ninth, lane);
+                        const uint32_t word = (lane & 3u) == 0u ? lane >> 2 : lane == 1u ? 8u : kWords;
+                        const float v = lane == 1u ? ninth : sum;
+                        if (word < kWords && v != 0.0f)
+                            atomicAdd(grads + (recBase + sRec[j]) * kGradWords + word, v);
                     }
                 }
             }
-            __syncthreads();
-            // the moments -> dL/d(centre, conic) in the record's terms, then to the record
-            for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
-                const float* a = sAcc + k * kWords;
-                float out[kWords];
-                const float4 cn = sConic[k];
-                const float ca = cn.x * kUnscale, fr = cn.y, fs = cn.z * kUnscale;
-                const float mt = a[0], my = a[1], mtt = a[2], mty = a[3], myy = a[4];
-                out[kGradCx] = -2.0f * ca * mt;
-                out[kGradCy] = -2.0f * (fr * ca * mt + fs * my);
-                out[kGradA] = mtt - 2.0f * fr * mty + fr * fr * myy;   // sum dP dx^2, dx = t - fr dy
-                out[kGradB2] = 2.0f * (mty - fr * myy);                 // sum dP 2 dx dy
-                out[kGradC] = myy;                                      // sum dP dy^2
-                out[kGradAlpha] = a[5];
-                out[kGradR] = a[6];
-                out[kGradG] = a[7];
-                out[kGradB] = a[8];
-                float* dst = grads + (recBase + sRec[k]) * kGradWords;
-#pragma unroll
-                for (int q = 0; q < (int)kWords; ++q)
-                    if (out[q] != 0.0f) atomicAdd(dst + q, out[q]);
-            }
-            __syncthreads();   // the next batch's loads overwrite what the flush reads
+            __syncthreads();   // the next batch's staging overwrites what the walks read
             if (batchStart == range.x) break;
             batchEnd = batchStart;
             batchStart -= NB;
@@ -416,6 +399,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lossSum += __shfl_xor_sync(0xFFFFFFFFu, lossSum, o);
     if (kTrain && lane == 0 && lossSum != 0.0f) atomicAdd(loss, lossSum);
+    if constexpr (!kCount) return;
     // the work counts: a warp's sums, one atomic each
     const uint32_t visits = lane == 0;   // a warp's visits, once
     const uint32_t counts[7] = {evaluated, blended, adjVisited, adjLive, fwdVisits * visits, adjVisits * visits,
@@ -441,16 +425,19 @@ int residentGrid(K kernel, int threads, int sms) {
 template <uint32_t T, uint32_t NB>
 cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
                      const float* target, float* loss, float* grads, float* depth) {
-    if (target) {
-        const int grid = residentGrid(blendStepKernel<T, NB, true>, T * T / 2, L.sms);
-        blendStepKernel<T, NB, true><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values, L.recs,
-                                                                         colour, target, loss, grads, nullptr,
-                                                                         L.words, L.order);
+    if (target && L.count) {
+        const int grid = residentGrid(blendStepKernel<T, NB, true, true>, T * T / 2, L.sms);
+        blendStepKernel<T, NB, true, true><<<grid, T * T / 2, 0, stream>>>(
+            B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order);
+    } else if (target) {
+        const int grid = residentGrid(blendStepKernel<T, NB, true, false>, T * T / 2, L.sms);
+        blendStepKernel<T, NB, true, false><<<grid, T * T / 2, 0, stream>>>(
+            B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order);
     } else {
-        const int grid = residentGrid(blendStepKernel<T, NB, false>, T * T / 2, L.sms);
-        blendStepKernel<T, NB, false><<<grid, T * T / 2, 0, stream>>>(B, L.views, L.ranges, L.pairs, L.values,
-                                                                          L.recs, colour, nullptr, nullptr, nullptr,
-                                                                          depth, L.words, L.order);
+        const int grid = residentGrid(blendStepKernel<T, NB, false, false>, T * T / 2, L.sms);
+        blendStepKernel<T, NB, false, false><<<grid, T * T / 2, 0, stream>>>(
+            B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, nullptr, nullptr, nullptr, depth, L.words,
+            L.order);
     }
     return cudaGetLastError();
 }

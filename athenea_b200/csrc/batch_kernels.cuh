@@ -125,6 +125,21 @@ __device__ __forceinline__ uint32_t viewOf(const uint32_t* bases, uint32_t views
     return lo;
 }
 
+// The batched blend adjoint's words for a record (the warp sums it adds up):
+// [0..4] the moments of dL/dpower over the pixel offsets in the record's factored
+// frame t = dx + fr dy, dy (sum dP t, dP dy, dP t^2, dP t dy, dP dy^2), [5] dL/dalpha,
+// [6..8] dL/dcolour. To dL/d(centre, conic): the conic is ca (dx + fr dy)^2 + fs dy^2,
+// so dL/da = sum dP dx^2 with dx = t - fr dy, and so on; in place, in the plain
+// path's kGrad* layout.
+__device__ __forceinline__ void batchMomentsToRecordGrad(float ca, float fr, float fs, float g[10]) {
+    const float mt = g[0], my = g[1], mtt = g[2], mty = g[3], myy = g[4];
+    g[kGradCx] = -2.0f * ca * mt;
+    g[kGradCy] = -2.0f * (fr * ca * mt + fs * my);
+    g[kGradA] = mtt - 2.0f * fr * mty + fr * fr * myy;   // sum dP dx^2
+    g[kGradB2] = 2.0f * (mty - fr * myy);                 // sum dP 2 dx dy
+    g[kGradC] = myy;                                      // sum dP dy^2
+}
+
 // What the persistent blend of batch_blend.cu needs from a batch.
 struct BlendLaunch {
     const BatchView* views;
@@ -136,6 +151,7 @@ struct BlendLaunch {
     const uint32_t* order;   // the tiles, heaviest first
     int sms;
     uint32_t tile, blockBatch;
+    bool count;              // count the walks' work into `words` (a step timed stage by stage)
 };
 
 // A training step's blends over every view's tiles, in one kernel: the forward

@@ -342,6 +342,8 @@ typedef struct {
     uint32_t tile, block_batch;
     float ms_per_step;     /* ath_batch_tune: the chosen setting's time */
     uint32_t degenerate;   /* records whose 2D conic was inverted in FP64 (det < 1e-6 trace^2) */
+    /* The blends' work, counted by the last step ath_batch_time_stages ran (the
+     * captured steps do not count, to keep the counting out of their time). */
     uint64_t evaluated;    /* (pixel, record) evaluations of the forward blend */
     uint64_t blended;      /* of them, those that blended (inside the cutoff, alpha at least 1/255) */
     uint64_t adjoint_visited;  /* (pixel, record) evaluations of the blend adjoint (before the pixel's last contributor) */
