@@ -939,8 +939,16 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
                     reinterpret_cast<float4*>(gk.means), reinterpret_cast<float4*>(gk.scales),
                     reinterpret_cast<float4*>(gk.quats), gk.sh, 48, first, first + n);
             err = cudaGetLastError();
-            if (err == cudaSuccess && !b->bucketEvents.empty() && b->bucketEvents[k])
-                err = cudaEventRecord(b->bucketEvents[k], stream);
+            if (err == cudaSuccess && !b->bucketEvents.empty() && b->bucketEvents[k]) {
+                // in a captured step, an event record node of the graph (an external
+                // event: a stream outside the graph may wait on it after each replay)
+                cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+                err = cudaStreamIsCapturing(stream, &capturing);
+                if (err == cudaSuccess)
+                    err = capturing == cudaStreamCaptureStatusActive
+                              ? cudaEventRecordWithFlags(b->bucketEvents[k], stream, cudaEventRecordExternal)
+                              : cudaEventRecord(b->bucketEvents[k], stream);
+            }
         }
     }
     mark(5);
