@@ -219,31 +219,30 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                     if constexpr (kCount) ++fwdVisits;
                     const float2 ce = sCentre[j];
                     const float4 k = sConic[j];
-                    const float limit = sColour[j].w;
                     const float dx = pxc - ce.x;
+                    const float4 cc = sColour[j];
+                    // both pixels evaluated without branching: a pixel that does not blend the
+                    // record (done, outside the cutoff, or under 1/255) takes alpha 0, which
+                    // leaves its sums and transmittance as they were
 #pragma unroll
                     for (int p = 0; p < 2; ++p) {
-                        if (done[p]) continue;
-                        if constexpr (kCount) ++evaluated;
                         const float dy = pyc[p] - ce.y;
-                        // e = -log2(e)/2 * power; power > cutoff  <=>  e < -log2(e)/2 * cutoff
                         const float t = __fmaf_rn(k.y, dy, dx);
                         const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
-                        if (e < limit) continue;
-                        const float alpha = fminf(0.99f, k.w * fastExp2(e));
-                        if (alpha < kFaint) continue;
-                        if constexpr (kCount) ++blended;
+                        const float a0 = fminf(0.99f, k.w * fastExp2(e));
+                        const bool blend = !done[p] && e >= cc.w && a0 >= kFaint;
+                        if constexpr (kCount) { evaluated += done[p] ? 0u : 1u; blended += blend ? 1u : 0u; }
+                        const float alpha = blend ? a0 : 0.0f;
                         const float w = Tr[p] * alpha;
-                        const float4 c = sColour[j];
-                        r[p] = __fmaf_rn(w, c.x, r[p]);
-                        g[p] = __fmaf_rn(w, c.y, g[p]);
-                        bl[p] = __fmaf_rn(w, c.z, bl[p]);
+                        r[p] = __fmaf_rn(w, cc.x, r[p]);
+                        g[p] = __fmaf_rn(w, cc.y, g[p]);
+                        bl[p] = __fmaf_rn(w, cc.z, bl[p]);
                         if constexpr (!kTrain) depthSum[p] = __fmaf_rn(w, sDepth[j], depthSum[p]);
                         Tr[p] = Tr[p] * (1.0f - alpha);
-                        last[p] = first - range.x + j + 1;
+                        last[p] = blend ? first - range.x + j + 1 : last[p];
                         if constexpr (!kTrain)
-                            if (depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = sDepth[j];
-                        if (Tr[p] < 1e-4f) done[p] = true;
+                            if (blend && depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = sDepth[j];
+                        done[p] = done[p] || Tr[p] < 1e-4f;
                     }
                 }
                 if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
@@ -338,20 +337,20 @@ __global__ void __launch_bounds__(T * T / 2, 2)
 #pragma unroll
                         for (int q = 0; q < (int)kWords; ++q) gv[q] = 0.0f;
                         bool live = false;
+                        // as the forward, without branching: a pixel past its last contributor or
+                        // that does not blend the record takes alpha 0 (T unchanged, no terms)
 #pragma unroll
                         for (int p = 0; p < 2; ++p) {
-                            if (rel >= last[p]) continue;
-                            if constexpr (kCount) ++adjVisited;
                             const float dy = pyc[p] - ce.y;
                             const float t = __fmaf_rn(k.y, dy, dx);
                             const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
-                            if (e < c.w) continue;
                             const float G = fastExp2(e);
                             const float raw = k.w * G;
-                            const float alpha = fminf(0.99f, raw);
-                            if (alpha < kFaint) continue;
-                            live = true;
-                            if constexpr (kCount) ++adjLive;
+                            const float a0 = fminf(0.99f, raw);
+                            const bool on = rel < last[p] && e >= c.w && a0 >= kFaint;
+                            if constexpr (kCount) { adjVisited += rel < last[p] ? 1u : 0u; adjLive += on ? 1u : 0u; }
+                            live = live || on;
+                            const float alpha = on ? a0 : 0.0f;
                             const float inv = fastRcp(1.0f - alpha);
                             const float Tb = Tr[p] * inv;
                             const float w = Tb * alpha;
@@ -359,19 +358,17 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                             gv[7] = __fmaf_rn(w, dC[p][1], gv[7]);
                             gv[8] = __fmaf_rn(w, dC[p][2], gv[8]);
                             const float cd = (c.x * dC[p][0] + c.y * dC[p][1]) + c.z * dC[p][2];
-                            const float dAlpha = Tb * (cd - sd[p]);
+                            const float dAlpha = on && raw < 0.99f && k.w <= 1.0f ? Tb * (cd - sd[p]) : 0.0f;
                             sd[p] = __fmaf_rn(alpha, cd - sd[p], sd[p]);
                             Tr[p] = Tb;
-                            if (raw < 0.99f && k.w <= 1.0f) {
-                                gv[5] = __fmaf_rn(dAlpha, G, gv[5]);
-                                const float dP = -0.5f * alpha * dAlpha;
-                                const float dPt = dP * t, dPy = dP * dy;
-                                gv[0] += dPt;
-                                gv[1] += dPy;
-                                gv[2] = __fmaf_rn(dPt, t, gv[2]);
-                                gv[3] = __fmaf_rn(dPt, dy, gv[3]);
-                                gv[4] = __fmaf_rn(dPy, dy, gv[4]);
-                            }
+                            gv[5] = __fmaf_rn(dAlpha, G, gv[5]);
+                            const float dP = -0.5f * alpha * dAlpha;
+                            const float dPt = dP * t, dPy = dP * dy;
+                            gv[0] += dPt;
+                            gv[1] += dPy;
+                            gv[2] = __fmaf_rn(dPt, t, gv[2]);
+                            gv[3] = __fmaf_rn(dPt, dy, gv[3]);
+                            gv[4] = __fmaf_rn(dPy, dy, gv[4]);
                         }
                         const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, live);
                         if (!lanes) continue;

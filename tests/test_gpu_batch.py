@@ -430,7 +430,8 @@ def test_batched_render_depth_is_the_plain_paths(mode):
 def test_gradient_buckets_give_the_same_gradients_and_signal_each_bucket():
     """ath_batch_set_buckets: the projection adjoint bucket by bucket, an event after each. A
     side stream that waits on bucket k's event and copies that bucket out (where a multi-GPU
-    step posts its all-reduce) sees it final; the gradients equal the one-set step's bit for bit."""
+    step posts its all-reduce) sees it final; the gradients equal the one-set step's to the rounding
+    of their atomic sums, whose order varies from run to run."""
     Pq, M = _scene(40_000, 21)
     views = _views()
     gen = torch.Generator().manual_seed(8)
@@ -458,7 +459,8 @@ def test_gradient_buckets_give_the_same_gradients_and_signal_each_bucket():
             np.testing.assert_array_equal(copies[k].cpu().numpy(), buckets.slices[k].cpu().numpy())
         got = buckets.gather()
         for name in ("means", "scales", "quats", "sh"):
-            np.testing.assert_array_equal(getattr(got, name).cpu().numpy(), getattr(grads_one, name).cpu().numpy(),
-                                          err_msg=name)
-        assert loss.item() == loss_one.item()
+            want = getattr(grads_one, name).cpu().numpy()
+            np.testing.assert_allclose(getattr(got, name).cpu().numpy(), want, rtol=1e-4,
+                                       atol=1e-5 * float(np.abs(want).max()), err_msg=name)
+        assert abs(loss.item() - loss_one.item()) <= 1e-6 * loss_one.item()
     b.set_buckets(None)
