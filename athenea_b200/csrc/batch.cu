@@ -709,7 +709,7 @@ struct ath_batch {
     std::vector<uint32_t> widths, heights, tileBases;
     uint32_t lastSorted = 0, lastSlotBits = 0;
     // scratch
-    DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges, tileOrder;
+    DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges, tileOrder, live;
     uint32_t keyMode = 0;      // 0 automatic; 1 packed; 2 wide; 3 packed, depth exponent renumbered
     bool lastWide = false;
     // the pairs' form, planned by each sizing from its depths' exponents
@@ -857,6 +857,7 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
     L.recs = static_cast<const float4*>(b->recs.ptr);
     L.words = static_cast<uint32_t*>(b->words.ptr);
     L.order = static_cast<const uint32_t*>(b->tileOrder.ptr);
+    L.live = static_cast<uint32_t*>(b->live.ptr);
     L.sms = b->sms;
     L.tile = b->tile;
     L.blockBatch = b->blockBatch;
@@ -1034,6 +1035,9 @@ ath_status sizePairs(ath_batch* b, const ath_mixed_params& P, cudaStream_t strea
     const uint32_t bits = b->depthBits + b->tileBits;
     err = b->sortFlags.reserve(sortFlagWords((uint32_t)b->capacity, bits) * 8);
     if (err != cudaSuccess) return failCuda(err, "reserving the sort's look-back words");
+    // the blends' live bits (written by the forward before the adjoint reads them; no clearing)
+    err = b->live.reserve(liveWords(b->capacity, b->totalTiles, b->tile) * sizeof(uint32_t));
+    if (err != cudaSuccess) return failCuda(err, "reserving the blends' live bits");
     // the look-back words carry epochs: start them all at "not ready"
     err = cudaMemsetAsync(b->sortFlags.ptr, 0, sortFlagWords((uint32_t)b->capacity, bits) * 8, stream);
     if (err == cudaSuccess) err = cudaMemsetAsync(b->words.ptr, 0, kBatchWords * sizeof(uint32_t), stream);

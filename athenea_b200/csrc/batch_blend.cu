@@ -60,18 +60,6 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
     return mask;
 }
 
-// The Gaussian indices of pairs [first, end) that this thread stages (k = thread + q threads,
-// k < NB), for a load issued ahead of their use; 0 past the end.
-template <uint32_t kThreads, uint32_t NB, uint32_t kPer>
-__device__ __forceinline__ void prefetchIndices(const uint64_t* pairs, const uint32_t* values, uint64_t slotMask,
-                                                uint32_t first, uint32_t end, uint32_t (&out)[kPer]) {
-#pragma unroll
-    for (uint32_t q = 0; q < kPer; ++q) {
-        const uint32_t k = threadIdx.x + q * kThreads;
-        out[q] = k < NB && first + k < end ? gaussianOf(pairs, values, slotMask, first + k) : 0u;
-    }
-}
-
 // Nine values summed over a warp: the first eight by a transposed reduction
 // (each level sends half of the values still held and keeps the other half,
 // so three levels leave value (lane >> 2) spread over lanes differing in their
@@ -115,17 +103,18 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth, uint32_t lan
 // per-pixel test decides, the box test only skips records no pixel of the box can
 // pass. So the image does not depend on the tile size.
 //
-// Adjoint: the same boxes and masks, walked in reverse, in batches aligned with
-// the forward's (the forward's last batch, still staged, is the adjoint's first
-// when it holds the tile's last contributor): a warp takes the records marked for
-// its box from its pixels' last contributor down. What a lane sums over its two
-// pixels, and the warp over its 64, are moments of dL/dpower over the pixel
-// offsets in the factored frame (t = dx + fr dy, dy): sum dP t, sum dP dy,
-// sum dP t^2, sum dP t dy, sum dP dy^2. Each visit's warp sums are added into the
-// record's gradient words in global memory as they are (moments, dL/dalpha,
-// dL/dcolour); the projection's adjoint turns the moments into the centre and
-// conic gradients (batchMomentsToRecordGrad), once a record. The loss has
-// no alpha term, so dL/d(alpha out) is 0 and the colour behind a record enters
+// Adjoint: each warp on its own once its pixels' loss gradients are known (no
+// block barrier): the forward marked, for each 32-record chunk of the tile's list
+// a warp walked, the records some pixel of its box blended (`live`, one word a
+// chunk and box); the warp gathers those records, last first, 32 at a time into
+// slots of its own and walks them from its pixels' last contributor down. What a
+// lane sums over its two pixels, and the warp over its 64, are moments of
+// dL/dpower over the pixel offsets in the factored frame (t = dx + fr dy, dy): sum
+// dP t, sum dP dy, sum dP t^2, sum dP t dy, sum dP dy^2. Each visit's warp sums are
+// added into the record's gradient words in global memory as they are (moments,
+// dL/dalpha, dL/dcolour); the projection's adjoint turns the moments into the
+// centre and conic gradients (batchMomentsToRecordGrad), once a record. The loss
+// has no alpha term, so dL/d(alpha out) is 0 and the colour behind a record enters
 // only through S.dC, one value a pixel.
 //
 // kTrain false: the forward blend alone (a batched render: colour and, when
@@ -138,11 +127,11 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
                     const float4* __restrict__ recs, float4* __restrict__ colour, const float* __restrict__ target,
                     float* __restrict__ loss, float* __restrict__ grads, float* __restrict__ depth,
-                    uint32_t* __restrict__ words, const uint32_t* __restrict__ order) {
+                    uint32_t* __restrict__ words, const uint32_t* __restrict__ order, uint32_t* __restrict__ live) {
     constexpr uint32_t kThreads = T * T / 2;
     constexpr uint32_t kAcross = T / kBox;
+    constexpr uint32_t kBoxes = kAcross * kAcross;
     constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
-    constexpr uint32_t kPer = (NB + kThreads - 1) / kThreads;   // records a thread stages a batch
     __shared__ float2 sCentre[NB];
     __shared__ float4 sConic[NB];    // ca, fr, fs pre-scaled; alpha
     __shared__ float4 sColour[NB];   // r g b; the cutoff pre-scaled
@@ -150,7 +139,14 @@ __global__ void __launch_bounds__(T * T / 2, 2)
     __shared__ uint32_t sRec[NB];
     __shared__ float sDepth[kTrain ? 1 : NB];   // a render's record depths
     __shared__ uint32_t sTileBase[kMaxBatchViews];
-    __shared__ uint32_t sTile, sMaxLast;
+    __shared__ uint32_t sTile;
+    // the adjoint's gather slots, a warp's own: 32 records, their place in the tile's list
+    constexpr uint32_t kWarpsHere = kTrain ? kThreads / 32 : 1;
+    __shared__ float2 sWarpCentre[kWarpsHere][32];
+    __shared__ float4 sWarpConic[kWarpsHere][32];
+    __shared__ float4 sWarpColour[kWarpsHere][32];
+    __shared__ uint32_t sWarpRec[kWarpsHere][32];
+    __shared__ uint32_t sWarpRel[kWarpsHere][32];
     for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
     const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
     const float kScale = -0.5f * 1.4426950408889634f;   // power -> base-2 exponent
@@ -166,7 +162,6 @@ __global__ void __launch_bounds__(T * T / 2, 2)
         if (threadIdx.x == 0) {
             const uint32_t ticket = atomicAdd(&words[kBatchBlendTicket], 1u);
             sTile = ticket < B.totalTiles ? order[ticket] : ticket;
-            sMaxLast = 0;
         }
         __syncthreads();
         const uint32_t tile = sTile;
@@ -202,17 +197,16 @@ __global__ void __launch_bounds__(T * T / 2, 2)
         bool done[2];
 #pragma unroll
         for (int p = 0; p < 2; ++p) done[p] = !(px < V.width && py[p] < V.height);
-        uint32_t staged = 0xFFFFFFFFu;   // the first pair of the batch in shared memory
         for (uint32_t first = range.x; first < range.y; first += NB) {
             if (__syncthreads_count(done[0] && done[1]) == kThreads) break;
             const uint32_t count = min(NB, range.y - first);
             for (uint32_t k = threadIdx.x; k < count; k += kThreads) stage(k, gaussianOf(pairs, values, slotMask, first + k));
-            staged = first;
             __syncthreads();
             if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) continue;
             for (uint32_t base = 0; base < count; base += 32) {
                 const uint32_t m = base + lane < count ? sMask[base + lane] : 0u;
                 uint32_t todo = __ballot_sync(0xFFFFFFFFu, (m >> warp) & 1u);
+                uint32_t liveWord = 0;   // the records of this chunk some pixel of the box blended
                 while (todo) {
                     const uint32_t j = base + (uint32_t)__ffs(todo) - 1u;
                     todo &= todo - 1u;
@@ -221,6 +215,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                     const float4 k = sConic[j];
                     const float dx = pxc - ce.x;
                     const float4 cc = sColour[j];
+                    bool hit = false;
                     // both pixels evaluated without branching: a pixel that does not blend the
                     // record (done, outside the cutoff, or under 1/255) takes alpha 0, which
                     // leaves its sums and transmittance as they were
@@ -243,8 +238,14 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                         if constexpr (!kTrain)
                             if (blend && depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = sDepth[j];
                         done[p] = done[p] || Tr[p] < 1e-4f;
+                        hit = hit || blend;
                     }
+                    if constexpr (kTrain)
+                        if (__any_sync(0xFFFFFFFFu, hit)) liveWord |= 1u << (j - base);
                 }
+                if constexpr (kTrain)
+                    if (lane == 0)
+                        live[((size_t)(range.x >> 5) + tile + ((first - range.x + base) >> 5)) * kBoxes + warp] = liveWord;
                 if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
             }
         }
@@ -286,111 +287,111 @@ __global__ void __launch_bounds__(T * T / 2, 2)
             sd[p] = (B.bg[0] * dC[p][0] + B.bg[1] * dC[p][1]) + B.bg[2] * dC[p][2];   // S.dC, S the colour behind
         }
 
-        // ---- adjoint
+        // ---- adjoint: each warp on its own, over the records its box blended, last first
+        // (the forward's live bits), gathered 32 at a time into the warp's own slots; no
+        // block barrier, no staging and no box tests
         const uint32_t warpLast = __reduce_max_sync(0xFFFFFFFFu, max(last[0], last[1]));
-        if (lane == 0 && warpLast) atomicMax(&sMaxLast, warpLast);
-        __syncthreads();
-        const uint32_t end = range.x + sMaxLast;
-        if (end == range.x) continue;
-        uint32_t batchStart = range.x + ((end - 1u - range.x) / NB) * NB, batchEnd = end;
-        bool stagedAlready = batchStart == staged;   // the forward's last batch holds the last contributor
-        uint32_t ahead[kPer];   // the next batch's Gaussian indices, loaded a batch ahead
-        if (!stagedAlready) prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, batchStart, batchEnd, ahead);
-        while (true) {
-            const uint32_t count = batchEnd - batchStart;
-            if (!stagedAlready) {
-                uint32_t gauss[kPer];
+        const uint32_t nChunks = (warpLast + 31u) >> 5;
+        const uint32_t* liveOf = live + ((size_t)(range.x >> 5) + tile) * kBoxes + warp;   // chunk c: [c * kBoxes]
+        for (int32_t hi = (int32_t)nChunks - 1; hi >= 0; hi -= 32) {
+            // lane l: the live bits of chunk hi - l (records 32 c .. 32 c + 31 of the tile)
+            const int32_t ch = hi - (int32_t)lane;
+            const uint32_t word = ch >= 0 ? liveOf[(size_t)ch * kBoxes] : 0u;
+            const uint32_t n = __popc(word);
+            uint32_t incl = n;
 #pragma unroll
-                for (uint32_t q = 0; q < kPer; ++q) gauss[q] = ahead[q];
-                if (batchStart > range.x)
-                    prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, batchStart - NB, batchStart, ahead);
-#pragma unroll
-                for (uint32_t q = 0; q < kPer; ++q) {
-                    const uint32_t k = threadIdx.x + q * kThreads;
-                    if (k >= count) break;
-                    stage(k, gauss[q]);
-                }
-            } else if (batchStart > range.x) {
-                prefetchIndices<kThreads, NB, kPer>(pairs, values, slotMask, batchStart - NB, batchStart, ahead);
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= (uint32_t)o) incl += u;
             }
-            stagedAlready = false;
-            __syncthreads();
-            const uint32_t relStart = batchStart - range.x;
-            if (relStart < warpLast) {
-                for (int base = (int)((count - 1) & ~31u); base >= 0; base -= 32) {
-                    if (relStart + (uint32_t)base >= warpLast) continue;
-                    // the records marked for this warp's box, up to its pixels' last contributor
-                    const uint32_t m = (uint32_t)base + lane < count && relStart + (uint32_t)base + lane < warpLast
-                                           ? sMask[base + lane] : 0u;
-                    uint32_t todo = __ballot_sync(0xFFFFFFFFu, (m >> warp) & 1u);
-                    while (todo) {
-                        const uint32_t hb = 31u - (uint32_t)__clz(todo);
-                        todo &= ~(1u << hb);
-                        if constexpr (kCount) ++adjVisits;
-                        const uint32_t j = (uint32_t)base + hb;
-                        const uint32_t rel = relStart + j;
-                        const float2 ce = sCentre[j];
-                        const float4 k = sConic[j];
-                        const float4 c = sColour[j];
-                        const float dx = pxc - ce.x;
-                        float gv[kWords];
-#pragma unroll
-                        for (int q = 0; q < (int)kWords; ++q) gv[q] = 0.0f;
-                        bool live = false;
-                        // as the forward, without branching: a pixel past its last contributor or
-                        // that does not blend the record takes alpha 0 (T unchanged, no terms)
-#pragma unroll
-                        for (int p = 0; p < 2; ++p) {
-                            const float dy = pyc[p] - ce.y;
-                            const float t = __fmaf_rn(k.y, dy, dx);
-                            const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
-                            const float G = fastExp2(e);
-                            const float raw = k.w * G;
-                            const float a0 = fminf(0.99f, raw);
-                            const bool on = rel < last[p] && e >= c.w && a0 >= kFaint;
-                            if constexpr (kCount) { adjVisited += rel < last[p] ? 1u : 0u; adjLive += on ? 1u : 0u; }
-                            live = live || on;
-                            const float alpha = on ? a0 : 0.0f;
-                            const float inv = fastRcp(1.0f - alpha);
-                            const float Tb = Tr[p] * inv;
-                            const float w = Tb * alpha;
-                            gv[6] = __fmaf_rn(w, dC[p][0], gv[6]);
-                            gv[7] = __fmaf_rn(w, dC[p][1], gv[7]);
-                            gv[8] = __fmaf_rn(w, dC[p][2], gv[8]);
-                            const float cd = (c.x * dC[p][0] + c.y * dC[p][1]) + c.z * dC[p][2];
-                            const float dAlpha = on && raw < 0.99f && k.w <= 1.0f ? Tb * (cd - sd[p]) : 0.0f;
-                            sd[p] = __fmaf_rn(alpha, cd - sd[p], sd[p]);
-                            Tr[p] = Tb;
-                            gv[5] = __fmaf_rn(dAlpha, G, gv[5]);
-                            const float dP = -0.5f * alpha * dAlpha;
-                            const float dPt = dP * t, dPy = dP * dy;
-                            gv[0] += dPt;
-                            gv[1] += dPy;
-                            gv[2] = __fmaf_rn(dPt, t, gv[2]);
-                            gv[3] = __fmaf_rn(dPt, dy, gv[3]);
-                            gv[4] = __fmaf_rn(dPy, dy, gv[4]);
-                        }
-                        const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, live);
-                        if (!lanes) continue;
-                        if constexpr (kCount) ++adjSummed;
-                        // the warp's sums, however few lanes are live, added by nine lanes at once
-                        // into the record's words in global memory (reductions, not read back):
-                        // the five moments, dL/dalpha and dL/dcolour, which the projection's
-                        // adjoint turns into centre and conic gradients (linear in the moments,
-                        // so sums from every box, tile and batch add up)
-                        float ninth;
-                        const float sum = warpSum9(gv, ninth, lane);
-                        const uint32_t word = (lane & 3u) == 0u ? lane >> 2 : lane == 1u ? 8u : kWords;
-                        const float v = lane == 1u ? ninth : sum;
-                        if (word < kWords && v != 0.0f)
-                            atomicAdd(grads + (recBase + sRec[j]) * kGradWords + word, v);
+            const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            const uint32_t excl = incl - n;
+            for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+                // the records of ranks r0 .. r0 + 31 (ranked last first) into the warp's slots
+                if (excl < r0 + 32u && excl + n > r0) {
+                    uint32_t w = word, rank = excl;
+                    while (w && rank < r0 + 32u) {
+                        const uint32_t bit = 31u - (uint32_t)__clz(w);
+                        w &= ~(1u << bit);
+                        if (rank >= r0) sWarpRel[warp][rank - r0] = (uint32_t)ch * 32u + bit;
+                        ++rank;
                     }
                 }
+                __syncwarp();
+                const uint32_t cnt = min(32u, total - r0);
+                if (lane < cnt) {
+                    const uint32_t rel = sWarpRel[warp][lane];
+                    const uint32_t gs = gaussianOf(pairs, values, slotMask, range.x + rel);
+                    const size_t at = (recBase + gs) * 3;
+                    const float4 sc = recs[at + 0];
+                    const float4 c = recs[at + 1];
+                    const float4 rgb = recs[at + 2];
+                    sWarpCentre[warp][lane] = make_float2(sc.x, sc.y);
+                    sWarpConic[warp][lane] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
+                    sWarpColour[warp][lane] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
+                    sWarpRec[warp][lane] = (uint32_t)(recBase + gs);
+                }
+                __syncwarp();
+                for (uint32_t q = 0; q < cnt; ++q) {
+                    if constexpr (kCount) ++adjVisits;
+                    const uint32_t rel = sWarpRel[warp][q];
+                    const float2 ce = sWarpCentre[warp][q];
+                    const float4 k = sWarpConic[warp][q];
+                    const float4 c = sWarpColour[warp][q];
+                    const float dx = pxc - ce.x;
+                    float gv[kWords];
+#pragma unroll
+                    for (int e = 0; e < (int)kWords; ++e) gv[e] = 0.0f;
+                    bool live = false;
+                    // as the forward, without branching: a pixel past its last contributor or
+                    // that does not blend the record takes alpha 0 (T unchanged, no terms)
+#pragma unroll
+                    for (int p = 0; p < 2; ++p) {
+                        const float dy = pyc[p] - ce.y;
+                        const float t = __fmaf_rn(k.y, dy, dx);
+                        const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
+                        const float G = fastExp2(e);
+                        const float raw = k.w * G;
+                        const float a0 = fminf(0.99f, raw);
+                        const bool on = rel < last[p] && e >= c.w && a0 >= kFaint;
+                        if constexpr (kCount) { adjVisited += rel < last[p] ? 1u : 0u; adjLive += on ? 1u : 0u; }
+                        live = live || on;
+                        const float alpha = on ? a0 : 0.0f;
+                        const float inv = fastRcp(1.0f - alpha);
+                        const float Tb = Tr[p] * inv;
+                        const float w = Tb * alpha;
+                        gv[6] = __fmaf_rn(w, dC[p][0], gv[6]);
+                        gv[7] = __fmaf_rn(w, dC[p][1], gv[7]);
+                        gv[8] = __fmaf_rn(w, dC[p][2], gv[8]);
+                        const float cd = (c.x * dC[p][0] + c.y * dC[p][1]) + c.z * dC[p][2];
+                        const float dAlpha = on && raw < 0.99f && k.w <= 1.0f ? Tb * (cd - sd[p]) : 0.0f;
+                        sd[p] = __fmaf_rn(alpha, cd - sd[p], sd[p]);
+                        Tr[p] = Tb;
+                        gv[5] = __fmaf_rn(dAlpha, G, gv[5]);
+                        const float dP = -0.5f * alpha * dAlpha;
+                        const float dPt = dP * t, dPy = dP * dy;
+                        gv[0] += dPt;
+                        gv[1] += dPy;
+                        gv[2] = __fmaf_rn(dPt, t, gv[2]);
+                        gv[3] = __fmaf_rn(dPt, dy, gv[3]);
+                        gv[4] = __fmaf_rn(dPy, dy, gv[4]);
+                    }
+                    if (!__any_sync(0xFFFFFFFFu, live)) continue;
+                    if constexpr (kCount) ++adjSummed;
+                    // the warp's sums, however few lanes are live, added by nine lanes at once
+                    // into the record's words in global memory (reductions, not read back):
+                    // the five moments, dL/dalpha and dL/dcolour, which the projection's
+                    // adjoint turns into centre and conic gradients (linear in the moments,
+                    // so sums from every box, tile and batch add up)
+                    float ninth;
+                    const float sum = warpSum9(gv, ninth, lane);
+                    const uint32_t slot = (lane & 3u) == 0u ? lane >> 2 : lane == 1u ? 8u : kWords;
+                    const float val = lane == 1u ? ninth : sum;
+                    if (slot < kWords && val != 0.0f)
+                        atomicAdd(grads + (size_t)sWarpRec[warp][q] * kGradWords + slot, val);
+                }
+                __syncwarp();   // the next round's gathers overwrite the slots
             }
-            __syncthreads();   // the next batch's staging overwrites what the walks read
-            if (batchStart == range.x) break;
-            batchEnd = batchStart;
-            batchStart -= NB;
         }
     }
 #pragma unroll
@@ -425,16 +426,18 @@ cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t str
     if (target && L.count) {
         const int grid = residentGrid(blendStepKernel<T, NB, true, true>, T * T / 2, L.sms);
         blendStepKernel<T, NB, true, true><<<grid, T * T / 2, 0, stream>>>(
-            B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order);
+            B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order,
+            L.live);
     } else if (target) {
         const int grid = residentGrid(blendStepKernel<T, NB, true, false>, T * T / 2, L.sms);
         blendStepKernel<T, NB, true, false><<<grid, T * T / 2, 0, stream>>>(
-            B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order);
+            B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order,
+            L.live);
     } else {
         const int grid = residentGrid(blendStepKernel<T, NB, false, false>, T * T / 2, L.sms);
         blendStepKernel<T, NB, false, false><<<grid, T * T / 2, 0, stream>>>(
             B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, nullptr, nullptr, nullptr, depth, L.words,
-            L.order);
+            L.order, nullptr);
     }
     return cudaGetLastError();
 }

@@ -149,10 +149,19 @@ struct BlendLaunch {
     const float4* recs;
     uint32_t* words;
     const uint32_t* order;   // the tiles, heaviest first
+    uint32_t* live;          // a training step's live bits: per tile, one word a 32-record chunk and box
     int sms;
     uint32_t tile, blockBatch;
     bool count;              // count the walks' work into `words` (a step timed stage by stage)
 };
+
+// The live bits' words a batch needs: chunk c of tile t's list (records 32 c ..
+// 32 c + 31 after its range's start) and box b at word ((start >> 5) + t + c) boxes + b,
+// so tiles never overlap (each takes at most one word-row past start / 32).
+inline size_t liveWords(uint64_t capacity, uint32_t totalTiles, uint32_t tile) {
+    const size_t boxes = (size_t)(tile / 8) * (tile / 8);
+    return (size_t)(capacity / 32 + totalTiles + 2) * boxes;
+}
 
 // A training step's blends over every view's tiles, in one kernel: the forward
 // blend into `colour`; the loss, each view's mean L2 against `target` (float3 a
