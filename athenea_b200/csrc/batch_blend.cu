@@ -16,6 +16,10 @@ namespace {
 
 // A warp's box of pixels: 8x8, two pixels a lane.
 constexpr uint32_t kBox = 8;
+// The pixels a block takes of a tile: a span of kBlendSpan x kBlendSpan (or the
+// whole tile when it is smaller), so that a block's barriers wait on fewer boxes
+// and a span whose pixels are done stops staging the tile's records.
+constexpr uint32_t kBlendSpan = 16;
 
 // The footprint's half extents from the factored conic: the covariance's
 // diagonal a' = cutoff (1/ca + fr^2/fs) and c' = cutoff / fs.
@@ -121,16 +125,17 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth, uint32_t lan
 // given, depth as the plain blend makes it; no target, loss or gradients).
 // kCount: also count the walks' work (evaluations and warp visits) into the
 // batch's words; a step timed stage by stage counts, the captured steps do not.
-template <uint32_t T, uint32_t NB, bool kTrain, bool kCount>
-__global__ void __launch_bounds__(T * T / 2, 2)
+template <uint32_t T, uint32_t S, uint32_t NB, bool kTrain, bool kCount>
+__global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
     blendStepKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
                     const float4* __restrict__ recs, float4* __restrict__ colour, const float* __restrict__ target,
                     float* __restrict__ loss, float* __restrict__ grads, float* __restrict__ depth,
                     uint32_t* __restrict__ words, const uint32_t* __restrict__ order, uint32_t* __restrict__ live) {
-    constexpr uint32_t kThreads = T * T / 2;
-    constexpr uint32_t kAcross = T / kBox;
-    constexpr uint32_t kBoxes = kAcross * kAcross;
+    constexpr uint32_t kThreads = S * S / 2;
+    constexpr uint32_t kAcross = S / kBox;            // boxes across a block's span
+    constexpr uint32_t kSpans = (T / S) * (T / S);    // spans (blocks' work units) a tile
+    constexpr uint32_t kBoxes = (T / kBox) * (T / kBox);   // boxes a tile (the live words' row)
     constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
     __shared__ float2 sCentre[NB];
     __shared__ float4 sConic[NB];    // ca, fr, fs pre-scaled; alpha
@@ -161,17 +166,18 @@ __global__ void __launch_bounds__(T * T / 2, 2)
         __syncthreads();
         if (threadIdx.x == 0) {
             const uint32_t ticket = atomicAdd(&words[kBatchBlendTicket], 1u);
-            sTile = ticket < B.totalTiles ? order[ticket] : ticket;
+            sTile = ticket < B.totalTiles * kSpans ? order[ticket / kSpans] * kSpans + ticket % kSpans : 0xFFFFFFFFu;
         }
         __syncthreads();
-        const uint32_t tile = sTile;
-        if (tile >= B.totalTiles) break;
+        if (sTile == 0xFFFFFFFFu) break;
+        const uint32_t tile = sTile / kSpans, span = sTile % kSpans;   // the block's span of the tile
         const uint32_t v = viewOf(sTileBase, B.views, tile);
         const BatchView& V = views[v];
         const uint32_t local = tile - V.tileBase;
         const uint32_t tx = local % V.tilesX, ty = local / V.tilesX;
-        const float tileX0 = (float)(tx * T), tileY0 = (float)(ty * T);
-        const uint32_t px = tx * T + lx, py[2] = {ty * T + ly, ty * T + ly + 4};
+        const uint32_t spanX = tx * T + (span % (T / S)) * S, spanY = ty * T + (span / (T / S)) * S;
+        const float tileX0 = (float)spanX, tileY0 = (float)spanY;   // the span's first pixel
+        const uint32_t px = spanX + lx, py[2] = {spanY + ly, spanY + ly + 4};
         const uint2 range = ranges[tile];
         const float pxc = (float)px + 0.5f, pyc[2] = {(float)py[0] + 0.5f, (float)py[1] + 0.5f};
         const size_t recBase = (size_t)v * B.count;
@@ -186,7 +192,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
             sCentre[k] = make_float2(sc.x, sc.y);
             sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
             sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
-            sMask[k] = boxMask<T>(tileX0, tileY0, sc, c.x, c.y, c.z);
+            sMask[k] = boxMask<S>(tileX0, tileY0, sc, c.x, c.y, c.z);
             if constexpr (!kTrain) sDepth[k] = sc.z;
         };
 
@@ -245,7 +251,8 @@ __global__ void __launch_bounds__(T * T / 2, 2)
                 }
                 if constexpr (kTrain)
                     if (lane == 0)
-                        live[((size_t)(range.x >> 5) + tile + ((first - range.x + base) >> 5)) * kBoxes + warp] = liveWord;
+                        live[((size_t)(range.x >> 5) + tile + ((first - range.x + base) >> 5)) * kBoxes +
+                             span * (kAcross * kAcross) + warp] = liveWord;
                 if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
             }
         }
@@ -292,7 +299,7 @@ __global__ void __launch_bounds__(T * T / 2, 2)
         // block barrier, no staging and no box tests
         const uint32_t warpLast = __reduce_max_sync(0xFFFFFFFFu, max(last[0], last[1]));
         const uint32_t nChunks = (warpLast + 31u) >> 5;
-        const uint32_t* liveOf = live + ((size_t)(range.x >> 5) + tile) * kBoxes + warp;   // chunk c: [c * kBoxes]
+        const uint32_t* liveOf = live + ((size_t)(range.x >> 5) + tile) * kBoxes + span * (kAcross * kAcross) + warp;
         for (int32_t hi = (int32_t)nChunks - 1; hi >= 0; hi -= 32) {
             // lane l: the live bits of chunk hi - l (records 32 c .. 32 c + 31 of the tile)
             const int32_t ch = hi - (int32_t)lane;
@@ -420,22 +427,22 @@ int residentGrid(K kernel, int threads, int sms) {
     return (n > 0 ? n : 1) * sms;
 }
 
-template <uint32_t T, uint32_t NB>
+template <uint32_t T, uint32_t S, uint32_t NB>
 cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
                      const float* target, float* loss, float* grads, float* depth) {
     if (target && L.count) {
-        const int grid = residentGrid(blendStepKernel<T, NB, true, true>, T * T / 2, L.sms);
-        blendStepKernel<T, NB, true, true><<<grid, T * T / 2, 0, stream>>>(
+        const int grid = residentGrid(blendStepKernel<T, S, NB, true, true>, S * S / 2, L.sms);
+        blendStepKernel<T, S, NB, true, true><<<grid, S * S / 2, 0, stream>>>(
             B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order,
             L.live);
     } else if (target) {
-        const int grid = residentGrid(blendStepKernel<T, NB, true, false>, T * T / 2, L.sms);
-        blendStepKernel<T, NB, true, false><<<grid, T * T / 2, 0, stream>>>(
+        const int grid = residentGrid(blendStepKernel<T, S, NB, true, false>, S * S / 2, L.sms);
+        blendStepKernel<T, S, NB, true, false><<<grid, S * S / 2, 0, stream>>>(
             B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order,
             L.live);
     } else {
-        const int grid = residentGrid(blendStepKernel<T, NB, false, false>, T * T / 2, L.sms);
-        blendStepKernel<T, NB, false, false><<<grid, T * T / 2, 0, stream>>>(
+        const int grid = residentGrid(blendStepKernel<T, S, NB, false, false>, S * S / 2, L.sms);
+        blendStepKernel<T, S, NB, false, false><<<grid, S * S / 2, 0, stream>>>(
             B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, nullptr, nullptr, nullptr, depth, L.words,
             L.order, nullptr);
     }
@@ -451,7 +458,8 @@ cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t str
 cudaError_t launchBatchBlendStep(const BatchConst& B, const BlendLaunch& L, cudaStream_t stream, float4* colour,
                                  const float* target, float* loss, float* grads, float* depth) {
 #define ATH_CASE(T_, NB_) \
-    if (L.tile == T_ && L.blockBatch == NB_) return stepWith<T_, NB_>(B, L, stream, colour, target, loss, grads, depth);
+    if (L.tile == T_ && L.blockBatch == NB_) \
+        return stepWith<T_, (T_ > kBlendSpan ? kBlendSpan : T_), NB_>(B, L, stream, colour, target, loss, grads, depth);
     ATH_BLEND_CASES(ATH_CASE)
 #undef ATH_CASE
     return cudaErrorInvalidValue;
