@@ -117,7 +117,8 @@ class BatchStats(C.Structure):
                 ("block_batch", C.c_uint32), ("ms_per_step", C.c_float), ("degenerate", C.c_uint32),
                 ("evaluated", C.c_uint64), ("blended", C.c_uint64), ("adjoint_visited", C.c_uint64),
                 ("adjoint_live", C.c_uint64), ("warp_visits_forward", C.c_uint64),
-                ("warp_visits_adjoint", C.c_uint64), ("warp_visits_adjoint_summed", C.c_uint64)]
+                ("warp_visits_adjoint", C.c_uint64), ("warp_visits_adjoint_summed", C.c_uint64),
+                ("records_staged", C.c_uint64)]
 
 
 class BatchBuffers(C.Structure):

@@ -1305,6 +1305,7 @@ extern "C" ath_status ath_batch_check(ath_batch* b, ath_batch_stats* out, void* 
     out->warp_visits_forward = word64(kBatchFwdVisits);
     out->warp_visits_adjoint = word64(kBatchAdjVisits);
     out->warp_visits_adjoint_summed = word64(kBatchAdjSummed);
+    out->records_staged = word64(kBatchStaged);
     out->degenerate = w[kBatchDegenerate];
     out->tile = b->tile;
     out->block_batch = b->blockBatch;
@@ -1344,7 +1345,7 @@ extern "C" ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params
     uint32_t* words = static_cast<uint32_t*>(b->words.ptr);
     cudaError_t err = cudaMemsetAsync(words + kBatchEvaluated, 0, 2 * sizeof(uint32_t), stream);
     if (err == cudaSuccess)
-        err = cudaMemsetAsync(words + kBatchBlended, 0, (kBatchAdjSummed + 2 - kBatchBlended) * sizeof(uint32_t),
+        err = cudaMemsetAsync(words + kBatchBlended, 0, (kBatchStaged + 2 - kBatchBlended) * sizeof(uint32_t),
                               stream);
     if (err == cudaSuccess)
         err = enqueueStep(b, *params, target, reinterpret_cast<float4*>(colour), loss, g, stream, false, marks);

@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
     uint32_t blended = 0;     // of them, those that blended
     uint32_t adjVisited = 0, adjLive = 0;   // the adjoint's evaluations, and those that blended
     uint32_t fwdVisits = 0, adjVisits = 0, adjSummed = 0;   // a warp's record visits (counted by lane 0)
+    uint32_t staged = 0;      // records this thread staged
     float lossSum = 0.0f;     // this thread's pixels' share of the loss
     while (true) {
         __syncthreads();
@@ -184,6 +185,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
         // record s of this view into slot k: the factored conic's two weights and the
         // cutoff pre-scaled to base-2 exponent units, and the boxes it can reach
         auto stage = [&](uint32_t k, uint32_t s) {
+            if constexpr (kCount) ++staged;
             sRec[k] = s;
             const size_t at = (recBase + s) * 3;
             const float4 sc = recs[at + 0];
@@ -411,12 +413,12 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
     if constexpr (!kCount) return;
     // the work counts: a warp's sums, one atomic each
     const uint32_t visits = lane == 0;   // a warp's visits, once
-    const uint32_t counts[7] = {evaluated, blended, adjVisited, adjLive, fwdVisits * visits, adjVisits * visits,
-                                adjSummed * visits};
-    const uint32_t at[7] = {kBatchEvaluated, kBatchBlended, kBatchAdjVisited, kBatchAdjLive, kBatchFwdVisits,
-                            kBatchAdjVisits, kBatchAdjSummed};
+    const uint32_t counts[8] = {evaluated, blended, adjVisited, adjLive, fwdVisits * visits, adjVisits * visits,
+                                adjSummed * visits, staged};
+    const uint32_t at[8] = {kBatchEvaluated, kBatchBlended, kBatchAdjVisited, kBatchAdjLive, kBatchFwdVisits,
+                            kBatchAdjVisits, kBatchAdjSummed, kBatchStaged};
 #pragma unroll
-    for (int c = 0; c < 7; ++c) {
+    for (int c = 0; c < 8; ++c) {
         uint64_t e = counts[c];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xFFFFFFFFu, e, o);

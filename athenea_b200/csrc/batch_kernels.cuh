@@ -65,6 +65,7 @@ enum BatchWord : uint32_t {
     kBatchFwdVisits = 32,    // 64-bit (32, 33): (warp, record) visits of the forward walk
     kBatchAdjVisits = 34,    // 64-bit (34, 35): (warp, record) visits of the adjoint walk
     kBatchAdjSummed = 36,    // 64-bit (36, 37): adjoint visits with a live lane, whose sums the warp reduced
+    kBatchStaged = 38,       // 64-bit (38, 39): records a block staged (loaded and box-tested) for the forward
     kBatchWords = 48,
 };
 

@@ -670,7 +670,7 @@ class BatchTrainer:
                     degenerate=st.degenerate, evaluated=st.evaluated, blended=st.blended,
                     adjoint_visited=st.adjoint_visited, adjoint_live=st.adjoint_live,
                     warp_visits_forward=st.warp_visits_forward, warp_visits_adjoint=st.warp_visits_adjoint,
-                    warp_visits_adjoint_summed=st.warp_visits_adjoint_summed)
+                    warp_visits_adjoint_summed=st.warp_visits_adjoint_summed, records_staged=st.records_staged)
 
     def tune(self, params: MixedParams, target, colour, loss, grads: "Params", repeats: int = 3,
              stream: torch.cuda.Stream | None = None) -> dict:

@@ -569,7 +569,8 @@ def main():
         "blended": stats["blended"], "adjoint_visited": stats["adjoint_visited"],
         "adjoint_live": stats["adjoint_live"], "warp_visits": {
             "forward": stats["warp_visits_forward"], "adjoint": stats["warp_visits_adjoint"],
-            "adjoint_summed": stats["warp_visits_adjoint_summed"]}, "arith_peaks": res["arith"],
+            "adjoint_summed": stats["warp_visits_adjoint_summed"]}, "records_staged": stats["records_staged"],
+        "arith_peaks": res["arith"],
         "degenerate_fp64": stats["degenerate"], "loss": res["loss"],
         "roofline": roofline,
         "e2e": {"value": res["e2e_ms"] / V, "unit": "ms/view", "h2d_bytes_per_step": res["h2d"],

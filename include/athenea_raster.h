@@ -351,6 +351,7 @@ typedef struct {
     uint64_t warp_visits_forward;   /* (warp, record) visits of the forward walk (a warp: 64 pixels) */
     uint64_t warp_visits_adjoint;   /* (warp, record) visits of the adjoint walk */
     uint64_t warp_visits_adjoint_summed;  /* of them, those with a live pixel, whose sums the warp reduced */
+    uint64_t records_staged;        /* records the blends' blocks loaded and box-tested for the forward walk */
 } ath_batch_stats;
 
 ath_status ath_batch_create(ath_batch** out);
