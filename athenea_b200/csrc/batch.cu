@@ -319,9 +319,9 @@ __global__ void __launch_bounds__(kProjThreads, 5)   // five blocks an SM: the k
     if (i < B.count && gb < gaussBlocks) {
         // the record's gradient words, which the blend adjoint sums into, start at zero (a training step's)
         if (grads) {
-            float4* zero = reinterpret_cast<float4*>(grads + ((size_t)v * B.count + i) * kBatchGradWords);
+            float2* zero = reinterpret_cast<float2*>(grads + ((size_t)v * B.count + i) * kGradWords);
 #pragma unroll
-            for (uint32_t k = 0; k < kBatchGradWords / 4; ++k) zero[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            for (uint32_t k = 0; k < kGradWords / 2; ++k) zero[k] = make_float2(0.0f, 0.0f);
         }
         InstanceConst I = B.inst;
 #pragma unroll
@@ -594,11 +594,16 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
         for (int k = 0; k < 48; ++k) dSh[k] = 0.0f;
         // each view's colour gradient loaded a view ahead, so its latency overlaps the work
-        const float4* gv4 = reinterpret_cast<const float4*>(grads);   // a record's words: three float4
-        float4 next = gv4[(size_t)i * 3 + 2];                            // dL/dcolour r g b
+        const float* gr0 = grads + (size_t)i * kGradWords;
+        float next[3] = {gr0[kGradR], gr0[kGradG], gr0[kGradB]};
         for (uint32_t v = 0; v < B.views; ++v) {
-            const float gc[3] = {next.x, next.y, next.z};
-            if (v + 1 < B.views) next = gv4[((size_t)(v + 1) * B.count + i) * 3 + 2];
+            const float gc[3] = {next[0], next[1], next[2]};
+            if (v + 1 < B.views) {
+                const float* gr = grads + ((size_t)(v + 1) * B.count + i) * kGradWords;
+                next[0] = gr[kGradR];
+                next[1] = gr[kGradG];
+                next[2] = gr[kGradB];
+            }
             if (gc[0] == 0.0f && gc[1] == 0.0f && gc[2] == 0.0f) continue;
             colourAdjointFast(sh, g, degree, I.linear, views[v].eye, gc, dSh, dp);
         }
@@ -614,15 +619,21 @@ __global__ void __launch_bounds__(128)
     acc.dQuat[0] = acc.dQuat[1] = acc.dQuat[2] = acc.dQuat[3] = 0.0f;
     float dMsum[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
     bool shaped = false;
-    const float4* gv4 = reinterpret_cast<const float4*>(grads);
-    float4 next0 = gv4[(size_t)i * 3], next1 = gv4[(size_t)i * 3 + 1];   // the moments and dL/dalpha
+    float next[kGradWords];
+#pragma unroll
+    for (int k = 0; k < (int)kGradWords; ++k) next[k] = grads[(size_t)i * kGradWords + k];
     for (uint32_t v = 0; v < B.views; ++v) {
-        const float4 m0 = next0, m1 = next1;
-        const bool any = m0.x != 0.0f || m0.y != 0.0f || m0.z != 0.0f || m0.w != 0.0f || m1.x != 0.0f ||
-                         m1.y != 0.0f;
+        float gw[kGradWords];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < (int)kGradWords; ++k) {
+            gw[k] = next[k];
+            any |= gw[k] != 0.0f;
+        }
         if (v + 1 < B.views) {
-            next0 = gv4[((size_t)(v + 1) * B.count + i) * 3];
-            next1 = gv4[((size_t)(v + 1) * B.count + i) * 3 + 1];
+            const float* gr = grads + ((size_t)(v + 1) * B.count + i) * kGradWords;
+#pragma unroll
+            for (int k = 0; k < (int)kGradWords; ++k) next[k] = gr[k];
         }
         if (!any) continue;
         const BatchView& V = views[v];
@@ -634,8 +645,7 @@ __global__ void __launch_bounds__(128)
         for (int k = 0; k < 12; ++k) I.m[k] = V.m[k];
         I.eye[0] = V.eye[0]; I.eye[1] = V.eye[1]; I.eye[2] = V.eye[2];
         const Geometry G = projectGeometry<true>(F, I, g, g.opacity);
-        float gw[kGradWords];
-        batchMomentsToRecordGrad(G.ca, G.fr, G.fs, m0, m1, gw);   // the blend's moments, to the record's terms
+        batchMomentsToRecordGrad(G.ca, G.fr, G.fs, gw);   // the blend's moments, to the record's terms
         float dpv[3] = {0.0f, 0.0f, 0.0f};
         float dM[3][3];
         geometryAdjointToM(F, I, g, G, gw, dpv, acc, dM);
@@ -952,7 +962,7 @@ ath_status reserveBatch(ath_batch* b, uint32_t count) {
     cudaError_t err = b->words.reserve(kBatchWords * sizeof(uint32_t));
     if (err == cudaSuccess && b->count == 0) err = cudaMemset(b->words.ptr, 0, kBatchWords * sizeof(uint32_t));
     if (err == cudaSuccess) err = b->recs.reserve((size_t)V * count * 48);
-    if (err == cudaSuccess) err = b->grads.reserve((size_t)V * count * kBatchGradWords * sizeof(float));
+    if (err == cudaSuccess) err = b->grads.reserve((size_t)V * count * kGradWords * sizeof(float));
     if (err == cudaSuccess) err = b->projFlags.reserve((size_t)std::max(1u, gaussBlocks * V) * 8);
     if (err == cudaSuccess) err = b->ranges.reserve((size_t)std::max(1u, b->totalTiles) * 8);
     if (err == cudaSuccess) err = b->tileOrder.reserve((size_t)std::max(1u, b->totalTiles) * 4);

@@ -394,14 +394,10 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
                     // so sums from every box, tile and batch add up)
                     float ninth;
                     const float sum = warpSum9(gv, ninth, lane);
-                    // sums 0..7 (moments, alpha, r, g) at lanes 0, 4, .. 28, the ninth (b) at lane 1;
-                    // to the record's words (kBatchGradWords layout)
-                    const uint32_t sumAt = lane >> 2;
-                    const uint32_t slot = lane == 1u ? (uint32_t)kBgB
-                                          : (lane & 3u) == 0u ? (sumAt < 6u ? sumAt : sumAt + 2u) : 32u;
+                    const uint32_t slot = (lane & 3u) == 0u ? lane >> 2 : lane == 1u ? 8u : kWords;
                     const float val = lane == 1u ? ninth : sum;
-                    if (slot < kBatchGradWords && val != 0.0f)
-                        atomicAdd(grads + (size_t)sWarpRec[warp][q] * kBatchGradWords + slot, val);
+                    if (slot < kWords && val != 0.0f)
+                        atomicAdd(grads + (size_t)sWarpRec[warp][q] * kGradWords + slot, val);
                 }
                 __syncwarp();   // the next round's gathers overwrite the slots
             }

@@ -126,30 +126,19 @@ __device__ __forceinline__ uint32_t viewOf(const uint32_t* bases, uint32_t views
     return lo;
 }
 
-// A batched record's gradient words: twelve floats (three 16-byte vectors, so
-// the projection's adjoint reads them with three loads), the sums the blend
-// adjoint adds up: [0..3] the moments of dL/dpower over the pixel offsets in the
-// record's factored frame t = dx + fr dy, dy: sum dP t, sum dP dy, sum dP t^2,
-// sum dP t dy; [4] sum dP dy^2; [5] dL/dalpha; [8..10] dL/dcolour; 6, 7 and 11 unused.
-constexpr uint32_t kBatchGradWords = 12;
-enum BatchGradWord : uint32_t {
-    kBgMt = 0, kBgMy = 1, kBgMtt = 2, kBgMty = 3, kBgMyy = 4, kBgAlpha = 5, kBgR = 8, kBgG = 9, kBgB = 10,
-};
-
-// A record's moments to dL/d(centre, conic) in the plain path's kGrad* layout:
-// the conic is ca (dx + fr dy)^2 + fs dy^2, so dL/da = sum dP dx^2 with
-// dx = t - fr dy, and so on. `m`: words 0..7 of the record's gradient.
-__device__ __forceinline__ void batchMomentsToRecordGrad(float ca, float fr, float fs, float4 m0, float4 m1,
-                                                         float g[kGradWords]) {
-    const float mt = m0.x, my = m0.y, mtt = m0.z, mty = m0.w, myy = m1.x;
+// The batched blend adjoint's words for a record (the warp sums it adds up):
+// [0..4] the moments of dL/dpower over the pixel offsets in the record's factored
+// frame t = dx + fr dy, dy (sum dP t, dP dy, dP t^2, dP t dy, dP dy^2), [5] dL/dalpha,
+// [6..8] dL/dcolour. To dL/d(centre, conic): the conic is ca (dx + fr dy)^2 + fs dy^2,
+// so dL/da = sum dP dx^2 with dx = t - fr dy, and so on; in place, in the plain
+// path's kGrad* layout.
+__device__ __forceinline__ void batchMomentsToRecordGrad(float ca, float fr, float fs, float g[10]) {
+    const float mt = g[0], my = g[1], mtt = g[2], mty = g[3], myy = g[4];
     g[kGradCx] = -2.0f * ca * mt;
     g[kGradCy] = -2.0f * (fr * ca * mt + fs * my);
     g[kGradA] = mtt - 2.0f * fr * mty + fr * fr * myy;   // sum dP dx^2
     g[kGradB2] = 2.0f * (mty - fr * myy);                 // sum dP 2 dx dy
     g[kGradC] = myy;                                      // sum dP dy^2
-    g[kGradAlpha] = m1.y;
-    g[kGradR] = g[kGradG] = g[kGradB] = 0.0f;             // the colour's adjoint reads words 8..10 itself
-    g[kGradZ] = 0.0f;
 }
 
 // What the persistent blend of batch_blend.cu needs from a batch.
