@@ -32,6 +32,7 @@ cudaError_t launchRanges(uint32_t pairs, const uint32_t* pairsDevice, uint32_t t
                          uint2* ranges, uint32_t* status, cudaStream_t stream);
 
 // sort.cu
+constexpr uint32_t kSortTileKeys = 8192;   // keys a onesweep block ranks (the look-back's unit)
 uint32_t sortPasses(uint32_t bits);
 uint32_t sortTiles(uint32_t n);
 size_t sortFlagWords(uint32_t n, uint32_t bits);

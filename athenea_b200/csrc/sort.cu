@@ -19,10 +19,11 @@ namespace ath {
 namespace {
 
 constexpr uint32_t kRadix = 256;
-constexpr uint32_t kSortThreads = 256;
+constexpr uint32_t kSortThreads = 512;
 constexpr uint32_t kWarps = kSortThreads / 32;
 constexpr uint32_t kItems = 16;
-constexpr uint32_t kTileKeys = kSortThreads * kItems;   // 4096
+constexpr uint32_t kTileKeys = kSortThreads * kItems;   // 8192: fewer tiles for the look-back to walk
+static_assert(kTileKeys == kSortTileKeys, "kernels.h states the sort's tile size");
 // A warp ranks its items in kChains independent chains (items 0-7 and 8-15),
 // each with its own digit counters, so the two chains' shared-memory round
 // trips overlap instead of queueing behind each other; the chains are ordered
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(256)
         if (sHist[j]) atomicAdd(&hist[j], sHist[j]);
 }
 
-// Exclusive scan of one value a thread over the block (256 threads).
+// Exclusive scan of one value a thread over the block (kSortThreads threads).
 __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* sWarp) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t incl = v;
@@ -73,7 +74,7 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* sWa
 }
 
 template <bool kValues>
-__global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
+__global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     onesweepKernel(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
                    uint64_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, uint32_t n, uint32_t shift,
                    const uint32_t* __restrict__ globalHist, uint64_t* __restrict__ flags, uint32_t* __restrict__ ticket,
@@ -140,23 +141,27 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
     }
     __syncthreads();
 
-    // One thread a digit: the warps' counts to exclusive offsets, the tile's count.
-    const uint32_t t = tid;
+    // One thread a digit (the first kRadix threads): the warps' counts to exclusive
+    // offsets, the tile's count; every thread takes part in the block scans.
+    const bool digit = tid < kRadix;
+    const uint32_t t = digit ? tid : 0u;
     uint32_t count = 0;
+    if (digit) {
 #pragma unroll
-    for (uint32_t w = 0; w < kCounters; ++w) {
-        const uint32_t c = sWarpCnt[w * kRadix + t];
-        sWarpCnt[w * kRadix + t] = count;
-        count += c;
+        for (uint32_t w = 0; w < kCounters; ++w) {
+            const uint32_t c = sWarpCnt[w * kRadix + t];
+            sWarpCnt[w * kRadix + t] = count;
+            count += c;
+        }
     }
     // Where this tile's share of digit t starts in the output.
     uint64_t* flag = flags + (size_t)tile * kRadix + t;
-    uint32_t exclusive;
+    uint32_t exclusive = 0;
     const uint64_t tag = (uint64_t)epoch << 34;
     if (tile == 0) {
-        exclusive = blockExclusiveScan(globalHist[t], sScan);
-        storeRelaxed(flag, tag | (2ull << 32) | (uint64_t)(exclusive + count));
-    } else {
+        exclusive = blockExclusiveScan(digit ? globalHist[t] : 0u, sScan);
+        if (digit) storeRelaxed(flag, tag | (2ull << 32) | (uint64_t)(exclusive + count));
+    } else if (digit) {
         storeRelaxed(flag, tag | (1ull << 32) | (uint64_t)count);
         uint64_t sum = 0;
         int64_t j = (int64_t)tile - 1;
@@ -180,8 +185,10 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
         storeRelaxed(flag, tag | (2ull << 32) | (uint64_t)(exclusive + count));
     }
     const uint32_t start = blockExclusiveScan(count, sScan);
-    sStart[t] = start;
-    sAdjust[t] = exclusive - start;
+    if (digit) {
+        sStart[t] = start;
+        sAdjust[t] = exclusive - start;
+    }
     __syncthreads();
 
     // Scatter into shared memory in the tile's sorted order, then out.

@@ -11,7 +11,7 @@
 // with the library on every GPU that loads it, and allocates nothing.
 //
 // The limit follows from that array's size: at most kStaticMaxCount pairs a
-// call, 4 MiB of device memory a GPU for the library's lifetime. Every call
+// call, 2 MiB of device memory a GPU for the library's lifetime. Every call
 // shares the array and it keeps the last call's contents, so each call clears
 // what must start at zero (histograms, look-back words, tickets); calls that
 // overlap on the GPU (on different streams, or from different threads without
@@ -32,7 +32,7 @@ namespace {
 
 constexpr uint32_t kStaticMaxCount = 1u << 20;              // pairs a call
 constexpr uint32_t kStaticMaxPasses = 8;                    // 64-bit keys, 8 bits a pass
-constexpr size_t kStaticTiles = kStaticMaxCount / 4096;     // the onesweep's 4096-key tiles
+constexpr size_t kStaticTiles = kStaticMaxCount / kSortTileKeys;   // the onesweep's tiles
 constexpr size_t kFlagWords = kStaticMaxPasses * kStaticTiles * 256;   // look-back words (u64)
 constexpr size_t kHistWords = kStaticMaxPasses * 256 / 2;               // 8 x 256 u32 histograms, as u64
 constexpr size_t kCounterWords = 8;                                     // 16 u32: 8 pass tickets, status
