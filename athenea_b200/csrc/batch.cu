@@ -594,15 +594,16 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
         for (int k = 0; k < 48; ++k) dSh[k] = 0.0f;
         // each view's colour gradient loaded a view ahead, so its latency overlaps the work
+        // words 6..8 of a record (8-byte aligned: a record is 40 bytes): a pair and one
         const float* gr0 = grads + (size_t)i * kGradWords;
-        float next[3] = {gr0[kGradR], gr0[kGradG], gr0[kGradB]};
+        float2 nextRG = *reinterpret_cast<const float2*>(gr0 + kGradR);
+        float nextB = gr0[kGradB];
         for (uint32_t v = 0; v < B.views; ++v) {
-            const float gc[3] = {next[0], next[1], next[2]};
+            const float gc[3] = {nextRG.x, nextRG.y, nextB};
             if (v + 1 < B.views) {
                 const float* gr = grads + ((size_t)(v + 1) * B.count + i) * kGradWords;
-                next[0] = gr[kGradR];
-                next[1] = gr[kGradG];
-                next[2] = gr[kGradB];
+                nextRG = *reinterpret_cast<const float2*>(gr + kGradR);
+                nextB = gr[kGradB];
             }
             if (gc[0] == 0.0f && gc[1] == 0.0f && gc[2] == 0.0f) continue;
             colourAdjointFast(sh, g, degree, I.linear, views[v].eye, gc, dSh, dp);
@@ -619,21 +620,25 @@ __global__ void __launch_bounds__(128)
     acc.dQuat[0] = acc.dQuat[1] = acc.dQuat[2] = acc.dQuat[3] = 0.0f;
     float dMsum[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
     bool shaped = false;
-    float next[kGradWords];
+    // words 0..5 of a record (the moments and dL/dalpha) as three 8-byte pairs, a view ahead
+    float2 next[3];
 #pragma unroll
-    for (int k = 0; k < (int)kGradWords; ++k) next[k] = grads[(size_t)i * kGradWords + k];
+    for (int k = 0; k < 3; ++k) next[k] = reinterpret_cast<const float2*>(grads + (size_t)i * kGradWords)[k];
     for (uint32_t v = 0; v < B.views; ++v) {
         float gw[kGradWords];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            gw[2 * k] = next[k].x;
+            gw[2 * k + 1] = next[k].y;
+        }
+        gw[6] = gw[7] = gw[8] = gw[9] = 0.0f;
         bool any = false;
 #pragma unroll
-        for (int k = 0; k < (int)kGradWords; ++k) {
-            gw[k] = next[k];
-            any |= gw[k] != 0.0f;
-        }
+        for (int k = 0; k < 6; ++k) any |= gw[k] != 0.0f;
         if (v + 1 < B.views) {
-            const float* gr = grads + ((size_t)(v + 1) * B.count + i) * kGradWords;
+            const float2* gr = reinterpret_cast<const float2*>(grads + ((size_t)(v + 1) * B.count + i) * kGradWords);
 #pragma unroll
-            for (int k = 0; k < (int)kGradWords; ++k) next[k] = gr[k];
+            for (int k = 0; k < 3; ++k) next[k] = gr[k];
         }
         if (!any) continue;
         const BatchView& V = views[v];
