@@ -971,7 +971,7 @@ ath_status reserveBatch(ath_batch* b, uint32_t count) {
     if (err == cudaSuccess) err = b->projFlags.reserve((size_t)std::max(1u, gaussBlocks * V) * 8);
     if (err == cudaSuccess) err = b->ranges.reserve((size_t)std::max(1u, b->totalTiles) * 8);
     if (err == cudaSuccess) err = b->tileOrder.reserve((size_t)std::max(1u, b->totalTiles) * 4);
-    if (err == cudaSuccess) err = b->sortHist.reserve(8 * 256 * sizeof(uint32_t));
+    if (err == cudaSuccess) err = b->sortHist.reserve(sortHistWords() * sizeof(uint32_t));
     if (err == cudaSuccess) err = b->viewsDev.reserve(std::max<size_t>(1, b->views.size()) * sizeof(BatchView));
     if (err != cudaSuccess) return failCuda(err, "reserving the batch's scratch");
     b->count = count;
@@ -1022,7 +1022,17 @@ ath_status sizePairs(ath_batch* b, const ath_mixed_params& P, cudaStream_t strea
                                            "(packed keys asked for; the wide form has no such limit)");
         wide = false;
     } else {
-        wide = 24 + slot + b->tileBits > 64 && !renumbered();
+        // packed with the 24-bit depth key while it fits, unless the renumbered depth
+        // sorts in fewer passes (C1: 14 tile bits + 20 depth bits sort in four passes
+        // of 9, 9, 8, 8 bits; with the 24-bit key, 38 bits take five); else renumbered; else wide
+        const bool packedFits = 24 + slot + b->tileBits <= 64;
+        if (renumbered() && (!packedFits || sortPasses(depthBits + b->tileBits) < sortPasses(24 + b->tileBits))) {
+            wide = false;
+        } else {
+            wide = !packedFits;
+            depthBits = 24;
+            expBase = 0;
+        }
     }
     b->planned = true;
     b->planWide = wide;

@@ -427,7 +427,7 @@ ath_status reservePairs(ath_raster* r, uint32_t pairs, uint32_t bits) {   // res
         r->pairCapacity = n;
     }
     cudaError_t err = r->sortFlags.reserve(sortFlagWords(std::max(r->pairCapacity, pairs), std::max(bits, 8u)) * 8);
-    if (err == cudaSuccess) err = r->sortHist.reserve(8 * 256 * sizeof(uint32_t));
+    if (err == cudaSuccess) err = r->sortHist.reserve(sortHistWords() * sizeof(uint32_t));
     if (err != cudaSuccess) return failCuda(err, "reserving the sort's scratch");
     return ATH_OK;
 }
@@ -853,7 +853,7 @@ extern "C" ath_status ath_sorter_create(ath_sorter** out) {
     if (!s) return fail(ATH_E_OUT_OF_MEMORY, "ath_sorter_create: host allocation failed");
     cudaError_t err = cudaGetDevice(&s->device);
     if (err == cudaSuccess) err = sortPrepare();
-    if (err == cudaSuccess) err = s->hist.reserve(8 * 256 * sizeof(uint32_t));
+    if (err == cudaSuccess) err = s->hist.reserve(sortHistWords() * sizeof(uint32_t));
     if (err == cudaSuccess) err = s->words.reserve(16 * sizeof(uint32_t));
     if (err == cudaSuccess) err = s->wordsHost.reserve(16 * sizeof(uint32_t));
     if (err == cudaSuccess) err = cudaMemset(s->words.ptr, 0, 16 * sizeof(uint32_t));

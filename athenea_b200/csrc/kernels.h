@@ -33,7 +33,8 @@ cudaError_t launchRanges(uint32_t pairs, const uint32_t* pairsDevice, uint32_t t
 
 // sort.cu
 constexpr uint32_t kSortTileKeys = 8192;   // keys a onesweep block ranks (the look-back's unit)
-uint32_t sortPasses(uint32_t bits);
+uint32_t sortPasses(uint32_t bits);      // 8-bit passes, or 9-bit ones where that saves a pass
+uint32_t sortHistWords();                // the words of a sort's digit histograms (every pass)
 uint32_t sortTiles(uint32_t n);
 size_t sortFlagWords(uint32_t n, uint32_t bits);
 uint32_t sortResultIndex(uint32_t n, uint32_t bits);

@@ -1,5 +1,5 @@
 // Stage (c): a stable LSD radix sort of 64-bit keys with 32-bit values, eight
-// bits a pass, in the onesweep form (Adinets and Merrill, "Onesweep: A Faster
+// (or nine) bits a pass, in the onesweep form (Adinets and Merrill, "Onesweep: A Faster
 // Least Significant Digit Radix Sort for GPUs", 2022): one read of the keys
 // makes every pass's digit histogram, then each pass is a single kernel whose
 // tiles rank their keys in shared memory, find where each digit of theirs
@@ -18,19 +18,17 @@
 namespace ath {
 namespace {
 
-constexpr uint32_t kRadix = 256;
+constexpr uint32_t kRadix = 256;        // an 8-bit pass's digits
+constexpr uint32_t kMaxRadix = 512;     // a 9-bit pass's digits: the histograms' stride a pass
 constexpr uint32_t kSortThreads = 512;
 constexpr uint32_t kWarps = kSortThreads / 32;
 constexpr uint32_t kItems = 16;
 constexpr uint32_t kTileKeys = kSortThreads * kItems;   // 8192: fewer tiles for the look-back to walk
 static_assert(kTileKeys == kSortTileKeys, "kernels.h states the sort's tile size");
-// A warp ranks its items in kChains independent chains (items 0-7 and 8-15),
-// each with its own digit counters, so the two chains' shared-memory round
+// A warp ranks its items in independent chains (an 8-bit pass: items 0-7 and
+// 8-15), each with its own digit counters, so the chains' shared-memory round
 // trips overlap instead of queueing behind each other; the chains are ordered
 // after each other like warps.
-constexpr uint32_t kChains = 2;
-constexpr uint32_t kChainItems = kItems / kChains;
-constexpr uint32_t kCounters = kWarps * kChains;
 constexpr uint32_t kMaxPasses = 8;
 
 // `nDevice`, when given, holds the key count (a count only the device knows, as
@@ -39,19 +37,27 @@ __device__ __forceinline__ uint32_t countOf(uint32_t n, const uint32_t* nDevice)
     return nDevice ? min(n, *nDevice) : n;
 }
 
+// A sort's passes: their digit widths (8 or 9 bits) over bits [firstBit, firstBit + bits).
+struct SortPlan {
+    uint32_t passes;
+    uint32_t width[kMaxPasses];
+    uint32_t shift[kMaxPasses];   // from firstBit
+};
+
 __global__ void __launch_bounds__(256)
     histogramKernel(const uint64_t* __restrict__ keys, uint32_t n, const uint32_t* __restrict__ nDevice,
-                    uint32_t firstBit, uint32_t passes, uint32_t* __restrict__ hist) {
-    __shared__ uint32_t sHist[kMaxPasses * kRadix];
+                    uint32_t firstBit, const SortPlan plan, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t sHist[kMaxPasses * kMaxRadix];
     n = countOf(n, nDevice);
-    for (uint32_t j = threadIdx.x; j < passes * kRadix; j += blockDim.x) sHist[j] = 0;
+    for (uint32_t j = threadIdx.x; j < plan.passes * kMaxRadix; j += blockDim.x) sHist[j] = 0;
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint64_t key = keys[i] >> firstBit;
-        for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p * kRadix + (uint32_t)((key >> (8 * p)) & 0xFFu)], 1u);
+        for (uint32_t p = 0; p < plan.passes; ++p)
+            atomicAdd(&sHist[p * kMaxRadix + (uint32_t)((key >> plan.shift[p]) & ((1u << plan.width[p]) - 1u))], 1u);
     }
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < passes * kRadix; j += blockDim.x)
+    for (uint32_t j = threadIdx.x; j < plan.passes * kMaxRadix; j += blockDim.x)
         if (sHist[j]) atomicAdd(&hist[j], sHist[j]);
 }
 
@@ -73,13 +79,20 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* sWa
     return base + incl - v;
 }
 
-template <bool kValues>
+// kBits: the pass's digit width, 8 or 9 (kRadixT digits, one thread each in the
+// digit phase; a 9-bit pass ranks in one chain, so that its counters fit beside the keys).
+template <bool kValues, uint32_t kBits>
 __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     onesweepKernel(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
                    uint64_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, uint32_t n, uint32_t shift,
                    const uint32_t* __restrict__ globalHist, uint64_t* __restrict__ flags, uint32_t* __restrict__ ticket,
                    uint32_t* __restrict__ status, const uint32_t* __restrict__ nDevice,
                    const uint32_t* __restrict__ epochDevice) {
+    constexpr uint32_t kRadix = 1u << kBits;
+    constexpr uint32_t kDigitMask = kRadix - 1u;
+    constexpr uint32_t kChains = kBits == 8 ? 2 : 1;
+    constexpr uint32_t kChainItems = kItems / kChains;
+    constexpr uint32_t kCounters = kWarps * kChains;
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(sKeys + kTileKeys);
@@ -124,7 +137,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
         for (uint32_t c = 0; c < kChains; ++c) {
             const uint32_t k = c * kChainItems + i;
             valid[c] = base + warp * 32 * kItems + k * 32 + lane < n;
-            d[c] = valid[c] ? (uint32_t)((key[k] >> shift) & 0xFFu) : kRadix + lane;
+            d[c] = valid[c] ? (uint32_t)((key[k] >> shift) & kDigitMask) : kRadix + lane;
             peers[c] = __match_any_sync(0xFFFFFFFFu, d[c]);
         }
 #pragma unroll
@@ -196,7 +209,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     for (uint32_t k = 0; k < kItems; ++k) {
         const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
         if (idx < n) {
-            const uint32_t d = (uint32_t)((key[k] >> shift) & 0xFFu);
+            const uint32_t d = (uint32_t)((key[k] >> shift) & kDigitMask);
             const uint32_t s = sStart[d] + sWarpCnt[(warp * kChains + k / kChainItems) * kRadix + d] + rank[k];
             sKeys[s] = key[k];
             if constexpr (kValues) sVals[s] = val[k];
@@ -206,7 +219,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     const uint32_t tileN = min(kTileKeys, n - base);
     for (uint32_t s = tid; s < tileN; s += kSortThreads) {
         const uint64_t k = sKeys[s];
-        const uint32_t dst = sAdjust[(uint32_t)((k >> shift) & 0xFFu)] + s;
+        const uint32_t dst = sAdjust[(uint32_t)((k >> shift) & kDigitMask)] + s;
         if (dst < n) {
             keysOut[dst] = k;
             if constexpr (kValues) valsOut[dst] = sVals[s];
@@ -216,40 +229,72 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     }
 }
 
-constexpr size_t kOnesweepSmem = (size_t)kTileKeys * 8 + (size_t)kTileKeys * 4 + (size_t)kCounters * kRadix * 4;
-constexpr size_t kOnesweepKeysSmem = (size_t)kTileKeys * 8 + (size_t)kCounters * kRadix * 4;
+// A pass's dynamic shared memory: its keys (and values) and its chains' digit counters.
+constexpr size_t onesweepSmem(bool values, uint32_t bits) {
+    return (size_t)kTileKeys * 8 + (values ? (size_t)kTileKeys * 4 : 0) +
+           (size_t)kWarps * (bits == 8 ? 2 : 1) * ((size_t)1 << bits) * 4;
+}
+
+// The passes of a sort of `bits` bits: eight bits a pass, or, where that takes a
+// pass fewer, nine bits in as many passes as needed and eight in the rest
+// (34 bits: 9 + 9 + 8 + 8 in four passes, not five).
+SortPlan planSort(uint32_t bits) {
+    SortPlan p{};
+    const uint32_t eights = (bits + 7) / 8, nines = (bits + 8) / 9;
+    p.passes = nines < eights ? nines : eights;
+    const uint32_t wide = nines < eights ? (bits > 8 * p.passes ? bits - 8 * p.passes : 0) : 0;
+    uint32_t at = 0;
+    for (uint32_t k = 0; k < p.passes && k < kMaxPasses; ++k) {
+        p.width[k] = k < wide ? 9u : 8u;
+        p.shift[k] = at;
+        at += p.width[k];
+    }
+    return p;
+}
 
 }   // namespace
 
-uint32_t sortPasses(uint32_t bits) { return (bits + 7) / 8; }
+uint32_t sortPasses(uint32_t bits) { return planSort(bits).passes; }
 uint32_t sortTiles(uint32_t n) { return (n + kTileKeys - 1) / kTileKeys; }
-size_t sortFlagWords(uint32_t n, uint32_t bits) { return (size_t)sortTiles(n) * kRadix * sortPasses(bits); }
+size_t sortFlagWords(uint32_t n, uint32_t bits) {
+    const SortPlan p = planSort(bits);
+    size_t words = 0;
+    for (uint32_t k = 0; k < p.passes; ++k) words += (size_t)sortTiles(n) << p.width[k];
+    return words;
+}
 
 cudaError_t sortPrepare() {
-    cudaError_t err =
-        cudaFuncSetAttribute(onesweepKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOnesweepSmem);
+    cudaError_t err = cudaFuncSetAttribute(onesweepKernel<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)onesweepSmem(true, 8));
     if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(onesweepKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kOnesweepKeysSmem);
+        err = cudaFuncSetAttribute(onesweepKernel<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)onesweepSmem(false, 8));
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(onesweepKernel<true, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)onesweepSmem(true, 9));
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(onesweepKernel<false, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)onesweepSmem(false, 9));
     return err;
 }
 
 // keys/vals[0] hold the input; the sorted result lands in keys/vals[passes & 1]
 // (the caller reads sortResultIndex). vals may be null (keys only). The passes
-// sort bits [firstBit, firstBit + bits) of the keys, eight at a time. hist:
-// kMaxPasses*256 words, flags: sortFlagWords words, tickets: one word a pass;
-// all three are zeroed here.
+// sort bits [firstBit, firstBit + bits) of the keys, eight or nine at a time
+// (planSort). hist: kMaxPasses * kSortHistStride words, flags: sortFlagWords
+// words, tickets: one word a pass; all three are zeroed here.
 cudaError_t launchSortDevice(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, const uint32_t* nDevice,
                              const uint32_t* epochDevice, uint32_t firstBit, uint32_t bits, uint32_t* hist,
                              uint64_t* flags, uint32_t* tickets, uint32_t* status, cudaStream_t stream) {
     if (n <= 1 && !nDevice) return cudaSuccess;
-    const uint32_t passes = sortPasses(bits);
-    if (passes > kMaxPasses || firstBit + 8 * passes > 64 + 7) return cudaErrorInvalidValue;
+    const SortPlan plan = planSort(bits);
+    const uint32_t passes = plan.passes;
+    if (passes > kMaxPasses || firstBit + bits > 64) return cudaErrorInvalidValue;
     const uint32_t tiles = sortTiles(n);
-    cudaError_t err = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kRadix * passes, stream);
+    cudaError_t err = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kMaxRadix * passes, stream);
     if (err != cudaSuccess) return err;
     if (!epochDevice) {
-        err = cudaMemsetAsync(flags, 0, sizeof(uint64_t) * (size_t)tiles * kRadix * passes, stream);
+        err = cudaMemsetAsync(flags, 0, sizeof(uint64_t) * sortFlagWords(n, bits), stream);
         if (err != cudaSuccess) return err;
     }
     err = cudaMemsetAsync(tickets, 0, sizeof(uint32_t) * passes, stream);
@@ -258,18 +303,24 @@ cudaError_t launchSortDevice(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, c
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const uint32_t hblocks = min((n + 255) / 256, (uint32_t)sms * 4);
-    histogramKernel<<<hblocks, 256, 0, stream>>>(keys[0], n, nDevice, firstBit, passes, hist);
+    histogramKernel<<<hblocks, 256, 0, stream>>>(keys[0], n, nDevice, firstBit, plan, hist);
     const bool withValues = vals != nullptr && vals[0] != nullptr;
+    size_t flagAt = 0;
     for (uint32_t p = 0; p < passes; ++p) {
         const uint32_t in = p & 1u, out = in ^ 1u;
-        if (withValues)
-            onesweepKernel<true><<<tiles, kSortThreads, kOnesweepSmem, stream>>>(
-                keys[in], vals[in], keys[out], vals[out], n, firstBit + 8 * p, hist + p * kRadix,
-                flags + (size_t)p * tiles * kRadix, tickets + p, status, nDevice, epochDevice);
-        else
-            onesweepKernel<false><<<tiles, kSortThreads, kOnesweepKeysSmem, stream>>>(
-                keys[in], nullptr, keys[out], nullptr, n, firstBit + 8 * p, hist + p * kRadix,
-                flags + (size_t)p * tiles * kRadix, tickets + p, status, nDevice, epochDevice);
+        const uint32_t shift = firstBit + plan.shift[p];
+        const uint32_t* h = hist + p * kMaxRadix;
+        uint64_t* f = flags + flagAt;
+        flagAt += (size_t)tiles << plan.width[p];
+#define ATH_PASS(V_, W_)                                                                                          \
+    onesweepKernel<V_, W_><<<tiles, kSortThreads, onesweepSmem(V_, W_), stream>>>(                             \
+        keys[in], V_ ? vals[in] : nullptr, keys[out], V_ ? vals[out] : nullptr, n, shift, h, f, tickets + p, status, \
+        nDevice, epochDevice)
+        if (withValues && plan.width[p] == 9) ATH_PASS(true, 9);
+        else if (withValues) ATH_PASS(true, 8);
+        else if (plan.width[p] == 9) ATH_PASS(false, 9);
+        else ATH_PASS(false, 8);
+#undef ATH_PASS
     }
     return cudaGetLastError();
 }
@@ -285,5 +336,6 @@ cudaError_t launchSort(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, uint32_
 }
 
 uint32_t sortResultIndex(uint32_t n, uint32_t bits) { return n <= 1 ? 0u : (sortPasses(bits) & 1u); }
+uint32_t sortHistWords() { return kMaxPasses * kMaxRadix; }
 
 }   // namespace ath

@@ -11,7 +11,7 @@
 // with the library on every GPU that loads it, and allocates nothing.
 //
 // The limit follows from that array's size: at most kStaticMaxCount pairs a
-// call, 2 MiB of device memory a GPU for the library's lifetime. Every call
+// call, 3.5 MiB of device memory a GPU for the library's lifetime. Every call
 // shares the array and it keeps the last call's contents, so each call clears
 // what must start at zero (histograms, look-back words, tickets); calls that
 // overlap on the GPU (on different streams, or from different threads without
@@ -33,8 +33,10 @@ namespace {
 constexpr uint32_t kStaticMaxCount = 1u << 20;              // pairs a call
 constexpr uint32_t kStaticMaxPasses = 8;                    // 64-bit keys, 8 bits a pass
 constexpr size_t kStaticTiles = kStaticMaxCount / kSortTileKeys;   // the onesweep's tiles
-constexpr size_t kFlagWords = kStaticMaxPasses * kStaticTiles * 256;   // look-back words (u64)
-constexpr size_t kHistWords = kStaticMaxPasses * 256 / 2;               // 8 x 256 u32 histograms, as u64
+// look-back words (u64): a tile's words over every pass, at most 3584 (63 key bits
+// sort in seven 9-bit passes of 512 digits; 64 bits in eight 8-bit passes of 256)
+constexpr size_t kFlagWords = kStaticTiles * 7 * 512;
+constexpr size_t kHistWords = kStaticMaxPasses * 512 / 2;               // 8 x 512 u32 histograms, as u64
 constexpr size_t kCounterWords = 8;                                     // 16 u32: 8 pass tickets, status
 constexpr size_t kScratchWords = kFlagWords + kHistWords + kCounterWords;
 
@@ -94,6 +96,8 @@ extern "C" ath_status ath_sort_pairs_static(uint64_t* keys, uint32_t* values, ui
     uint32_t* hist = reinterpret_cast<uint32_t*>(scratch + kFlagWords);
     uint32_t* counters = reinterpret_cast<uint32_t*>(scratch + kFlagWords + kHistWords);
     uint32_t* status = counters + 8;
+    if (sortFlagWords(count, keyBits) > kFlagWords || sortHistWords() > 2 * kHistWords)
+        return fail(ATH_E_INTERNAL, "ath_sort_pairs_static: the static working memory is too small for this sort");
     // The status word is not read here: the call enqueues its work and returns.
     // What a call raises (a look-back that gave up, an index outside the buffers)
     // stays in the word until ath_sort_pairs_static_status reads and clears it.

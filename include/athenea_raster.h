@@ -532,7 +532,7 @@ ath_status ath_sorter_check(ath_sorter* s);
  * sort: a plugin whose host application owns the device memory and holds it to
  * a fixed budget mid-frame, or a real-time frame that cannot take the stall of
  * an allocation. It has no counterpart in the reference. The sort's own working
- * memory (histograms, look-back words, tickets, a status word) is a fixed 2 MiB
+ * memory (histograms, look-back words, tickets, a status word) is a fixed 3.5 MiB
  * array every GPU that loads the library holds until exit; nothing is
  * allocated. At most 1,048,576 pairs a call (larger counts return
  * ATH_E_INVALID_ARGUMENT). The first call on a device (or the first status

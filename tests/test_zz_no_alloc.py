@@ -38,9 +38,9 @@ def _sort(N, fn, keys, vals, key_bits, handle=None):
     return k.cpu().numpy().view(np.uint64), v.cpu().numpy().view(np.uint32)
 
 
-# (LIMIT, 64) fills the whole static array: 128 tiles x 8 passes of look-back words;
+# (LIMIT, 64) sorts in eight 8-bit passes, 63 bits in seven 9-bit passes (the most look-back words);
 # 48 bits is an even pass count (6) at the limit, whose result needs no copy back.
-@pytest.mark.parametrize("count,key_bits", [(65537, 40), (LIMIT, 37), (LIMIT, 64), (LIMIT, 48)])
+@pytest.mark.parametrize("count,key_bits", [(65537, 40), (LIMIT, 37), (LIMIT, 64), (LIMIT, 63), (LIMIT, 48)])
 def test_static_sort_equals_the_allocating_sort_twice_in_a_row(native, count, key_bits):
     N = native
     lib = N.lib()
