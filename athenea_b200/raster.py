@@ -682,10 +682,12 @@ class BatchTrainer:
                                      C.byref(g), repeats, C.byref(st), C.c_void_p(s.cuda_stream)))
         return dict(pairs=st.pairs, tile=st.tile, block_batch=st.block_batch, ms_per_step=st.ms_per_step)
 
-    def time_stages(self, params: MixedParams, target, colour, loss, grads: "Params",
+    def time_stages(self, params: MixedParams, target, colour, loss, grads: "Params | None",
                     stream: torch.cuda.Stream | None = None) -> dict:
-        """ath_batch_time_stages: one step, not captured, with events between its stages (ms)."""
-        g = N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
+        """ath_batch_time_stages: one step, not captured, with events between its stages (ms);
+        `grads` None when gradient buckets are set."""
+        g = N.ParamGrads(None, None, None, None) if grads is None else \
+            N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
         ms = (C.c_float * 5)()
         s = stream if stream is not None else torch.cuda.current_stream(colour.device)
         self._keep = (params, target, colour, loss, grads)
