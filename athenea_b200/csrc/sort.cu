@@ -85,11 +85,11 @@ template <bool kValues, uint32_t kBits>
 __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     onesweepKernel(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
                    uint64_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, uint32_t n, uint32_t shift,
-                   const uint32_t* __restrict__ globalHist, uint64_t* __restrict__ flags, uint32_t* __restrict__ ticket,
+                   uint32_t digitMask, const uint32_t* __restrict__ globalHist, uint64_t* __restrict__ flags,
+                   uint32_t* __restrict__ ticket,
                    uint32_t* __restrict__ status, const uint32_t* __restrict__ nDevice,
                    const uint32_t* __restrict__ epochDevice) {
     constexpr uint32_t kRadix = 1u << kBits;
-    constexpr uint32_t kDigitMask = kRadix - 1u;
     constexpr uint32_t kChains = kBits == 8 ? 2 : 1;
     constexpr uint32_t kChainItems = kItems / kChains;
     constexpr uint32_t kCounters = kWarps * kChains;
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
         for (uint32_t c = 0; c < kChains; ++c) {
             const uint32_t k = c * kChainItems + i;
             valid[c] = base + warp * 32 * kItems + k * 32 + lane < n;
-            d[c] = valid[c] ? (uint32_t)((key[k] >> shift) & kDigitMask) : kRadix + lane;
+            d[c] = valid[c] ? (uint32_t)((key[k] >> shift) & digitMask) : kRadix + lane;
             peers[c] = __match_any_sync(0xFFFFFFFFu, d[c]);
         }
 #pragma unroll
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     for (uint32_t k = 0; k < kItems; ++k) {
         const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
         if (idx < n) {
-            const uint32_t d = (uint32_t)((key[k] >> shift) & kDigitMask);
+            const uint32_t d = (uint32_t)((key[k] >> shift) & digitMask);
             const uint32_t s = sStart[d] + sWarpCnt[(warp * kChains + k / kChainItems) * kRadix + d] + rank[k];
             sKeys[s] = key[k];
             if constexpr (kValues) sVals[s] = val[k];
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     const uint32_t tileN = min(kTileKeys, n - base);
     for (uint32_t s = tid; s < tileN; s += kSortThreads) {
         const uint64_t k = sKeys[s];
-        const uint32_t dst = sAdjust[(uint32_t)((k >> shift) & kDigitMask)] + s;
+        const uint32_t dst = sAdjust[(uint32_t)((k >> shift) & digitMask)] + s;
         if (dst < n) {
             keysOut[dst] = k;
             if constexpr (kValues) valsOut[dst] = sVals[s];
@@ -310,12 +310,13 @@ cudaError_t launchSortDevice(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, c
         const uint32_t in = p & 1u, out = in ^ 1u;
         const uint32_t shift = firstBit + plan.shift[p];
         const uint32_t* h = hist + p * kMaxRadix;
+        const uint32_t digitMask = (1u << plan.width[p]) - 1u;
         uint64_t* f = flags + flagAt;
         flagAt += (size_t)tiles << plan.width[p];
 #define ATH_PASS(V_, W_)                                                                                          \
     onesweepKernel<V_, W_><<<tiles, kSortThreads, onesweepSmem(V_, W_), stream>>>(                             \
-        keys[in], V_ ? vals[in] : nullptr, keys[out], V_ ? vals[out] : nullptr, n, shift, h, f, tickets + p, status, \
-        nDevice, epochDevice)
+        keys[in], V_ ? vals[in] : nullptr, keys[out], V_ ? vals[out] : nullptr, n, shift, digitMask, h, f,         \
+        tickets + p, status, nDevice, epochDevice)
         if (withValues && plan.width[p] == 9) ATH_PASS(true, 9);
         else if (withValues) ATH_PASS(true, 8);
         else if (plan.width[p] == 9) ATH_PASS(false, 9);
