@@ -43,11 +43,11 @@ METRIC = "fwd+bwd ms/view, 1.5M Gaussians 1080p, batched+BF16 vs plain FP32, err
 
 # DRAM bytes a launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # batched kernels, from an ncu capture of this workload at 2 views (tile 32,
-# 512 records a batch), scaled by 4 to its 8 views: records and pairs grow
+# 128 records a batch), scaled by 4 to its 8 views: records and pairs grow
 # with the views.
 NCU_TRAFFIC: dict = {
-    "blendStepKernel": 4 * 161.94e6,
-    "projectEmitKernel": 4 * 489.20e6,
+    "blendStepKernel": 4 * 147.60e6,
+    "projectEmitKernel": 4 * 473.22e6,
 }
 
 
@@ -488,9 +488,10 @@ def main():
     ap.add_argument("--block-batch", type=int, choices=[64, 128, 256, 512], default=256,
                     help="records a block stages at once, with --tile")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
-    ap.add_argument("--workload", type=int, choices=[1, 3, 4], default=1,
-                    help="1: 1.5M clustered, 8 views of 1920x1080 (the headline); 3: 2.36M clustered, 64 views of "
-                         "mixed sizes; 4: 50M clustered, 8 views of 3840x2160")
+    ap.add_argument("--workload", type=int, choices=[0, 1, 2, 3, 4], default=1,
+                    help="0: 100k uniform, one 960x540 view; 1: 1.5M clustered, 8 views of 1920x1080 (the "
+                         "headline); 2: 500k clustered, one 1280x720 view; 3: 2.36M clustered, 64 views of mixed "
+                         "sizes; 4: 50M clustered, 8 views of 3840x2160")
     args = ap.parse_args()
     if args.workload != 1:
         from athenea_b200 import scenes

@@ -462,5 +462,6 @@ def test_gradient_buckets_give_the_same_gradients_and_signal_each_bucket():
             want = getattr(grads_one, name).cpu().numpy()
             np.testing.assert_allclose(getattr(got, name).cpu().numpy(), want, rtol=1e-4,
                                        atol=1e-5 * float(np.abs(want).max()), err_msg=name)
-        assert abs(loss.item() - loss_one.item()) <= 1e-6 * loss_one.item()
+        # the loss is a float atomic sum over blocks, in an order that varies from run to run
+        assert abs(loss.item() - loss_one.item()) <= 2e-5 * loss_one.item()
     b.set_buckets(None)
