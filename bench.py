@@ -428,9 +428,9 @@ def run_ours(args) -> dict | None:
     total_tiles = sum(((W + T - 1) // T) * ((H + T - 1) // T) for _, W, H in views)
     passes = sort_passes(buf["depth_bits"] + max(1, math.ceil(math.log2(max(2, total_tiles)))))
     # the step's kernels: begin, projectEmit, histogram, the sort's passes, ranges,
-    # the tile order, the blends (forward, loss and adjoint), projection adjoint
-    # (memsets are not counted)
-    launches = (2 + 1 + passes + 1 + 1 + 1 + 1) * args.steps
+    # the tile order, the blends (forward, loss and adjoint), and the projection
+    # adjoint once for each gradient bucket (memsets are not counted)
+    launches = (2 + 1 + passes + 1 + 1 + 1 + (BUCKETS if world > 1 else 1)) * args.steps
     arith = A.measure_peaks(5, stream=stream)   # the blends' denominators: FP32 FMA and ex2 rates, measured here
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
                arith=arith,
@@ -515,12 +515,13 @@ def main():
         line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms/view", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "clustered-1.5M-1920x1080", "gaussians": WORKLOAD["count"],
+                "config": {"workload": WORKLOAD["name"], "gaussians": WORKLOAD["count"],
                            "width": WORKLOAD["width"], "height": WORKLOAD["height"],
                            "path": "the CPU restatement of the reference's path (oracle/, OpenMP): forward, "
                                    "mean-L2 loss gradient, the reference's colour-gradient backward"},
                 "cpu_baseline": {"value": ms, "unit": "ms/view", "cores": runs[0]["cores"], "kind": "port",
-                                 "sample": "one 1920x1080 view of the 1.5M-Gaussian scene a step"},
+                                 "sample": f"one {WORKLOAD['width']}x{WORKLOAD['height']} view of the "
+                                           f"{WORKLOAD['count']}-Gaussian scene a step"},
                 "e2e": {"value": ms, "unit": "ms/view", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -608,8 +609,8 @@ def main():
     }
     if cpu:
         line["cpu_baseline"] = {"value": cpu["ms"], "unit": "ms/view", "cores": cpu["cores"], "kind": "port",
-                                "sample": "one 1920x1080 view of the same scene: forward, loss gradient and the "
-                                          "reference's colour-gradient backward"}
+                                "sample": f"one {WORKLOAD['width']}x{WORKLOAD['height']} view of the same scene: "
+                                          "forward, loss gradient and the reference's colour-gradient backward"}
     print(json.dumps(line))
 
 
