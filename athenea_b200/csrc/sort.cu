@@ -18,7 +18,6 @@
 namespace ath {
 namespace {
 
-constexpr uint32_t kRadix = 256;        // an 8-bit pass's digits
 constexpr uint32_t kMaxRadix = 512;     // a 9-bit pass's digits: the histograms' stride a pass
 constexpr uint32_t kSortThreads = 512;
 constexpr uint32_t kWarps = kSortThreads / 32;
@@ -36,6 +35,13 @@ constexpr uint32_t kMaxPasses = 8;
 __device__ __forceinline__ uint32_t countOf(uint32_t n, const uint32_t* nDevice) {
     return nDevice ? min(n, *nDevice) : n;
 }
+
+// Digit d's slot in a per-digit table in shared memory: d with its low five bits
+// XORed with the next five (a permutation within each run of 32). A warp's keys
+// often hold digits 32 or 64 apart and little else (a pass over an exponent byte's
+// few values beside a tile index's low bits); unswizzled, those all fall in one
+// bank and their counter reads serialise.
+__device__ __forceinline__ uint32_t digitSlot(uint32_t d) { return d ^ ((d >> 5) & 31u); }
 
 // A sort's passes: their digit widths (8 or 9 bits) over bits [firstBit, firstBit + bits).
 struct SortPlan {
@@ -69,13 +75,15 @@ __global__ void __launch_bounds__(256)
             for (uint32_t p = 0; p < kMaxPasses; ++p)
                 if (p < plan.passes) {
                     const uint32_t d = (uint32_t)((key[k] >> plan.shift[p]) & ((1u << plan.width[p]) - 1u));
-                    atomicAdd(&sHist[p * kMaxRadix + d], 1u);
+                    atomicAdd(&sHist[p * kMaxRadix + digitSlot(d)], 1u);
                 }
         }
     }
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < plan.passes * kMaxRadix; j += blockDim.x)
-        if (sHist[j]) atomicAdd(&hist[j], sHist[j]);
+    for (uint32_t j = threadIdx.x; j < plan.passes * kMaxRadix; j += blockDim.x) {
+        const uint32_t c = sHist[(j / kMaxRadix) * kMaxRadix + digitSlot(j % kMaxRadix)];
+        if (c) atomicAdd(&hist[j], c);
+    }
 }
 
 // Exclusive scan of one value a thread over the block (kSortThreads threads).
@@ -159,12 +167,12 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
         }
 #pragma unroll
         for (uint32_t c = 0; c < kChains; ++c)
-            before[c] = valid[c] ? sWarpCnt[(warp * kChains + c) * kRadix + d[c]] : 0u;
+            before[c] = valid[c] ? sWarpCnt[(warp * kChains + c) * kRadix + digitSlot(d[c])] : 0u;
         __syncwarp();
 #pragma unroll
         for (uint32_t c = 0; c < kChains; ++c)
             if (valid[c] && lane == (uint32_t)(__ffs(peers[c]) - 1))
-                sWarpCnt[(warp * kChains + c) * kRadix + d[c]] = before[c] + __popc(peers[c]);
+                sWarpCnt[(warp * kChains + c) * kRadix + digitSlot(d[c])] = before[c] + __popc(peers[c]);
         __syncwarp();
 #pragma unroll
         for (uint32_t c = 0; c < kChains; ++c) rank[c * kChainItems + i] = before[c] + __popc(peers[c] & ltMask);
@@ -179,8 +187,8 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     if (digit) {
 #pragma unroll
         for (uint32_t w = 0; w < kCounters; ++w) {
-            const uint32_t c = sWarpCnt[w * kRadix + t];
-            sWarpCnt[w * kRadix + t] = count;
+            const uint32_t c = sWarpCnt[w * kRadix + digitSlot(t)];
+            sWarpCnt[w * kRadix + digitSlot(t)] = count;
             count += c;
         }
     }
@@ -216,8 +224,8 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     }
     const uint32_t start = blockExclusiveScan(count, sScan);
     if (digit) {
-        sStart[t] = start;
-        sAdjust[t] = exclusive - start;
+        sStart[digitSlot(t)] = start;
+        sAdjust[digitSlot(t)] = exclusive - start;
     }
     __syncthreads();
 
@@ -227,7 +235,9 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
         const uint32_t idx = base + warp * 32 * kItems + k * 32 + lane;
         if (idx < n) {
             const uint32_t d = (uint32_t)((key[k] >> shift) & digitMask);
-            const uint32_t s = sStart[d] + sWarpCnt[(warp * kChains + k / kChainItems) * kRadix + d] + rank[k];
+            const uint32_t at = digitSlot(d);
+            const uint32_t s =
+                sStart[at] + sWarpCnt[(warp * kChains + k / kChainItems) * kRadix + at] + rank[k];
             sKeys[s] = key[k];
             if constexpr (kValues) sVals[s] = val[k];
         }
@@ -236,7 +246,7 @@ __global__ void __launch_bounds__(kSortThreads, kValues ? 1 : 2)
     const uint32_t tileN = min(kTileKeys, n - base);
     for (uint32_t s = tid; s < tileN; s += kSortThreads) {
         const uint64_t k = sKeys[s];
-        const uint32_t dst = sAdjust[(uint32_t)((k >> shift) & digitMask)] + s;
+        const uint32_t dst = sAdjust[digitSlot((uint32_t)((k >> shift) & digitMask))] + s;
         if (dst < n) {
             keysOut[dst] = k;
             if constexpr (kValues) valsOut[dst] = sVals[s];
