@@ -568,6 +568,84 @@ __global__ void __launch_bounds__(256)
 }
 
 
+// ---- Gaussians grouped by the views whose records took a gradient ----------------
+// The projection's adjoint runs a Gaussian a thread over every view and skips a view
+// whose record got no gradient (on C1 most records lie behind the pixels' early stop
+// and get none); a warp of Gaussians with different such views runs each view's work
+// for a few lanes. The forward blend sets `seen[v count + i]` for every record (v, i)
+// some pixel blends (the records the blend adjoint gives a gradient); ordering the Gaussians [first, end) by the word of those
+// views (bit v mod 32, folded to 8 bits: exactly the views for up to 8) lets whole
+// warps skip a view. Within a group the Gaussians keep their order inside each block of 256; the
+// blocks' runs follow in the order the blocks reserve them. The adjoint's results do
+// not depend on the order (each Gaussian's gradient is its own thread's).
+__device__ __forceinline__ uint32_t seenGroup(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count,
+                                              uint32_t i) {
+    uint32_t m = 0;
+    for (uint32_t v = 0; v < views; ++v) m |= (uint32_t)(seen[(size_t)v * count + i] != 0u) << (v & 31u);
+    m ^= m >> 16;
+    m ^= m >> 8;
+    return m & 255u;
+}
+
+__global__ void __launch_bounds__(256)
+    groupCountKernel(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count, uint32_t first, uint32_t end,
+                     uint32_t* __restrict__ counts) {
+    __shared__ uint32_t sCount[256];
+    sCount[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t i = first + blockIdx.x * 256 + threadIdx.x;
+    if (i < end) atomicAdd(&sCount[seenGroup(seen, views, count, i)], 1u);
+    __syncthreads();
+    if (sCount[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sCount[threadIdx.x]);
+}
+
+// order[first + k], k < end - first: the Gaussians of [first, end), group by group.
+__global__ void __launch_bounds__(256)
+    groupPlaceKernel(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count, uint32_t first, uint32_t end,
+                     const uint32_t* __restrict__ counts, uint32_t* __restrict__ cursors, uint32_t* __restrict__ order) {
+    __shared__ uint32_t sWarpCount[8][256];   // a warp's Gaussians of each group, then their offsets
+    __shared__ uint32_t sStart[256], sBase[256], sWarp[8];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    for (uint32_t w = 0; w < 8; ++w) sWarpCount[w][tid] = 0;
+    // where each group starts: the exclusive scan of the groups' sizes
+    const uint32_t c = counts[tid];
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += u;
+    }
+    if (lane == 31) sWarp[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < 8; ++w) before += w < warp ? sWarp[w] : 0u;
+    sStart[tid] = before + incl - c;
+    // a Gaussian's rank among the block's Gaussians of its group, in index order
+    const uint32_t i = first + blockIdx.x * 256 + tid;
+    const bool valid = i < end;
+    const uint32_t h = valid ? seenGroup(seen, views, count, i) : 256u + lane;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, h);
+    const uint32_t inWarp = __popc(peers & ((1u << lane) - 1u));
+    if (valid && inWarp == 0) sWarpCount[warp][h] = __popc(peers);
+    __syncthreads();
+    {
+        // group tid: its warps' counts to offsets, the block's total reserved at once
+        uint32_t sum = 0;
+        for (uint32_t w = 0; w < 8; ++w) {
+            const uint32_t k = sWarpCount[w][tid];
+            sWarpCount[w][tid] = sum;
+            sum += k;
+        }
+        if (sum) sBase[tid] = atomicAdd(&cursors[tid], sum);
+    }
+    __syncthreads();
+    if (valid) {
+        const uint32_t at = sStart[h] + sBase[h] + sWarpCount[warp][h] + inWarp;
+        if (at < end - first) order[first + at] = i;
+    }
+}
+
 // ---- the projection's adjoint over every view: one thread a Gaussian ---------
 // Two passes over the views, so that what is live across them stays small: the
 // colour's adjoint (the SH gradient, 48 values, and the position's share through
@@ -576,13 +654,18 @@ __global__ void __launch_bounds__(256)
 // scales and the rotation once). The cloud's loads and the SH (packed in
 // registers) are read once.
 // Gaussians [first, end) a launch (a gradient bucket, or the whole cloud), whose
-// gradients go to g*[i - first].
+// gradients go to g*[i - first]; thread k takes Gaussian order[first + k]
+// (groupPlaceKernel's order).
 __global__ void __launch_bounds__(128)
     projectAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float* __restrict__ grads,
                               float4* __restrict__ gMeans, float4* __restrict__ gScales, float4* __restrict__ gQuats,
-                              float* __restrict__ gSh, uint32_t shStride, uint32_t first, uint32_t end) {
-    const uint32_t i = first + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= min(end, B.count)) return;
+                              float* __restrict__ gSh, uint32_t shStride, uint32_t first, uint32_t end,
+                              const uint32_t* __restrict__ order) {
+    const uint32_t limit = min(end, B.count);
+    const uint32_t slot = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= limit) return;
+    const uint32_t i = order ? order[slot] : slot;   // a permutation of [first, end), grouped
+    if (i < first || i >= limit) return;
     const uint32_t o = i - first;   // the row in this launch's gradient arrays
     InstanceConst I = B.inst;
     const Gauss g = loadGauss<kLayoutMixed>(I, i);
@@ -715,6 +798,7 @@ struct ath_batch {
     uint32_t lastSorted = 0, lastSlotBits = 0;
     // scratch
     DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges, tileOrder, live;
+    DeviceBuffer seen, adjointOrder, groupWords;   // the projection adjoint's grouping of Gaussians
     uint32_t keyMode = 0;      // 0 automatic; 1 packed; 2 wide; 3 packed, depth exponent renumbered
     bool lastWide = false;
     // the pairs' form, planned by each sizing from its depths' exponents
@@ -863,6 +947,7 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
     L.words = static_cast<uint32_t*>(b->words.ptr);
     L.order = static_cast<const uint32_t*>(b->tileOrder.ptr);
     L.live = static_cast<uint32_t*>(b->live.ptr);
+    L.seen = static_cast<uint8_t*>(b->seen.ptr);
     L.sms = b->sms;
     L.tile = b->tile;
     L.blockBatch = b->blockBatch;
@@ -926,6 +1011,8 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     mark(3);
     const bool train = target != nullptr;
     if (err == cudaSuccess && train) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
+    if (err == cudaSuccess && train && P.count)
+        err = cudaMemsetAsync(b->seen.ptr, 0, (size_t)B.views * P.count, stream);
     // the forward blend, the loss and the blend adjoint (the record gradients were cleared by the projection)
     if (err == cudaSuccess)
         err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr), depth,
@@ -939,12 +1026,25 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
             uint32_t first = 0, n = P.count;
             if (!b->bucketGrads.empty()) ath_gradient_bucket(P.count, buckets, k, &first, &n);
             const ath_param_grads& gk = b->bucketGrads.empty() ? g : b->bucketGrads[k];
-            if (n)
-                projectAdjointBatchKernel<<<(n + 127) / 128, 128, 0, stream>>>(
-                    B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
-                    reinterpret_cast<float4*>(gk.means), reinterpret_cast<float4*>(gk.scales),
-                    reinterpret_cast<float4*>(gk.quats), gk.sh, 48, first, first + n);
-            err = cudaGetLastError();
+            if (n) {
+                // the bucket's Gaussians grouped by the views that gave them a gradient, then
+                // the adjoint in that order
+                const uint8_t* seen = static_cast<const uint8_t*>(b->seen.ptr);
+                uint32_t* counts = static_cast<uint32_t*>(b->groupWords.ptr);
+                uint32_t* order = static_cast<uint32_t*>(b->adjointOrder.ptr);
+                const uint32_t blocks = (n + 255) / 256;
+                err = cudaMemsetAsync(counts, 0, 2 * 256 * 4, stream);
+                if (err == cudaSuccess) {
+                    groupCountKernel<<<blocks, 256, 0, stream>>>(seen, B.views, P.count, first, first + n, counts);
+                    groupPlaceKernel<<<blocks, 256, 0, stream>>>(seen, B.views, P.count, first, first + n, counts,
+                                                                 counts + 256, order);
+                    projectAdjointBatchKernel<<<(n + 127) / 128, 128, 0, stream>>>(
+                        B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
+                        reinterpret_cast<float4*>(gk.means), reinterpret_cast<float4*>(gk.scales),
+                        reinterpret_cast<float4*>(gk.quats), gk.sh, 48, first, first + n, order);
+                    err = cudaGetLastError();
+                }
+            }
             if (err == cudaSuccess && !b->bucketEvents.empty() && b->bucketEvents[k]) {
                 // in a captured step, an event record node of the graph (an external
                 // event: a stream outside the graph may wait on it after each replay)
@@ -973,6 +1073,9 @@ ath_status reserveBatch(ath_batch* b, uint32_t count) {
     if (err == cudaSuccess) err = b->tileOrder.reserve((size_t)std::max(1u, b->totalTiles) * 4);
     if (err == cudaSuccess) err = b->sortHist.reserve(sortHistWords() * sizeof(uint32_t));
     if (err == cudaSuccess) err = b->viewsDev.reserve(std::max<size_t>(1, b->views.size()) * sizeof(BatchView));
+    if (err == cudaSuccess) err = b->seen.reserve(std::max<size_t>(1, (size_t)V * count));
+    if (err == cudaSuccess) err = b->adjointOrder.reserve((size_t)std::max(1u, count) * 4);
+    if (err == cudaSuccess) err = b->groupWords.reserve(2 * 256 * 4);
     if (err != cudaSuccess) return failCuda(err, "reserving the batch's scratch");
     b->count = count;
     return ATH_OK;

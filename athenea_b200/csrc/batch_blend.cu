@@ -131,7 +131,8 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
                     const float4* __restrict__ recs, float4* __restrict__ colour, const float* __restrict__ target,
                     float* __restrict__ loss, float* __restrict__ grads, float* __restrict__ depth,
-                    uint32_t* __restrict__ words, const uint32_t* __restrict__ order, uint32_t* __restrict__ live) {
+                    uint32_t* __restrict__ words, const uint32_t* __restrict__ order, uint32_t* __restrict__ live,
+                    uint8_t* __restrict__ seen) {
     constexpr uint32_t kThreads = S * S / 2;
     constexpr uint32_t kAcross = S / kBox;            // boxes across a block's span
     constexpr uint32_t kSpans = (T / S) * (T / S);    // spans (blocks' work units) a tile
@@ -251,10 +252,15 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
                     if constexpr (kTrain)
                         if (__any_sync(0xFFFFFFFFu, hit)) liveWord |= 1u << (j - base);
                 }
-                if constexpr (kTrain)
+                if constexpr (kTrain) {
                     if (lane == 0)
                         live[((size_t)(range.x >> 5) + tile + ((first - range.x + base) >> 5)) * kBoxes +
                              span * (kAcross * kAcross) + warp] = liveWord;
+                    // the records some pixel blended take a gradient in the adjoint: mark them
+                    // (lane l for record base + l; a plain store, every writer stores 1), by which
+                    // the projection's adjoint groups Gaussians
+                    if ((liveWord >> lane) & 1u) seen[recBase + sRec[base + lane]] = 1u;
+                }
                 if (__all_sync(0xFFFFFFFFu, done[0] && done[1])) break;
             }
         }
@@ -436,17 +442,17 @@ cudaError_t stepWith(const BatchConst& B, const BlendLaunch& L, cudaStream_t str
         const int grid = residentGrid(blendStepKernel<T, S, NB, true, true>, S * S / 2, L.sms);
         blendStepKernel<T, S, NB, true, true><<<grid, S * S / 2, 0, stream>>>(
             B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order,
-            L.live);
+            L.live, L.seen);
     } else if (target) {
         const int grid = residentGrid(blendStepKernel<T, S, NB, true, false>, S * S / 2, L.sms);
         blendStepKernel<T, S, NB, true, false><<<grid, S * S / 2, 0, stream>>>(
             B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, target, loss, grads, nullptr, L.words, L.order,
-            L.live);
+            L.live, L.seen);
     } else {
         const int grid = residentGrid(blendStepKernel<T, S, NB, false, false>, S * S / 2, L.sms);
         blendStepKernel<T, S, NB, false, false><<<grid, S * S / 2, 0, stream>>>(
             B, L.views, L.ranges, L.pairs, L.values, L.recs, colour, nullptr, nullptr, nullptr, depth, L.words,
-            L.order, nullptr);
+            L.order, nullptr, nullptr);
     }
     return cudaGetLastError();
 }

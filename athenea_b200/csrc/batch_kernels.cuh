@@ -151,6 +151,7 @@ struct BlendLaunch {
     uint32_t* words;
     const uint32_t* order;   // the tiles, heaviest first
     uint32_t* live;          // a training step's live bits: per tile, one word a 32-record chunk and box
+    uint8_t* seen;           // a training step's: per record (view, Gaussian), 1 once some pixel blended it
     int sms;
     uint32_t tile, blockBatch;
     bool count;              // count the walks' work into `words` (a step timed stage by stage)

@@ -428,9 +428,9 @@ def run_ours(args) -> dict | None:
     total_tiles = sum(((W + T - 1) // T) * ((H + T - 1) // T) for _, W, H in views)
     passes = sort_passes(buf["depth_bits"] + max(1, math.ceil(math.log2(max(2, total_tiles)))))
     # the step's kernels: begin, projectEmit, histogram, the sort's passes, ranges,
-    # the tile order, the blends (forward, loss and adjoint), and the projection
-    # adjoint once for each gradient bucket (memsets are not counted)
-    launches = (2 + 1 + passes + 1 + 1 + 1 + (BUCKETS if world > 1 else 1)) * args.steps
+    # the tile order, the blends (forward, loss and adjoint), and for each gradient
+    # bucket the two grouping kernels and the projection adjoint (memsets are not counted)
+    launches = (2 + 1 + passes + 1 + 1 + 1 + 3 * (BUCKETS if world > 1 else 1)) * args.steps
     arith = A.measure_peaks(5, stream=stream)   # the blends' denominators: FP32 FMA and ex2 rates, measured here
     out = dict(ms_batched=ms_batched, ms_plain=ms_plain, e2e_ms=e2e_ms, stages=stages, plain_stages=plain_stages,
                arith=arith,
