@@ -578,10 +578,14 @@ __global__ void __launch_bounds__(256)
 // warps skip a view. Within a group the Gaussians keep their order inside each block of 256; the
 // blocks' runs follow in the order the blocks reserve them. The adjoint's results do
 // not depend on the order (each Gaussian's gradient is its own thread's).
-__device__ __forceinline__ uint32_t seenGroup(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count,
+// Gaussian i's views whose record some pixel blended: bit v mod 32.
+__device__ __forceinline__ uint32_t seenViews(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count,
                                               uint32_t i) {
     uint32_t m = 0;
     for (uint32_t v = 0; v < views; ++v) m |= (uint32_t)(seen[(size_t)v * count + i] != 0u) << (v & 31u);
+    return m;
+}
+__device__ __forceinline__ uint32_t groupOf(uint32_t m) {
     m ^= m >> 16;
     m ^= m >> 8;
     return m & 255u;
@@ -594,15 +598,18 @@ __global__ void __launch_bounds__(256)
     sCount[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t i = first + blockIdx.x * 256 + threadIdx.x;
-    if (i < end) atomicAdd(&sCount[seenGroup(seen, views, count, i)], 1u);
+    if (i < end) atomicAdd(&sCount[groupOf(seenViews(seen, views, count, i))], 1u);
     __syncthreads();
     if (sCount[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sCount[threadIdx.x]);
 }
 
-// order[first + k], k < end - first: the Gaussians of [first, end), group by group.
+// order[first + k], k < end - first: the Gaussians of [first, end), group by group;
+// viewsOf[first + k]: that Gaussian's seenViews word (the views the adjoint visits
+// when there are at most 32).
 __global__ void __launch_bounds__(256)
     groupPlaceKernel(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count, uint32_t first, uint32_t end,
-                     const uint32_t* __restrict__ counts, uint32_t* __restrict__ cursors, uint32_t* __restrict__ order) {
+                     const uint32_t* __restrict__ counts, uint32_t* __restrict__ cursors, uint32_t* __restrict__ order,
+                     uint32_t* __restrict__ viewsOf) {
     __shared__ uint32_t sWarpCount[8][256];   // a warp's Gaussians of each group, then their offsets
     __shared__ uint32_t sStart[256], sBase[256], sWarp[8];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -624,7 +631,8 @@ __global__ void __launch_bounds__(256)
     // a Gaussian's rank among the block's Gaussians of its group, in index order
     const uint32_t i = first + blockIdx.x * 256 + tid;
     const bool valid = i < end;
-    const uint32_t h = valid ? seenGroup(seen, views, count, i) : 256u + lane;
+    const uint32_t m = valid ? seenViews(seen, views, count, i) : 0u;
+    const uint32_t h = valid ? groupOf(m) : 256u + lane;
     const uint32_t peers = __match_any_sync(0xFFFFFFFFu, h);
     const uint32_t inWarp = __popc(peers & ((1u << lane) - 1u));
     if (valid && inWarp == 0) sWarpCount[warp][h] = __popc(peers);
@@ -642,7 +650,10 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     if (valid) {
         const uint32_t at = sStart[h] + sBase[h] + sWarpCount[warp][h] + inWarp;
-        if (at < end - first) order[first + at] = i;
+        if (at < end - first) {
+            order[first + at] = i;
+            viewsOf[first + at] = m;
+        }
     }
 }
 
@@ -660,13 +671,23 @@ __global__ void __launch_bounds__(128)
     projectAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float* __restrict__ grads,
                               float4* __restrict__ gMeans, float4* __restrict__ gScales, float4* __restrict__ gQuats,
                               float* __restrict__ gSh, uint32_t shStride, uint32_t first, uint32_t end,
-                              const uint32_t* __restrict__ order) {
+                              const uint32_t* __restrict__ order, const uint32_t* __restrict__ viewsOf) {
     const uint32_t limit = min(end, B.count);
     const uint32_t slot = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= limit) return;
     const uint32_t i = order ? order[slot] : slot;   // a permutation of [first, end), grouped
     if (i < first || i >= limit) return;
     const uint32_t o = i - first;   // the row in this launch's gradient arrays
+    // the views whose record of this Gaussian took a gradient (up to 32 views; past 32,
+    // every view, the zero records skipped by their value): the other views' records
+    // are not even read
+    const bool masked = order && B.views <= 32;
+    const uint32_t seenMask = masked ? viewsOf[slot] : 0u;
+    auto nextView = [&](uint32_t from) -> uint32_t {   // the first such view >= from, or B.views
+        if (!masked) return from;
+        const uint32_t m = from < 32u ? seenMask >> from : 0u;
+        return m ? from + (uint32_t)__ffs(m) - 1u : B.views;
+    };
     InstanceConst I = B.inst;
     const Gauss g = loadGauss<kLayoutMixed>(I, i);
     const uint32_t degree = min(degreeOf(I.restPerColour), B.shLimit);
@@ -678,18 +699,25 @@ __global__ void __launch_bounds__(128)
         for (int k = 0; k < 48; ++k) dSh[k] = 0.0f;
         // each view's colour gradient loaded a view ahead, so its latency overlaps the work
         // words 6..8 of a record (8-byte aligned: a record is 40 bytes): a pair and one
-        const float* gr0 = grads + (size_t)i * kGradWords;
-        float2 nextRG = *reinterpret_cast<const float2*>(gr0 + kGradR);
-        float nextB = gr0[kGradB];
-        for (uint32_t v = 0; v < B.views; ++v) {
+        float2 nextRG = make_float2(0.0f, 0.0f);
+        float nextB = 0.0f;
+        uint32_t v = nextView(0);
+        if (v < B.views) {
+            const float* gr = grads + ((size_t)v * B.count + i) * kGradWords;
+            nextRG = *reinterpret_cast<const float2*>(gr + kGradR);
+            nextB = gr[kGradB];
+        }
+        while (v < B.views) {
             const float gc[3] = {nextRG.x, nextRG.y, nextB};
-            if (v + 1 < B.views) {
-                const float* gr = grads + ((size_t)(v + 1) * B.count + i) * kGradWords;
+            const uint32_t vn = nextView(v + 1);
+            if (vn < B.views) {
+                const float* gr = grads + ((size_t)vn * B.count + i) * kGradWords;
                 nextRG = *reinterpret_cast<const float2*>(gr + kGradR);
                 nextB = gr[kGradB];
             }
-            if (gc[0] == 0.0f && gc[1] == 0.0f && gc[2] == 0.0f) continue;
-            colourAdjointFast(sh, g, degree, I.linear, views[v].eye, gc, dSh, dp);
+            if (!(gc[0] == 0.0f && gc[1] == 0.0f && gc[2] == 0.0f))
+                colourAdjointFast(sh, g, degree, I.linear, views[v].eye, gc, dSh, dp);
+            v = vn;
         }
         float* row = gSh + (size_t)o * shStride;
 #pragma unroll
@@ -704,10 +732,14 @@ __global__ void __launch_bounds__(128)
     float dMsum[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
     bool shaped = false;
     // words 0..5 of a record (the moments and dL/dalpha) as three 8-byte pairs, a view ahead
-    float2 next[3];
+    float2 next[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+    uint32_t view = nextView(0);
+    if (view < B.views) {
+        const float2* gr = reinterpret_cast<const float2*>(grads + ((size_t)view * B.count + i) * kGradWords);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) next[k] = reinterpret_cast<const float2*>(grads + (size_t)i * kGradWords)[k];
-    for (uint32_t v = 0; v < B.views; ++v) {
+        for (int k = 0; k < 3; ++k) next[k] = gr[k];
+    }
+    for (uint32_t v = view, vn; v < B.views; v = vn) {
         float gw[kGradWords];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -718,8 +750,9 @@ __global__ void __launch_bounds__(128)
         bool any = false;
 #pragma unroll
         for (int k = 0; k < 6; ++k) any |= gw[k] != 0.0f;
-        if (v + 1 < B.views) {
-            const float2* gr = reinterpret_cast<const float2*>(grads + ((size_t)(v + 1) * B.count + i) * kGradWords);
+        vn = nextView(v + 1);
+        if (vn < B.views) {
+            const float2* gr = reinterpret_cast<const float2*>(grads + ((size_t)vn * B.count + i) * kGradWords);
 #pragma unroll
             for (int k = 0; k < 3; ++k) next[k] = gr[k];
         }
@@ -798,7 +831,7 @@ struct ath_batch {
     uint32_t lastSorted = 0, lastSlotBits = 0;
     // scratch
     DeviceBuffer words, recs, grads, projFlags, pairs[2], values[2], sortHist, sortFlags, ranges, tileOrder, live;
-    DeviceBuffer seen, adjointOrder, groupWords;   // the projection adjoint's grouping of Gaussians
+    DeviceBuffer seen, adjointOrder, adjointViews, groupWords;   // the projection adjoint's grouping
     uint32_t keyMode = 0;      // 0 automatic; 1 packed; 2 wide; 3 packed, depth exponent renumbered
     bool lastWide = false;
     // the pairs' form, planned by each sizing from its depths' exponents
@@ -1032,16 +1065,17 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
                 const uint8_t* seen = static_cast<const uint8_t*>(b->seen.ptr);
                 uint32_t* counts = static_cast<uint32_t*>(b->groupWords.ptr);
                 uint32_t* order = static_cast<uint32_t*>(b->adjointOrder.ptr);
+                uint32_t* viewsOf = static_cast<uint32_t*>(b->adjointViews.ptr);
                 const uint32_t blocks = (n + 255) / 256;
                 err = cudaMemsetAsync(counts, 0, 2 * 256 * 4, stream);
                 if (err == cudaSuccess) {
                     groupCountKernel<<<blocks, 256, 0, stream>>>(seen, B.views, P.count, first, first + n, counts);
                     groupPlaceKernel<<<blocks, 256, 0, stream>>>(seen, B.views, P.count, first, first + n, counts,
-                                                                 counts + 256, order);
+                                                                 counts + 256, order, viewsOf);
                     projectAdjointBatchKernel<<<(n + 127) / 128, 128, 0, stream>>>(
                         B, static_cast<const BatchView*>(b->viewsDev.ptr), static_cast<const float*>(b->grads.ptr),
                         reinterpret_cast<float4*>(gk.means), reinterpret_cast<float4*>(gk.scales),
-                        reinterpret_cast<float4*>(gk.quats), gk.sh, 48, first, first + n, order);
+                        reinterpret_cast<float4*>(gk.quats), gk.sh, 48, first, first + n, order, viewsOf);
                     err = cudaGetLastError();
                 }
             }
@@ -1075,6 +1109,7 @@ ath_status reserveBatch(ath_batch* b, uint32_t count) {
     if (err == cudaSuccess) err = b->viewsDev.reserve(std::max<size_t>(1, b->views.size()) * sizeof(BatchView));
     if (err == cudaSuccess) err = b->seen.reserve(std::max<size_t>(1, (size_t)V * count));
     if (err == cudaSuccess) err = b->adjointOrder.reserve((size_t)std::max(1u, count) * 4);
+    if (err == cudaSuccess) err = b->adjointViews.reserve((size_t)std::max(1u, count) * 4);
     if (err == cudaSuccess) err = b->groupWords.reserve(2 * 256 * 4);
     if (err != cudaSuccess) return failCuda(err, "reserving the batch's scratch");
     b->count = count;
