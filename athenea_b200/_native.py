@@ -161,6 +161,8 @@ SIGNATURES = {
     "ath_batch_set_tuning": (C.c_int32, [_P, C.c_uint32, C.c_uint32]),
     "ath_batch_pixels": (C.c_int32, [_P, C.POINTER(C.c_uint32)]),
     "ath_batch_train_step": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, C.POINTER(ParamGrads), _P]),
+    "ath_batch_train_step_after": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P, _P, C.POINTER(ParamGrads),
+                                               _P]),
     "ath_batch_render": (C.c_int32, [_P, C.POINTER(MixedParams), _P, _P, _P]),
     "ath_batch_check": (C.c_int32, [_P, C.POINTER(BatchStats), _P]),
     "ath_batch_buffers_of": (C.c_int32, [_P, C.POINTER(BatchBuffers), _P]),

@@ -846,7 +846,7 @@ struct ath_batch {
     static constexpr int kGraphs = 4;
     cudaStream_t captureStream = nullptr;
     cudaGraphExec_t exec[kGraphs] = {};
-    uintptr_t graphKey[kGraphs][13] = {};
+    uintptr_t graphKey[kGraphs][14] = {};
     int nextGraph = 0;   // the slot the next capture replaces
     // the gradient buckets (ath_batch_set_buckets): each bucket's arrays, and the event
     // the step records after its projection adjoint; empty: the whole cloud into `grads`
@@ -992,7 +992,7 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
 // A null `target`: a render, the forward blend alone (no loss, no backward).
 cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* target, float4* colour, float* loss,
                         ath_param_grads& g, cudaStream_t stream, bool countOnly, cudaEvent_t* marks = nullptr,
-                        float* depth = nullptr) {
+                        float* depth = nullptr, cudaEvent_t targetReady = nullptr) {
     auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], stream); };
     mark(0);
     BatchConst B = batchConst(b, P);
@@ -1043,6 +1043,14 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     }
     mark(3);
     const bool train = target != nullptr;
+    if (err == cudaSuccess && targetReady) {
+        // the target's upload overlapped the stages before: only the blends read it
+        cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+        err = cudaStreamIsCapturing(stream, &capturing);
+        if (err == cudaSuccess)
+            err = cudaStreamWaitEvent(stream, targetReady,
+                                      capturing == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0);
+    }
     if (err == cudaSuccess && train) err = cudaMemsetAsync(loss, 0, sizeof(float), stream);
     if (err == cudaSuccess && train && P.count)
         err = cudaMemsetAsync(b->seen.ptr, 0, (size_t)B.views * P.count, stream);
@@ -1310,7 +1318,8 @@ namespace {
 // A training step (target, loss and gradients given) or a render (all three
 // null), checked, its buffers sized, captured once for its arrays and replayed.
 ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour, float* loss,
-                   ath_param_grads* grads, float* depth, void* streamPtr, const char* what) {
+                   ath_param_grads* grads, float* depth, void* streamPtr, const char* what,
+                   cudaEvent_t targetReady = nullptr) {
     if (b->views.empty()) return fail(ATH_E_INVALID_ARGUMENT, std::string(what) + ": no views (ath_batch_set_views)");
     const ath_mixed_params& P = *params;
     if (P.count && (!P.means || !P.scales || !P.quats || !P.sh_low || !P.sh_high || !P.sh_scale))
@@ -1346,10 +1355,11 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
         if ((st = sizePairs(b, P, stream)) != ATH_OK) return st;
         dropGraph(b);
     }
-    const uintptr_t key[13] = {(uintptr_t)P.means, (uintptr_t)P.scales, (uintptr_t)P.quats, (uintptr_t)P.sh_low,
+    const uintptr_t key[14] = {(uintptr_t)P.means, (uintptr_t)P.scales, (uintptr_t)P.quats, (uintptr_t)P.sh_low,
                                (uintptr_t)P.sh_high, (uintptr_t)P.sh_scale, (uintptr_t)target, (uintptr_t)colour,
                                (uintptr_t)loss, (uintptr_t)(grads ? grads->means : nullptr),
-                               (uintptr_t)(grads ? grads->sh : nullptr), (uintptr_t)P.count, (uintptr_t)depth};
+                               (uintptr_t)(grads ? grads->sh : nullptr), (uintptr_t)P.count, (uintptr_t)depth,
+                               (uintptr_t)targetReady};
     int slot = -1;
     for (int k = 0; k < ath_batch::kGraphs && slot < 0; ++k)
         if (b->exec[k] && std::memcmp(key, b->graphKey[k], sizeof(key)) == 0) slot = k;
@@ -1372,7 +1382,7 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
             ath_param_grads g = grads ? *grads : ath_param_grads{};
             const cudaError_t enq =
                 enqueueStep(b, P, target, reinterpret_cast<float4*>(colour), loss, g, b->captureStream, false,
-                            nullptr, depth);
+                            nullptr, depth, targetReady);
             err = cudaStreamEndCapture(b->captureStream, &graph);
             if (enq != cudaSuccess) err = enq;
         }
@@ -1393,6 +1403,12 @@ ath_status runStep(ath_batch* b, const ath_mixed_params* params, const float* ta
 
 extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target,
                                            float* colour, float* loss, ath_param_grads* grads, void* streamPtr) {
+    return ath_batch_train_step_after(b, params, target, nullptr, colour, loss, grads, streamPtr);
+}
+
+extern "C" ath_status ath_batch_train_step_after(ath_batch* b, const ath_mixed_params* params, const float* target,
+                                                 void* targetReady, float* colour, float* loss, ath_param_grads* grads,
+                                                 void* streamPtr) {
     if (!b || !params || !target || !colour || !loss)
         return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_train_step: null argument");
     // with gradient buckets the buckets' arrays receive the gradients; an empty cloud
@@ -1405,7 +1421,7 @@ extern "C" ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params*
                                                 std::to_string(b->bucketCount) + " Gaussians, the cloud has " +
                                                 std::to_string(params->count));
     return runStep(b, params, target, colour, loss, b->bucketGrads.empty() ? grads : nullptr, nullptr, streamPtr,
-                   "ath_batch_train_step");
+                   "ath_batch_train_step", static_cast<cudaEvent_t>(targetReady));
 }
 
 // Bucket k of `buckets` over `count` Gaussians: consecutive ranges in whole blocks

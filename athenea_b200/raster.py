@@ -644,14 +644,20 @@ class BatchTrainer:
         check(N.lib().ath_batch_set_key_mode(self._h, mode))
 
     def step(self, params: MixedParams, target: torch.Tensor, colour: torch.Tensor, loss: torch.Tensor,
-             grads: "Params | None", stream: torch.cuda.Stream | None = None) -> None:
-        """ath_batch_train_step; `grads` None when gradient buckets are set."""
+             grads: "Params | None", stream: torch.cuda.Stream | None = None,
+             target_ready: torch.cuda.Event | None = None) -> None:
+        """ath_batch_train_step; `grads` None when gradient buckets are set. With `target_ready`
+        (ath_batch_train_step_after), only the blends wait for that event: the target's upload
+        overlaps the projection and the sort."""
         g = N.ParamGrads(None, None, None, None) if grads is None else \
             N.ParamGrads(_ptr(grads.means), _ptr(grads.scales), _ptr(grads.quats), _ptr(grads.sh))
         s = stream if stream is not None else torch.cuda.current_stream(colour.device)
-        self._keep = (params, target, colour, loss, grads)
-        check(N.lib().ath_batch_train_step(self._h, C.byref(params._native()), _ptr(target), _ptr(colour),
-                                           _ptr(loss), C.byref(g), C.c_void_p(s.cuda_stream)))
+        self._keep = (params, target, colour, loss, grads, target_ready)
+        if target_ready is not None and target_ready.cuda_event == 0:
+            target_ready.record(s)   # torch makes the event on its first record
+        ready = C.c_void_p(target_ready.cuda_event if target_ready is not None else None)
+        check(N.lib().ath_batch_train_step_after(self._h, C.byref(params._native()), _ptr(target), ready,
+                                                 _ptr(colour), _ptr(loss), C.byref(g), C.c_void_p(s.cuda_stream)))
 
     def render(self, params: MixedParams, colour: torch.Tensor, depth: torch.Tensor | None = None,
                stream: torch.cuda.Stream | None = None) -> None:

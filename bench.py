@@ -337,8 +337,10 @@ def run_ours(args) -> dict | None:
 
     # e2e through the public API: each step's target images copied in from pinned
     # host memory into one of two device buffers on a copy stream (overlapping the
-    # step before), the step reading that buffer directly (the library keeps one
-    # captured step for each); the loss read back to pinned host memory.
+    # step before, and the step's own projection and sort: only its blends wait for
+    # the copy, ath_batch_train_step_after), the step reading that buffer directly
+    # (the library keeps one captured step for each); the loss read back to pinned
+    # host memory.
     copy = torch.cuda.Stream(dev)
     staging = [torch.empty_like(target), torch.empty_like(target)]
     h2d_done = [torch.cuda.Event(), torch.cuda.Event()]
@@ -352,8 +354,7 @@ def run_ours(args) -> dict | None:
             h2d_done[k % 2].record(copy)
 
     def e2e_step(k):
-        stream.wait_event(h2d_done[k % 2])
-        bt.step(mixed, staging[k % 2], colour, loss, grads, stream=stream)
+        bt.step(mixed, staging[k % 2], colour, loss, grads, stream=stream, target_ready=h2d_done[k % 2])
         exchange()
         used[k % 2].record(stream)
         loss_host.copy_(loss, non_blocking=True)

@@ -397,6 +397,14 @@ ath_status ath_batch_set_key_mode(ath_batch* b, uint32_t mode);
  * (count 0) draws the background, and its gradient arrays may be null. */
 ath_status ath_batch_train_step(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
                                 float* loss, ath_param_grads* grads, void* stream);
+/* ath_batch_train_step with the target still arriving: the step's projection,
+ * sort and ranges start at once, and only its blends wait for `target_ready` (a
+ * cudaEvent_t the caller records after the target's upload, on any stream), so
+ * that the upload overlaps them. The event is part of the captured step: one
+ * event a target buffer, as for double-buffered uploads. */
+ath_status ath_batch_train_step_after(ath_batch* b, const ath_mixed_params* params, const float* target,
+                                      void* target_ready, float* colour, float* loss, ath_param_grads* grads,
+                                      void* stream);
 /* Gradient buckets, for a step whose gradients are summed over GPUs while it
  * still runs (no counterpart in the reference, which is single-device): with
  * `buckets` > 0, the step's projection adjoint runs bucket by bucket over

@@ -465,3 +465,41 @@ def test_gradient_buckets_give_the_same_gradients_and_signal_each_bucket():
         # the loss is a float atomic sum over blocks, in an order that varies from run to run
         assert abs(loss.item() - loss_one.item()) <= 2e-5 * loss_one.item()
     b.set_buckets(None)
+
+
+@pytest.mark.gpu
+def test_a_step_whose_blends_wait_for_the_target_upload_equals_the_step():
+    """ath_batch_train_step_after: the target is copied from pinned host memory on a side
+    stream while the step's projection and sort run; only the blends wait for its event.
+    Twice on each of two device buffers (captured, then replayed), the image, the loss and
+    the gradients equal the plain step's (to the rounding of atomic sums, whose order varies)."""
+    Pq, M = _scene(40_000, 23)
+    views = _views()
+    gen = torch.Generator().manual_seed(9)
+    targets = [torch.rand((W * H, 3), generator=gen).cuda() for _, W, H in views]
+    b, colour_one, loss_one, grads_one, _ = _batched(M, views, targets)
+    host = torch.cat(targets).cpu().pin_memory()
+    staging = [torch.empty_like(host, device="cuda") for _ in range(2)]
+    ready = [torch.cuda.Event() for _ in range(2)]
+    side = torch.cuda.Stream()
+    colour = torch.empty_like(colour_one)
+    loss = torch.zeros(1, device="cuda")
+    grads = A.Params(torch.zeros_like(M.means), torch.zeros_like(M.scales), torch.zeros_like(M.quats),
+                     torch.zeros((M.count, 48), device="cuda"), 3)
+    main = torch.cuda.current_stream()
+    for k in range(4):
+        torch.cuda.synchronize()
+        staging[k % 2].zero_()
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            staging[k % 2].copy_(host, non_blocking=True)
+            ready[k % 2].record(side)
+        b.step(M, staging[k % 2], colour, loss, grads, stream=main, target_ready=ready[k % 2])
+        b.check()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(colour.cpu().numpy(), colour_one.cpu().numpy())
+        assert abs(loss.item() - loss_one.item()) <= 2e-5 * loss_one.item()
+        for name in ("means", "scales", "quats", "sh"):
+            want = getattr(grads_one, name).cpu().numpy()
+            np.testing.assert_allclose(getattr(grads, name).cpu().numpy(), want, rtol=1e-4,
+                                       atol=1e-5 * float(np.abs(want).max()), err_msg=name)
