@@ -574,21 +574,22 @@ __global__ void __launch_bounds__(256)
 // and get none); a warp of Gaussians with different such views runs each view's work
 // for a few lanes. The forward blend sets `seen[v count + i]` for every record (v, i)
 // some pixel blends (the records the blend adjoint gives a gradient); ordering the Gaussians [first, end) by the word of those
-// views (bit v mod 32, folded to 8 bits: exactly the views for up to 8) lets whole
+// views (bit v mod 64, folded to 8 bits: exactly the views for up to 8) lets whole
 // warps skip a view. Within a group the Gaussians keep their order inside each block of 256; the
 // blocks' runs follow in the order the blocks reserve them. The adjoint's results do
 // not depend on the order (each Gaussian's gradient is its own thread's).
-// Gaussian i's views whose record some pixel blended: bit v mod 32.
-__device__ __forceinline__ uint32_t seenViews(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count,
+// Gaussian i's views whose record some pixel blended: bit v mod 64.
+__device__ __forceinline__ uint64_t seenViews(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count,
                                               uint32_t i) {
-    uint32_t m = 0;
-    for (uint32_t v = 0; v < views; ++v) m |= (uint32_t)(seen[(size_t)v * count + i] != 0u) << (v & 31u);
+    uint64_t m = 0;
+    for (uint32_t v = 0; v < views; ++v) m |= (uint64_t)(seen[(size_t)v * count + i] != 0u) << (v & 63u);
     return m;
 }
-__device__ __forceinline__ uint32_t groupOf(uint32_t m) {
+__device__ __forceinline__ uint32_t groupOf(uint64_t m) {
+    m ^= m >> 32;
     m ^= m >> 16;
     m ^= m >> 8;
-    return m & 255u;
+    return (uint32_t)m & 255u;
 }
 
 __global__ void __launch_bounds__(256)
@@ -605,11 +606,11 @@ __global__ void __launch_bounds__(256)
 
 // order[first + k], k < end - first: the Gaussians of [first, end), group by group;
 // viewsOf[first + k]: that Gaussian's seenViews word (the views the adjoint visits
-// when there are at most 32).
+// when there are at most 64).
 __global__ void __launch_bounds__(256)
     groupPlaceKernel(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count, uint32_t first, uint32_t end,
                      const uint32_t* __restrict__ counts, uint32_t* __restrict__ cursors, uint32_t* __restrict__ order,
-                     uint32_t* __restrict__ viewsOf) {
+                     uint64_t* __restrict__ viewsOf) {
     __shared__ uint32_t sWarpCount[8][256];   // a warp's Gaussians of each group, then their offsets
     __shared__ uint32_t sStart[256], sBase[256], sWarp[8];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -631,7 +632,7 @@ __global__ void __launch_bounds__(256)
     // a Gaussian's rank among the block's Gaussians of its group, in index order
     const uint32_t i = first + blockIdx.x * 256 + tid;
     const bool valid = i < end;
-    const uint32_t m = valid ? seenViews(seen, views, count, i) : 0u;
+    const uint64_t m = valid ? seenViews(seen, views, count, i) : 0ull;
     const uint32_t h = valid ? groupOf(m) : 256u + lane;
     const uint32_t peers = __match_any_sync(0xFFFFFFFFu, h);
     const uint32_t inWarp = __popc(peers & ((1u << lane) - 1u));
@@ -671,22 +672,22 @@ __global__ void __launch_bounds__(128)
     projectAdjointBatchKernel(const BatchConst B, const BatchView* __restrict__ views, const float* __restrict__ grads,
                               float4* __restrict__ gMeans, float4* __restrict__ gScales, float4* __restrict__ gQuats,
                               float* __restrict__ gSh, uint32_t shStride, uint32_t first, uint32_t end,
-                              const uint32_t* __restrict__ order, const uint32_t* __restrict__ viewsOf) {
+                              const uint32_t* __restrict__ order, const uint64_t* __restrict__ viewsOf) {
     const uint32_t limit = min(end, B.count);
     const uint32_t slot = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= limit) return;
     const uint32_t i = order ? order[slot] : slot;   // a permutation of [first, end), grouped
     if (i < first || i >= limit) return;
     const uint32_t o = i - first;   // the row in this launch's gradient arrays
-    // the views whose record of this Gaussian took a gradient (up to 32 views; past 32,
+    // the views whose record of this Gaussian took a gradient (up to 64 views; past 64,
     // every view, the zero records skipped by their value): the other views' records
     // are not even read
-    const bool masked = order && B.views <= 32;
-    const uint32_t seenMask = masked ? viewsOf[slot] : 0u;
+    const bool masked = order && B.views <= 64;
+    const uint64_t seenMask = masked ? viewsOf[slot] : 0ull;
     auto nextView = [&](uint32_t from) -> uint32_t {   // the first such view >= from, or B.views
         if (!masked) return from;
-        const uint32_t m = from < 32u ? seenMask >> from : 0u;
-        return m ? from + (uint32_t)__ffs(m) - 1u : B.views;
+        const uint64_t m = from < 64u ? seenMask >> from : 0ull;
+        return m ? from + (uint32_t)__ffsll((long long)m) - 1u : B.views;
     };
     InstanceConst I = B.inst;
     const Gauss g = loadGauss<kLayoutMixed>(I, i);
@@ -1073,7 +1074,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
                 const uint8_t* seen = static_cast<const uint8_t*>(b->seen.ptr);
                 uint32_t* counts = static_cast<uint32_t*>(b->groupWords.ptr);
                 uint32_t* order = static_cast<uint32_t*>(b->adjointOrder.ptr);
-                uint32_t* viewsOf = static_cast<uint32_t*>(b->adjointViews.ptr);
+                uint64_t* viewsOf = static_cast<uint64_t*>(b->adjointViews.ptr);
                 const uint32_t blocks = (n + 255) / 256;
                 err = cudaMemsetAsync(counts, 0, 2 * 256 * 4, stream);
                 if (err == cudaSuccess) {
@@ -1117,7 +1118,7 @@ ath_status reserveBatch(ath_batch* b, uint32_t count) {
     if (err == cudaSuccess) err = b->viewsDev.reserve(std::max<size_t>(1, b->views.size()) * sizeof(BatchView));
     if (err == cudaSuccess) err = b->seen.reserve(std::max<size_t>(1, (size_t)V * count));
     if (err == cudaSuccess) err = b->adjointOrder.reserve((size_t)std::max(1u, count) * 4);
-    if (err == cudaSuccess) err = b->adjointViews.reserve((size_t)std::max(1u, count) * 4);
+    if (err == cudaSuccess) err = b->adjointViews.reserve((size_t)std::max(1u, count) * 8);
     if (err == cudaSuccess) err = b->groupWords.reserve(2 * 256 * 4);
     if (err != cudaSuccess) return failCuda(err, "reserving the batch's scratch");
     b->count = count;

@@ -503,3 +503,27 @@ def test_a_step_whose_blends_wait_for_the_target_upload_equals_the_step():
             want = getattr(grads_one, name).cpu().numpy()
             np.testing.assert_allclose(getattr(grads, name).cpu().numpy(), want, rtol=1e-4,
                                        atol=1e-5 * float(np.abs(want).max()), err_msg=name)
+
+
+@pytest.mark.gpu
+def test_gradients_of_many_views_are_the_sums_of_their_halves():
+    """The projection adjoint reads only the records of the views that gave a Gaussian a
+    gradient, from a word of view bits (up to 64 views; past 64, every view). 70 small
+    views in one step (past 64) and as two steps of 35 (within 64): the gradients and the
+    loss of the whole are the sums of the halves' (to the rounding of atomic sums)."""
+    _, M = _scene(20_000, 27)
+    views = []
+    for v in range(70):
+        cam = A.pinhole_for_vertical_fov(scenes.circle_eye(v, 70, 3.0, 0.3), (0, 0, 0), 64, 48, 60.0)
+        views.append((cam.projection_for(64, 48), 64, 48))
+    gen = torch.Generator().manual_seed(27)
+    targets = [torch.rand((64 * 48, 3), generator=gen).cuda() for _ in views]
+    _, _, loss_all, grads_all, _ = _batched(M, views, targets, 16, 128)
+    _, _, loss_a, grads_a, _ = _batched(M, views[:35], targets[:35], 16, 128)
+    _, _, loss_b, grads_b, _ = _batched(M, views[35:], targets[35:], 16, 128)
+    assert abs(loss_all.item() - (loss_a.item() + loss_b.item())) <= 1e-4 * loss_all.item()
+    for name in ("means", "scales", "quats", "sh"):
+        want = (getattr(grads_a, name) + getattr(grads_b, name)).cpu().numpy()
+        got = getattr(grads_all, name).cpu().numpy()
+        assert np.abs(want).max() > 0, name
+        np.testing.assert_allclose(got, want, rtol=1e-3, atol=1e-5 * float(np.abs(want).max()), err_msg=name)
