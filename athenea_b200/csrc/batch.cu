@@ -673,17 +673,23 @@ __global__ void __launch_bounds__(128)
                               float4* __restrict__ gMeans, float4* __restrict__ gScales, float4* __restrict__ gQuats,
                               float* __restrict__ gSh, uint32_t shStride, uint32_t first, uint32_t end,
                               const uint32_t* __restrict__ order, const uint64_t* __restrict__ viewsOf) {
+    // a warp's SH gradient rows (stride 49: lane l's value k at bank (17 l + k) mod 32), written
+    // out a row at a time so that each store covers whole sectors: the rows of a grouped
+    // warp's Gaussians lie far apart, and a lane storing its own row touches a sector a value
+    __shared__ float sSh[4][32 * 49];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t limit = min(end, B.count);
     const uint32_t slot = first + blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= limit) return;
-    const uint32_t i = order ? order[slot] : slot;   // a permutation of [first, end), grouped
-    if (i < first || i >= limit) return;
+    const uint32_t picked = slot < limit ? (order ? order[slot] : slot) : first;
+    const bool active = slot < limit && picked >= first && picked < limit;
+    if (!__any_sync(0xFFFFFFFFu, active)) return;
+    const uint32_t i = active ? picked : first;   // a permutation of [first, end), grouped
     const uint32_t o = i - first;   // the row in this launch's gradient arrays
     // the views whose record of this Gaussian took a gradient (up to 64 views; past 64,
     // every view, the zero records skipped by their value): the other views' records
     // are not even read
     const bool masked = order && B.views <= 64;
-    const uint64_t seenMask = masked ? viewsOf[slot] : 0ull;
+    const uint64_t seenMask = masked && active ? viewsOf[slot] : 0ull;
     auto nextView = [&](uint32_t from) -> uint32_t {   // the first such view >= from, or B.views
         if (!masked) return from;
         const uint64_t m = from < 64u ? seenMask >> from : 0ull;
@@ -693,7 +699,7 @@ __global__ void __launch_bounds__(128)
     const Gauss g = loadGauss<kLayoutMixed>(I, i);
     const uint32_t degree = min(degreeOf(I.restPerColour), B.shLimit);
     float dp[3] = {0.0f, 0.0f, 0.0f};
-    {
+    if (active) {
         const MixedSh sh = loadMixedSh(I, i);
         float dSh[48];
 #pragma unroll
@@ -720,11 +726,22 @@ __global__ void __launch_bounds__(128)
                 colourAdjointFast(sh, g, degree, I.linear, views[v].eye, gc, dSh, dp);
             v = vn;
         }
-        float* row = gSh + (size_t)o * shStride;
+        float* mine = sSh[warp] + lane * 49;
 #pragma unroll
-        for (uint32_t k = 0; k < 48; ++k)
-            if (k < shStride) row[k] = dSh[k];
+        for (uint32_t k = 0; k < 48; ++k) mine[k] = dSh[k];
     }
+    __syncwarp();
+    {
+        // row r is lane r's, for the active lanes
+        const uint32_t cols = min(48u, shStride), lanes = __ballot_sync(0xFFFFFFFFu, active);
+        for (uint32_t r = 0; r < 32; ++r) {
+            const uint32_t orow = __shfl_sync(0xFFFFFFFFu, o, r);
+            if (!((lanes >> r) & 1u)) continue;
+            float* row = gSh + (size_t)orow * shStride;
+            for (uint32_t c = lane; c < cols; c += 32) row[c] = sSh[warp][r * 49 + c];
+        }
+    }
+    if (!active) return;
     ParamGrad acc;
     acc.dp[0] = acc.dp[1] = acc.dp[2] = 0.0f;
     acc.dLogit = 0.0f;
