@@ -1010,7 +1010,7 @@ cudaError_t launchBlendsFor(const ath_batch* b, const BatchConst& B, uint32_t so
 // A null `target`: a render, the forward blend alone (no loss, no backward).
 cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* target, float4* colour, float* loss,
                         ath_param_grads& g, cudaStream_t stream, bool countOnly, cudaEvent_t* marks = nullptr,
-                        float* depth = nullptr, cudaEvent_t targetReady = nullptr) {
+                        float* depth = nullptr, cudaEvent_t targetReady = nullptr, bool countWork = false) {
     auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], stream); };
     mark(0);
     BatchConst B = batchConst(b, P);
@@ -1075,7 +1075,7 @@ cudaError_t enqueueStep(ath_batch* b, const ath_mixed_params& P, const float* ta
     // the forward blend, the loss and the blend adjoint (the record gradients were cleared by the projection)
     if (err == cudaSuccess)
         err = launchBlendsFor(b, B, sorted, stream, colour, target, loss, static_cast<float*>(b->grads.ptr), depth,
-                              marks != nullptr);
+                              countWork);
     mark(4);
     if (err == cudaSuccess && train && P.count) {
         // the whole cloud into `g`, or bucket by bucket into each bucket's arrays, each
@@ -1530,7 +1530,9 @@ extern "C" ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params
                                             void* streamPtr) {
     // A step as ath_batch_train_step enqueues it, uncaptured, with events between
     // its stages, waited for: project+emit, sort, ranges, blends (forward, loss and
-    // adjoint in one kernel), projection adjoint.
+    // adjoint in one kernel), projection adjoint. The blends' work is counted in a step
+    // run just before on the same inputs (the counting kernel is slower), so the timed
+    // step runs the kernels a captured step runs.
     if (!b || !params || !grads || !ms) return fail(ATH_E_INVALID_ARGUMENT, "ath_batch_time_stages: null argument");
     ath_status st = ath_batch_train_step(b, params, target, colour, loss, grads, streamPtr);   // sized and placed
     if (st != ATH_OK) return st;
@@ -1544,6 +1546,9 @@ extern "C" ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params
     if (err == cudaSuccess)
         err = cudaMemsetAsync(words + kBatchBlended, 0, (kBatchStaged + 2 - kBatchBlended) * sizeof(uint32_t),
                               stream);
+    if (err == cudaSuccess)
+        err = enqueueStep(b, *params, target, reinterpret_cast<float4*>(colour), loss, g, stream, false, nullptr,
+                          nullptr, nullptr, true);
     if (err == cudaSuccess)
         err = enqueueStep(b, *params, target, reinterpret_cast<float4*>(colour), loss, g, stream, false, marks);
     if (err == cudaSuccess) err = cudaEventSynchronize(marks[5]);

@@ -342,8 +342,9 @@ typedef struct {
     uint32_t tile, block_batch;
     float ms_per_step;     /* ath_batch_tune: the chosen setting's time */
     uint32_t degenerate;   /* records whose 2D conic was inverted in FP64 (det < 1e-6 trace^2) */
-    /* The blends' work, counted by the last step ath_batch_time_stages ran (the
-     * captured steps do not count, to keep the counting out of their time). */
+    /* The blends' work, counted by the step ath_batch_time_stages runs before its
+     * timed one on the same inputs (neither the captured steps nor the timed step
+     * count, to keep the counting out of their time). */
     uint64_t evaluated;    /* (pixel, record) evaluations of the forward blend */
     uint64_t blended;      /* of them, those that blended (inside the cutoff, alpha at least 1/255) */
     uint64_t adjoint_visited;  /* (pixel, record) evaluations of the blend adjoint (before the pixel's last contributor) */
@@ -446,7 +447,8 @@ ath_status ath_batch_tune(ath_batch* b, const ath_mixed_params* params, const fl
 /* One step as ath_batch_train_step runs it, not captured, with events between
  * its stages, waited for: ms[] = project+emit (with the record gradients'
  * clearing), sort, ranges, blends (the forward blend, the loss and the blend
- * adjoint, one kernel), projection adjoint. For measurement. */
+ * adjoint, one kernel), projection adjoint. For measurement. A step that counts
+ * the blends' work (ath_batch_stats) runs first, untimed. */
 ath_status ath_batch_time_stages(ath_batch* b, const ath_mixed_params* params, const float* target, float* colour,
                                  float* loss, ath_param_grads* grads, float ms[5], void* stream);
 
