@@ -322,16 +322,27 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
             const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
             const uint32_t excl = incl - n;
             for (uint32_t r0 = 0; r0 < total; r0 += 32) {
-                // the records of ranks r0 .. r0 + 31 (ranked last first) into the warp's slots
-                if (excl < r0 + 32u && excl + n > r0) {
-                    uint32_t w = word, rank = excl;
-                    while (w && rank < r0 + 32u) {
-                        const uint32_t bit = 31u - (uint32_t)__clz(w);
-                        w &= ~(1u << bit);
-                        if (rank >= r0) sWarpRel[warp][rank - r0] = (uint32_t)ch * 32u + bit;
-                        ++rank;
+                // the records of ranks r0 .. r0 + 31 (ranked last first) into the warp's slots:
+                // lane q takes rank r0 + q. Its chunk is the last lane c whose exclusive count
+                // is at most the rank (a search over the lanes' counts); in that chunk's word,
+                // the record is the set bit of the remaining rank, counted down from bit 31 (a
+                // search over the word's halves, quarters, ...). No lane walks bits one by one.
+                const uint32_t want = r0 + lane;
+                uint32_t c = 0;
+#pragma unroll
+                for (uint32_t step = 16; step; step >>= 1)
+                    if (__shfl_sync(0xFFFFFFFFu, excl, c + step) <= want) c += step;
+                const uint32_t wc = __shfl_sync(0xFFFFFFFFu, word, c);
+                uint32_t rem = want - __shfl_sync(0xFFFFFFFFu, excl, c), bit = 31;
+#pragma unroll
+                for (uint32_t step = 16; step; step >>= 1) {
+                    const uint32_t below = __popc((wc >> (bit - step + 1u)) & ((1u << step) - 1u));
+                    if (below <= rem) {
+                        rem -= below;
+                        bit -= step;
                     }
                 }
+                if (want < total) sWarpRel[warp][lane] = (uint32_t)(hi - (int32_t)c) * 32u + bit;
                 __syncwarp();
                 const uint32_t cnt = min(32u, total - r0);
                 if (lane < cnt) {
