@@ -573,11 +573,13 @@ __global__ void __launch_bounds__(256)
 // whose record got no gradient (on C1 most records lie behind the pixels' early stop
 // and get none); a warp of Gaussians with different such views runs each view's work
 // for a few lanes. The forward blend sets `seen[v count + i]` for every record (v, i)
-// some pixel blends (the records the blend adjoint gives a gradient); ordering the Gaussians [first, end) by the word of those
-// views (bit v mod 64, folded to 8 bits: exactly the views for up to 8) lets whole
-// warps skip a view. Within a group the Gaussians keep their order inside each block of 256; the
-// blocks' runs follow in the order the blocks reserve them. The adjoint's results do
-// not depend on the order (each Gaussian's gradient is its own thread's).
+// some pixel blends (the records the blend adjoint gives a gradient). Ordering the
+// Gaussians [first, end) by their word of those views (bit v mod 64, folded to 8 bits:
+// exactly the views for up to 8) lets whole warps skip a view. Within a group the
+// Gaussians keep their order inside each block of 256; the blocks' runs follow in the
+// order the blocks reserve them. The adjoint's results do not depend on the order
+// (each Gaussian's gradient is its own thread's).
+
 // Gaussian i's views whose record some pixel blended: bit v mod 64.
 __device__ __forceinline__ uint64_t seenViews(const uint8_t* __restrict__ seen, uint32_t views, uint32_t count,
                                               uint32_t i) {
