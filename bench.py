@@ -509,7 +509,8 @@ def main():
         if rank != 0:
             return
         runs = []
-        cpu_baseline()   # one untimed run: builds the checker, pages the scene in
+        for _ in range(args.warmup):   # untimed: builds the checker, pages the scene in
+            cpu_baseline()
         for _ in range(args.steps):
             runs.append(cpu_baseline())
         ms = statistics.median(r["ms"] for r in runs)
