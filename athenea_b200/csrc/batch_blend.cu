@@ -126,7 +126,7 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth, uint32_t lan
 // kCount: also count the walks' work (evaluations and warp visits) into the
 // batch's words; a step timed stage by stage counts, the captured steps do not.
 template <uint32_t T, uint32_t S, uint32_t NB, bool kTrain, bool kCount>
-__global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 8 : 16)
+__global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   // 16x16 spans: 71 registers, no spill
     blendStepKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
                     const float4* __restrict__ recs, float4* __restrict__ colour, const float* __restrict__ target,
