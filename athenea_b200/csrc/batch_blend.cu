@@ -368,7 +368,6 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                     float gv[kWords];
 #pragma unroll
                     for (int e = 0; e < (int)kWords; ++e) gv[e] = 0.0f;
-                    bool live = false;
                     // as the forward, without branching: a pixel past its last contributor or
                     // that does not blend the record takes alpha 0 (T unchanged, no terms)
 #pragma unroll
@@ -381,7 +380,6 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                         const float a0 = fminf(0.99f, raw);
                         const bool on = rel < last[p] && e >= c.w && a0 >= kFaint;
                         if constexpr (kCount) { adjVisited += rel < last[p] ? 1u : 0u; adjLive += on ? 1u : 0u; }
-                        live = live || on;
                         const float alpha = on ? a0 : 0.0f;
                         const float inv = fastRcp(1.0f - alpha);
                         const float Tb = Tr[p] * inv;
@@ -402,7 +400,9 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                         gv[3] = __fmaf_rn(dPt, dy, gv[3]);
                         gv[4] = __fmaf_rn(dPy, dy, gv[4]);
                     }
-                    if (!__any_sync(0xFFFFFFFFu, live)) continue;
+                    // no test that some lane is live: a gathered record's forward live bit says a
+                    // pixel of this box blended it, and the adjoint decides that pixel the same way
+                    // (a record with no live lane would only add zeros, which are not stored)
                     if constexpr (kCount) ++adjSummed;
                     // the warp's sums, however few lanes are live, added by nine lanes at once
                     // into the record's words in global memory (reductions, not read back):
