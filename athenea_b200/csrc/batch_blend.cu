@@ -67,9 +67,12 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
 // Nine values summed over a warp: the first eight by a transposed reduction
 // (each level sends half of the values still held and keeps the other half,
 // so three levels leave value (lane >> 2) spread over lanes differing in their
-// two low bits), the ninth by a butterfly. Lanes with lane % 4 == 0 hold value
-// lane >> 2; every lane holds the ninth.
-__device__ __forceinline__ float warpSum9(float v[9], float& ninth, uint32_t lane) {
+// two low bits), the ninth by a butterfly over the same three levels; the last
+// two levels take the pair (value lane >> 2, the ninth) transposed as well.
+// Lanes with lane % 4 == 0 end with value lane >> 2, lanes with lane % 4 == 2
+// with the ninth. Every sum adds the same terms in the same pairs as a
+// butterfly over each value alone, so the results are those of one.
+__device__ __forceinline__ float warpSum9(float v[9], uint32_t lane) {
 #pragma unroll
     for (int half = 4, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
         const bool upper = (lane & (uint32_t)bit) != 0;
@@ -80,13 +83,12 @@ __device__ __forceinline__ float warpSum9(float v[9], float& ninth, uint32_t lan
             v[k] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, bit);
         }
     }
-    float s = v[0];
-    s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
-    s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
     float n = v[8];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
-    ninth = n;
+    for (int o = 16; o > 2; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
+    const bool upper = (lane & 2u) != 0;
+    float s = (upper ? n : v[0]) + __shfl_xor_sync(0xFFFFFFFFu, upper ? v[0] : n, 2);
+    s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
     return s;
 }
 
@@ -146,13 +148,13 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
     __shared__ float sDepth[kTrain ? 1 : NB];   // a render's record depths
     __shared__ uint32_t sTileBase[kMaxBatchViews];
     __shared__ uint32_t sTile;
-    // the adjoint's gather slots, a warp's own: 32 records, their place in the tile's list
+    // the adjoint's gather slots, a warp's own: 32 records, each its centre with its
+    // place in the tile's list and its record index (one 16-byte load a visit), its
+    // conic and its colour
     constexpr uint32_t kWarpsHere = kTrain ? kThreads / 32 : 1;
-    __shared__ float2 sWarpCentre[kWarpsHere][32];
+    __shared__ float4 sWarpCentre[kWarpsHere][32];
     __shared__ float4 sWarpConic[kWarpsHere][32];
     __shared__ float4 sWarpColour[kWarpsHere][32];
-    __shared__ uint32_t sWarpRec[kWarpsHere][32];
-    __shared__ uint32_t sWarpRel[kWarpsHere][32];
     for (uint32_t k = threadIdx.x; k < B.views; k += kThreads) sTileBase[k] = views[k].tileBase;
     const uint64_t slotMask = (1ull << B.slotBits) - 1ull;
     const float kScale = -0.5f * 1.4426950408889634f;   // power -> base-2 exponent
@@ -342,32 +344,32 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                         bit -= step;
                     }
                 }
-                if (want < total) sWarpRel[warp][lane] = (uint32_t)(hi - (int32_t)c) * 32u + bit;
-                __syncwarp();
-                const uint32_t cnt = min(32u, total - r0);
+                const uint32_t cnt = min(32u, total - r0);   // lane < cnt exactly when want < total
                 if (lane < cnt) {
-                    const uint32_t rel = sWarpRel[warp][lane];
+                    const uint32_t rel = (uint32_t)(hi - (int32_t)c) * 32u + bit;
                     const uint32_t gs = gaussianOf(pairs, values, slotMask, range.x + rel);
                     const size_t at = (recBase + gs) * 3;
                     const float4 sc = recs[at + 0];
-                    const float4 c = recs[at + 1];
+                    const float4 k = recs[at + 1];
                     const float4 rgb = recs[at + 2];
-                    sWarpCentre[warp][lane] = make_float2(sc.x, sc.y);
-                    sWarpConic[warp][lane] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
+                    sWarpCentre[warp][lane] =
+                        make_float4(sc.x, sc.y, __uint_as_float(rel), __uint_as_float((uint32_t)(recBase + gs)));
+                    sWarpConic[warp][lane] = make_float4(k.x * kScale, k.y, k.z * kScale, k.w);
                     sWarpColour[warp][lane] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
-                    sWarpRec[warp][lane] = (uint32_t)(recBase + gs);
                 }
                 __syncwarp();
                 for (uint32_t q = 0; q < cnt; ++q) {
                     if constexpr (kCount) ++adjVisits;
-                    const uint32_t rel = sWarpRel[warp][q];
-                    const float2 ce = sWarpCentre[warp][q];
+                    const float4 ce = sWarpCentre[warp][q];
+                    const uint32_t rel = __float_as_uint(ce.z);
                     const float4 k = sWarpConic[warp][q];
                     const float4 c = sWarpColour[warp][q];
                     const float dx = pxc - ce.x;
+                    // the sums start at -0, which adding leaves any value as it is (+0 would
+                    // turn a -0 term into +0): the first pixel's terms are taken as they come
                     float gv[kWords];
 #pragma unroll
-                    for (int e = 0; e < (int)kWords; ++e) gv[e] = 0.0f;
+                    for (int e = 0; e < (int)kWords; ++e) gv[e] = -0.0f;
                     // as the forward, without branching: a pixel past its last contributor or
                     // that does not blend the record takes alpha 0 (T unchanged, no terms)
 #pragma unroll
@@ -409,12 +411,10 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                     // the five moments, dL/dalpha and dL/dcolour, which the projection's
                     // adjoint turns into centre and conic gradients (linear in the moments,
                     // so sums from every box, tile and batch add up)
-                    float ninth;
-                    const float sum = warpSum9(gv, ninth, lane);
-                    const uint32_t slot = (lane & 3u) == 0u ? lane >> 2 : lane == 1u ? 8u : kWords;
-                    const float val = lane == 1u ? ninth : sum;
+                    const float val = warpSum9(gv, lane);
+                    const uint32_t slot = (lane & 3u) == 0u ? lane >> 2 : lane == 2u ? 8u : kWords;
                     if (slot < kWords && val != 0.0f)
-                        atomicAdd(grads + (size_t)sWarpRec[warp][q] * kGradWords + slot, val);
+                        atomicAdd(grads + (size_t)__float_as_uint(ce.w) * kGradWords + slot, val);
                 }
                 __syncwarp();   // the next round's gathers overwrite the slots
             }
