@@ -64,6 +64,18 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
     return mask;
 }
 
+// The least base-2 exponent e = -power / (2 ln 2) at which a pixel blends a
+// record: the larger of the cutoff's and the one at which opacity * 2^e reaches
+// 1/255 (log2(1/255) - log2(opacity); every record's opacity is at least 1/255).
+// One comparison a pixel then stands for both tests. Both walks take it from
+// the same record values, so the forward and the adjoint decide alike.
+__device__ __forceinline__ float blendFloor(float cutoffExp, float opacity) {
+    constexpr float kLog2Faint = -7.99435344f;   // log2(1/255)
+    float lg;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(lg) : "f"(opacity));
+    return fmaxf(cutoffExp, kLog2Faint - lg);
+}
+
 // Nine values summed over a warp: the first eight by a transposed reduction
 // (each level sends half of the values still held and keeps the other half,
 // so three levels leave value (lane >> 2) spread over lanes differing in their
@@ -142,7 +154,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
     constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
     __shared__ float2 sCentre[NB];
     __shared__ float4 sConic[NB];    // ca, fr, fs pre-scaled; alpha
-    __shared__ float4 sColour[NB];   // r g b; the cutoff pre-scaled
+    __shared__ float4 sColour[NB];   // r g b; the least exponent that blends (blendFloor)
     __shared__ uint32_t sMask[NB];
     __shared__ uint32_t sRec[NB];
     __shared__ float sDepth[kTrain ? 1 : NB];   // a render's record depths
@@ -186,7 +198,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
         const float pxc = (float)px + 0.5f, pyc[2] = {(float)py[0] + 0.5f, (float)py[1] + 0.5f};
         const size_t recBase = (size_t)v * B.count;
         // record s of this view into slot k: the factored conic's two weights and the
-        // cutoff pre-scaled to base-2 exponent units, and the boxes it can reach
+        // least base-2 exponent that blends, and the boxes it can reach
         auto stage = [&](uint32_t k, uint32_t s) {
             if constexpr (kCount) ++staged;
             sRec[k] = s;
@@ -196,7 +208,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
             const float4 rgb = recs[at + 2];
             sCentre[k] = make_float2(sc.x, sc.y);
             sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
-            sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
+            sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, blendFloor(kScale * sc.w, c.w));
             sMask[k] = boxMask<S>(tileX0, tileY0, sc, c.x, c.y, c.z);
             if constexpr (!kTrain) sDepth[k] = sc.z;
         };
@@ -236,7 +248,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                         const float t = __fmaf_rn(k.y, dy, dx);
                         const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
                         const float a0 = fminf(0.99f, k.w * fastExp2(e));
-                        const bool blend = !done[p] && e >= cc.w && a0 >= kFaint;
+                        const bool blend = !done[p] && e >= cc.w;
                         if constexpr (kCount) { evaluated += done[p] ? 0u : 1u; blended += blend ? 1u : 0u; }
                         const float alpha = blend ? a0 : 0.0f;
                         const float w = Tr[p] * alpha;
@@ -244,7 +256,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                         g[p] = __fmaf_rn(w, cc.y, g[p]);
                         bl[p] = __fmaf_rn(w, cc.z, bl[p]);
                         if constexpr (!kTrain) depthSum[p] = __fmaf_rn(w, sDepth[j], depthSum[p]);
-                        Tr[p] = Tr[p] * (1.0f - alpha);
+                        Tr[p] = __fmaf_rn(-Tr[p], alpha, Tr[p]);   // T (1 - alpha), one rounding
                         last[p] = blend ? first - range.x + j + 1 : last[p];
                         if constexpr (!kTrain)
                             if (blend && depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = sDepth[j];
@@ -355,7 +367,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                     sWarpCentre[warp][lane] =
                         make_float4(sc.x, sc.y, __uint_as_float(rel), __uint_as_float((uint32_t)(recBase + gs)));
                     sWarpConic[warp][lane] = make_float4(k.x * kScale, k.y, k.z * kScale, k.w);
-                    sWarpColour[warp][lane] = make_float4(rgb.x, rgb.y, rgb.z, kScale * sc.w);
+                    sWarpColour[warp][lane] = make_float4(rgb.x, rgb.y, rgb.z, blendFloor(kScale * sc.w, k.w));
                 }
                 __syncwarp();
                 for (uint32_t q = 0; q < cnt; ++q) {
@@ -380,7 +392,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                         const float G = fastExp2(e);
                         const float raw = k.w * G;
                         const float a0 = fminf(0.99f, raw);
-                        const bool on = rel < last[p] && e >= c.w && a0 >= kFaint;
+                        const bool on = rel < last[p] && e >= c.w;
                         if constexpr (kCount) { adjVisited += rel < last[p] ? 1u : 0u; adjLive += on ? 1u : 0u; }
                         const float alpha = on ? a0 : 0.0f;
                         const float inv = fastRcp(1.0f - alpha);
