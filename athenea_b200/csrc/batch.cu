@@ -787,6 +787,7 @@ __global__ void __launch_bounds__(128)
         I.eye[0] = V.eye[0]; I.eye[1] = V.eye[1]; I.eye[2] = V.eye[2];
         const Geometry G = projectGeometry<true>(F, I, g, g.opacity);
         batchMomentsToRecordGrad(G.ca, G.fr, G.fs, gw);   // the blend's moments, to the record's terms
+        gw[5] = gw[5] / G.alpha;   // the blend summed the opacity times dL/dopacity (alpha >= 1/255)
         float dpv[3] = {0.0f, 0.0f, 0.0f};
         float dM[3][3];
         geometryAdjointToM(F, I, g, G, gw, dpv, acc, dM);

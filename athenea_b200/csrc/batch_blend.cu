@@ -64,16 +64,21 @@ __device__ __forceinline__ uint32_t boxMask(float tileX0, float tileY0, float4 s
     return mask;
 }
 
-// The least base-2 exponent e = -power / (2 ln 2) at which a pixel blends a
-// record: the larger of the cutoff's and the one at which opacity * 2^e reaches
-// 1/255 (log2(1/255) - log2(opacity); every record's opacity is at least 1/255).
-// One comparison a pixel then stands for both tests. Both walks take it from
-// the same record values, so the forward and the adjoint decide alike.
-__device__ __forceinline__ float blendFloor(float cutoffExp, float opacity) {
-    constexpr float kLog2Faint = -7.99435344f;   // log2(1/255)
+// A walk's exponent e = log2(opacity) - power / (2 ln 2), so that alpha =
+// min(0.99, 2^e) takes no multiply a pixel: each staged record carries
+// log2(opacity) in place of its opacity (every record's opacity is at least 1/255).
+__device__ __forceinline__ float log2Of(float x) {
     float lg;
-    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(lg) : "f"(opacity));
-    return fmaxf(cutoffExp, kLog2Faint - lg);
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(lg) : "f"(x));
+    return lg;
+}
+// The least such exponent at which a pixel blends a record: the larger of the
+// cutoff's (power at the cutoff) and log2(1/255), where alpha reaches 1/255. One
+// comparison a pixel then stands for both tests. Both walks take it from the same
+// record values, so the forward and the adjoint decide alike.
+__device__ __forceinline__ float blendFloor(float cutoffExp, float lgOpacity) {
+    constexpr float kLog2Faint = -7.99435344f;   // log2(1/255)
+    return fmaxf(cutoffExp + lgOpacity, kLog2Faint);
 }
 
 // Nine values summed over a warp: the first eight by a transposed reduction
@@ -127,11 +132,12 @@ __device__ __forceinline__ float warpSum9(float v[9], uint32_t lane) {
 // chunk and box); the warp gathers those records, last first, 32 at a time into
 // slots of its own and walks them from its pixels' last contributor down. What a
 // lane sums over its two pixels, and the warp over its 64, are moments of
-// dL/dpower over the pixel offsets in the factored frame (t = dx + fr dy, dy): sum
-// dP t, sum dP dy, sum dP t^2, sum dP t dy, sum dP dy^2. Each visit's warp sums are
-// added into the record's gradient words in global memory as they are (moments,
-// dL/dalpha, dL/dcolour); the projection's adjoint turns the moments into the
-// centre and conic gradients (batchMomentsToRecordGrad), once a record. The loss
+// dP = -2 dL/dpower over the pixel offsets in the factored frame (t = dx + fr dy,
+// dy): sum dP t, sum dP dy, sum dP t^2, sum dP t dy, sum dP dy^2. Each visit's warp
+// sums are added into the record's gradient words in global memory as they are
+// (moments, opacity times dL/dopacity, dL/dcolour); the projection's adjoint turns
+// the moments into the centre and conic gradients (batchMomentsToRecordGrad, which
+// applies the -1/2) and divides the opacity's word by the opacity, once a record. The loss
 // has no alpha term, so dL/d(alpha out) is 0 and the colour behind a record enters
 // only through S.dC, one value a pixel.
 //
@@ -153,7 +159,7 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
     constexpr uint32_t kBoxes = (T / kBox) * (T / kBox);   // boxes a tile (the live words' row)
     constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
     __shared__ float2 sCentre[NB];
-    __shared__ float4 sConic[NB];    // ca, fr, fs pre-scaled; alpha
+    __shared__ float4 sConic[NB];    // ca, fs pre-scaled, fr; log2 of the opacity (alpha)
     __shared__ float4 sColour[NB];   // r g b; the least exponent that blends (blendFloor)
     __shared__ uint32_t sMask[NB];
     __shared__ uint32_t sRec[NB];
@@ -197,8 +203,9 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
         const uint2 range = ranges[tile];
         const float pxc = (float)px + 0.5f, pyc[2] = {(float)py[0] + 0.5f, (float)py[1] + 0.5f};
         const size_t recBase = (size_t)v * B.count;
-        // record s of this view into slot k: the factored conic's two weights and the
-        // least base-2 exponent that blends, and the boxes it can reach
+        // record s of this view into slot k: the factored conic's two weights pre-scaled
+        // to base-2 exponent units, log2 of its opacity, the least exponent that blends,
+        // and the boxes it can reach
         auto stage = [&](uint32_t k, uint32_t s) {
             if constexpr (kCount) ++staged;
             sRec[k] = s;
@@ -207,8 +214,9 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
             const float4 c = recs[at + 1];
             const float4 rgb = recs[at + 2];
             sCentre[k] = make_float2(sc.x, sc.y);
-            sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, c.w);
-            sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, blendFloor(kScale * sc.w, c.w));
+            const float lgo = log2Of(c.w);
+            sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, lgo);
+            sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, blendFloor(kScale * sc.w, lgo));
             sMask[k] = boxMask<S>(tileX0, tileY0, sc, c.x, c.y, c.z);
             if constexpr (!kTrain) sDepth[k] = sc.z;
         };
@@ -246,8 +254,8 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                     for (int p = 0; p < 2; ++p) {
                         const float dy = pyc[p] - ce.y;
                         const float t = __fmaf_rn(k.y, dy, dx);
-                        const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
-                        const float a0 = fminf(0.99f, k.w * fastExp2(e));
+                        const float e = __fmaf_rn(k.x * t, t, __fmaf_rn(k.z * dy, dy, k.w));
+                        const float a0 = fminf(0.99f, fastExp2(e));
                         const bool blend = !done[p] && e >= cc.w;
                         if constexpr (kCount) { evaluated += done[p] ? 0u : 1u; blended += blend ? 1u : 0u; }
                         const float alpha = blend ? a0 : 0.0f;
@@ -366,8 +374,9 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                     const float4 rgb = recs[at + 2];
                     sWarpCentre[warp][lane] =
                         make_float4(sc.x, sc.y, __uint_as_float(rel), __uint_as_float((uint32_t)(recBase + gs)));
-                    sWarpConic[warp][lane] = make_float4(k.x * kScale, k.y, k.z * kScale, k.w);
-                    sWarpColour[warp][lane] = make_float4(rgb.x, rgb.y, rgb.z, blendFloor(kScale * sc.w, k.w));
+                    const float lgo = log2Of(k.w);
+                    sWarpConic[warp][lane] = make_float4(k.x * kScale, k.y, k.z * kScale, lgo);
+                    sWarpColour[warp][lane] = make_float4(rgb.x, rgb.y, rgb.z, blendFloor(kScale * sc.w, lgo));
                 }
                 __syncwarp();
                 for (uint32_t q = 0; q < cnt; ++q) {
@@ -388,9 +397,8 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                     for (int p = 0; p < 2; ++p) {
                         const float dy = pyc[p] - ce.y;
                         const float t = __fmaf_rn(k.y, dy, dx);
-                        const float e = __fmaf_rn(k.x * t, t, (k.z * dy) * dy);
-                        const float G = fastExp2(e);
-                        const float raw = k.w * G;
+                        const float e = __fmaf_rn(k.x * t, t, __fmaf_rn(k.z * dy, dy, k.w));
+                        const float raw = fastExp2(e);
                         const float a0 = fminf(0.99f, raw);
                         const bool on = rel < last[p] && e >= c.w;
                         if constexpr (kCount) { adjVisited += rel < last[p] ? 1u : 0u; adjLive += on ? 1u : 0u; }
@@ -402,11 +410,11 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                         gv[7] = __fmaf_rn(w, dC[p][1], gv[7]);
                         gv[8] = __fmaf_rn(w, dC[p][2], gv[8]);
                         const float cd = (c.x * dC[p][0] + c.y * dC[p][1]) + c.z * dC[p][2];
-                        const float dAlpha = on && raw < 0.99f && k.w <= 1.0f ? Tb * (cd - sd[p]) : 0.0f;
+                        const float dAlpha = on && raw < 0.99f && k.w <= 0.0f ? Tb * (cd - sd[p]) : 0.0f;
                         sd[p] = __fmaf_rn(alpha, cd - sd[p], sd[p]);
                         Tr[p] = Tb;
-                        gv[5] = __fmaf_rn(dAlpha, G, gv[5]);
-                        const float dP = -0.5f * alpha * dAlpha;
+                        gv[5] = __fmaf_rn(dAlpha, raw, gv[5]);   // opacity times dL/dopacity
+                        const float dP = alpha * dAlpha;   // -2 dL/dpower: the -1/2 is the record's, once
                         const float dPt = dP * t, dPy = dP * dy;
                         gv[0] += dPt;
                         gv[1] += dPy;

@@ -127,13 +127,14 @@ __device__ __forceinline__ uint32_t viewOf(const uint32_t* bases, uint32_t views
 }
 
 // The batched blend adjoint's words for a record (the warp sums it adds up):
-// [0..4] the moments of dL/dpower over the pixel offsets in the record's factored
-// frame t = dx + fr dy, dy (sum dP t, dP dy, dP t^2, dP t dy, dP dy^2), [5] dL/dalpha,
-// [6..8] dL/dcolour. To dL/d(centre, conic): the conic is ca (dx + fr dy)^2 + fs dy^2,
-// so dL/da = sum dP dx^2 with dx = t - fr dy, and so on; in place, in the plain
-// path's kGrad* layout.
+// [0..4] the moments of -2 dL/dpower over the pixel offsets in the record's factored
+// frame t = dx + fr dy, dy (sum t, dy, t^2, t dy, dy^2 times it), [5] the opacity
+// times dL/dopacity, [6..8] dL/dcolour. To dL/d(centre, conic), with the -1/2 applied
+// here (exact: a power of two): the conic is ca (dx + fr dy)^2 + fs dy^2, so
+// dL/da = sum dP dx^2 with dx = t - fr dy, and so on; in place, in the plain path's
+// kGrad* layout. Word [5] is left for the caller, which knows the opacity.
 __device__ __forceinline__ void batchMomentsToRecordGrad(float ca, float fr, float fs, float g[10]) {
-    const float mt = g[0], my = g[1], mtt = g[2], mty = g[3], myy = g[4];
+    const float mt = -0.5f * g[0], my = -0.5f * g[1], mtt = -0.5f * g[2], mty = -0.5f * g[3], myy = -0.5f * g[4];
     g[kGradCx] = -2.0f * ca * mt;
     g[kGradCy] = -2.0f * (fr * ca * mt + fs * my);
     g[kGradA] = mtt - 2.0f * fr * mty + fr * fr * myy;   // sum dP dx^2
