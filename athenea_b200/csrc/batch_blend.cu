@@ -146,7 +146,7 @@ __device__ __forceinline__ float warpSum9(float v[9], uint32_t lane) {
 // kCount: also count the walks' work (evaluations and warp visits) into the
 // batch's words; a step timed stage by stage counts, the captured steps do not.
 template <uint32_t T, uint32_t S, uint32_t NB, bool kTrain, bool kCount>
-__global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   // 16x16 spans: 71 registers, no spill
+__global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? (kTrain ? 8 : 7) : 16)   // 16x16 spans: no spill
     blendStepKernel(const BatchConst B, const BatchView* __restrict__ views, const uint2* __restrict__ ranges,
                     const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ values,
                     const float4* __restrict__ recs, float4* __restrict__ colour, const float* __restrict__ target,
@@ -410,11 +410,13 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? 7 : 16)   /
                         gv[7] = __fmaf_rn(w, dC[p][1], gv[7]);
                         gv[8] = __fmaf_rn(w, dC[p][2], gv[8]);
                         const float cd = (c.x * dC[p][0] + c.y * dC[p][1]) + c.z * dC[p][2];
-                        const float dAlpha = on && raw < 0.99f && k.w <= 0.0f ? Tb * (cd - sd[p]) : 0.0f;
-                        sd[p] = __fmaf_rn(alpha, cd - sd[p], sd[p]);
+                        // alpha dL/dalpha where alpha is not clamped (dL/dalpha = T before it
+                        // times (c - S).dC): the opacity times dL/dopacity, and -2 dL/dpower
+                        const float u = cd - sd[p];
+                        const float dP = on && raw < 0.99f && k.w <= 0.0f ? w * u : 0.0f;
+                        sd[p] = __fmaf_rn(alpha, u, sd[p]);
                         Tr[p] = Tb;
-                        gv[5] = __fmaf_rn(dAlpha, raw, gv[5]);   // opacity times dL/dopacity
-                        const float dP = alpha * dAlpha;   // -2 dL/dpower: the -1/2 is the record's, once
+                        gv[5] += dP;
                         const float dPt = dP * t, dPy = dP * dy;
                         gv[0] += dPt;
                         gv[1] += dPy;
