@@ -158,12 +158,11 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? (kTrain ? 8
     constexpr uint32_t kSpans = (T / S) * (T / S);    // spans (blocks' work units) a tile
     constexpr uint32_t kBoxes = (T / kBox) * (T / kBox);   // boxes a tile (the live words' row)
     constexpr uint32_t kWords = 9;   // moments t, dy, tt, t dy, dy dy; alpha; colour r g b
-    __shared__ float2 sCentre[NB];
-    __shared__ float4 sConic[NB];    // ca, fs pre-scaled, fr; log2 of the opacity (alpha)
-    __shared__ float4 sColour[NB];   // r g b; the least exponent that blends (blendFloor)
+    // a staged record, 48 bytes at one address: centre (cx, cy, depth); conic (ca, fs
+    // pre-scaled, fr; log2 of the opacity); colour (r g b; the least exponent that blends)
+    __shared__ float4 sStaged[NB][3];
     __shared__ uint32_t sMask[NB];
     __shared__ uint32_t sRec[NB];
-    __shared__ float sDepth[kTrain ? 1 : NB];   // a render's record depths
     __shared__ uint32_t sTileBase[kMaxBatchViews];
     __shared__ uint32_t sTile;
     // the adjoint's gather slots, a warp's own: 32 records, each its centre with its
@@ -213,12 +212,11 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? (kTrain ? 8
             const float4 sc = recs[at + 0];
             const float4 c = recs[at + 1];
             const float4 rgb = recs[at + 2];
-            sCentre[k] = make_float2(sc.x, sc.y);
+            sStaged[k][0] = make_float4(sc.x, sc.y, sc.z, 0.0f);
             const float lgo = log2Of(c.w);
-            sConic[k] = make_float4(c.x * kScale, c.y, c.z * kScale, lgo);
-            sColour[k] = make_float4(rgb.x, rgb.y, rgb.z, blendFloor(kScale * sc.w, lgo));
+            sStaged[k][1] = make_float4(c.x * kScale, c.y, c.z * kScale, lgo);
+            sStaged[k][2] = make_float4(rgb.x, rgb.y, rgb.z, blendFloor(kScale * sc.w, lgo));
             sMask[k] = boxMask<S>(tileX0, tileY0, sc, c.x, c.y, c.z);
-            if constexpr (!kTrain) sDepth[k] = sc.z;
         };
 
         // ---- forward
@@ -237,15 +235,15 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? (kTrain ? 8
             for (uint32_t base = 0; base < count; base += 32) {
                 const uint32_t m = base + lane < count ? sMask[base + lane] : 0u;
                 uint32_t todo = __ballot_sync(0xFFFFFFFFu, (m >> warp) & 1u);
-                uint32_t liveWord = 0;   // the records of this chunk some pixel of the box blended
+                uint32_t laneBits = 0;   // the records of this chunk a pixel of this lane blended
                 while (todo) {
                     const uint32_t j = base + (uint32_t)__ffs(todo) - 1u;
                     todo &= todo - 1u;
                     if constexpr (kCount) ++fwdVisits;
-                    const float2 ce = sCentre[j];
-                    const float4 k = sConic[j];
+                    const float4 ce = sStaged[j][0];
+                    const float4 k = sStaged[j][1];
                     const float dx = pxc - ce.x;
-                    const float4 cc = sColour[j];
+                    const float4 cc = sStaged[j][2];
                     bool hit = false;
                     // both pixels evaluated without branching: a pixel that does not blend the
                     // record (done, outside the cutoff, or under 1/255) takes alpha 0, which
@@ -263,17 +261,18 @@ __global__ void __launch_bounds__(S * S / 2, S == 32 ? 2 : S == 16 ? (kTrain ? 8
                         r[p] = __fmaf_rn(w, cc.x, r[p]);
                         g[p] = __fmaf_rn(w, cc.y, g[p]);
                         bl[p] = __fmaf_rn(w, cc.z, bl[p]);
-                        if constexpr (!kTrain) depthSum[p] = __fmaf_rn(w, sDepth[j], depthSum[p]);
+                        if constexpr (!kTrain) depthSum[p] = __fmaf_rn(w, ce.z, depthSum[p]);
                         Tr[p] = __fmaf_rn(-Tr[p], alpha, Tr[p]);   // T (1 - alpha), one rounding
                         last[p] = blend ? first - range.x + j + 1 : last[p];
                         if constexpr (!kTrain)
-                            if (blend && depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = sDepth[j];
+                            if (blend && depthAt[p] < 0.0f && 1.0f - Tr[p] >= B.depthThreshold) depthAt[p] = ce.z;
                         done[p] = done[p] || Tr[p] < 1e-4f;
                         hit = hit || blend;
                     }
-                    if constexpr (kTrain)
-                        if (__any_sync(0xFFFFFFFFu, hit)) liveWord |= 1u << (j - base);
+                    if constexpr (kTrain) laneBits |= hit ? 1u << (j - base) : 0u;
                 }
+                // the records of this chunk some pixel of the box blended
+                const uint32_t liveWord = kTrain ? __reduce_or_sync(0xFFFFFFFFu, laneBits) : 0u;
                 if constexpr (kTrain) {
                     if (lane == 0)
                         live[((size_t)(range.x >> 5) + tile + ((first - range.x + base) >> 5)) * kBoxes +
